@@ -1,0 +1,246 @@
+/*
+ * pmb.h — C ABI of libpmb, the B200 (sm_100a) implementation of polars-metal's
+ * filter -> group_by -> fused-aggregate path.
+ *
+ * Every entry point is plain C: pointers, sizes and status codes, no C++ or torch
+ * types. Each declaration names the reference interface it replaces
+ * (file:line inside the dbfclark/polars-metal tree).
+ *
+ * Conventions shared by all entry points
+ *   - Return value: PMB_OK (0) or a PMB_E_* code; pmb_last_error() gives text.
+ *   - Columns follow the Arrow layout the reference's buffer crate uses
+ *     (crates/polars-metal-buffer/src/null_bitmap.rs:29-92): dense little-endian
+ *     values (Bool bit-packed LSB-first) and an optional validity bitmap,
+ *     LSB-first, 1 = valid, NULL = all rows valid.
+ *   - `on_device` = 1 means the pointer is CUDA device memory on the handle's
+ *     device; 0 means host memory (pinned or pageable), copied in by the call.
+ *   - A handle owns one CUDA stream and one device workspace; it is not
+ *     thread-safe. Use one handle per host thread.
+ *   - Results are owned by the library until pmb_result_free(). Device-resident
+ *     result buffers live in the handle's workspace and stay valid until the next
+ *     call on the same handle.
+ */
+#ifndef PMB_H
+#define PMB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (EngineError mapping: crates/polars-metal-core/src/error.rs:19-34) ---- */
+enum {
+  PMB_OK = 0,
+  PMB_E_INVALID = 1,     /* bad argument / buffer too short  (PyValueError)          */
+  PMB_E_OOM = 2,         /* device or host allocation failed                          */
+  PMB_E_TIMEOUT = 3,     /* a bounded device wait gave up; the context stays usable   */
+  PMB_E_CUDA = 4,        /* a CUDA runtime call failed                                */
+  PMB_E_UNSUPPORTED = 5, /* valid request outside this build (PyNotImplementedError)  */
+  PMB_E_NOT_FOUND = 6    /* a referenced column index does not exist (PyKeyError)     */
+};
+
+/* ---- dtypes: the reference's wire tags (crates/polars-metal-core/src/plan/mod.rs MetalDtype) ---- */
+enum {
+  PMB_BOOL = 0,
+  PMB_I8 = 1,
+  PMB_I16 = 2,
+  PMB_I32 = 3,
+  PMB_I64 = 4,
+  PMB_U8 = 5,
+  PMB_U16 = 6,
+  PMB_U32 = 7,
+  PMB_U64 = 8,
+  PMB_F32 = 9,
+  PMB_F64 = 10
+};
+
+/* One Arrow-layout column (replaces the `(name, tag, data: bytes, valid: bytes)` tuples of
+ * `_native.execute_groupby`, crates/polars-metal-core/src/udf/groupby/mod.rs:747-820). */
+typedef struct pmb_column {
+  const void* data;        /* values at row 0 of the array (before `offset`)          */
+  const uint8_t* validity; /* Arrow validity bitmap or NULL (= all valid)              */
+  int64_t length;          /* rows in this column                                      */
+  int64_t offset;          /* Arrow row offset applied to data and validity            */
+  int32_t dtype;           /* PMB_* dtype                                              */
+  int32_t on_device;       /* 1 = device pointers, 0 = host pointers                   */
+} pmb_column;
+
+/* ---- predicate expression (PredicateAst, crates/polars-metal-core/src/plan/mod.rs:42-60,
+ *      plus the Arith / Not / IsNull nodes this build adds) ---- */
+enum {
+  PMB_EXPR_COLUMN = 0,
+  PMB_EXPR_LIT_I64 = 1,
+  PMB_EXPR_LIT_F64 = 2,
+  PMB_EXPR_LIT_BOOL = 3,
+  PMB_EXPR_COMPARE = 4,
+  PMB_EXPR_AND = 5,
+  PMB_EXPR_OR = 6,
+  PMB_EXPR_NOT = 7,
+  PMB_EXPR_ARITH = 8,
+  PMB_EXPR_IS_NULL = 9,
+  PMB_EXPR_IS_NOT_NULL = 10
+};
+enum { PMB_CMP_EQ = 0, PMB_CMP_NE = 1, PMB_CMP_LT = 2, PMB_CMP_LE = 3, PMB_CMP_GT = 4, PMB_CMP_GE = 5 };
+enum {
+  PMB_ARITH_ADD = 0,
+  PMB_ARITH_SUB = 1,
+  PMB_ARITH_MUL = 2,
+  PMB_ARITH_TRUEDIV = 3,  /* always F64 */
+  PMB_ARITH_FLOORDIV = 4,
+  PMB_ARITH_MOD = 5       /* floor modulo: result takes the divisor's sign; x % 0 is null for ints */
+};
+
+typedef struct pmb_expr_node {
+  int32_t kind;    /* PMB_EXPR_*                                                  */
+  int32_t op;      /* PMB_CMP_* for COMPARE, PMB_ARITH_* for ARITH                */
+  int32_t lhs;     /* child node index (-1 when unused)                           */
+  int32_t rhs;     /* child node index (-1 when unused)                           */
+  int32_t column;  /* column index for PMB_EXPR_COLUMN                            */
+  int32_t dtype;   /* operand dtype for COMPARE / ARITH: PMB_I64 or PMB_F64       */
+  int64_t lit_i64; /* LIT_I64 value; LIT_BOOL uses 0/1                            */
+  double lit_f64;  /* LIT_F64 value                                               */
+} pmb_expr_node;
+
+typedef struct pmb_expr {
+  const pmb_expr_node* nodes;
+  int32_t n_nodes;
+  int32_t root;
+} pmb_expr;
+
+/* ---- aggregations (AggOp, crates/polars-metal-core/src/plan/mod.rs:62-70) ---- */
+enum { PMB_AGG_SUM = 0, PMB_AGG_MEAN = 1, PMB_AGG_COUNT = 2, PMB_AGG_MIN = 3, PMB_AGG_MAX = 4, PMB_AGG_LEN = 5 };
+typedef struct pmb_agg {
+  int32_t op;     /* PMB_AGG_*                                  */
+  int32_t column; /* input column index; ignored for PMB_AGG_LEN */
+} pmb_agg;
+
+/* ---- group-by strategies (build archetypes A1/A2/A3 of crates/polars-metal-kernels/src/groupby.rs:450-538) ---- */
+enum {
+  PMB_STRATEGY_AUTO = 0,        /* sketch + learned selector, heuristic fallback   */
+  PMB_STRATEGY_SMEM_HASH = 1,   /* per-CTA shared-memory tables + small global merge */
+  PMB_STRATEGY_GLOBAL_HASH = 2, /* global open addressing with a shared-memory hot cache */
+  PMB_STRATEGY_SORT = 3         /* packed-key LSD radix sort + segmented reduce   */
+};
+
+typedef struct pmb_query {
+  const int32_t* key_columns; /* indices into the column array                     */
+  int32_t n_keys;
+  const pmb_agg* aggs;
+  int32_t n_aggs;
+  const pmb_expr* predicate;  /* NULL = no filter                                  */
+  int32_t strategy;           /* PMB_STRATEGY_*                                    */
+  int32_t output_on_device;   /* 1 = result columns in device memory               */
+  int64_t capacity_hint;      /* expected distinct groups; 0 = let the library pick */
+} pmb_query;
+
+typedef struct pmb_out_column {
+  void* data;        /* values; Bool outputs bit-packed                             */
+  uint8_t* validity; /* bitmap, LSB-first, padded to a 4-byte multiple (never NULL) */
+  int64_t length;
+  int32_t dtype;
+  int32_t on_device;
+} pmb_out_column;
+
+typedef struct pmb_result {
+  int64_t n_groups;         /* rows in every output column                        */
+  int32_t n_columns;        /* group-by: keys then aggs; filter: one per input   */
+  pmb_out_column* columns;
+  int32_t strategy_used;    /* PMB_STRATEGY_* actually executed                   */
+  int32_t rehash_count;     /* capacity overflows retried with a larger table     */
+  int64_t capacity;         /* hash slots of the final attempt (0 for sort)       */
+} pmb_result;
+
+typedef struct pmb_handle pmb_handle;
+
+/* Per-call timing record, filled when profiling is enabled (pmb_set_profiling). */
+#define PMB_MAX_STAT_KERNELS 16
+typedef struct pmb_stats {
+  int32_t n_kernels;
+  int32_t launches[PMB_MAX_STAT_KERNELS];
+  float ms[PMB_MAX_STAT_KERNELS];        /* device time per kernel name, summed over launches */
+  char names[PMB_MAX_STAT_KERNELS][32];
+  float total_ms;                        /* device time of the whole call                     */
+  int64_t h2d_bytes;
+  int64_t d2h_bytes;
+  int32_t kernel_launches;               /* every kernel this call launched                   */
+} pmb_stats;
+
+/* ---- lifetime ---- */
+
+/* Creates a handle on `device` with an initial device workspace (grown on demand).
+ * Replaces MetalDevice::system_default + CommandQueue::new
+ * (crates/polars-metal-core/src/udf/groupby/mod.rs:996-1000, crates/polars-metal-kernels/src/command.rs:95). */
+int pmb_open(pmb_handle** out, int32_t device, uint64_t workspace_bytes);
+void pmb_close(pmb_handle* h);
+/* Last error text of this handle (EngineError's Display, crates/polars-metal-core/src/error.rs:19-34). */
+const char* pmb_last_error(const pmb_handle* h);
+/* Makes the handle launch on an existing cudaStream_t (NULL = the handle's own stream). */
+int pmb_set_stream(pmb_handle* h, void* cuda_stream);
+/* 1 = record per-kernel CUDA-event timings of every call (readable with pmb_last_stats). */
+int pmb_set_profiling(pmb_handle* h, int32_t enabled);
+int pmb_last_stats(const pmb_handle* h, pmb_stats* out);
+/* Library version string. */
+const char* pmb_version(void);
+
+/* ---- the hot path ---- */
+
+/* filter -> group_by -> fused aggregate in one call.
+ * Replaces `_native.execute_groupby(plan_dict, n_rows, columns)`
+ * (crates/polars-metal-core/src/udf/groupby/mod.rs:747-1144) together with the CPU
+ * filter it is fed from (`_filter_via_polars`, python/polars_metal/_udf.py:550-597).
+ * Output columns: keys (in key order) then one column per aggregation. */
+int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols,
+                pmb_result** out);
+
+/* Many independent queries in one persistent launch over a device work queue.
+ * No reference counterpart (new batching layer); each query follows pmb_groupby's
+ * semantics. cols[i] holds n_cols[i] columns of query i. */
+int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb_column* const* cols,
+                        const int32_t* n_cols, int32_t n_queries, pmb_result** outs);
+
+void pmb_result_free(pmb_result* r);
+
+/* ---- the operator surface on the filter side ---- */
+
+/* Null-aware comparison -> bit-packed (data, validity); rhs == NULL compares with the scalar
+ * (rhs_i64 for PMB_I64 columns, rhs_f64 for PMB_F64). Output buffers must hold
+ * max(4, round_up_4(ceil(n/8))) bytes each and live where `out_on_device` says.
+ * Replaces `_native.cmp_{i64,f64}_col_{col,scalar}` (crates/polars-metal-core/src/udf/compare.rs:23-145)
+ * and dispatch_cmp_* (crates/polars-metal-kernels/src/cmp.rs:180-641). */
+int pmb_compare(pmb_handle* h, const pmb_column* lhs, const pmb_column* rhs, int64_t rhs_i64,
+                double rhs_f64, int32_t op, uint8_t* out_data, uint8_t* out_valid,
+                int32_t out_on_device);
+
+/* Kleene AND / OR of two bit-packed nullable Boolean columns of n rows.
+ * Replaces `_native.bool_{and,or}_dispatch` (crates/polars-metal-core/src/udf/logical.rs:26-55). */
+int pmb_bool_and(pmb_handle* h, const uint8_t* lhs_data, const uint8_t* lhs_valid,
+                 const uint8_t* rhs_data, const uint8_t* rhs_valid, int64_t n, uint8_t* out_data,
+                 uint8_t* out_valid, int32_t on_device);
+int pmb_bool_or(pmb_handle* h, const uint8_t* lhs_data, const uint8_t* lhs_valid,
+                const uint8_t* rhs_data, const uint8_t* rhs_valid, int64_t n, uint8_t* out_data,
+                uint8_t* out_valid, int32_t on_device);
+
+/* Stream compaction of `cols` by a bit-packed predicate (keep = data & valid).
+ * Replaces `_native.execute_filter_compact(pred_data, pred_valid, n_rows, columns)`
+ * (crates/polars-metal-core/src/udf/compact.rs:46-147) and compute_keep_and_prefix +
+ * compact_* (crates/polars-metal-kernels/src/pipeline.rs:103-270). */
+int pmb_filter_compact(pmb_handle* h, const uint8_t* pred_data, const uint8_t* pred_valid,
+                       int64_t n_rows, int32_t pred_on_device, const pmb_column* cols,
+                       int32_t n_cols, int32_t output_on_device, pmb_result** out);
+
+/* Same compaction with the predicate evaluated on the device from an expression. */
+int pmb_filter_compact_expr(pmb_handle* h, const pmb_expr* predicate, const pmb_column* cols,
+                            int32_t n_cols, int32_t output_on_device, pmb_result** out);
+
+/* Inclusive prefix sum of n bytes into n uint32 values.
+ * Replaces polars-metal-mlx-sys `cumsum_u8_to_u32(&[u8], &mut [u32])`
+ * (crates/polars-metal-mlx-sys/src/lib.rs:47, cxx/mlx_bridge.cc:59-89). */
+int pmb_cumsum_u8_to_u32(pmb_handle* h, const uint8_t* in, uint32_t* out, int64_t n,
+                         int32_t on_device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PMB_H */

@@ -1,0 +1,432 @@
+// pmb_expr.cuh — device-side row access, predicate evaluation, key packing and the
+// aggregation-state update/merge primitives shared by the group-by and filter kernels.
+//
+// Predicate semantics follow the reference: IEEE compares (NaN compares false except !=,
+// -0.0 == +0.0; crates/polars-metal-kernels/src/cmp.rs:14-28), a compare is null when an
+// operand is null (cmp.rs:9-13), Kleene AND/OR (shaders/logical_bool.metal:3-26), and a row
+// survives the filter iff the predicate is valid and true. Each leaf term yields a pair of
+// bits (T = "valid and true", F = "valid and false"); AND/OR/NOT on those pairs is exactly
+// Kleene logic, so the circuit runs on two small bit stacks held in registers.
+#pragma once
+
+#include "pmb_internal.cuh"
+
+// Where the current tile's column chunks live: a shared-memory stage (sbase != nullptr, with
+// per-column offsets doff/voff) or global memory starting at row `row0`.
+struct TileCtx {
+  const uint8_t* sbase;
+  const int32_t* doff;
+  const int32_t* voff;
+  int64_t row0;
+};
+
+__device__ __forceinline__ const uint8_t* tc_data(const DQuery& q, const TileCtx& t, int c) {
+  if (t.sbase) return t.sbase + t.doff[c];
+  int e = q.col[c].elem;
+  return q.col[c].data + (e ? t.row0 * e : t.row0 / 8);
+}
+__device__ __forceinline__ const uint8_t* tc_valid(const DQuery& q, const TileCtx& t, int c) {
+  const uint8_t* v = q.col[c].valid;
+  if (!v) return nullptr;
+  return t.sbase ? t.sbase + t.voff[c] : v + t.row0 / 8;
+}
+__device__ __forceinline__ uint64_t tc_bits(const DQuery& q, const TileCtx& t, int c, int64_t lr) {
+  return pmb_load_bits(tc_data(q, t, c), q.col[c].elem, lr);
+}
+__device__ __forceinline__ bool tc_isvalid(const DQuery& q, const TileCtx& t, int c, int64_t lr) {
+  return pmb_valid_bit(tc_valid(q, t, c), lr);
+}
+
+// ------------------------------------------------------------------ predicate
+struct OpVal {
+  bool valid;
+  int64_t i;
+  double f;
+};
+
+__device__ __forceinline__ OpVal eval_leaf(const DQuery& q, const TileCtx& t, const DLeaf& L, int dt, int64_t lr) {
+  OpVal v;
+  if (L.col < 0) {
+    v.valid = true;
+    v.i = L.i;
+    v.f = L.f;
+    return v;
+  }
+  v.valid = tc_isvalid(q, t, L.col, lr);
+  uint64_t b = tc_bits(q, t, L.col, lr);
+  int cdt = q.col[L.col].dtype;
+  if (dt == PMB_F64) v.f = pmb_bits_to_f64(b, cdt), v.i = 0;
+  else v.i = pmb_bits_to_i64(b, cdt), v.f = 0.0;
+  return v;
+}
+
+__device__ __forceinline__ double pmb_py_fmod(double a, double b) {
+  double r = fmod(a, b);
+  if (r != 0.0 && ((r < 0.0) != (b < 0.0))) r += b;
+  return r;
+}
+
+__device__ __forceinline__ OpVal eval_operand(const DQuery& q, const TileCtx& t, const DOperand& o, int dt, int64_t lr) {
+  OpVal a = eval_leaf(q, t, o.a, dt, lr);
+  if (o.arith < 0) return a;
+  OpVal b = eval_leaf(q, t, o.b, dt, lr);
+  OpVal r;
+  r.valid = a.valid && b.valid;
+  r.i = 0;
+  r.f = 0.0;
+  if (dt == PMB_F64) {
+    switch (o.arith) {
+      case PMB_ARITH_ADD: r.f = a.f + b.f; break;
+      case PMB_ARITH_SUB: r.f = a.f - b.f; break;
+      case PMB_ARITH_MUL: r.f = a.f * b.f; break;
+      case PMB_ARITH_TRUEDIV: r.f = a.f / b.f; break;
+      case PMB_ARITH_FLOORDIV: r.f = floor(a.f / b.f); break;
+      default: r.f = pmb_py_fmod(a.f, b.f); break;
+    }
+  } else {
+    uint64_t x = (uint64_t)a.i, y = (uint64_t)b.i;
+    switch (o.arith) {
+      case PMB_ARITH_ADD: r.i = (int64_t)(x + y); break;
+      case PMB_ARITH_SUB: r.i = (int64_t)(x - y); break;
+      case PMB_ARITH_MUL: r.i = (int64_t)(x * y); break;
+      case PMB_ARITH_FLOORDIV:
+        if (b.i == 0) r.valid = false;
+        else if (a.i == INT64_MIN && b.i == -1) r.i = INT64_MIN;
+        else {
+          int64_t qq = a.i / b.i;
+          if ((a.i % b.i != 0) && ((a.i < 0) != (b.i < 0))) qq -= 1;
+          r.i = qq;
+        }
+        break;
+      default:
+        if (b.i == 0) r.valid = false;
+        else if (b.i == -1) r.i = 0;
+        else {
+          int64_t m = a.i % b.i;
+          if (m != 0 && ((m < 0) != (b.i < 0))) m += b.i;
+          r.i = m;
+        }
+        break;
+    }
+  }
+  return r;
+}
+
+__device__ __forceinline__ void eval_term(const DQuery& q, const TileCtx& t, const DTerm& T, int64_t lr,uint32_t& tt,
+                                          uint32_t& ff) {
+  switch (T.kind) {
+    case T_CMP: {
+      OpVal a = eval_operand(q, t, T.lhs, T.dtype, lr);
+      OpVal b = eval_operand(q, t, T.rhs, T.dtype, lr);
+      if (!(a.valid && b.valid)) {
+        tt = ff = 0;
+        return;
+      }
+      bool c;
+      if (T.dtype == PMB_F64) {
+        switch (T.op) {
+          case PMB_CMP_EQ: c = a.f == b.f; break;
+          case PMB_CMP_NE: c = a.f != b.f; break;
+          case PMB_CMP_LT: c = a.f < b.f; break;
+          case PMB_CMP_LE: c = a.f <= b.f; break;
+          case PMB_CMP_GT: c = a.f > b.f; break;
+          default: c = a.f >= b.f; break;
+        }
+      } else {
+        switch (T.op) {
+          case PMB_CMP_EQ: c = a.i == b.i; break;
+          case PMB_CMP_NE: c = a.i != b.i; break;
+          case PMB_CMP_LT: c = a.i < b.i; break;
+          case PMB_CMP_LE: c = a.i <= b.i; break;
+          case PMB_CMP_GT: c = a.i > b.i; break;
+          default: c = a.i >= b.i; break;
+        }
+      }
+      tt = c;
+      ff = !c;
+      return;
+    }
+    case T_BOOLCOL: {
+      int c = T.lhs.a.col;
+      bool v = tc_isvalid(q, t, c, lr);
+      bool b = tc_bits(q, t, c, lr) != 0;
+      tt = v && b;
+      ff = v && !b;
+      return;
+    }
+    case T_ISNULL:
+    case T_ISNOTNULL: {
+      bool v = eval_operand(q, t, T.lhs, T.dtype, lr).valid;
+      bool isnull = !v;
+      tt = (T.kind == T_ISNULL) ? isnull : !isnull;
+      ff = !tt;
+      return;
+    }
+    default:  // T_LITBOOL
+      tt = T.lhs.a.i != 0;
+      ff = !tt;
+      return;
+  }
+}
+
+// true iff the row survives the filter (predicate valid and true)
+__device__ __forceinline__ bool eval_keep(const DQuery& q, const TileCtx& t, int64_t lr) {
+  const DProgram& P = q.prog;
+  if (P.n_ops == 0) return true;
+  uint32_t ts = 0, fs = 0;
+  for (int i = 0; i < P.n_ops; i++) {
+    int op = P.ops[i];
+    if (op >= 0) {
+      uint32_t a, b;
+      eval_term(q, t, P.term[op], lr, a, b);
+      ts = (ts << 1) | a;
+      fs = (fs << 1) | b;
+    } else if (op == OP_NOT) {
+      uint32_t a = ts & 1u, b = fs & 1u;
+      ts = (ts & ~1u) | b;
+      fs = (fs & ~1u) | a;
+    } else {
+      uint32_t tb = ts & 1u, fb = fs & 1u;
+      ts >>= 1;
+      fs >>= 1;
+      uint32_t ta = ts & 1u, fa = fs & 1u, r_t, r_f;
+      if (op == OP_AND) {
+        r_t = ta & tb;
+        r_f = fa | fb;
+      } else {
+        r_t = ta | tb;
+        r_f = fa & fb;
+      }
+      ts = (ts & ~1u) | r_t;
+      fs = (fs & ~1u) | r_f;
+    }
+  }
+  return (ts & 1u) != 0;
+}
+
+// Kleene (T, F) of the whole predicate, for bit-packed (data, validity) outputs
+__device__ __forceinline__ void eval_pred_tf(const DQuery& q, const TileCtx& t, int64_t lr,bool& valid, bool& truth) {
+  const DProgram& P = q.prog;
+  uint32_t ts = 0, fs = 0;
+  for (int i = 0; i < P.n_ops; i++) {
+    int op = P.ops[i];
+    if (op >= 0) {
+      uint32_t a, b;
+      eval_term(q, t, P.term[op], lr, a, b);
+      ts = (ts << 1) | a;
+      fs = (fs << 1) | b;
+    } else if (op == OP_NOT) {
+      uint32_t a = ts & 1u, b = fs & 1u;
+      ts = (ts & ~1u) | b;
+      fs = (fs & ~1u) | a;
+    } else {
+      uint32_t tb = ts & 1u, fb = fs & 1u;
+      ts >>= 1;
+      fs >>= 1;
+      uint32_t ta = ts & 1u, fa = fs & 1u, r_t, r_f;
+      if (op == OP_AND) {
+        r_t = ta & tb;
+        r_f = fa | fb;
+      } else {
+        r_t = ta | tb;
+        r_f = fa & fb;
+      }
+      ts = (ts & ~1u) | r_t;
+      fs = (fs & ~1u) | r_f;
+    }
+  }
+  truth = (ts & 1u) != 0;
+  valid = truth || (fs & 1u);
+}
+
+// ------------------------------------------------------------------ keys
+#define PMB_EMPTY64 0xFFFFFFFFFFFFFFFFULL
+
+__device__ __forceinline__ uint64_t pack_key64(const DQuery& q, const TileCtx& t, int64_t lr) {
+  uint64_t k = 0;
+  for (int i = 0; i < q.n_keys; i++) {
+    const DKey& K = q.key[i];
+    if (K.nullable && !tc_isvalid(q, t, K.col, lr)) {
+      k |= 1ULL << K.null_off;
+      continue;
+    }
+    uint64_t v = tc_bits(q, t, K.col, lr);
+    if (K.bits < 64) v &= (1ULL << K.bits) - 1ULL;
+    k |= v << K.data_off;
+  }
+  return k;
+}
+
+struct Key128 {
+  uint64_t lo, hi;
+};
+__device__ __forceinline__ Key128 pack_key128(const DQuery& q, const TileCtx& t, int64_t lr) {
+  Key128 k{0, 0};
+  for (int i = 0; i < q.n_keys; i++) {
+    const DKey& K = q.key[i];
+    if (K.nullable && !tc_isvalid(q, t, K.col, lr)) {
+      if (K.null_off < 64) k.lo |= 1ULL << K.null_off;
+      else k.hi |= 1ULL << (K.null_off - 64);
+      continue;
+    }
+    uint64_t v = tc_bits(q, t, K.col, lr);
+    if (K.bits < 64) v &= (1ULL << K.bits) - 1ULL;
+    int o = K.data_off;
+    if (o < 64) {
+      k.lo |= v << o;
+      if (o > 0 && o + K.bits > 64) k.hi |= v >> (64 - o);
+    } else {
+      k.hi |= v << (o - 64);
+    }
+  }
+  return k;
+}
+
+// decode the raw data bits of key field K from a packed key; returns false when null
+__device__ __forceinline__ bool unpack_field(const DKey& K, uint64_t lo, uint64_t hi, uint64_t& v) {
+  if (K.nullable) {
+    uint64_t nb = K.null_off < 64 ? (lo >> K.null_off) & 1ULL : (hi >> (K.null_off - 64)) & 1ULL;
+    if (nb) {
+      v = 0;
+      return false;
+    }
+  }
+  int o = K.data_off;
+  if (o < 64) {
+    v = lo >> o;
+    if (o > 0 && o + K.bits > 64) v |= hi << (64 - o);
+  } else {
+    v = hi >> (o - 64);
+  }
+  if (K.bits < 64) v &= (1ULL << K.bits) - 1ULL;
+  return true;
+}
+
+// ------------------------------------------------------------------ aggregation state
+// Exact-to-double-double accumulation: atomicAdd returns the old partial sum, so the rounding
+// error of that very addition is recovered with TwoSum (Knuth) and added into the low word.
+__device__ __forceinline__ void dd_atomic_add(double* hi, double* lo, double x) {
+  double old = atomicAdd(hi, x);
+  double s = old + x;
+  if (!isfinite(s)) return;
+  double bp = s - old;
+  double err = (old - (s - bp)) + (x - bp);
+  if (err != 0.0) atomicAdd(lo, err);
+}
+
+// identity value word(s) of a field, written at record init
+__host__ __device__ inline void field_identity(int kind, uint64_t* w0, uint64_t* w1, int* nwords, int* bytes) {
+  *w1 = 0;
+  *nwords = 1;
+  switch (kind) {
+    case F_LEN: case F_CNT: *w0 = 0; *bytes = 4; break;
+    case F_SUM_DD: *w0 = 0; *nwords = 2; *bytes = 16; break;
+    case F_SUM_I: *w0 = 0; *bytes = 8; break;
+    case F_MIN_I: case F_MIN_F: *w0 = 0x7FFFFFFFFFFFFFFFULL; *bytes = 8; break;
+    case F_MAX_I: case F_MAX_F: *w0 = 0x8000000000000000ULL; *bytes = 8; break;
+    case F_MIN_U: *w0 = 0xFFFFFFFFFFFFFFFFULL; *bytes = 8; break;
+    default: *w0 = 0; *bytes = 8; break;  // F_MAX_U
+  }
+}
+
+// Adds one row to a group record (in shared or global memory).
+template <bool SMEM>
+__device__ __forceinline__ void apply_row(const DQuery& q, const TileCtx& t, uint8_t* rec, int64_t lr) {
+  for (int i = 0; i < q.n_fields; i++) {
+    const DField F = q.field[i];
+    uint8_t* p = rec + F.off;
+    if (F.kind == F_LEN) {
+      atomicAdd((unsigned int*)p, 1u);
+      continue;
+    }
+    if (!tc_isvalid(q, t, F.col, lr)) continue;
+    if (F.kind == F_CNT) {
+      atomicAdd((unsigned int*)p, 1u);
+      continue;
+    }
+    uint64_t b = tc_bits(q, t, F.col, lr);
+    int dt = q.col[F.col].dtype;
+    switch (F.kind) {
+      case F_SUM_DD: dd_atomic_add((double*)p, (double*)(p + 8), pmb_bits_to_f64(b, dt)); break;
+      case F_SUM_I: atomicAdd((unsigned long long*)p, (unsigned long long)pmb_bits_to_i64(b, dt)); break;
+      case F_MIN_I: {
+        long long v = (long long)pmb_bits_to_i64(b, dt);
+        if (!SMEM || v < *(volatile long long*)p) atomicMin((long long*)p, v);
+        break;
+      }
+      case F_MAX_I: {
+        long long v = (long long)pmb_bits_to_i64(b, dt);
+        if (!SMEM || v > *(volatile long long*)p) atomicMax((long long*)p, v);
+        break;
+      }
+      case F_MIN_U:
+        if (!SMEM || b < *(volatile unsigned long long*)p) atomicMin((unsigned long long*)p, (unsigned long long)b);
+        break;
+      case F_MAX_U:
+        if (!SMEM || b > *(volatile unsigned long long*)p) atomicMax((unsigned long long*)p, (unsigned long long)b);
+        break;
+      case F_MIN_F: {
+        double x = pmb_bits_to_f64(b, dt);
+        long long k = isnan(x) ? (long long)0x8000000000000000LL : pmb_f64_key(x);
+        if (!SMEM || k < *(volatile long long*)p) atomicMin((long long*)p, k);
+        break;
+      }
+      default: {  // F_MAX_F
+        double x = pmb_bits_to_f64(b, dt);
+        long long k = isnan(x) ? (long long)0x7FFFFFFFFFFFFFFFLL : pmb_f64_key(x);
+        if (!SMEM || k > *(volatile long long*)p) atomicMax((long long*)p, k);
+        break;
+      }
+    }
+  }
+}
+
+// Merges a finished record `src` into `dst` (global memory).
+__device__ __forceinline__ void merge_record(const DQuery& q, uint8_t* dst, const uint8_t* src) {
+  for (int i = 0; i < q.n_fields; i++) {
+    const DField F = q.field[i];
+    uint8_t* d = dst + F.off;
+    const uint8_t* s = src + F.off;
+    switch (F.kind) {
+      case F_LEN:
+      case F_CNT: {
+        unsigned int v = *(const unsigned int*)s;
+        if (v) atomicAdd((unsigned int*)d, v);
+        break;
+      }
+      case F_SUM_DD: {
+        double hi = *(const double*)s, lo = *(const double*)(s + 8);
+        if (hi != 0.0) dd_atomic_add((double*)d, (double*)(d + 8), hi);
+        if (lo != 0.0) atomicAdd((double*)(d + 8), lo);
+        break;
+      }
+      case F_SUM_I: {
+        unsigned long long v = *(const unsigned long long*)s;
+        if (v) atomicAdd((unsigned long long*)d, v);
+        break;
+      }
+      case F_MIN_I:
+      case F_MIN_F: {
+        long long v = *(const long long*)s;
+        if (v != 0x7FFFFFFFFFFFFFFFLL) atomicMin((long long*)d, v);
+        break;
+      }
+      case F_MAX_I:
+      case F_MAX_F: {
+        long long v = *(const long long*)s;
+        if (v != (long long)0x8000000000000000LL) atomicMax((long long*)d, v);
+        break;
+      }
+      case F_MIN_U: {
+        unsigned long long v = *(const unsigned long long*)s;
+        if (v != 0xFFFFFFFFFFFFFFFFULL) atomicMin((unsigned long long*)d, v);
+        break;
+      }
+      default: {
+        unsigned long long v = *(const unsigned long long*)s;
+        if (v) atomicMax((unsigned long long*)d, v);
+        break;
+      }
+    }
+  }
+}

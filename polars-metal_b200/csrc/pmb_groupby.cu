@@ -1,0 +1,709 @@
+// pmb_groupby.cu — filter -> group_by -> fused aggregate on sm_100a.
+//
+// Replaces, for this path: `_native.execute_groupby` (crates/polars-metal-core/src/udf/groupby/mod.rs:747-1144),
+// the CPU compaction it is fed from (python/polars_metal/_udf.py:550-597), key encoding
+// (crates/polars-metal-kernels/src/groupby.rs:155-302), the build strategies A1/A3
+// (groupby.rs:450-538, src/groupby_build_partitioned/gpu.rs:115-258, src/groupby_global_hash/gpu.rs:34-123),
+// the per-aggregation CPU folds (groupby.rs:1268-1700) and the fused-aggregate kernel
+// (groupby.rs:2599-2833, src/aggregate_fused/emitter.rs:189-393).
+//
+// Design (one pass over the input, no row_to_group materialisation):
+//   k_sketch     — 65,536 sampled rows -> distinct / singleton counts -> group estimate
+//   k_table_init — global open-addressing table: keys = EMPTY, records = identity
+//   k_hash_agg   — persistent CTAs; each column tile arrives in shared memory by 1-D TMA bulk
+//                  copies (cp.async.bulk + mbarrier, multi-stage ring); per row: predicate in
+//                  registers -> packed key -> per-CTA shared-memory table (hot keys) or the
+//                  global table -> fused state update with atomics; at exit the shared table is
+//                  merged into the global one.
+//   k_finalize   — occupied slots -> dense output columns in slot order (single pass,
+//                  decoupled look-back), keys decoded, aggregates finalised (Arrow layout).
+// A capacity overflow (probe limit) sets a status bit; the host re-runs with 4x capacity, so
+// the estimate can only cost time, never change results.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pmb_groupby.h"
+
+// ============================================================================ sketch
+#define SK_SAMPLES 65536
+#define SK_SLOTS (1 << 18)
+
+template <bool K128>
+__global__ void k_sketch(const __grid_constant__ DQuery q, int64_t m, unsigned long long* __restrict__ set_keys,
+                         unsigned int* __restrict__ set_cnt) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  int64_t row = (m == q.n_rows) ? i : (int64_t)((double)i * (double)q.n_rows / (double)m);
+  if (row >= q.n_rows) row = q.n_rows - 1;
+  TileCtx t{nullptr, nullptr, nullptr, 0};
+  uint64_t k;
+  if (K128) {
+    Key128 kk = pack_key128(q, t, row);
+    k = pmb_fmix64(kk.lo ^ pmb_fmix64(kk.hi + 0x9E3779B97F4A7C15ULL));
+  } else {
+    k = pack_key64(q, t, row);
+  }
+  if (k == PMB_EMPTY64) k = PMB_EMPTY64 - 1;
+  uint32_t s = (uint32_t)(pmb_fmix64(k) & (SK_SLOTS - 1));
+  for (int p = 0; p < SK_SLOTS; p++) {
+    unsigned long long cur = set_keys[s];
+    if (cur == k) break;
+    if (cur == PMB_EMPTY64) {
+      unsigned long long old = atomicCAS(&set_keys[s], PMB_EMPTY64, k);
+      if (old == PMB_EMPTY64 || old == k) break;
+    }
+    s = (s + 1) & (SK_SLOTS - 1);
+  }
+  atomicAdd(&set_cnt[s], 1u);
+}
+
+// distinct count, singletons and doubletons of the sample
+__global__ void k_sketch_reduce(const unsigned long long* __restrict__ set_keys,
+                                const unsigned int* __restrict__ set_cnt, unsigned long long* __restrict__ out) {
+  __shared__ unsigned long long acc[3];
+  if (threadIdx.x < 3) acc[threadIdx.x] = 0;
+  __syncthreads();
+  unsigned long long d = 0, f1 = 0, f2 = 0;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < SK_SLOTS; s += gridDim.x * blockDim.x) {
+    if (set_keys[s] != PMB_EMPTY64) {
+      d++;
+      unsigned int c = set_cnt[s];
+      f1 += c == 1;
+      f2 += c == 2;
+    }
+  }
+  atomicAdd(&acc[0], d);
+  atomicAdd(&acc[1], f1);
+  atomicAdd(&acc[2], f2);
+  __syncthreads();
+  if (threadIdx.x < 3) atomicAdd(&out[threadIdx.x], acc[threadIdx.x]);
+}
+
+// ============================================================================ table init
+__global__ void k_table_init(unsigned long long* __restrict__ keys, int64_t key_words, uint64_t* __restrict__ recs,
+                             int64_t n_recs, int rec_words, const __grid_constant__ RecInit ri) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t k = i; k < key_words; k += stride) keys[k] = PMB_EMPTY64;
+  int64_t total = n_recs * rec_words;
+  for (int64_t w = i; w < total; w += stride) recs[w] = ri.w[w % rec_words];
+}
+
+// ============================================================================ global table
+__device__ __forceinline__ int64_t gfind64(const HashParams& P, uint64_t key, uint64_t h) {
+  if (key == PMB_EMPTY64) {
+    if (*(volatile unsigned int*)&P.status[1] == 0) atomicOr(&P.status[1], 1u);
+    return (int64_t)P.gcap;
+  }
+  uint64_t mask = P.gcap - 1, i = h & mask;
+  unsigned long long* keys = P.gkeys;
+  for (int p = 0; p < P.gprobe; p++) {
+    unsigned long long k = keys[i];
+    if (k == key) return (int64_t)i;
+    if (k == PMB_EMPTY64) {
+      unsigned long long old = atomicCAS(&keys[i], PMB_EMPTY64, key);
+      if (old == PMB_EMPTY64 || old == key) return (int64_t)i;
+    }
+    i = (i + 1) & mask;
+  }
+  atomicOr(P.status, PMB_ST_OVERFLOW);
+  return -1;
+}
+
+struct __align__(16) K128Slot {
+  unsigned long long lo, hi;
+};
+
+__device__ __forceinline__ int64_t gfind128(const HashParams& P, Key128 key, uint64_t h) {
+  if (key.lo == PMB_EMPTY64 && key.hi == PMB_EMPTY64) {
+    if (*(volatile unsigned int*)&P.status[1] == 0) atomicOr(&P.status[1], 1u);
+    return (int64_t)P.gcap;
+  }
+  uint64_t mask = P.gcap - 1, i = h & mask;
+  K128Slot* keys = reinterpret_cast<K128Slot*>(P.gkeys);
+  for (int p = 0; p < P.gprobe; p++) {
+    K128Slot cur = keys[i];
+    if (cur.lo == key.lo && cur.hi == key.hi) return (int64_t)i;
+    // a 16-byte load may observe a slot mid-publication: any EMPTY half means "ask the CAS"
+    if (cur.lo == PMB_EMPTY64 || cur.hi == PMB_EMPTY64) {
+      K128Slot want{key.lo, key.hi}, empty{PMB_EMPTY64, PMB_EMPTY64};
+      K128Slot old = atomicCAS(&keys[i], empty, want);
+      if ((old.lo == PMB_EMPTY64 && old.hi == PMB_EMPTY64) || (old.lo == key.lo && old.hi == key.hi))
+        return (int64_t)i;
+    }
+    i = (i + 1) & mask;
+  }
+  atomicOr(P.status, PMB_ST_OVERFLOW);
+  return -1;
+}
+
+// ============================================================================ fused hash aggregation
+__device__ __forceinline__ int sfind64(unsigned long long* skeys, int S, int probes, uint64_t key, uint64_t h) {
+  if (key == PMB_EMPTY64) return -1;
+  int i = (int)((h >> 40) & (uint64_t)(S - 1));
+  for (int p = 0; p < probes; p++) {
+    unsigned long long k = skeys[i];
+    if (k == key) return i;
+    if (k == PMB_EMPTY64) {
+      unsigned long long old = atomicCAS(&skeys[i], PMB_EMPTY64, (unsigned long long)key);
+      if (old == PMB_EMPTY64 || old == key) return i;
+    }
+    i = (i + 1) & (S - 1);
+  }
+  return -1;
+}
+
+template <bool K128>
+__device__ __forceinline__ void process_row(const HashParams& P, const TileCtx& t, int lr,
+                                            unsigned long long* skeys, uint8_t* srecs) {
+  const DQuery& q = P.q;
+  if (!eval_keep(q, t, lr)) return;
+  const int rb = q.rec_bytes;
+  if (!K128) {
+    uint64_t key = pack_key64(q, t, lr);
+    uint64_t h = pmb_fmix64(key);
+    if (P.smem_slots) {
+      int si = sfind64(skeys, P.smem_slots, P.smem_probe, key, h);
+      if (si >= 0) {
+        apply_row<true>(q, t, srecs + (size_t)si * rb, lr);
+        return;
+      }
+    }
+    int64_t gi = gfind64(P, key, h);
+    if (gi >= 0) apply_row<false>(q, t, P.grecs + (size_t)gi * rb, lr);
+  } else {
+    Key128 key = pack_key128(q, t, lr);
+    uint64_t h = pmb_fmix64(key.lo ^ pmb_fmix64(key.hi + 0x9E3779B97F4A7C15ULL));
+    int64_t gi = gfind128(P, key, h);
+    if (gi >= 0) apply_row<false>(q, t, P.grecs + (size_t)gi * rb, lr);
+  }
+}
+
+template <int NT, bool K128>
+__global__ void __launch_bounds__(NT, 1) k_hash_agg(const __grid_constant__ HashParams P) {
+  extern __shared__ __align__(128) uint8_t sm[];
+  __shared__ int32_t s_doff[PMB_MAX_COLS];
+  __shared__ int32_t s_voff[PMB_MAX_COLS];
+  __shared__ int s_abort;
+  const DQuery& q = P.q;
+  const int tid = threadIdx.x;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm);
+  unsigned long long* skeys = reinterpret_cast<unsigned long long*>(sm + P.smem_keys_off);
+  uint8_t* srecs = sm + P.smem_recs_off;
+  const int S = P.smem_slots;
+  const int TILE = P.tile_rows;
+  const int STAGES = P.stages;
+
+  // shared table: keys EMPTY, records identity (so a claim needs no record publication)
+  for (int i = tid; i < S; i += NT) skeys[i] = PMB_EMPTY64;
+  const int rw = q.rec_bytes / 8;
+  for (int w = tid; w < S * rw; w += NT) reinterpret_cast<uint64_t*>(srecs)[w] = P.rec_init.w[w % rw];
+  if (tid < PMB_MAX_COLS) {
+    s_doff[tid] = P.stage_data_off[tid];
+    s_voff[tid] = P.stage_valid_off[tid];
+  }
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+    s_abort = 0;
+  }
+  __syncthreads();
+
+  const int64_t G = gridDim.x;
+  const int64_t n_full = P.n_full_tiles;
+  const int64_t my_tiles = n_full > (int64_t)blockIdx.x ? (n_full - 1 - blockIdx.x) / G + 1 : 0;
+
+  auto issue = [&](int64_t k) {
+    int s = (int)(k % STAGES);
+    int64_t tile = blockIdx.x + k * G;
+    uint8_t* base = sm + P.stage_region_off + (size_t)s * P.stage_bytes;
+    mbar_arrive_expect_tx(&bars[s], (uint32_t)P.stage_bytes_used);
+    for (int j = 0; j < P.n_staged; j++) {
+      int c = P.staged_col[j];
+      const DCol& C = q.col[c];
+      uint32_t db = C.elem ? (uint32_t)(TILE * C.elem) : (uint32_t)(TILE / 8);
+      const uint8_t* src = C.data + (C.elem ? tile * TILE * C.elem : tile * TILE / 8);
+      bulk_g2s(base + P.stage_data_off[c], src, db, &bars[s]);
+      if (C.valid) bulk_g2s(base + P.stage_valid_off[c], C.valid + tile * TILE / 8, (uint32_t)(TILE / 8), &bars[s]);
+    }
+  };
+
+  if (tid == 0) {
+    for (int64_t k = 0; k < STAGES && k < my_tiles; k++) issue(k);
+  }
+
+  int64_t k = 0;
+  for (; k < my_tiles; k++) {
+    int s = (int)(k % STAGES);
+    uint32_t parity = (uint32_t)((k / STAGES) & 1);
+    bool ok = mbar_wait_bounded(&bars[s], parity);
+    if (!ok) s_abort = 1;
+    if (ok) {
+      TileCtx t{sm + P.stage_region_off + (size_t)s * P.stage_bytes, s_doff, s_voff, 0};
+      for (int lr = tid; lr < TILE; lr += NT) process_row<K128>(P, t, lr, skeys, srecs);
+    }
+    __syncthreads();
+    if (s_abort) break;
+    if (tid == 0 && k + STAGES < my_tiles) {
+      fence_proxy_async();
+      issue(k + STAGES);
+    }
+  }
+  if (s_abort) {
+    // report, then wait (bounded) for this CTA's copies still in flight before exiting
+    if (tid == 0) {
+      atomicOr(P.status, PMB_ST_TIMEOUT);
+      for (int64_t j = k; j < my_tiles && j < k + STAGES; j++)
+        mbar_wait_bounded(&bars[j % STAGES], (uint32_t)((j / STAGES) & 1));
+    }
+    __syncthreads();
+    return;
+  }
+
+  // ragged tail tile straight from global memory
+  if (P.tail_rows > 0 && (int64_t)blockIdx.x == n_full % G) {
+    TileCtx t{nullptr, s_doff, s_voff, n_full * TILE};
+    for (int lr = tid; lr < P.tail_rows; lr += NT) process_row<K128>(P, t, lr, skeys, srecs);
+  }
+  __syncthreads();
+
+  // merge the shared table into the global table
+  if (!K128) {
+    for (int i = tid; i < S; i += NT) {
+      unsigned long long key = skeys[i];
+      if (key == PMB_EMPTY64) continue;
+      int64_t gi = gfind64(P, key, pmb_fmix64(key));
+      if (gi >= 0) merge_record(q, P.grecs + (size_t)gi * q.rec_bytes, srecs + (size_t)i * q.rec_bytes);
+    }
+  }
+}
+
+// ============================================================================ finalize
+template <int NT, int PER, bool K128>
+__global__ void __launch_bounds__(NT) k_finalize(const __grid_constant__ FinParams F) {
+  __shared__ int s_cnt[PER][NT / 32];
+  __shared__ int s_off[PER][NT / 32];
+  __shared__ long long s_tile;
+  __shared__ unsigned long long s_base;
+  const DQuery& q = F.q;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = (long long)atomicAdd(F.ticket, 1ULL);
+  __syncthreads();
+  const long long tile = s_tile;
+  const int64_t nslots = (int64_t)F.gcap + 1;  // + sentinel slot
+  bool occ[PER];
+  int64_t slot[PER];
+  const bool sentinel_used = F.status[1] != 0;
+  for (int j = 0; j < PER; j++) {
+    slot[j] = tile * (NT * PER) + (int64_t)j * NT + tid;
+    bool o = false;
+    if (slot[j] < (int64_t)F.gcap) {
+      if (K128) {
+        const unsigned long long* kk = F.gkeys + 2 * slot[j];
+        o = !(kk[0] == PMB_EMPTY64 && kk[1] == PMB_EMPTY64);
+      } else {
+        o = F.gkeys[slot[j]] != PMB_EMPTY64;
+      }
+    } else if (slot[j] == (int64_t)F.gcap) {
+      o = sentinel_used;
+    }
+    occ[j] = o && slot[j] < nslots;
+    unsigned b = __ballot_sync(0xffffffffu, occ[j]);
+    if (lane == 0) s_cnt[j][warp] = __popc(b);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int j = 0; j < PER; j++)
+      for (int w = 0; w < NT / 32; w++) {
+        s_off[j][w] = acc;
+        acc += s_cnt[j][w];
+      }
+    unsigned long long base = pmb_lookback(F.lb_status, tile, (unsigned long long)acc, F.status);
+    s_base = base;
+    if (tile == (long long)gridDim.x - 1) *F.n_groups = base + acc;
+  }
+  __syncthreads();
+  const unsigned long long base = s_base;
+  for (int j = 0; j < PER; j++) {
+    unsigned b = __ballot_sync(0xffffffffu, occ[j]);
+    if (b == 0) continue;
+    int rank = __popc(b & ((1u << lane) - 1u));
+    int64_t p = (int64_t)(base + s_off[j][warp] + rank);
+    int64_t p_first = (int64_t)(base + s_off[j][warp]);
+    uint64_t klo = PMB_EMPTY64, khi = PMB_EMPTY64;
+    const uint8_t* rec = nullptr;
+    if (occ[j]) {
+      if (slot[j] < (int64_t)F.gcap) {
+        if (K128) {
+          klo = F.gkeys[2 * slot[j]];
+          khi = F.gkeys[2 * slot[j] + 1];
+        } else {
+          klo = F.gkeys[slot[j]];
+          khi = 0;
+        }
+      } else if (!K128) {
+        khi = 0;
+      }
+      rec = F.grecs + (size_t)slot[j] * q.rec_bytes;
+    }
+    int oc = 0;
+    // keys
+    for (int k = 0; k < q.n_keys; k++, oc++) {
+      const DKey& K = q.key[k];
+      uint64_t v = 0;
+      bool valid = false;
+      if (occ[j]) valid = unpack_field(K, klo, khi, v);
+      int dt = q.col[K.col].dtype;
+      uint8_t* d = F.out_data[oc];
+      if (occ[j]) {
+        switch (pmb_dtype_bytes(dt)) {
+          case 0: break;
+          case 1: d[p] = (uint8_t)v; break;
+          case 2: reinterpret_cast<uint16_t*>(d)[p] = (uint16_t)v; break;
+          case 4: reinterpret_cast<uint32_t*>(d)[p] = (uint32_t)v; break;
+          default: reinterpret_cast<uint64_t*>(d)[p] = v; break;
+        }
+      }
+      if (dt == PMB_BOOL) warp_set_bits(reinterpret_cast<unsigned int*>(d), p, p_first, occ[j] && valid && v);
+      warp_set_bits(reinterpret_cast<unsigned int*>(F.out_valid[oc]), p, p_first, occ[j] && valid);
+    }
+    // aggregates
+    for (int a = 0; a < q.n_aggs; a++, oc++) {
+      const DAggOut& A = q.agg[a];
+      bool valid = true;
+      uint64_t bits = 0;
+      if (occ[j]) finalize_agg(q, A, rec, valid, bits);
+      uint8_t* d = F.out_data[oc];
+      if (occ[j]) {
+        switch (pmb_dtype_bytes(A.out_dtype)) {
+          case 0: break;
+          case 1: d[p] = (uint8_t)bits; break;
+          case 2: reinterpret_cast<uint16_t*>(d)[p] = (uint16_t)bits; break;
+          case 4: reinterpret_cast<uint32_t*>(d)[p] = (uint32_t)bits; break;
+          default: reinterpret_cast<uint64_t*>(d)[p] = bits; break;
+        }
+      }
+      warp_set_bits(reinterpret_cast<unsigned int*>(F.out_valid[oc]), p, p_first, occ[j] && valid);
+    }
+  }
+}
+
+// ============================================================================ host side
+static int smem_table_bytes(int S, int rec) { return S * (8 + rec); }
+
+struct Plan {
+  int tile = 1024;
+  int stages = 3;
+  int nt = 512;
+  int smem_slots = 0;
+  int smem_probe = 8;
+  uint64_t gcap = 1024;
+  int strategy = PMB_STRATEGY_GLOBAL_HASH;
+};
+
+static uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// stage layout in shared memory for the columns the query touches
+static int layout_stage(const CompiledQuery& cq, int tile, HashParams& P) {
+  const DQuery& q = cq.dq;
+  int off = 0;
+  int used = 0;
+  P.n_staged = 0;
+  for (int c = 0; c < PMB_MAX_COLS; c++) {
+    P.stage_data_off[c] = 0;
+    P.stage_valid_off[c] = 0;
+  }
+  for (int c = 0; c < q.n_cols; c++) {
+    int db = q.col[c].elem ? tile * q.col[c].elem : tile / 8;
+    P.stage_data_off[c] = off;
+    off += (int)pmb_align((size_t)db, 16);
+    used += db;
+    if (q.col[c].valid) {
+      P.stage_valid_off[c] = off;
+      off += (int)pmb_align((size_t)(tile / 8), 16);
+      used += tile / 8;
+    }
+    P.staged_col[P.n_staged++] = c;
+  }
+  P.stage_bytes = (int)pmb_align((size_t)off, 128);
+  P.stage_bytes_used = used;
+  return P.stage_bytes;
+}
+
+template <int NT, bool K128>
+static int launch_hash(pmb_handle* h, const HashParams& P, int smem, int grid) {
+  auto kern = k_hash_agg<NT, K128>;
+  PMB_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  pmb_kernel_begin(h, "hash_agg");
+  kern<<<grid, NT, smem, h->stream>>>(P);
+  pmb_kernel_end(h);
+  PMB_CUDA(h, cudaGetLastError());
+  return PMB_OK;
+}
+
+template <bool K128>
+static int launch_finalize(pmb_handle* h, const FinParams& F, int64_t nslots) {
+  constexpr int NT = 256, PER = 4;
+  int64_t tiles = (nslots + NT * PER - 1) / (NT * PER);
+  pmb_kernel_begin(h, "finalize");
+  k_finalize<NT, PER, K128><<<(unsigned)tiles, NT, 0, h->stream>>>(F);
+  pmb_kernel_end(h);
+  PMB_CUDA(h, cudaGetLastError());
+  return PMB_OK;
+}
+
+int pmb_groupby_sketch(pmb_handle* h, const CompiledQuery& cq, SketchOut* out) {
+  const DQuery& q = cq.dq;
+  int64_t m = std::min<int64_t>(q.n_rows, SK_SAMPLES);
+  out->samples = m;
+  out->distinct = out->singletons = out->doubletons = 0;
+  if (m == 0) return PMB_OK;
+  unsigned long long* keys = (unsigned long long*)pmb_ws_alloc(h, sizeof(unsigned long long) * SK_SLOTS);
+  unsigned int* cnt = (unsigned int*)pmb_ws_alloc(h, sizeof(unsigned int) * SK_SLOTS);
+  unsigned long long* res = (unsigned long long*)pmb_ws_alloc(h, 64);
+  if (!keys || !cnt || !res) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sketch)");
+  PMB_CUDA(h, cudaMemsetAsync(keys, 0xFF, sizeof(unsigned long long) * SK_SLOTS, h->stream));
+  PMB_CUDA(h, cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * SK_SLOTS, h->stream));
+  PMB_CUDA(h, cudaMemsetAsync(res, 0, 64, h->stream));
+  pmb_kernel_begin(h, "sketch");
+  if (q.key_bits > 64) k_sketch<true><<<(unsigned)((m + 255) / 256), 256, 0, h->stream>>>(q, m, keys, cnt);
+  else k_sketch<false><<<(unsigned)((m + 255) / 256), 256, 0, h->stream>>>(q, m, keys, cnt);
+  pmb_kernel_end(h);
+  PMB_CUDA(h, cudaGetLastError());
+  pmb_kernel_begin(h, "sketch_reduce");
+  k_sketch_reduce<<<64, 256, 0, h->stream>>>(keys, cnt, res);
+  pmb_kernel_end(h);
+  PMB_CUDA(h, cudaGetLastError());
+  PMB_CUDA(h, cudaMemcpyAsync(h->pinned, res, 24, cudaMemcpyDeviceToHost, h->stream));
+  PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+  const unsigned long long* r = (const unsigned long long*)h->pinned;
+  out->distinct = (int64_t)r[0];
+  out->singletons = (int64_t)r[1];
+  out->doubletons = (int64_t)r[2];
+  return PMB_OK;
+}
+
+// Distinct-group estimate from the sample: exact when the sample is the whole input, else the
+// GEE estimator (Charikar, Chaudhuri, Motwani, Narasayya 2000): sqrt(n/m) * f1 + (d - f1).
+int64_t pmb_estimate_groups(const SketchOut& s, int64_t n_rows) {
+  if (s.samples <= 0) return 0;
+  if (s.samples >= n_rows) return s.distinct;
+  double scale = std::sqrt((double)n_rows / (double)s.samples);
+  double est = scale * (double)s.singletons + (double)(s.distinct - s.singletons);
+  if ((double)s.singletons > 0.9 * (double)s.samples) est = (double)n_rows;  // near-unique keys
+  est = std::max(est, (double)s.distinct);
+  est = std::min(est, (double)n_rows);
+  return (int64_t)est;
+}
+
+static void build_output_columns(const CompiledQuery& cq, pmb_result* r, const pmb_column* cols) {
+  const DQuery& q = cq.dq;
+  int oc = 0;
+  for (int k = 0; k < q.n_keys; k++, oc++) r->columns[oc].dtype = q.col[q.key[k].col].dtype;
+  for (int a = 0; a < q.n_aggs; a++, oc++) r->columns[oc].dtype = q.agg[a].out_dtype;
+  (void)cols;
+}
+
+int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
+                     pmb_result* r) {
+  DQuery& q = cq.dq;
+  const bool K128 = q.key_bits > 64;
+  const int rec = q.rec_bytes;
+  Plan pl;
+  pl.strategy = strategy;
+  if (K128 && strategy == PMB_STRATEGY_SMEM_HASH) pl.strategy = PMB_STRATEGY_GLOBAL_HASH;
+  HashParams P;
+  memset(&P, 0, sizeof(P));
+  P.q = q;
+  P.tile_rows = pl.tile;
+  layout_stage(cq, pl.tile, P);
+  // shared memory budget: mbarriers, stages, table
+  const int budget = h->max_smem_optin - 1024;
+  int stages = 3;
+  while (stages > 1 && 128 + stages * P.stage_bytes > budget / 2) stages--;
+  int smem_fixed = 128 + stages * P.stage_bytes;
+  if (smem_fixed > budget) {
+    // very wide queries: smaller tiles
+    pl.tile = 512;
+    P.tile_rows = pl.tile;
+    layout_stage(cq, pl.tile, P);
+    stages = 2;
+    smem_fixed = 128 + stages * P.stage_bytes;
+    if (smem_fixed > budget) return pmb_fail(h, PMB_E_UNSUPPORTED, "query touches too many columns for one tile");
+  }
+  int S = 0;
+  if (!K128) {
+    int room = budget - smem_fixed;
+    S = 1;
+    while (smem_table_bytes(S * 2, rec) <= room && S * 2 <= 4096) S *= 2;
+    if (S < 64) S = 0;
+    if (strategy == PMB_STRATEGY_SMEM_HASH && est > 0) {
+      int want = (int)next_pow2((uint64_t)std::max<int64_t>(2 * est, 64));
+      if (want < S) S = want;
+    }
+  }
+  P.stages = stages;
+  P.smem_slots = S;
+  P.smem_probe = S ? std::min(S, (strategy == PMB_STRATEGY_SMEM_HASH) ? 64 : 16) : 0;
+  P.stage_region_off = 128;
+  P.smem_keys_off = (int)pmb_align((size_t)(128 + stages * P.stage_bytes), 16);
+  P.smem_recs_off = P.smem_keys_off + S * 8;
+  int smem = P.smem_recs_off + S * rec;
+  const int64_t n = q.n_rows;
+  P.n_full_tiles = n / pl.tile;
+  P.tail_rows = (int32_t)(n % pl.tile);
+  if (cq.rec_words > (int)(sizeof(P.rec_init.w) / 8)) return pmb_fail(h, PMB_E_UNSUPPORTED, "record too large");
+  for (int w = 0; w < cq.rec_words; w++) P.rec_init.w[w] = cq.rec_init[w];
+
+  uint64_t cap = next_pow2((uint64_t)std::max<int64_t>(2 * est, 1024));
+  if (uq->capacity_hint > 0) cap = next_pow2((uint64_t)std::max<int64_t>(2 * uq->capacity_hint, 1024));
+  const uint64_t cap_max = next_pow2((uint64_t)std::max<int64_t>(2 * n, 1024));
+  cap = std::min(cap, cap_max);
+
+  const int n_out = q.n_keys + q.n_aggs;
+  for (int attempt = 0;; attempt++) {
+    const int key_words = K128 ? 2 : 1;
+    size_t keys_bytes = (size_t)(cap + 1) * 8 * key_words;
+    size_t recs_bytes = (size_t)(cap + 1) * rec;
+    unsigned long long* gkeys = (unsigned long long*)pmb_ws_alloc(h, keys_bytes);
+    uint8_t* grecs = (uint8_t*)pmb_ws_alloc(h, recs_bytes);
+    unsigned int* status = (unsigned int*)pmb_ws_alloc(h, 64);
+    int64_t nslots = (int64_t)cap + 1;
+    int64_t fin_tiles = (nslots + 1024 - 1) / 1024;
+    unsigned long long* lb = (unsigned long long*)pmb_ws_alloc(h, (size_t)fin_tiles * 8 + 64);
+    if (!gkeys || !grecs || !status || !lb) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (hash table)");
+    FinParams F;
+    memset(&F, 0, sizeof(F));
+    F.q = q;
+    for (int c = 0; c < n_out; c++) {
+      int dt = r->columns[c].dtype;
+      size_t db = dt == PMB_BOOL ? (size_t)((nslots + 31) / 32 * 4) : (size_t)nslots * pmb_dtype_bytes(dt);
+      F.out_data[c] = (uint8_t*)pmb_ws_alloc(h, db + 16);
+      F.out_valid[c] = (uint8_t*)pmb_ws_alloc(h, (size_t)((nslots + 31) / 32 * 4) + 16);
+      if (!F.out_data[c] || !F.out_valid[c]) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (outputs)");
+      PMB_CUDA(h, cudaMemsetAsync(F.out_valid[c], 0, (size_t)((nslots + 31) / 32 * 4), h->stream));
+      if (dt == PMB_BOOL) PMB_CUDA(h, cudaMemsetAsync(F.out_data[c], 0, db, h->stream));
+    }
+    PMB_CUDA(h, cudaMemsetAsync(status, 0, 64, h->stream));
+    PMB_CUDA(h, cudaMemsetAsync(lb, 0, (size_t)fin_tiles * 8 + 64, h->stream));
+    // table init
+    {
+      int64_t work = std::max<int64_t>((int64_t)(cap + 1) * key_words, (int64_t)(cap + 1) * cq.rec_words);
+      int blocks = (int)std::min<int64_t>((work + 255) / 256, (int64_t)h->sm_count * 16);
+      pmb_kernel_begin(h, "table_init");
+      k_table_init<<<blocks, 256, 0, h->stream>>>(gkeys, (int64_t)(cap + 1) * key_words, (uint64_t*)grecs,
+                                                  (int64_t)(cap + 1), cq.rec_words, P.rec_init);
+      pmb_kernel_end(h);
+      PMB_CUDA(h, cudaGetLastError());
+    }
+    P.gkeys = gkeys;
+    P.grecs = grecs;
+    P.gcap = cap;
+    P.gprobe = (int)std::min<uint64_t>(cap, 1u << 14);
+    P.status = status;
+    int grid = (int)std::max<int64_t>(1, std::min<int64_t>(P.n_full_tiles, (int64_t)h->sm_count));
+    int rc = K128 ? launch_hash<512, true>(h, P, smem, grid) : launch_hash<512, false>(h, P, smem, grid);
+    if (rc) return rc;
+    F.gkeys = gkeys;
+    F.grecs = grecs;
+    F.gcap = cap;
+    F.status = status;
+    F.lb_status = lb;
+    F.ticket = lb + fin_tiles;
+    F.n_groups = lb + fin_tiles + 1;
+    rc = K128 ? launch_finalize<true>(h, F, nslots) : launch_finalize<false>(h, F, nslots);
+    if (rc) return rc;
+    PMB_CUDA(h, cudaMemcpyAsync(h->pinned, status, 8, cudaMemcpyDeviceToHost, h->stream));
+    PMB_CUDA(h, cudaMemcpyAsync(h->pinned + 8, F.n_groups, 8, cudaMemcpyDeviceToHost, h->stream));
+    PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+    unsigned int st = *(unsigned int*)h->pinned;
+    if (st & PMB_ST_TIMEOUT) return pmb_fail(h, PMB_E_TIMEOUT, "a bounded device wait timed out");
+    if (st & PMB_ST_OVERFLOW) {
+      if (cap >= cap_max) return pmb_fail(h, PMB_E_OOM, "hash table overflow at maximum capacity");
+      cap = std::min(cap * 4, cap_max);
+      r->rehash_count++;
+      continue;
+    }
+    r->n_groups = (int64_t) * (unsigned long long*)(h->pinned + 8);
+    r->capacity = (int64_t)cap;
+    r->strategy_used = pl.strategy;
+    for (int c = 0; c < n_out; c++) {
+      r->columns[c].data = F.out_data[c];
+      r->columns[c].validity = F.out_valid[c];
+    }
+    return PMB_OK;
+  }
+}
+
+extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols,
+                           pmb_result** out) {
+  if (!h) return PMB_E_INVALID;
+  if (!out) return pmb_fail(h, PMB_E_INVALID, "out is NULL");
+  *out = nullptr;
+  PMB_CUDA(h, cudaSetDevice(h->device));
+  CompiledQuery cq;
+  int rc = pmb_compile_groupby(h, q, cols, n_cols, &cq);
+  if (rc) return rc;
+  rc = pmb_ws_begin(h);
+  if (rc) return rc;
+  pmb_call_begin(h);
+  pmb_result* r = pmb_result_new(cq.dq.n_keys + cq.dq.n_aggs);
+  if (!r) return pmb_fail(h, PMB_E_OOM, "host allocation failed");
+  build_output_columns(cq, r, cols);
+  auto bail = [&](int code) {
+    pmb_result_free(r);
+    return code;
+  };
+  // stage the touched columns
+  for (int c = 0; c < cq.dq.n_cols; c++) {
+    rc = pmb_stage_column(h, cols[cq.map.user[c]], cq.dq.n_rows, &cq.dq.col[c]);
+    if (rc) return bail(rc);
+  }
+  if (cq.dq.n_rows == 0) {
+    r->n_groups = 0;
+    r->strategy_used = q->strategy ? q->strategy : PMB_STRATEGY_GLOBAL_HASH;
+    for (int c = 0; c < r->n_columns; c++) {
+      r->columns[c].data = pmb_ws_alloc(h, 16);
+      r->columns[c].validity = (uint8_t*)pmb_ws_alloc(h, 16);
+    }
+  } else {
+    int strategy = q->strategy;
+    int64_t est = q->capacity_hint;
+    if (est <= 0 || strategy == PMB_STRATEGY_AUTO) {
+      SketchOut sk;
+      rc = pmb_groupby_sketch(h, cq, &sk);
+      if (rc) return bail(rc);
+      int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
+      if (est <= 0) est = e;
+      if (strategy == PMB_STRATEGY_AUTO) strategy = pmb_choose_strategy(h, cq, sk, est);
+    }
+    if (strategy == PMB_STRATEGY_SORT) strategy = PMB_STRATEGY_GLOBAL_HASH;  // sort path: see pmb_sort.cu
+    rc = pmb_groupby_hash(h, cq, q, strategy, est, r);
+    if (rc) return bail(rc);
+  }
+  rc = pmb_finish_outputs(h, r, q->output_on_device == 0);
+  if (rc) return bail(rc);
+  PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+  pmb_call_end(h);
+  *out = r;
+  return PMB_OK;
+}
+
+// Plain cardinality heuristic (the fallback of the learned selector): shared-memory tables
+// when every group fits a CTA's table, else the global table with a hot-key cache.
+int pmb_choose_strategy(pmb_handle* h, const CompiledQuery& cq, const SketchOut& sk, int64_t est) {
+  (void)h;
+  (void)sk;
+  if (cq.dq.key_bits > 64) return PMB_STRATEGY_GLOBAL_HASH;
+  return est <= 1024 ? PMB_STRATEGY_SMEM_HASH : PMB_STRATEGY_GLOBAL_HASH;
+}

@@ -1,0 +1,138 @@
+// pmb_groupby.h — kernel parameter blocks and finalisation helpers of the hash group-by.
+#pragma once
+
+#include "pmb_plan.h"
+
+struct RecInit {
+  uint64_t w[48];  // identity record words (records up to 384 bytes)
+};
+
+// parameters of k_hash_agg (passed as a __grid_constant__ kernel parameter)
+struct HashParams {
+  DQuery q;
+  RecInit rec_init;
+  int32_t tile_rows;
+  int32_t stages;
+  int32_t n_staged;
+  int32_t staged_col[PMB_MAX_COLS];
+  int32_t stage_data_off[PMB_MAX_COLS];  // per compact column, offset inside a stage
+  int32_t stage_valid_off[PMB_MAX_COLS];
+  int32_t stage_bytes;       // bytes per stage (padded)
+  int32_t stage_bytes_used;  // bytes the bulk copies of one tile deliver
+  int32_t stage_region_off;
+  int32_t smem_slots;        // shared table slots (0 = no shared table)
+  int32_t smem_probe;
+  int32_t smem_keys_off;
+  int32_t smem_recs_off;
+  int32_t tail_rows;
+  int64_t n_full_tiles;
+  unsigned long long* gkeys;  // global table keys, gcap + 1 slots (the last is the EMPTY-key slot)
+  uint8_t* grecs;             // global records, (gcap + 1) * rec_bytes
+  uint64_t gcap;
+  int32_t gprobe;
+  unsigned int* status;       // [0] status bits, [1] EMPTY-key slot used
+};
+
+#define PMB_MAX_OUT (PMB_MAX_KEYS + PMB_MAX_AGGS)
+
+struct FinParams {
+  DQuery q;
+  const unsigned long long* gkeys;
+  const uint8_t* grecs;
+  uint64_t gcap;
+  unsigned int* status;
+  unsigned long long* lb_status;  // look-back tile states
+  unsigned long long* ticket;     // tile ticket counter
+  unsigned long long* n_groups;
+  uint8_t* out_data[PMB_MAX_OUT];
+  uint8_t* out_valid[PMB_MAX_OUT];
+};
+
+struct SketchOut {
+  int64_t samples;
+  int64_t distinct;
+  int64_t singletons;
+  int64_t doubletons;
+};
+
+int pmb_groupby_sketch(pmb_handle* h, const CompiledQuery& cq, SketchOut* out);
+int64_t pmb_estimate_groups(const SketchOut& s, int64_t n_rows);
+int pmb_choose_strategy(pmb_handle* h, const CompiledQuery& cq, const SketchOut& sk, int64_t est);
+int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
+                     pmb_result* r);
+
+// Sets bit p of a bitmap for every lane whose `bit` is true. The warp's positions are
+// consecutive from p_first, so they touch at most two 32-bit words: one atomicOr each.
+__device__ __forceinline__ void warp_set_bits(unsigned int* words, int64_t p, int64_t p_first, bool bit) {
+  const int64_t w0 = p_first >> 5;
+  unsigned m0 = __reduce_or_sync(0xffffffffu, (bit && (p >> 5) == w0) ? (1u << (p & 31)) : 0u);
+  unsigned m1 = __reduce_or_sync(0xffffffffu, (bit && (p >> 5) == w0 + 1) ? (1u << (p & 31)) : 0u);
+  if ((threadIdx.x & 31) == 0) {
+    if (m0) atomicOr(&words[w0], m0);
+    if (m1) atomicOr(&words[w0 + 1], m1);
+  }
+}
+
+// Final value of aggregation A from a group record (Polars rules: all-null sum = 0, mean /
+// min / max of no valid value = null, NaN poisons float min / max, ints wrap).
+__device__ __forceinline__ void finalize_agg(const DQuery& q, const DAggOut& A, const uint8_t* rec, bool& valid,
+                                             uint64_t& bits) {
+  valid = true;
+  bits = 0;
+  auto u32 = [&](int f) { return *reinterpret_cast<const unsigned int*>(rec + q.field[f].off); };
+  auto u64 = [&](int f) { return *reinterpret_cast<const unsigned long long*>(rec + q.field[f].off); };
+  auto ddv = [&](int f) {
+    const double* p = reinterpret_cast<const double*>(rec + q.field[f].off);
+    return p[0] + p[1];
+  };
+  const bool fl = pmb_is_float(A.in_dtype);
+  switch (A.op) {
+    case PMB_AGG_LEN: bits = u32(A.f_len); return;
+    case PMB_AGG_COUNT: bits = u32(A.f_cnt); return;
+    case PMB_AGG_SUM:
+      if (fl) {
+        double v = ddv(A.f_main);
+        if (A.out_dtype == PMB_F32) bits = __float_as_uint((float)v);
+        else bits = (uint64_t)__double_as_longlong(v);
+      } else {
+        bits = u64(A.f_main);
+      }
+      return;
+    case PMB_AGG_MEAN: {
+      unsigned int c = u32(A.f_cnt);
+      if (c == 0) {
+        valid = false;
+        return;
+      }
+      double v;
+      if (fl) v = ddv(A.f_main) / (double)c;
+      else if (pmb_is_signed(A.in_dtype) || A.in_dtype == PMB_BOOL) v = (double)(long long)u64(A.f_main) / (double)c;
+      else v = (double)u64(A.f_main) / (double)c;
+      if (A.out_dtype == PMB_F32) bits = __float_as_uint((float)v);
+      else bits = (uint64_t)__double_as_longlong(v);
+      return;
+    }
+    default: {  // min / max
+      long long k = (long long)u64(A.f_main);
+      if (fl) {
+        bool mn = A.op == PMB_AGG_MIN;
+        long long ident = mn ? 0x7FFFFFFFFFFFFFFFLL : (long long)0x8000000000000000LL;
+        long long nanm = mn ? (long long)0x8000000000000000LL : 0x7FFFFFFFFFFFFFFFLL;
+        if (k == ident) {
+          valid = false;
+          return;
+        }
+        double v = (k == nanm) ? __longlong_as_double(0x7FF8000000000000LL) : pmb_f64_from_key(k);
+        if (A.in_dtype == PMB_F32) bits = __float_as_uint((float)v);
+        else bits = (uint64_t)__double_as_longlong(v);
+        return;
+      }
+      if (A.f_cnt >= 0 && u32(A.f_cnt) == 0) {
+        valid = false;
+        return;
+      }
+      bits = (uint64_t)k;
+      return;
+    }
+  }
+}

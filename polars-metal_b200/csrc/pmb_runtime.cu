@@ -1,0 +1,376 @@
+// pmb_runtime.cu — handle lifetime, device workspace, column staging, results, profiling.
+//
+// Replaces the reference's Metal runtime pieces for this path: MetalDevice / CommandQueue
+// (crates/polars-metal-kernels/src/command.rs:95-231), the Arrow -> device buffer bridge
+// (crates/polars-metal-buffer/src/bridge.rs:1-60) and the per-call buffer allocation the
+// reference does for every dispatch. Here one handle owns a stream and one growable device
+// workspace; each call bump-allocates from it and synchronises once at the end.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "pmb_internal.cuh"
+
+int pmb_fail(pmb_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int pmb_cuda_check(pmb_handle* h, cudaError_t e, const char* what) {
+  std::string m = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return pmb_fail(h, PMB_E_OOM, m);
+  return pmb_fail(h, PMB_E_CUDA, m);
+}
+
+// ------------------------------------------------------------------ workspace
+static void ws_free_all(pmb_handle* h) {
+  for (auto& b : h->ws) cudaFree(b.ptr);
+  h->ws.clear();
+}
+
+int pmb_ws_begin(pmb_handle* h) {
+  if (h->ws.size() > 1) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return pmb_cuda_check(h, e, "cudaStreamSynchronize");
+    size_t total = 0;
+    for (auto& b : h->ws) total += b.cap;
+    ws_free_all(h);
+    uint8_t* p = nullptr;
+    if (cudaMalloc((void**)&p, total) != cudaSuccess) {
+      cudaGetLastError();
+      return PMB_OK;  // blocks are added again on demand
+    }
+    h->ws.push_back({p, total, 0});
+  }
+  for (auto& b : h->ws) b.top = 0;
+  return PMB_OK;
+}
+
+void* pmb_ws_alloc(pmb_handle* h, size_t bytes) {
+  bytes = pmb_align(bytes ? bytes : 1, 256);
+  if (!h->ws.empty()) {
+    auto& b = h->ws.back();
+    if (b.top + bytes <= b.cap) {
+      void* p = b.ptr + b.top;
+      b.top += bytes;
+      return p;
+    }
+  }
+  size_t last = h->ws.empty() ? 0 : h->ws.back().cap;
+  size_t want = std::max(std::max(bytes, (size_t)64 << 20), last);
+  uint8_t* p = nullptr;
+  if (cudaMalloc((void**)&p, want) != cudaSuccess) {
+    cudaGetLastError();
+    if (want == bytes || cudaMalloc((void**)&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    want = bytes;
+  }
+  h->ws.push_back({p, want, bytes});
+  return p;
+}
+
+// ------------------------------------------------------------------ profiling
+static cudaEvent_t take_event(pmb_handle* h) {
+  if (h->event_next == h->event_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    h->event_pool.push_back(e);
+  }
+  return h->event_pool[h->event_next++];
+}
+
+void pmb_call_begin(pmb_handle* h) {
+  h->timings.clear();
+  h->event_next = 0;
+  h->launches = 0;
+  h->h2d = h->d2h = 0;
+  if (h->profiling) cudaEventRecord(h->call_start, h->stream);
+}
+
+void pmb_kernel_begin(pmb_handle* h, const char* name) {
+  h->launches++;
+  if (!h->profiling) return;
+  KernelTiming t;
+  t.name = name;
+  t.start = take_event(h);
+  t.stop = take_event(h);
+  cudaEventRecord(t.start, h->stream);
+  h->timings.push_back(t);
+}
+
+void pmb_kernel_end(pmb_handle* h) {
+  if (!h->profiling || h->timings.empty()) return;
+  cudaEventRecord(h->timings.back().stop, h->stream);
+}
+
+void pmb_call_end(pmb_handle* h) {
+  pmb_stats s{};
+  s.kernel_launches = h->launches;
+  s.h2d_bytes = h->h2d;
+  s.d2h_bytes = h->d2h;
+  if (h->profiling) {
+    cudaEventRecord(h->call_stop, h->stream);
+    cudaEventSynchronize(h->call_stop);
+    cudaEventElapsedTime(&s.total_ms, h->call_start, h->call_stop);
+    for (const KernelTiming& t : h->timings) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, t.start, t.stop);
+      int k = 0;
+      for (; k < s.n_kernels; k++)
+        if (t.name == s.names[k]) break;
+      if (k == s.n_kernels) {
+        if (s.n_kernels == PMB_MAX_STAT_KERNELS) continue;
+        strncpy(s.names[k], t.name.c_str(), 31);
+        s.names[k][31] = 0;
+        s.n_kernels++;
+      }
+      s.ms[k] += ms;
+      s.launches[k]++;
+    }
+  }
+  h->last_stats = s;
+}
+
+// ------------------------------------------------------------------ staging kernels
+// out bit i = in bit (i + shift), shift in [0, 8); out is zero-padded to whole bytes
+__global__ void k_bitmap_shift(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, int64_t n_bits,
+                               int shift, int64_t in_bytes) {
+  int64_t ob = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t n_out = (n_bits + 7) / 8;
+  for (; ob < n_out; ob += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = in[ob];
+    uint32_t hi = (ob + 1 < in_bytes) ? in[ob + 1] : 0u;
+    uint32_t v = ((hi << 8) | lo) >> shift;
+    int64_t rem = n_bits - ob * 8;
+    if (rem < 8) v &= (1u << rem) - 1u;
+    out[ob] = (uint8_t)v;
+  }
+}
+
+static int launch_shift(pmb_handle* h, const uint8_t* in, uint8_t* out, int64_t n_bits, int shift,
+                        int64_t in_bytes) {
+  int64_t n_out = (n_bits + 7) / 8;
+  if (n_out == 0) return PMB_OK;
+  int blocks = (int)std::min<int64_t>((n_out + 255) / 256, 4096);
+  pmb_kernel_begin(h, "bitmap_shift");
+  k_bitmap_shift<<<blocks, 256, 0, h->stream>>>(in, out, n_bits, shift, in_bytes);
+  pmb_kernel_end(h);
+  PMB_CUDA(h, cudaGetLastError());
+  return PMB_OK;
+}
+
+// copies `bytes` into the workspace (H2D when !on_device, D2D otherwise)
+static int copy_in(pmb_handle* h, const void* src, size_t bytes, bool on_device, uint8_t** dst) {
+  *dst = (uint8_t*)pmb_ws_alloc(h, bytes + 16);
+  if (!*dst) return pmb_fail(h, PMB_E_OOM, "workspace exhausted while staging a column");
+  if (bytes == 0) return PMB_OK;
+  PMB_CUDA(h, cudaMemcpyAsync(*dst, src, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                              h->stream));
+  if (!on_device) h->h2d += (int64_t)bytes;
+  return PMB_OK;
+}
+
+static int stage_bits(pmb_handle* h, const uint8_t* base, int64_t offset, int64_t n, bool on_device,
+                      const uint8_t** out) {
+  const uint8_t* first = base + offset / 8;
+  int shift = (int)(offset % 8);
+  int64_t bytes = (n + shift + 7) / 8;
+  if (on_device && shift == 0 && ((uintptr_t)first % 16) == 0) {
+    *out = first;
+    return PMB_OK;
+  }
+  uint8_t* raw;
+  int rc = copy_in(h, first, (size_t)bytes, on_device, &raw);
+  if (rc) return rc;
+  if (shift == 0) {
+    *out = raw;
+    return PMB_OK;
+  }
+  uint8_t* aligned = (uint8_t*)pmb_ws_alloc(h, (size_t)((n + 7) / 8) + 16);
+  if (!aligned) return pmb_fail(h, PMB_E_OOM, "workspace exhausted while staging a bitmap");
+  rc = launch_shift(h, raw, aligned, n, shift, bytes);
+  if (rc) return rc;
+  *out = aligned;
+  return PMB_OK;
+}
+
+int pmb_stage_column(pmb_handle* h, const pmb_column& c, int64_t n, DCol* out) {
+  out->dtype = c.dtype;
+  out->elem = pmb_dtype_bytes(c.dtype);
+  if (c.offset < 0) return pmb_fail(h, PMB_E_INVALID, "negative column offset");
+  if (n > 0 && c.data == nullptr) return pmb_fail(h, PMB_E_INVALID, "column data pointer is NULL");
+  bool dev = c.on_device != 0;
+  if (c.dtype == PMB_BOOL) {
+    int rc = stage_bits(h, (const uint8_t*)c.data, c.offset, n, dev, &out->data);
+    if (rc) return rc;
+  } else {
+    const uint8_t* p = (const uint8_t*)c.data + c.offset * out->elem;
+    if (dev && ((uintptr_t)p % 16) == 0) {
+      out->data = p;
+    } else {
+      uint8_t* d;
+      int rc = copy_in(h, p, (size_t)(n * out->elem), dev, &d);
+      if (rc) return rc;
+      out->data = d;
+    }
+  }
+  if (c.validity == nullptr) {
+    out->valid = nullptr;
+  } else {
+    int rc = stage_bits(h, c.validity, c.offset, n, dev, &out->valid);
+    if (rc) return rc;
+  }
+  return PMB_OK;
+}
+
+// ------------------------------------------------------------------ results
+pmb_result* pmb_result_new(int32_t n_columns) {
+  pmb_result* r = (pmb_result*)calloc(1, sizeof(pmb_result));
+  if (!r) return nullptr;
+  r->n_columns = n_columns;
+  r->columns = (pmb_out_column*)calloc((size_t)std::max(n_columns, 1), sizeof(pmb_out_column));
+  if (!r->columns) {
+    free(r);
+    return nullptr;
+  }
+  return r;
+}
+
+static size_t bitmap_bytes(int64_t n) {
+  size_t b = (size_t)((n + 7) / 8);
+  b = (b + 3) & ~(size_t)3;
+  return b < 4 ? 4 : b;
+}
+
+int pmb_finish_outputs(pmb_handle* h, pmb_result* r, bool to_host) {
+  int64_t n = r->n_groups;
+  for (int c = 0; c < r->n_columns; c++) {
+    pmb_out_column& oc = r->columns[c];
+    oc.length = n;
+    if (!to_host) {
+      oc.on_device = 1;
+      continue;
+    }
+    size_t db = oc.dtype == PMB_BOOL ? bitmap_bytes(n) : (size_t)n * pmb_dtype_bytes(oc.dtype);
+    size_t vb = bitmap_bytes(n);
+    void* hd = malloc(db ? db : 1);
+    uint8_t* hv = (uint8_t*)malloc(vb);
+    if (!hd || !hv) {
+      free(hd);
+      free(hv);
+      return pmb_fail(h, PMB_E_OOM, "host output allocation failed");
+    }
+    memset(hd, 0, db ? db : 1);
+    memset(hv, 0, vb);
+    if (n > 0) {
+      size_t copy_d = oc.dtype == PMB_BOOL ? (size_t)((n + 7) / 8) : db;
+      PMB_CUDA(h, cudaMemcpyAsync(hd, oc.data, copy_d, cudaMemcpyDeviceToHost, h->stream));
+      PMB_CUDA(h, cudaMemcpyAsync(hv, oc.validity, (size_t)((n + 7) / 8), cudaMemcpyDeviceToHost, h->stream));
+      h->d2h += (int64_t)(copy_d + (size_t)((n + 7) / 8));
+    }
+    oc.data = hd;
+    oc.validity = hv;
+    oc.on_device = 0;
+  }
+  if (to_host) PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return PMB_OK;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char* pmb_version(void) { return "pmb 0.1.0 (sm_100a)"; }
+
+int pmb_open(pmb_handle** out, int32_t device, uint64_t workspace_bytes) {
+  if (!out) return PMB_E_INVALID;
+  *out = nullptr;
+  pmb_handle* h = new pmb_handle();
+  h->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    delete h;
+    return PMB_E_CUDA;
+  }
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) {
+    delete h;
+    return PMB_E_CUDA;
+  }
+  if (prop.major < 10) {
+    delete h;
+    return PMB_E_UNSUPPORTED;  // built for sm_100a only
+  }
+  h->sm_count = prop.multiProcessorCount;
+  h->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&h->call_start) != cudaSuccess || cudaEventCreate(&h->call_stop) != cudaSuccess ||
+      cudaMallocHost((void**)&h->pinned, 4096) != cudaSuccess) {
+    pmb_close(h);
+    return PMB_E_CUDA;
+  }
+  h->stream = h->own_stream;
+  if (workspace_bytes) {
+    uint8_t* p = nullptr;
+    if (cudaMalloc((void**)&p, workspace_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      pmb_close(h);
+      return PMB_E_OOM;
+    }
+    h->ws.push_back({p, (size_t)workspace_bytes, 0});
+  }
+  *out = h;
+  return PMB_OK;
+}
+
+void pmb_close(pmb_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  ws_free_all(h);
+  if (h->pinned) cudaFreeHost(h->pinned);
+  for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
+  if (h->call_start) cudaEventDestroy(h->call_start);
+  if (h->call_stop) cudaEventDestroy(h->call_stop);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+}
+
+const char* pmb_last_error(const pmb_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int pmb_set_stream(pmb_handle* h, void* stream) {
+  if (!h) return PMB_E_INVALID;
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return PMB_OK;
+}
+
+int pmb_set_profiling(pmb_handle* h, int32_t enabled) {
+  if (!h) return PMB_E_INVALID;
+  h->profiling = enabled != 0;
+  return PMB_OK;
+}
+
+int pmb_last_stats(const pmb_handle* h, pmb_stats* out) {
+  if (!h || !out) return PMB_E_INVALID;
+  *out = h->last_stats;
+  return PMB_OK;
+}
+
+void pmb_result_free(pmb_result* r) {
+  if (!r) return;
+  for (int c = 0; c < r->n_columns; c++) {
+    if (!r->columns[c].on_device) {
+      free(r->columns[c].data);
+      free(r->columns[c].validity);
+    }
+  }
+  free(r->columns);
+  free(r);
+}
+
+}  // extern "C"

@@ -1,0 +1,580 @@
+"""Python surface of libpmb, mirroring the reference's PyO3 `_native` module for this path.
+
+Reference functions mirrored (same names, argument meaning and error classes):
+  - execute_groupby(plan_dict, n_rows, columns)      crates/polars-metal-core/src/udf/groupby/mod.rs:747-1144
+  - cmp_{i64,f64}_col_{col,scalar}(...)               crates/polars-metal-core/src/udf/compare.rs:23-145
+  - bool_and_dispatch / bool_or_dispatch(...)          crates/polars-metal-core/src/udf/logical.rs:26-55
+  - execute_filter_compact(pred_data, pred_valid, n_rows, columns)
+                                                       crates/polars-metal-core/src/udf/compact.rs:46-147
+Errors: ValueError (parse / length), KeyError (missing column), NotImplementedError (outside
+this build), MemoryError, RuntimeError (device failures; the reference's ComputeError).
+
+Beyond the wire-format functions, `groupby()` takes numpy arrays or CUDA tensors directly
+(zero-copy for device-resident columns) and `Handle` exposes streams and per-kernel timings.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from dataclasses import dataclass, field
+from typing import Any, Sequence
+
+import numpy as np
+
+from . import _abi as A
+
+_ERRORS = {
+    A.PMB_E_INVALID: ValueError,
+    A.PMB_E_OOM: MemoryError,
+    A.PMB_E_TIMEOUT: RuntimeError,
+    A.PMB_E_CUDA: RuntimeError,
+    A.PMB_E_UNSUPPORTED: NotImplementedError,
+    A.PMB_E_NOT_FOUND: KeyError,
+}
+
+
+class Handle:
+    """One device context: a CUDA stream plus a growable device workspace (libpmb handle)."""
+
+    def __init__(self, device: int = 0, workspace_bytes: int = 0):
+        self._lib = A.lib()
+        self._h = C.c_void_p()
+        rc = self._lib.pmb_open(C.byref(self._h), device, workspace_bytes)
+        if rc != A.PMB_OK:
+            raise _ERRORS.get(rc, RuntimeError)(f"polars_b200: pmb_open failed with status {rc}")
+        self.device = device
+
+    @property
+    def raw(self) -> C.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.pmb_close(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc: int) -> None:
+        if rc != A.PMB_OK:
+            msg = self._lib.pmb_last_error(self._h).decode(errors="replace")
+            raise _ERRORS.get(rc, RuntimeError)(f"polars_b200: {msg}")
+
+    def set_stream(self, cuda_stream: int | None) -> None:
+        self.check(self._lib.pmb_set_stream(self._h, C.c_void_p(cuda_stream or 0)))
+
+    def set_profiling(self, on: bool) -> None:
+        self.check(self._lib.pmb_set_profiling(self._h, 1 if on else 0))
+
+    def last_stats(self) -> dict:
+        s = A.Stats()
+        self.check(self._lib.pmb_last_stats(self._h, C.byref(s)))
+        kernels = {}
+        for i in range(s.n_kernels):
+            kernels[s.names[i].value.decode()] = {"launches": s.launches[i], "ms": s.ms[i]}
+        return {
+            "kernels": kernels,
+            "total_ms": s.total_ms,
+            "h2d_bytes": s.h2d_bytes,
+            "d2h_bytes": s.d2h_bytes,
+            "kernel_launches": s.kernel_launches,
+        }
+
+
+_local = threading.local()
+
+
+def default_handle() -> Handle:
+    h = getattr(_local, "handle", None)
+    if h is None:
+        h = Handle(0)
+        _local.handle = h
+    return h
+
+
+# ------------------------------------------------------------------------------- column inputs
+@dataclass
+class ColumnData:
+    """An Arrow-layout column: values plus an optional LSB-first validity bitmap.
+
+    `data` / `validity` are numpy arrays (host) or CUDA torch tensors (device, zero-copy).
+    Bool columns are bit-packed uint8 (LSB first). `length` defaults to len(data)."""
+
+    data: Any
+    validity: Any = None
+    dtype: int | None = None
+    length: int | None = None
+    offset: int = 0
+
+    def __post_init__(self):
+        if self.dtype is None:
+            self.dtype = _infer_dtype(self.data)
+        if self.length is None:
+            if self.dtype == A.BOOL:
+                raise ValueError("Bool columns need an explicit length")
+            self.length = int(_nelem(self.data)) - self.offset
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _nelem(x) -> int:
+    return int(x.numel()) if _is_torch(x) else int(np.asarray(x).size)
+
+
+def _infer_dtype(x) -> int:
+    if _is_torch(x):
+        name = str(x.dtype).replace("torch.", "")
+    else:
+        name = np.asarray(x).dtype.name
+    table = {v: k for k, v in A.NUMPY_NAME.items()}
+    if name == "bool":
+        raise ValueError("pass Bool columns bit-packed with dtype=BOOL")
+    if name not in table:
+        raise NotImplementedError(f"polars_b200: unsupported dtype {name}")
+    return table[name]
+
+
+def _ptr(x) -> tuple[int, int, Any]:
+    """(address, on_device, keepalive) of a numpy array or torch tensor."""
+    if x is None:
+        return 0, 0, None
+    if _is_torch(x):
+        if not x.is_contiguous():
+            x = x.contiguous()
+        return int(x.data_ptr()), 1 if x.is_cuda else 0, x
+    arr = np.ascontiguousarray(x)
+    return int(arr.ctypes.data), 0, arr
+
+
+def _to_abi_columns(cols: Sequence[ColumnData]):
+    arr = (A.Column * max(1, len(cols)))()
+    keep = []
+    for i, c in enumerate(cols):
+        dp, dd, k1 = _ptr(c.data)
+        vp, vd, k2 = _ptr(c.validity)
+        if c.validity is not None and vd != dd:
+            raise ValueError("data and validity of a column must live in the same memory space")
+        arr[i].data = dp
+        arr[i].validity = vp if c.validity is not None else None
+        arr[i].length = c.length
+        arr[i].offset = c.offset
+        arr[i].dtype = c.dtype
+        arr[i].on_device = dd
+        keep += [k1, k2]
+    return arr, keep
+
+
+# ------------------------------------------------------------------------------- predicates
+def compile_predicate(pred: dict | None, col_index: dict[str, int]):
+    """Lowers a predicate dict (the walker's PredicateAst wire shape, python/polars_metal/_walker.py:1508-1644,
+    plus "Arith", "Not", "IsNull", "IsNotNull") into expression nodes."""
+    if pred is None:
+        return None, None
+    nodes: list[A.ExprNode] = []
+
+    def add(**kw) -> int:
+        n = A.ExprNode()
+        n.lhs = n.rhs = -1
+        for k, v in kw.items():
+            setattr(n, k, v)
+        nodes.append(n)
+        return len(nodes) - 1
+
+    def dtype_of(tag):
+        if tag is None:
+            return 0
+        if tag not in ("I64", "F64"):
+            raise ValueError(f"polars_b200: operand dtype must be I64 or F64, got {tag!r}")
+        return A.TAG_TO_DTYPE[tag]
+
+    def walk(p: dict) -> int:
+        kind = p.get("kind")
+        if kind == "Column":
+            name = p["name"]
+            if name not in col_index:
+                raise KeyError(f"polars_b200: predicate column {name!r} not found in upstream columns")
+            return add(kind=A.EXPR_COLUMN, column=col_index[name])
+        if kind == "LiteralI64":
+            return add(kind=A.EXPR_LIT_I64, lit_i64=int(p["value"]), dtype=A.I64)
+        if kind == "LiteralF64":
+            return add(kind=A.EXPR_LIT_F64, lit_f64=float(p["value"]), dtype=A.F64)
+        if kind == "LiteralBool":
+            return add(kind=A.EXPR_LIT_BOOL, lit_i64=1 if p["value"] else 0)
+        if kind == "Compare":
+            if p["op"] not in A.CMP_OPS:
+                raise ValueError(f"polars_b200: unknown compare op {p['op']!r}")
+            l, r = walk(p["lhs"]), walk(p["rhs"])
+            return add(kind=A.EXPR_COMPARE, op=A.CMP_OPS[p["op"]], lhs=l, rhs=r, dtype=dtype_of(p.get("dtype")))
+        if kind in ("And", "Or"):
+            l, r = walk(p["lhs"]), walk(p["rhs"])
+            return add(kind=A.EXPR_AND if kind == "And" else A.EXPR_OR, lhs=l, rhs=r)
+        if kind == "Not":
+            return add(kind=A.EXPR_NOT, lhs=walk(p["arg"]))
+        if kind in ("IsNull", "IsNotNull"):
+            return add(kind=A.EXPR_IS_NULL if kind == "IsNull" else A.EXPR_IS_NOT_NULL, lhs=walk(p["arg"]))
+        if kind == "Arith":
+            if p["op"] not in A.ARITH_OPS:
+                raise ValueError(f"polars_b200: unknown arithmetic op {p['op']!r}")
+            l, r = walk(p["lhs"]), walk(p["rhs"])
+            return add(kind=A.EXPR_ARITH, op=A.ARITH_OPS[p["op"]], lhs=l, rhs=r, dtype=dtype_of(p.get("dtype")))
+        raise ValueError(f"polars_b200: unknown predicate node kind {kind!r}")
+
+    root = walk(pred)
+    arr = (A.ExprNode * len(nodes))(*nodes)
+    expr = A.Expr(C.cast(arr, C.POINTER(A.ExprNode)), len(nodes), root)
+    return expr, arr
+
+
+# ------------------------------------------------------------------------------- group-by
+@dataclass
+class GroupByResult:
+    n_groups: int
+    names: list[str]
+    dtypes: list[int]
+    data: list[Any]  # numpy arrays (host) or device addresses (int) when output_on_device
+    validity: list[Any]
+    strategy: str
+    rehash_count: int
+    capacity: int
+    stats: dict = field(default_factory=dict)
+
+    def column(self, name: str) -> tuple[np.ndarray, np.ndarray]:
+        i = self.names.index(name)
+        return self.data[i], self.validity[i]
+
+
+def _bitmap_bytes(n: int) -> int:
+    b = (n + 7) // 8
+    b = (b + 3) & ~3
+    return max(b, 4)
+
+
+def _read_result(res: A.Result, names, to_host: bool) -> tuple[list, list, list]:
+    n = res.n_groups
+    data, valid, dts = [], [], []
+    for i in range(res.n_columns):
+        oc = res.columns[i]
+        dts.append(oc.dtype)
+        if not to_host:
+            data.append(int(oc.data or 0))
+            valid.append(int(oc.validity or 0))
+            continue
+        vb = _bitmap_bytes(n)
+        v = np.frombuffer(C.string_at(oc.validity, vb), dtype=np.uint8).copy() if oc.validity else np.zeros(vb, np.uint8)
+        if oc.dtype == A.BOOL:
+            d = np.frombuffer(C.string_at(oc.data, vb), dtype=np.uint8).copy() if oc.data else np.zeros(vb, np.uint8)
+        else:
+            nb = n * A.DTYPE_BYTES[oc.dtype]
+            raw = C.string_at(oc.data, nb) if (oc.data and nb) else b""
+            d = np.frombuffer(raw, dtype=A.NUMPY_NAME[oc.dtype]).copy()
+        data.append(d)
+        valid.append(v)
+    return data, valid, dts
+
+
+def groupby(
+    columns: dict[str, ColumnData | Any],
+    keys: Sequence[str],
+    aggs: Sequence[tuple[str, str | None, str]],
+    predicate: dict | None = None,
+    strategy: str = "auto",
+    output: str = "host",
+    capacity_hint: int = 0,
+    handle: Handle | None = None,
+) -> GroupByResult:
+    """filter -> group_by -> aggregate through libpmb.
+
+    columns: name -> ColumnData (or a bare array with no nulls); aggs: (op, input column, alias)
+    with op in Sum/Mean/Count/Min/Max/Len (input None for Len); predicate: a predicate dict.
+    """
+    names = list(columns)
+    index = {n: i for i, n in enumerate(names)}
+    cols = [c if isinstance(c, ColumnData) else ColumnData(c) for c in columns.values()]
+    for k in keys:
+        if k not in index:
+            raise KeyError(f"polars_b200: key column {k!r} not found in upstream columns")
+    key_arr = (C.c_int32 * max(1, len(keys)))(*[index[k] for k in keys])
+    agg_arr = (A.Agg * max(1, len(aggs)))()
+    for i, (op, col, _alias) in enumerate(aggs):
+        if op not in A.AGG_OPS:
+            raise ValueError(f"polars_b200: unknown aggregation op {op!r}")
+        agg_arr[i].op = A.AGG_OPS[op]
+        if op == "Len":
+            agg_arr[i].column = -1
+        else:
+            if col not in index:
+                raise KeyError(f"polars_b200: agg input column {col!r} not found in upstream columns")
+            agg_arr[i].column = index[col]
+    expr, expr_keep = compile_predicate(predicate, index)
+    q = A.Query()
+    q.key_columns = key_arr
+    q.n_keys = len(keys)
+    q.aggs = agg_arr
+    q.n_aggs = len(aggs)
+    q.predicate = C.pointer(expr) if expr is not None else None
+    if strategy not in A.STRATEGIES:
+        raise ValueError(f"polars_b200: unknown strategy {strategy!r}")
+    q.strategy = A.STRATEGIES[strategy]
+    q.output_on_device = 1 if output == "device" else 0
+    q.capacity_hint = capacity_hint
+    h = handle or default_handle()
+    abi_cols, keep = _to_abi_columns(cols)
+    res_p = C.POINTER(A.Result)()
+    h.check(h._lib.pmb_groupby(h.raw, C.byref(q), abi_cols, len(cols), C.byref(res_p)))
+    try:
+        res = res_p.contents
+        out_names = list(keys) + [a[2] for a in aggs]
+        data, valid, dts = _read_result(res, out_names, output != "device")
+        return GroupByResult(
+            n_groups=res.n_groups,
+            names=out_names,
+            dtypes=dts,
+            data=data,
+            validity=valid,
+            strategy=A.STRATEGY_NAMES.get(res.strategy_used, str(res.strategy_used)),
+            rehash_count=res.rehash_count,
+            capacity=res.capacity,
+        )
+    finally:
+        h._lib.pmb_result_free(res_p)
+        del keep, expr_keep
+
+
+# ------------------------------------------------------------------------------- wire format
+def _all_valid(valid: bytes, n: int) -> bool:
+    if n == 0:
+        return True
+    v = np.frombuffer(valid, dtype=np.uint8, count=(n + 7) // 8)
+    full = n // 8
+    if full and not np.all(v[:full] == 0xFF):
+        return False
+    rem = n % 8
+    if rem:
+        m = (1 << rem) - 1
+        return (int(v[full]) & m) == m
+    return True
+
+
+def _wire_column(tag: str, data: bytes, valid: bytes, n_rows: int, name: str) -> ColumnData:
+    if tag in ("Utf8", "String"):
+        raise NotImplementedError(f"polars_b200: Utf8 columns are not supported on this path ({name!r})")
+    if tag not in A.TAG_TO_DTYPE:
+        raise ValueError(f"polars_b200: unknown dtype tag {tag!r} for column {name!r}")
+    dt = A.TAG_TO_DTYPE[tag]
+    if dt == A.BOOL:
+        need = (n_rows + 7) // 8
+        arr = np.frombuffer(data, dtype=np.uint8, count=need) if need else np.zeros(1, np.uint8)
+    else:
+        need = n_rows * A.DTYPE_BYTES[dt]
+        if len(data) < need:
+            raise ValueError(f"polars_b200: data buffer is {len(data)} B, need at least {need} B for {n_rows} rows")
+        arr = np.frombuffer(data, dtype=A.NUMPY_NAME[dt], count=n_rows)
+    if len(valid) < (n_rows + 7) // 8:
+        raise ValueError(
+            f"polars_b200: validity buffer is {len(valid)} B, need at least {(n_rows + 7) // 8} B for {n_rows} rows"
+        )
+    v = None if _all_valid(valid, n_rows) else np.frombuffer(valid, dtype=np.uint8, count=(n_rows + 7) // 8)
+    return ColumnData(arr, v, dtype=dt, length=n_rows)
+
+
+def execute_groupby(plan_dict: dict, n_rows: int, columns: list) -> list[tuple[str, str, bytes, bytes]]:
+    """Wire-compatible `_native.execute_groupby` (crates/polars-metal-core/src/udf/groupby/mod.rs:720-746).
+
+    plan_dict: {"keys": [[name, tag], ...], "aggs": [{"input_col", "op", "output_alias", "kind"?}],
+                "predicate": <predicate dict>?}
+    columns:   [(name, tag, data: bytes, valid: bytes), ...]
+    returns:   [(name, tag, data, valid), ...] keys then aggs; Count/Len as U32 with all-valid bitmaps.
+    """
+    if "keys" not in plan_dict:
+        raise ValueError("polars_b200: plan parse error: missing field keys")
+    if "aggs" not in plan_dict:
+        raise ValueError("polars_b200: plan parse error: missing field aggs")
+    by_name: dict[str, ColumnData] = {}
+    for idx, entry in enumerate(columns):
+        if not isinstance(entry, tuple) or len(entry) != 4:
+            raise ValueError(
+                f"polars_b200: execute_groupby columns[{idx}] must have 4 elements (name, dtype, data, valid)"
+            )
+        name, tag, data, valid = entry
+        if not isinstance(data, (bytes, bytearray, memoryview)) or not isinstance(valid, (bytes, bytearray, memoryview)):
+            raise ValueError(f"polars_b200: execute_groupby columns[{idx}] data and valid must be bytes")
+        by_name[name] = (tag, bytes(data), bytes(valid))
+    keys = []
+    for k in plan_dict["keys"]:
+        if not isinstance(k, (list, tuple)) or len(k) < 2:
+            raise ValueError("polars_b200: plan parse error: wrong type for key entry")
+        keys.append(str(k[0]))
+    aggs = []
+    for a in plan_dict["aggs"]:
+        if "output_alias" not in a:
+            raise ValueError("polars_b200: plan parse error: wrong type for output_alias")
+        kind = a.get("kind") or ("Length" if a.get("op") == "Len" else "Simple")
+        if kind == "Length":
+            aggs.append(("Len", None, a["output_alias"]))
+        elif kind == "Simple":
+            if a.get("op") not in A.AGG_OPS:
+                raise ValueError(f"polars_b200: plan parse error: unknown op {a.get('op')!r}")
+            aggs.append((a["op"], a.get("input_col", ""), a["output_alias"]))
+        elif kind == "Expression":
+            raise NotImplementedError("polars_b200: Expression aggregations are not on this path")
+        else:
+            raise ValueError(f"polars_b200: plan parse error: unknown op kind={kind}")
+    for k in keys:
+        if k not in by_name:
+            raise KeyError(f"polars_b200: key column {k!r} not found in upstream columns")
+    for op, col, _ in aggs:
+        if op != "Len" and col not in by_name:
+            raise KeyError(f"polars_b200: agg input column {col!r} not found in upstream columns")
+    needed = list(dict.fromkeys(keys + [c for _, c, _ in aggs if c] + _predicate_columns(plan_dict.get("predicate"))))
+    cols = {}
+    for name in needed:
+        if name not in by_name:
+            raise KeyError(f"polars_b200: column {name!r} not found in upstream columns")
+        tag, data, valid = by_name[name]
+        cols[name] = _wire_column(tag, data, valid, n_rows, name)
+    res = groupby(cols, keys, aggs, plan_dict.get("predicate"), strategy=plan_dict.get("strategy", "auto"))
+    out = []
+    n = res.n_groups
+    for i, name in enumerate(res.names):
+        dt = res.dtypes[i]
+        tag = A.DTYPE_TO_TAG[dt]
+        d = res.data[i]
+        if dt == A.BOOL:
+            db = bytes(d[: _bitmap_bytes(n)])
+        else:
+            db = d.tobytes()
+        is_count = i >= len(keys) and aggs[i - len(keys)][0] in ("Count", "Len")
+        vb = b"\xff" * _bitmap_bytes(n) if is_count else bytes(res.validity[i][: _bitmap_bytes(n)])
+        out.append((name, tag, db, vb))
+    return out
+
+
+def _predicate_columns(p: dict | None) -> list[str]:
+    if p is None:
+        return []
+    out = []
+    if p.get("kind") == "Column":
+        out.append(p["name"])
+    for k in ("lhs", "rhs", "arg"):
+        if isinstance(p.get(k), dict):
+            out += _predicate_columns(p[k])
+    return out
+
+
+# ------------------------------------------------------------------------------- filter side
+def _cmp_common(lhs_data, lhs_valid, rhs_data, rhs_valid, scalar, op, n_rows, dtype) -> tuple[bytes, bytes]:
+    h = default_handle()
+    width = 8
+    if len(lhs_data) < n_rows * width:
+        raise ValueError(f"polars_b200: data buffer is {len(lhs_data)} B, need at least {n_rows * width} B")
+    if len(lhs_valid) < (n_rows + 7) // 8:
+        raise ValueError(f"polars_b200: validity buffer is {len(lhs_valid)} B, need at least {(n_rows + 7) // 8} B")
+    if op not in A.CMP_OPS:
+        raise ValueError(f"polars_b200: unknown compare op {op!r}")
+    npdt = "int64" if dtype == A.I64 else "float64"
+    lc = ColumnData(np.frombuffer(lhs_data, dtype=npdt, count=n_rows), np.frombuffer(lhs_valid, np.uint8), dtype=dtype,
+                    length=n_rows)
+    cols = [lc]
+    if rhs_data is not None:
+        if len(rhs_data) < n_rows * width or len(rhs_valid) < (n_rows + 7) // 8:
+            raise ValueError("polars_b200: rhs buffers too short")
+        cols.append(ColumnData(np.frombuffer(rhs_data, dtype=npdt, count=n_rows), np.frombuffer(rhs_valid, np.uint8),
+                               dtype=dtype, length=n_rows))
+    abi, keep = _to_abi_columns(cols)
+    nb = _bitmap_bytes(n_rows)
+    od = (C.c_uint8 * nb)()
+    ov = (C.c_uint8 * nb)()
+    rhs_ptr = C.pointer(abi[1]) if rhs_data is not None else None
+    si = int(scalar) if (scalar is not None and dtype == A.I64) else 0
+    sf = float(scalar) if (scalar is not None and dtype == A.F64) else 0.0
+    h.check(h._lib.pmb_compare(h.raw, C.pointer(abi[0]), rhs_ptr, si, sf, A.CMP_OPS[op], od, ov, 0))
+    del keep
+    return bytes(od), bytes(ov)
+
+
+def cmp_i64_col_scalar(data: bytes, valid: bytes, rhs: int, op: str, n_rows: int) -> tuple[bytes, bytes]:
+    return _cmp_common(data, valid, None, None, rhs, op, n_rows, A.I64)
+
+
+def cmp_f64_col_scalar(data: bytes, valid: bytes, rhs: float, op: str, n_rows: int) -> tuple[bytes, bytes]:
+    return _cmp_common(data, valid, None, None, rhs, op, n_rows, A.F64)
+
+
+def cmp_i64_col_col(lhs: bytes, lhs_valid: bytes, rhs: bytes, rhs_valid: bytes, op: str, n_rows: int):
+    return _cmp_common(lhs, lhs_valid, rhs, rhs_valid, None, op, n_rows, A.I64)
+
+
+def cmp_f64_col_col(lhs: bytes, lhs_valid: bytes, rhs: bytes, rhs_valid: bytes, op: str, n_rows: int):
+    return _cmp_common(lhs, lhs_valid, rhs, rhs_valid, None, op, n_rows, A.F64)
+
+
+def _bool_common(fn_name, ld, lv, rd, rv, n_rows):
+    h = default_handle()
+    need = (n_rows + 7) // 8
+    for label, b in (("lhs data", ld), ("lhs valid", lv), ("rhs data", rd), ("rhs valid", rv)):
+        if len(b) < need:
+            raise ValueError(f"polars_b200: {label} buffer is {len(b)} B, need at least {need} B for {n_rows} rows")
+    nb = _bitmap_bytes(n_rows)
+    od = (C.c_uint8 * nb)()
+    ov = (C.c_uint8 * nb)()
+    bufs = [np.frombuffer(x, np.uint8) if len(x) else np.zeros(1, np.uint8) for x in (ld, lv, rd, rv)]
+    ptrs = [b.ctypes.data for b in bufs]
+    h.check(getattr(h._lib, fn_name)(h.raw, *ptrs, n_rows, od, ov, 0))
+    return bytes(od), bytes(ov)
+
+
+def bool_and_dispatch(lhs_data: bytes, lhs_valid: bytes, rhs_data: bytes, rhs_valid: bytes, n_rows: int):
+    return _bool_common("pmb_bool_and", lhs_data, lhs_valid, rhs_data, rhs_valid, n_rows)
+
+
+def bool_or_dispatch(lhs_data: bytes, lhs_valid: bytes, rhs_data: bytes, rhs_valid: bytes, n_rows: int):
+    return _bool_common("pmb_bool_or", lhs_data, lhs_valid, rhs_data, rhs_valid, n_rows)
+
+
+def execute_filter_compact(pred_data: bytes, pred_valid: bytes, n_rows: int, columns: list) -> list:
+    """Wire-compatible `_native.execute_filter_compact` (crates/polars-metal-core/src/udf/compact.rs:46-147):
+    columns [(tag, data, valid)] -> [(data, valid, n_out)] compacted by keep = pred_data & pred_valid."""
+    h = default_handle()
+    need = (n_rows + 7) // 8
+    if len(pred_data) < need or len(pred_valid) < need:
+        raise ValueError("polars_b200: predicate buffers too short")
+    cols = []
+    for idx, entry in enumerate(columns):
+        tag, data, valid = entry
+        cols.append(_wire_column(tag, bytes(data), bytes(valid), n_rows, f"columns[{idx}]"))
+    abi, keep = _to_abi_columns(cols)
+    pd = np.frombuffer(pred_data, np.uint8) if need else np.zeros(1, np.uint8)
+    pv = np.frombuffer(pred_valid, np.uint8) if need else np.zeros(1, np.uint8)
+    res_p = C.POINTER(A.Result)()
+    h.check(h._lib.pmb_filter_compact(h.raw, pd.ctypes.data, pv.ctypes.data, n_rows, 0, abi, len(cols), 0,
+                                      C.byref(res_p)))
+    try:
+        res = res_p.contents
+        data, valid, dts = _read_result(res, None, True)
+        n = res.n_groups
+        out = []
+        for i in range(res.n_columns):
+            d = data[i]
+            db = bytes(d[: _bitmap_bytes(n)]) if dts[i] == A.BOOL else d.tobytes()
+            out.append((db, bytes(valid[i][: _bitmap_bytes(n)]), n))
+        return out
+    finally:
+        h._lib.pmb_result_free(res_p)
+        del keep
+
+
+def cumsum_u8_to_u32(data: np.ndarray) -> np.ndarray:
+    """Inclusive prefix sum u8 -> u32 (the MLX call the reference makes, mlx-sys/src/lib.rs:47)."""
+    h = default_handle()
+    a = np.ascontiguousarray(data, dtype=np.uint8)
+    out = np.empty(a.size, dtype=np.uint32)
+    h.check(h._lib.pmb_cumsum_u8_to_u32(h.raw, a.ctypes.data if a.size else None,
+                                        out.ctypes.data if a.size else None, a.size, 0))
+    return out

@@ -1,0 +1,110 @@
+"""The C ABI without a GPU: the library loads, exports every symbol include/pmb.h declares, and
+the ctypes mirror has the C layout; host-side argument checks run before any device call."""
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from polars_b200 import _abi as A
+from polars_b200 import _native as N
+from polars_b200 import datagen
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "pmb.h"
+
+
+def header_functions() -> list[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pmb_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib_path():
+    from polars_b200 import build
+
+    return build.build()
+
+
+def test_library_exports_every_declared_symbol(lib_path):
+    lib = C.CDLL(str(lib_path))
+    names = header_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_ctypes_mirror_covers_the_header(lib_path):
+    assert set(header_functions()) == set(A.SIGNATURES)
+    A.lib()  # binds every signature
+
+
+def test_struct_layouts_match_c(tmp_path):
+    src = tmp_path / "sz.c"
+    structs = ["pmb_column", "pmb_expr_node", "pmb_expr", "pmb_agg", "pmb_query", "pmb_out_column", "pmb_result",
+               "pmb_stats"]
+    src.write_text('#include <stdio.h>\n#include "pmb.h"\nint main(void){\n' +
+                   "".join(f'printf("%zu\\n", sizeof({s}));\n' for s in structs) + "return 0;}\n")
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    mirror = [A.Column, A.ExprNode, A.Expr, A.Agg, A.Query, A.OutColumn, A.Result, A.Stats]
+    assert sizes == [C.sizeof(m) for m in mirror]
+
+
+def test_oracle_library_loads():
+    from oracle import pyoracle
+
+    L = pyoracle.lib()
+    for sym in ("orc_groupby", "orc_filter_mask", "orc_predicate_bits", "orc_bool_logic", "orc_filter_compact",
+                "orc_cumsum_u8_to_u32"):
+        assert hasattr(L, sym)
+
+
+def test_predicate_lowering_of_the_hash_workload():
+    expr, keep = N.compile_predicate(datagen.PRED_HASH, {"key": 0, "v1": 1, "v2": 2, "v3": 3})
+    kinds = [expr.nodes[i].kind for i in range(expr.n_nodes)]
+    assert kinds == [A.EXPR_COLUMN, A.EXPR_LIT_F64, A.EXPR_COMPARE, A.EXPR_COLUMN, A.EXPR_LIT_I64, A.EXPR_ARITH,
+                     A.EXPR_LIT_I64, A.EXPR_COMPARE, A.EXPR_AND]
+    root = expr.nodes[expr.root]
+    assert root.kind == A.EXPR_AND
+    assert expr.nodes[5].op == A.ARITH_OPS["Mod"]
+
+
+def test_wire_errors_are_raised_before_any_device_call():
+    cols = [("k", "I64", np.arange(4, dtype=np.int64).tobytes(), b"\xff")]
+    with pytest.raises(ValueError):
+        N.execute_groupby({"aggs": []}, 4, cols)
+    with pytest.raises(KeyError):
+        N.execute_groupby({"keys": [["missing", "I64"]], "aggs": []}, 4, cols)
+    with pytest.raises(KeyError):
+        N.execute_groupby({"keys": [["k", "I64"]], "aggs": [{"input_col": "nope", "op": "Sum", "output_alias": "s"}]},
+                          4, cols)
+    with pytest.raises(NotImplementedError):
+        N.execute_groupby({"keys": [["s", "Utf8"]], "aggs": []}, 4, cols + [("s", "Utf8", b"\0" * 8, b"\xff")])
+    with pytest.raises(ValueError):
+        N.execute_groupby({"keys": [["k", "I64"]], "aggs": []}, 8, cols)  # data too short
+    with pytest.raises(ValueError):
+        N.execute_groupby({"keys": [["k", "I64"]], "aggs": [{"input_col": "k", "op": "Median", "output_alias": "m"}]},
+                          4, cols)
+    with pytest.raises(ValueError):
+        N.compile_predicate({"kind": "Compare", "op": "Like", "lhs": {}, "rhs": {}}, {})
+
+
+def test_all_valid_bitmap_detection():
+    assert N._all_valid(b"\xff\x07", 11)
+    assert not N._all_valid(b"\xff\x03", 11)
+    assert N._all_valid(b"", 0)
+
+
+def test_pack_bits_matches_numpy():
+    import torch
+
+    m = torch.rand(1003) > 0.3
+    got = datagen.pack_bits(m).numpy()
+    want = np.packbits(m.numpy(), bitorder="little")
+    assert np.array_equal(got, want)

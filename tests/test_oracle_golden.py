@@ -1,0 +1,106 @@
+"""Pins the CPU oracle to the reference's own known-answer tests (no GPU needed)."""
+
+import math
+
+import numpy as np
+import pytest
+
+from helpers import (assert_results_match, case_columns, expected_to_result, formula_columns, load_golden, pack,
+                     unpack)
+from oracle import pyoracle
+
+GOLD = load_golden()
+
+
+@pytest.mark.parametrize("case", GOLD["groupby"], ids=lambda c: c["name"])
+def test_oracle_groupby_known_answers(case):
+    got = pyoracle.groupby(case_columns(case), case["keys"], [tuple(a) for a in case["aggs"]])
+    want = expected_to_result(case)
+    assert_results_match(got, want, len(case["keys"]), case["aggs"], case["name"])
+
+
+@pytest.mark.parametrize("case", GOLD["integration"], ids=lambda c: c["name"])
+def test_oracle_integration_shapes(case):
+    cols = formula_columns(case["formula"], case["n"])
+    got = pyoracle.groupby(cols, case["keys"], [tuple(a) for a in case["aggs"]])
+    if case["formula"] == "all_unique":
+        assert got["n_groups"] == case["expected"]["n_groups"]
+        assert np.all(got["data"][1] == 1)
+        return
+    want = expected_to_result(case)
+    assert_results_match(got, want, len(case["keys"]), case["aggs"], case["name"])
+
+
+def _cmp_pred(op, scalar=None):
+    rhs = {"kind": "LiteralF64", "value": scalar} if scalar is not None else {"kind": "Column", "name": "r"}
+    return {"kind": "Compare", "op": op, "dtype": "F64", "lhs": {"kind": "Column", "name": "l"}, "rhs": rhs}
+
+
+@pytest.mark.parametrize("case", GOLD["compare"], ids=lambda c: c["name"])
+def test_oracle_compare_semantics(case):
+    n = len(case["lhs"])
+    cols = {"l": (np.array(case["lhs"], np.float64), pack(case["lhs_valid"]))}
+    if "rhs" in case:
+        cols["r"] = (np.array(case["rhs"], np.float64), pack(case["rhs_valid"]))
+        pred = _cmp_pred(case["op"])
+    else:
+        pred = _cmp_pred(case["op"], case["scalar"])
+    d, v = pyoracle.predicate_bits(cols, pred)
+    assert list(unpack(d, n).astype(int)) == case["expected_data"]
+    assert list(unpack(v, n).astype(int)) == case["expected_valid"]
+
+
+def _tri_bits(vals):
+    data = pack([v == "T" for v in vals])
+    valid = pack([v != "N" for v in vals])
+    return data, valid
+
+
+def test_oracle_kleene_tables():
+    case = GOLD["kleene"][0]
+    ld, lv = _tri_bits(case["lhs"])
+    rd, rv = _tri_bits(case["rhs"])
+    n = len(case["lhs"])
+    for op in ("and", "or"):
+        d, v = pyoracle.bool_logic(op, ld.tobytes(), lv.tobytes(), rd.tobytes(), rv.tobytes(), n)
+        dd, vv = unpack(d, n), unpack(v, n)
+        got = ["N" if not vv[i] else ("T" if dd[i] else "F") for i in range(n)]
+        assert got == case[op], op
+
+
+def test_oracle_mod_predicate_floor_semantics():
+    # Polars integer `%` is a floor modulo (sign of the divisor); x % 0 is null
+    v = np.array([-7, -1, 0, 6, 7, 13, 5], np.int64)
+    cols = {"v": (v, None)}
+    pred = {"kind": "Compare", "op": "Eq", "dtype": "I64",
+            "lhs": {"kind": "Arith", "op": "Mod", "dtype": "I64", "lhs": {"kind": "Column", "name": "v"},
+                    "rhs": {"kind": "LiteralI64", "value": 7}},
+            "rhs": {"kind": "LiteralI64", "value": 6}}
+    keep = pyoracle.filter_mask(cols, pred)
+    assert list(keep) == [False, True, False, True, False, True, False]
+    pred0 = dict(pred)
+    pred0["lhs"] = dict(pred["lhs"], rhs={"kind": "LiteralI64", "value": 0})
+    d, vmask = pyoracle.predicate_bits(cols, pred0)
+    assert not unpack(vmask, 7).any()
+
+
+def test_oracle_filter_compact_and_cumsum():
+    rng = np.random.default_rng(0)
+    n = 1000
+    a = rng.integers(-5, 5, n).astype(np.int64)
+    va = rng.random(n) > 0.1
+    keep = rng.random(n) > 0.5
+    m, cols = pyoracle.filter_compact(keep, {"a": (a, pack(va))})
+    assert m == keep.sum()
+    assert np.array_equal(cols[0][1][:m], a[keep])
+    assert np.array_equal(unpack(cols[0][2], m), va[keep])
+    u8 = rng.integers(0, 2, n).astype(np.uint8)
+    assert np.array_equal(pyoracle.cumsum_u8_to_u32(u8), np.cumsum(u8).astype(np.uint32))
+
+
+def test_oracle_exact_sum_beats_naive_on_cancellation():
+    # compensated summation keeps an exactly representable cancelling sum exact
+    v = np.array([1e16, 1.0, -1e16, 1.0] * 1000, np.float64)
+    got = pyoracle.groupby({"k": (np.zeros(v.size, np.int32), None), "v": (v, None)}, ["k"], [("Sum", "v", "s")])
+    assert got["data"][1][0] == 2000.0
+    assert math.fsum(v) == 2000.0
