@@ -311,6 +311,7 @@ def main():
             "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": desc, "rows_per_gpu": n, "groups": n_groups, "strategy": r.strategy,
+                       "capacity": r.capacity, "rehash_count": r.rehash_count,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": f"inputs {alg_bytes / 1e9:.2f} GB per GPU > 126 MB L2, no flush needed",
                        "bytes_per_row": bytes_per_row},

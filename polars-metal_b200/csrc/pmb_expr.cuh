@@ -329,9 +329,78 @@ __host__ __device__ inline void field_identity(int kind, uint64_t* w0, uint64_t*
   }
 }
 
-// Adds one row to a group record (in shared or global memory).
-template <bool SMEM>
-__device__ __forceinline__ void apply_row(const DQuery& q, const TileCtx& t, uint8_t* rec, int64_t lr) {
+// One row's contribution to a group record. Three variants, by who may touch the record:
+//   apply_row_private — records owned by one warp, updated by a single lane (no atomics);
+//   apply_row_shared  — the CTA-shared table (shared-memory atomics; on sm_100 only 32-bit
+//                       adds and 64-bit min/max are native there, so min/max skip when the
+//                       stored value already dominates and the rest stays low-contention);
+//   apply_row_global  — the global table (native L2 atomics, fire-and-forget where possible:
+//                       adjacent 32-bit counters share one 64-bit add, min/max are issued only
+//                       when the row improves on a possibly stale read).
+__device__ __forceinline__ void dd_plain_add(double* hi, double* lo, double x) {
+  double old = *hi;
+  double s = old + x;
+  *hi = s;
+  if (!isfinite(s)) return;
+  double bp = s - old;
+  *lo += (old - (s - bp)) + (x - bp);
+}
+
+__device__ __forceinline__ long long minmax_key(const DField& F, uint64_t b, int dt, bool is_min) {
+  double x = pmb_bits_to_f64(b, dt);
+  if (isnan(x)) return is_min ? (long long)0x8000000000000000LL : 0x7FFFFFFFFFFFFFFFLL;
+  return pmb_f64_key(x);
+}
+
+__device__ __forceinline__ void apply_row_private(const DQuery& q, const TileCtx& t, uint8_t* rec, int64_t lr) {
+  for (int i = 0; i < q.n_fields; i++) {
+    const DField F = q.field[i];
+    uint8_t* p = rec + F.off;
+    if (F.kind == F_LEN) {
+      *(unsigned int*)p += 1u;
+      continue;
+    }
+    if (!tc_isvalid(q, t, F.col, lr)) continue;
+    if (F.kind == F_CNT) {
+      *(unsigned int*)p += 1u;
+      continue;
+    }
+    uint64_t b = tc_bits(q, t, F.col, lr);
+    int dt = q.col[F.col].dtype;
+    switch (F.kind) {
+      case F_SUM_DD: dd_plain_add((double*)p, (double*)(p + 8), pmb_bits_to_f64(b, dt)); break;
+      case F_SUM_I: *(unsigned long long*)p += (unsigned long long)pmb_bits_to_i64(b, dt); break;
+      case F_MIN_I: {
+        long long v = (long long)pmb_bits_to_i64(b, dt);
+        if (v < *(long long*)p) *(long long*)p = v;
+        break;
+      }
+      case F_MAX_I: {
+        long long v = (long long)pmb_bits_to_i64(b, dt);
+        if (v > *(long long*)p) *(long long*)p = v;
+        break;
+      }
+      case F_MIN_U:
+        if (b < *(unsigned long long*)p) *(unsigned long long*)p = b;
+        break;
+      case F_MAX_U:
+        if (b > *(unsigned long long*)p) *(unsigned long long*)p = b;
+        break;
+      case F_MIN_F: {
+        long long k = minmax_key(F, b, dt, true);
+        if (k < *(long long*)p) *(long long*)p = k;
+        break;
+      }
+      default: {
+        long long k = minmax_key(F, b, dt, false);
+        if (k > *(long long*)p) *(long long*)p = k;
+        break;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void apply_row_shared(const DQuery& q, const TileCtx& t, uint8_t* rec, int64_t lr) {
   for (int i = 0; i < q.n_fields; i++) {
     const DField F = q.field[i];
     uint8_t* p = rec + F.off;
@@ -351,37 +420,90 @@ __device__ __forceinline__ void apply_row(const DQuery& q, const TileCtx& t, uin
       case F_SUM_I: atomicAdd((unsigned long long*)p, (unsigned long long)pmb_bits_to_i64(b, dt)); break;
       case F_MIN_I: {
         long long v = (long long)pmb_bits_to_i64(b, dt);
-        if (!SMEM || v < *(volatile long long*)p) atomicMin((long long*)p, v);
+        if (v < *(volatile long long*)p) atomicMin((long long*)p, v);
         break;
       }
       case F_MAX_I: {
         long long v = (long long)pmb_bits_to_i64(b, dt);
-        if (!SMEM || v > *(volatile long long*)p) atomicMax((long long*)p, v);
+        if (v > *(volatile long long*)p) atomicMax((long long*)p, v);
         break;
       }
       case F_MIN_U:
-        if (!SMEM || b < *(volatile unsigned long long*)p) atomicMin((unsigned long long*)p, (unsigned long long)b);
+        if (b < *(volatile unsigned long long*)p) atomicMin((unsigned long long*)p, (unsigned long long)b);
         break;
       case F_MAX_U:
-        if (!SMEM || b > *(volatile unsigned long long*)p) atomicMax((unsigned long long*)p, (unsigned long long)b);
+        if (b > *(volatile unsigned long long*)p) atomicMax((unsigned long long*)p, (unsigned long long)b);
         break;
       case F_MIN_F: {
-        double x = pmb_bits_to_f64(b, dt);
-        long long k = isnan(x) ? (long long)0x8000000000000000LL : pmb_f64_key(x);
-        if (!SMEM || k < *(volatile long long*)p) atomicMin((long long*)p, k);
+        long long k = minmax_key(F, b, dt, true);
+        if (k < *(volatile long long*)p) atomicMin((long long*)p, k);
         break;
       }
-      default: {  // F_MAX_F
-        double x = pmb_bits_to_f64(b, dt);
-        long long k = isnan(x) ? (long long)0x7FFFFFFFFFFFFFFFLL : pmb_f64_key(x);
-        if (!SMEM || k > *(volatile long long*)p) atomicMax((long long*)p, k);
+      default: {
+        long long k = minmax_key(F, b, dt, false);
+        if (k > *(volatile long long*)p) atomicMax((long long*)p, k);
         break;
       }
     }
   }
 }
 
-// Merges a finished record `src` into `dst` (global memory).
+__device__ __forceinline__ void apply_row_global(const DQuery& q, const TileCtx& t, uint8_t* rec, int64_t lr) {
+  unsigned long long pend = 0;  // packed 32-bit counter increments of one 8-byte word
+  int pend_off = -1;
+  for (int i = 0; i < q.n_fields; i++) {
+    const DField F = q.field[i];
+    uint8_t* p = rec + F.off;
+    if (F.kind == F_LEN || F.kind == F_CNT) {
+      unsigned long long inc = (F.kind == F_LEN || tc_isvalid(q, t, F.col, lr)) ? 1ULL : 0ULL;
+      int w = F.off & ~7;
+      if (w != pend_off) {
+        if (pend) atomicAdd((unsigned long long*)(rec + pend_off), pend);
+        pend = 0;
+        pend_off = w;
+      }
+      pend += inc << ((F.off & 4) ? 32 : 0);
+      continue;
+    }
+    if (!tc_isvalid(q, t, F.col, lr)) continue;
+    uint64_t b = tc_bits(q, t, F.col, lr);
+    int dt = q.col[F.col].dtype;
+    switch (F.kind) {
+      case F_SUM_DD: dd_atomic_add((double*)p, (double*)(p + 8), pmb_bits_to_f64(b, dt)); break;
+      case F_SUM_I: atomicAdd((unsigned long long*)p, (unsigned long long)pmb_bits_to_i64(b, dt)); break;
+      // a stale read can only be weaker than the stored extreme, so skipping is safe
+      case F_MIN_I: {
+        long long v = (long long)pmb_bits_to_i64(b, dt);
+        if (v < *(const long long*)p) atomicMin((long long*)p, v);
+        break;
+      }
+      case F_MAX_I: {
+        long long v = (long long)pmb_bits_to_i64(b, dt);
+        if (v > *(const long long*)p) atomicMax((long long*)p, v);
+        break;
+      }
+      case F_MIN_U:
+        if (b < *(const unsigned long long*)p) atomicMin((unsigned long long*)p, (unsigned long long)b);
+        break;
+      case F_MAX_U:
+        if (b > *(const unsigned long long*)p) atomicMax((unsigned long long*)p, (unsigned long long)b);
+        break;
+      case F_MIN_F: {
+        long long k = minmax_key(F, b, dt, true);
+        if (k < *(const long long*)p) atomicMin((long long*)p, k);
+        break;
+      }
+      default: {
+        long long k = minmax_key(F, b, dt, false);
+        if (k > *(const long long*)p) atomicMax((long long*)p, k);
+        break;
+      }
+    }
+  }
+  if (pend) atomicAdd((unsigned long long*)(rec + pend_off), pend);
+}
+
+// Merges a finished record `src` into `dst` (global memory, atomics).
 __device__ __forceinline__ void merge_record(const DQuery& q, uint8_t* dst, const uint8_t* src) {
   for (int i = 0; i < q.n_fields; i++) {
     const DField F = q.field[i];
@@ -425,6 +547,48 @@ __device__ __forceinline__ void merge_record(const DQuery& q, uint8_t* dst, cons
       default: {
         unsigned long long v = *(const unsigned long long*)s;
         if (v) atomicMax((unsigned long long*)d, v);
+        break;
+      }
+    }
+  }
+}
+
+// Merges record `src` into `dst` when one thread owns both (no atomics).
+__device__ __forceinline__ void merge_private(const DQuery& q, uint8_t* dst, const uint8_t* src) {
+  for (int i = 0; i < q.n_fields; i++) {
+    const DField F = q.field[i];
+    uint8_t* d = dst + F.off;
+    const uint8_t* s = src + F.off;
+    switch (F.kind) {
+      case F_LEN:
+      case F_CNT: *(unsigned int*)d += *(const unsigned int*)s; break;
+      case F_SUM_DD: {
+        double hi = *(const double*)s, lo = *(const double*)(s + 8);
+        dd_plain_add((double*)d, (double*)(d + 8), hi);
+        *(double*)(d + 8) += lo;
+        break;
+      }
+      case F_SUM_I: *(unsigned long long*)d += *(const unsigned long long*)s; break;
+      case F_MIN_I:
+      case F_MIN_F: {
+        long long v = *(const long long*)s;
+        if (v < *(long long*)d) *(long long*)d = v;
+        break;
+      }
+      case F_MAX_I:
+      case F_MAX_F: {
+        long long v = *(const long long*)s;
+        if (v > *(long long*)d) *(long long*)d = v;
+        break;
+      }
+      case F_MIN_U: {
+        unsigned long long v = *(const unsigned long long*)s;
+        if (v < *(unsigned long long*)d) *(unsigned long long*)d = v;
+        break;
+      }
+      default: {
+        unsigned long long v = *(const unsigned long long*)s;
+        if (v > *(unsigned long long*)d) *(unsigned long long*)d = v;
         break;
       }
     }

@@ -23,6 +23,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -62,11 +64,14 @@ __global__ void k_sketch(const __grid_constant__ DQuery q, int64_t m, unsigned l
   atomicAdd(&set_cnt[s], 1u);
 }
 
-// distinct count, singletons and doubletons of the sample
+// distinct count, singletons, doubletons and the histogram of per-key sample counts
 __global__ void k_sketch_reduce(const unsigned long long* __restrict__ set_keys,
-                                const unsigned int* __restrict__ set_cnt, unsigned long long* __restrict__ out) {
+                                const unsigned int* __restrict__ set_cnt, unsigned long long* __restrict__ out,
+                                unsigned int* __restrict__ hist) {
   __shared__ unsigned long long acc[3];
+  __shared__ unsigned int sh[SK_HIST];
   if (threadIdx.x < 3) acc[threadIdx.x] = 0;
+  for (int i = threadIdx.x; i < SK_HIST; i += blockDim.x) sh[i] = 0;
   __syncthreads();
   unsigned long long d = 0, f1 = 0, f2 = 0;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < SK_SLOTS; s += gridDim.x * blockDim.x) {
@@ -75,6 +80,7 @@ __global__ void k_sketch_reduce(const unsigned long long* __restrict__ set_keys,
       unsigned int c = set_cnt[s];
       f1 += c == 1;
       f2 += c == 2;
+      atomicAdd(&sh[c < SK_HIST ? c : SK_HIST - 1], 1u);
     }
   }
   atomicAdd(&acc[0], d);
@@ -82,6 +88,28 @@ __global__ void k_sketch_reduce(const unsigned long long* __restrict__ set_keys,
   atomicAdd(&acc[2], f2);
   __syncthreads();
   if (threadIdx.x < 3) atomicAdd(&out[threadIdx.x], acc[threadIdx.x]);
+  for (int i = threadIdx.x; i < SK_HIST; i += blockDim.x)
+    if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// keys of the sample with count >= t1 -> hot list, t2 <= count < t1 -> warm list
+__global__ void k_sketch_select(const unsigned long long* __restrict__ set_keys, const unsigned int* __restrict__ set_cnt,
+                                unsigned int t1, unsigned int t2, unsigned long long* __restrict__ hot,
+                                unsigned int* __restrict__ hot_n, unsigned int hot_cap,
+                                unsigned long long* __restrict__ warm, unsigned int* __restrict__ warm_n,
+                                unsigned int warm_cap) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < SK_SLOTS; s += gridDim.x * blockDim.x) {
+    unsigned long long k = set_keys[s];
+    if (k == PMB_EMPTY64) continue;
+    unsigned int c = set_cnt[s];
+    if (c >= t1) {
+      unsigned int i = atomicAdd(hot_n, 1u);
+      if (i < hot_cap) hot[i] = k;
+    } else if (c >= t2) {
+      unsigned int i = atomicAdd(warm_n, 1u);
+      if (i < warm_cap) warm[i] = k;
+    }
+  }
 }
 
 // ============================================================================ table init
@@ -158,30 +186,83 @@ __device__ __forceinline__ int sfind64(unsigned long long* skeys, int S, int pro
   return -1;
 }
 
-template <bool K128>
-__device__ __forceinline__ void process_row(const HashParams& P, const TileCtx& t, int lr,
-                                            unsigned long long* skeys, uint8_t* srecs) {
-  const DQuery& q = P.q;
-  if (!eval_keep(q, t, lr)) return;
+// read-only lookup in the hot-key table (built once per CTA); -1 when the key is not hot
+__device__ __forceinline__ int hot_find(const unsigned long long* lk, const int* li, int slots, uint64_t key, uint64_t h) {
+  int i = (int)((h >> 24) & (uint64_t)(slots - 1));
+  for (int p = 0; p < slots; p++) {
+    unsigned long long k = lk[i];
+    if (k == key) return li[i];
+    if (k == PMB_EMPTY64) return -1;
+    i = (i + 1) & (slots - 1);
+  }
+  return -1;
+}
+
+// per-thread cycle accumulators of the optional phase counters
+struct PathCycles {
+  long long pred = 0, hot = 0, smem = 0, sfind = 0, gfind = 0, apply = 0;
+};
+
+// Processes rows [base, base + NT) of a tile, one row per thread, the whole warp together:
+//   hot keys    -> warp-private records: lanes with the same hot key are grouped with
+//                  __match_any_sync and the group's first lane applies all their rows (no atomics);
+//   other keys  -> the CTA-shared table when the key is (or can be) there, else the global table.
+// Returns bit 0 = row went to the shared table, bit 1 = row went global (for phase counters).
+template <int NT, bool K128>
+__device__ __forceinline__ int process_rows(const HashParams& P, const DQuery& q, const TileCtx& t, int lr, bool in_range,
+                                            unsigned long long* skeys, uint8_t* srecs, const unsigned long long* hlk,
+                                            const int* hli, uint8_t* hrecs, int n_hot, PathCycles& pc) {
+  const int lane = threadIdx.x & 31;
   const int rb = q.rec_bytes;
-  if (!K128) {
-    uint64_t key = pack_key64(q, t, lr);
-    uint64_t h = pmb_fmix64(key);
-    if (P.smem_slots) {
-      int si = sfind64(skeys, P.smem_slots, P.smem_probe, key, h);
-      if (si >= 0) {
-        apply_row<true>(q, t, srecs + (size_t)si * rb, lr);
-        return;
-      }
-    }
-    int64_t gi = gfind64(P, key, h);
-    if (gi >= 0) apply_row<false>(q, t, P.grecs + (size_t)gi * rb, lr);
-  } else {
+  const bool ks = P.kstats != nullptr;
+  long long ck0 = ks ? clock64() : 0;
+  bool keep = in_range && eval_keep(q, t, lr);
+  if (K128) {
+    if (!keep) return 0;
     Key128 key = pack_key128(q, t, lr);
     uint64_t h = pmb_fmix64(key.lo ^ pmb_fmix64(key.hi + 0x9E3779B97F4A7C15ULL));
     int64_t gi = gfind128(P, key, h);
-    if (gi >= 0) apply_row<false>(q, t, P.grecs + (size_t)gi * rb, lr);
+    if (gi >= 0) apply_row_global(q, t, P.grecs + (size_t)gi * rb, lr);
+    return 2;
   }
+  uint64_t key = keep ? pack_key64(q, t, lr) : 0;
+  uint64_t h = pmb_fmix64(key);
+  int hot = -1;
+  if (n_hot && keep && key != PMB_EMPTY64) hot = hot_find(hlk, hli, P.hot_lut_slots, key, h);
+  long long ck1 = ks ? clock64() : 0;
+  unsigned hot_mask = __ballot_sync(0xffffffffu, hot >= 0);
+  if (hot_mask) {
+    unsigned peers = __match_any_sync(0xffffffffu, hot) & hot_mask;
+    if (hot >= 0 && lane == __ffs(peers) - 1) {
+      uint8_t* rec = hrecs + ((size_t)(threadIdx.x >> 5) * P.hot_cap + hot) * rb;
+      for (unsigned m = peers; m; m &= m - 1) apply_row_private(q, t, rec, lr - lane + (__ffs(m) - 1));
+    }
+  }
+  __syncwarp();
+  long long ck2 = ks ? clock64() : 0;
+  if (ks) {
+    pc.pred += ck1 - ck0;
+    pc.hot += ck2 - ck1;
+  }
+  if (!keep || hot >= 0) return 0;
+  if (P.smem_slots) {
+    int si = sfind64(skeys, P.smem_slots, P.smem_probe, key, h);
+    if (si >= 0) {
+      apply_row_shared(q, t, srecs + (size_t)si * rb, lr);
+      if (ks) pc.smem += clock64() - ck2;
+      return 1;
+    }
+  }
+  long long ck3 = ks ? clock64() : 0;
+  int64_t gi = gfind64(P, key, h);
+  long long ck4 = ks ? clock64() : 0;
+  if (gi >= 0) apply_row_global(q, t, P.grecs + (size_t)gi * rb, lr);
+  if (ks) {
+    pc.sfind += ck3 - ck2;
+    pc.gfind += ck4 - ck3;
+    pc.apply += clock64() - ck4;
+  }
+  return 2;
 }
 
 template <int NT, bool K128>
@@ -190,19 +271,37 @@ __global__ void __launch_bounds__(NT, 1) k_hash_agg(const __grid_constant__ Hash
   __shared__ int32_t s_doff[PMB_MAX_COLS];
   __shared__ int32_t s_voff[PMB_MAX_COLS];
   __shared__ int s_abort;
-  const DQuery& q = P.q;
+  // the query descriptor is read with data-dependent indices on every row: keep a copy in
+  // shared memory (parameter space would serialise those reads through the constant cache)
+  __shared__ __align__(16) DQuery sq;
   const int tid = threadIdx.x;
+  for (int i = tid; i < (int)(sizeof(DQuery) / 4); i += NT)
+    reinterpret_cast<uint32_t*>(&sq)[i] = reinterpret_cast<const uint32_t*>(&P.q)[i];
+  __syncthreads();
+  const DQuery& q = sq;
+  constexpr int W = NT / 32;
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm);
   unsigned long long* skeys = reinterpret_cast<unsigned long long*>(sm + P.smem_keys_off);
   uint8_t* srecs = sm + P.smem_recs_off;
+  unsigned long long* hlk = reinterpret_cast<unsigned long long*>(sm + P.hot_lut_off);
+  int* hli = reinterpret_cast<int*>(sm + P.hot_lut_off + 8 * P.hot_lut_slots);
+  uint8_t* hrecs = sm + P.hot_recs_off;
   const int S = P.smem_slots;
   const int TILE = P.tile_rows;
   const int STAGES = P.stages;
-
-  // shared table: keys EMPTY, records identity (so a claim needs no record publication)
-  for (int i = tid; i < S; i += NT) skeys[i] = PMB_EMPTY64;
   const int rw = q.rec_bytes / 8;
+  const int rb = q.rec_bytes;
+  const int n_hot = (K128 || !P.hot_keys) ? 0 : (int)min(*P.hot_n, (unsigned)P.hot_cap);
+  const int n_warm = (K128 || !P.warm_keys || !S) ? 0 : (int)min(*P.warm_n, (unsigned)(S / 2));
+
+  // shared table and hot records start at identity, so claiming a slot needs no publication
+  for (int i = tid; i < S; i += NT) skeys[i] = PMB_EMPTY64;
   for (int w = tid; w < S * rw; w += NT) reinterpret_cast<uint64_t*>(srecs)[w] = P.rec_init.w[w % rw];
+  if (n_hot) {
+    for (int i = tid; i < P.hot_lut_slots; i += NT) hlk[i] = PMB_EMPTY64;
+    for (int w = tid; w < W * P.hot_cap * rw; w += NT)
+      reinterpret_cast<uint64_t*>(hrecs)[w] = P.rec_init.w[w % rw];
+  }
   if (tid < PMB_MAX_COLS) {
     s_doff[tid] = P.stage_data_off[tid];
     s_voff[tid] = P.stage_valid_off[tid];
@@ -211,6 +310,24 @@ __global__ void __launch_bounds__(NT, 1) k_hash_agg(const __grid_constant__ Hash
     for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
     mbar_fence_init();
     s_abort = 0;
+  }
+  __syncthreads();
+  // hot-key lookup table (distinct keys: each insert claims its own slot)
+  for (int i = tid; i < n_hot; i += NT) {
+    unsigned long long k = P.hot_keys[i];
+    int j = (int)((pmb_fmix64(k) >> 24) & (uint64_t)(P.hot_lut_slots - 1));
+    for (int p = 0; p < P.hot_lut_slots; p++) {
+      if (atomicCAS(&hlk[j], PMB_EMPTY64, k) == PMB_EMPTY64) {
+        hli[j] = i;
+        break;
+      }
+      j = (j + 1) & (P.hot_lut_slots - 1);
+    }
+  }
+  // warm keys preloaded into the shared table
+  for (int i = tid; i < n_warm; i += NT) {
+    unsigned long long k = P.warm_keys[i];
+    sfind64(skeys, S, S, k, pmb_fmix64(k));
   }
   __syncthreads();
 
@@ -237,21 +354,55 @@ __global__ void __launch_bounds__(NT, 1) k_hash_agg(const __grid_constant__ Hash
     for (int64_t k = 0; k < STAGES && k < my_tiles; k++) issue(k);
   }
 
+  const bool ks = P.kstats != nullptr;
+  long long c_wait = 0, c_proc = 0, c0 = 0;
+  unsigned int n_smem = 0, n_glob = 0;
+  PathCycles pc;
   int64_t k = 0;
   for (; k < my_tiles; k++) {
     int s = (int)(k % STAGES);
     uint32_t parity = (uint32_t)((k / STAGES) & 1);
+    if (ks && tid == 0) c0 = clock64();
     bool ok = mbar_wait_bounded(&bars[s], parity);
+    if (ks && tid == 0) {
+      long long c1 = clock64();
+      c_wait += c1 - c0;
+      c0 = c1;
+    }
     if (!ok) s_abort = 1;
-    if (ok) {
+    __syncwarp();
+    // every lane of a warp takes the same path (the warp-level grouping needs all 32)
+    bool wok = __all_sync(0xffffffffu, ok);
+    if (wok) {
       TileCtx t{sm + P.stage_region_off + (size_t)s * P.stage_bytes, s_doff, s_voff, 0};
-      for (int lr = tid; lr < TILE; lr += NT) process_row<K128>(P, t, lr, skeys, srecs);
+      for (int base = 0; base < TILE; base += NT) {
+        int path = process_rows<NT, K128>(P, q, t, base + tid, base + tid < TILE, skeys, srecs, hlk, hli, hrecs, n_hot, pc);
+        n_smem += path == 1;
+        n_glob += path == 2;
+      }
     }
     __syncthreads();
+    if (ks && tid == 0) c_proc += clock64() - c0;
     if (s_abort) break;
     if (tid == 0 && k + STAGES < my_tiles) {
       fence_proxy_async();
       issue(k + STAGES);
+    }
+  }
+  if (ks) {
+    long long v[6] = {pc.pred, pc.hot, pc.smem, pc.sfind, pc.gfind, pc.apply};
+    for (int i = 0; i < 6; i++) {
+      long long x = v[i];
+      for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if ((tid & 31) == 0) atomicAdd(&P.kstats[6 + i], (unsigned long long)x);
+    }
+    atomicAdd(&P.kstats[4], (unsigned long long)n_smem);
+    atomicAdd(&P.kstats[5], (unsigned long long)n_glob);
+    if (tid == 0) {
+      atomicAdd(&P.kstats[0], (unsigned long long)c_wait);
+      atomicAdd(&P.kstats[1], (unsigned long long)c_proc);
+      atomicAdd(&P.kstats[3], (unsigned long long)my_tiles);
+      c0 = clock64();
     }
   }
   if (s_abort) {
@@ -268,18 +419,35 @@ __global__ void __launch_bounds__(NT, 1) k_hash_agg(const __grid_constant__ Hash
   // ragged tail tile straight from global memory
   if (P.tail_rows > 0 && (int64_t)blockIdx.x == n_full % G) {
     TileCtx t{nullptr, s_doff, s_voff, n_full * TILE};
-    for (int lr = tid; lr < P.tail_rows; lr += NT) process_row<K128>(P, t, lr, skeys, srecs);
+    for (int base = 0; base < P.tail_rows; base += NT)
+      process_rows<NT, K128>(P, q, t, base + tid, base + tid < P.tail_rows, skeys, srecs, hlk, hli, hrecs, n_hot, pc);
   }
   __syncthreads();
 
-  // merge the shared table into the global table
   if (!K128) {
+    // hot keys: fold the warps' private records, then one merge per touched key
+    const int len_off = q.field[0].off;  // field 0 is always the row count
+    for (int i = tid; i < n_hot; i += NT) {
+      uint8_t* r0 = hrecs + (size_t)i * rb;
+      for (int w = 1; w < W; w++) merge_private(q, r0, hrecs + ((size_t)w * P.hot_cap + i) * rb);
+      if (*reinterpret_cast<const unsigned int*>(r0 + len_off) == 0) continue;
+      unsigned long long key = P.hot_keys[i];
+      int64_t gi = gfind64(P, key, pmb_fmix64(key));
+      if (gi >= 0) merge_record(q, P.grecs + (size_t)gi * rb, r0);
+    }
+    // the shared table (preloaded warm keys may have seen no rows)
     for (int i = tid; i < S; i += NT) {
       unsigned long long key = skeys[i];
       if (key == PMB_EMPTY64) continue;
+      const uint8_t* r = srecs + (size_t)i * rb;
+      if (*reinterpret_cast<const unsigned int*>(r + len_off) == 0) continue;
       int64_t gi = gfind64(P, key, pmb_fmix64(key));
-      if (gi >= 0) merge_record(q, P.grecs + (size_t)gi * q.rec_bytes, srecs + (size_t)i * q.rec_bytes);
+      if (gi >= 0) merge_record(q, P.grecs + (size_t)gi * rb, r);
     }
+  }
+  if (ks) {
+    __syncthreads();
+    if (tid == 0) atomicAdd(&P.kstats[2], (unsigned long long)(clock64() - c0));
   }
 }
 
@@ -467,29 +635,36 @@ int pmb_groupby_sketch(pmb_handle* h, const CompiledQuery& cq, SketchOut* out) {
   int64_t m = std::min<int64_t>(q.n_rows, SK_SAMPLES);
   out->samples = m;
   out->distinct = out->singletons = out->doubletons = 0;
+  memset(out->hist, 0, sizeof(out->hist));
+  out->set_keys = nullptr;
+  out->set_cnt = nullptr;
   if (m == 0) return PMB_OK;
   unsigned long long* keys = (unsigned long long*)pmb_ws_alloc(h, sizeof(unsigned long long) * SK_SLOTS);
   unsigned int* cnt = (unsigned int*)pmb_ws_alloc(h, sizeof(unsigned int) * SK_SLOTS);
-  unsigned long long* res = (unsigned long long*)pmb_ws_alloc(h, 64);
+  unsigned long long* res = (unsigned long long*)pmb_ws_alloc(h, 64 + 4 * SK_HIST);
   if (!keys || !cnt || !res) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sketch)");
+  unsigned int* hist = (unsigned int*)(res + 8);
   PMB_CUDA(h, cudaMemsetAsync(keys, 0xFF, sizeof(unsigned long long) * SK_SLOTS, h->stream));
   PMB_CUDA(h, cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * SK_SLOTS, h->stream));
-  PMB_CUDA(h, cudaMemsetAsync(res, 0, 64, h->stream));
+  PMB_CUDA(h, cudaMemsetAsync(res, 0, 64 + 4 * SK_HIST, h->stream));
   pmb_kernel_begin(h, "sketch");
   if (q.key_bits > 64) k_sketch<true><<<(unsigned)((m + 255) / 256), 256, 0, h->stream>>>(q, m, keys, cnt);
   else k_sketch<false><<<(unsigned)((m + 255) / 256), 256, 0, h->stream>>>(q, m, keys, cnt);
   pmb_kernel_end(h);
   PMB_CUDA(h, cudaGetLastError());
   pmb_kernel_begin(h, "sketch_reduce");
-  k_sketch_reduce<<<64, 256, 0, h->stream>>>(keys, cnt, res);
+  k_sketch_reduce<<<64, 256, 0, h->stream>>>(keys, cnt, res, hist);
   pmb_kernel_end(h);
   PMB_CUDA(h, cudaGetLastError());
-  PMB_CUDA(h, cudaMemcpyAsync(h->pinned, res, 24, cudaMemcpyDeviceToHost, h->stream));
+  PMB_CUDA(h, cudaMemcpyAsync(h->pinned, res, 64 + 4 * SK_HIST, cudaMemcpyDeviceToHost, h->stream));
   PMB_CUDA(h, cudaStreamSynchronize(h->stream));
   const unsigned long long* r = (const unsigned long long*)h->pinned;
   out->distinct = (int64_t)r[0];
   out->singletons = (int64_t)r[1];
   out->doubletons = (int64_t)r[2];
+  memcpy(out->hist, h->pinned + 64, 4 * SK_HIST);
+  out->set_keys = keys;
+  out->set_cnt = cnt;
   return PMB_OK;
 }
 
@@ -515,12 +690,16 @@ static void build_output_columns(const CompiledQuery& cq, pmb_result* r, const p
 }
 
 int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
-                     pmb_result* r) {
+                     const SketchOut* sk, pmb_result* r) {
   DQuery& q = cq.dq;
   const bool K128 = q.key_bits > 64;
   const int rec = q.rec_bytes;
   Plan pl;
   pl.strategy = strategy;
+  if (const char* e = getenv("PMB_TILE")) {
+    int v = atoi(e);
+    if (v >= 256 && v <= 8192 && v % 128 == 0) pl.tile = v;
+  }
   if (K128 && strategy == PMB_STRATEGY_SMEM_HASH) pl.strategy = PMB_STRATEGY_GLOBAL_HASH;
   HashParams P;
   memset(&P, 0, sizeof(P));
@@ -528,8 +707,9 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
   P.tile_rows = pl.tile;
   layout_stage(cq, pl.tile, P);
   // shared memory budget: mbarriers, stages, table
-  const int budget = h->max_smem_optin - 1024;
-  int stages = 3;
+  const int budget = h->max_smem_optin - 4096;  // static shared memory (descriptor copy) comes on top
+  int stages = 2;
+  if (const char* e = getenv("PMB_STAGES")) stages = std::max(1, std::min(atoi(e), 4));
   while (stages > 1 && 128 + stages * P.stage_bytes > budget / 2) stages--;
   int smem_fixed = 128 + stages * P.stage_bytes;
   if (smem_fixed > budget) {
@@ -541,6 +721,20 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     smem_fixed = 128 + stages * P.stage_bytes;
     if (smem_fixed > budget) return pmb_fail(h, PMB_E_UNSUPPORTED, "query touches too many columns for one tile");
   }
+  // hot tier: per-warp private records for the heaviest sample keys
+  int nt = 1024;
+  if (const char* e = getenv("PMB_NT")) nt = atoi(e);
+  if (nt != 256 && nt != 512 && nt != 1024) nt = 1024;
+  if (K128) nt = 512;
+  int hot_cap = (K128 || !sk || !sk->set_keys) ? 0 : 32;
+  if (const char* e = getenv("PMB_HOT")) hot_cap = std::max(0, std::min(atoi(e), 128));
+  while (hot_cap > 0 && smem_fixed + (nt / 32) * hot_cap * rec + 16 * 2 * hot_cap > budget / 2) hot_cap /= 2;
+  int hot_lut = hot_cap ? (int)next_pow2((uint64_t)(2 * hot_cap)) : 0;
+  P.hot_cap = hot_cap;
+  P.hot_lut_slots = hot_lut;
+  P.hot_lut_off = (int)pmb_align((size_t)smem_fixed, 16);
+  P.hot_recs_off = (int)pmb_align((size_t)(P.hot_lut_off + hot_lut * 12), 16);
+  smem_fixed = P.hot_recs_off + (nt / 32) * hot_cap * rec;
   int S = 0;
   if (!K128) {
     int room = budget - smem_fixed;
@@ -551,14 +745,59 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
       int want = (int)next_pow2((uint64_t)std::max<int64_t>(2 * est, 64));
       if (want < S) S = want;
     }
+    // tuning override: PMB_SMEM_SLOTS=<pow2> (0 disables the shared-memory table)
+    if (const char* e = getenv("PMB_SMEM_SLOTS")) {
+      int v = atoi(e);
+      if (v == 0) S = 0;
+      else if (v > 0 && v < S) S = (int)next_pow2((uint64_t)v);
+    }
   }
   P.stages = stages;
   P.smem_slots = S;
   P.smem_probe = S ? std::min(S, (strategy == PMB_STRATEGY_SMEM_HASH) ? 64 : 16) : 0;
   P.stage_region_off = 128;
-  P.smem_keys_off = (int)pmb_align((size_t)(128 + stages * P.stage_bytes), 16);
+  P.smem_keys_off = (int)pmb_align((size_t)smem_fixed, 16);
   P.smem_recs_off = P.smem_keys_off + S * 8;
   int smem = P.smem_recs_off + S * rec;
+  // hot / warm key lists from the sample histogram
+  if (hot_cap || S) {
+    if (sk && sk->set_keys) {
+      unsigned int suffix[SK_HIST + 1];
+      suffix[SK_HIST] = 0;
+      for (int c = SK_HIST - 1; c >= 0; c--) suffix[c] = suffix[c + 1] + sk->hist[c];
+      unsigned int t1 = SK_HIST;
+      for (int c = 4; c < SK_HIST; c++)
+        if (suffix[c] <= (unsigned)hot_cap) {
+          t1 = c;
+          break;
+        }
+      if (!hot_cap) t1 = SK_HIST;
+      unsigned int warm_cap = (unsigned)(S / 2);
+      unsigned int t2 = t1;
+      for (int c = 2; c < (int)t1; c++)
+        if (suffix[c] - suffix[t1] <= warm_cap) {
+          t2 = c;
+          break;
+        }
+      unsigned long long* lists = (unsigned long long*)pmb_ws_alloc(h, 8 * ((size_t)hot_cap + warm_cap) + 64);
+      if (!lists) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (hot keys)");
+      unsigned int* counts = (unsigned int*)(lists + hot_cap + warm_cap);
+      PMB_CUDA(h, cudaMemsetAsync(counts, 0, 16, h->stream));
+      pmb_kernel_begin(h, "sketch_select");
+      k_sketch_select<<<64, 256, 0, h->stream>>>(sk->set_keys, sk->set_cnt, t1, t2, lists, counts, (unsigned)hot_cap,
+                                                 lists + hot_cap, counts + 1, warm_cap);
+      pmb_kernel_end(h);
+      PMB_CUDA(h, cudaGetLastError());
+      P.hot_keys = hot_cap ? lists : nullptr;
+      P.hot_n = counts;
+      P.warm_keys = warm_cap ? lists + hot_cap : nullptr;
+      P.warm_n = counts + 1;
+    }
+  }
+  if (!P.hot_keys) {
+    P.hot_cap = 0;
+    P.hot_lut_slots = 0;
+  }
   const int64_t n = q.n_rows;
   P.n_full_tiles = n / pl.tile;
   P.tail_rows = (int32_t)(n % pl.tile);
@@ -568,6 +807,11 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
   uint64_t cap = next_pow2((uint64_t)std::max<int64_t>(2 * est, 1024));
   if (uq->capacity_hint > 0) cap = next_pow2((uint64_t)std::max<int64_t>(2 * uq->capacity_hint, 1024));
   const uint64_t cap_max = next_pow2((uint64_t)std::max<int64_t>(2 * n, 1024));
+  // tuning override: PMB_GCAP_MULT=<k> multiplies the global table capacity
+  if (const char* e = getenv("PMB_GCAP_MULT")) {
+    int k = atoi(e);
+    if (k > 1) cap = next_pow2(cap * (uint64_t)k);
+  }
   cap = std::min(cap, cap_max);
 
   const int n_out = q.n_keys + q.n_aggs;
@@ -612,8 +856,33 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     P.gprobe = (int)std::min<uint64_t>(cap, 1u << 14);
     P.status = status;
     int grid = (int)std::max<int64_t>(1, std::min<int64_t>(P.n_full_tiles, (int64_t)h->sm_count));
-    int rc = K128 ? launch_hash<512, true>(h, P, smem, grid) : launch_hash<512, false>(h, P, smem, grid);
+    unsigned long long* kst = nullptr;
+    if (getenv("PMB_KSTATS")) {
+      kst = (unsigned long long*)pmb_ws_alloc(h, 128);
+      if (!kst) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (kstats)");
+      PMB_CUDA(h, cudaMemsetAsync(kst, 0, 128, h->stream));
+    }
+    P.kstats = kst;
+    int rc;
+    if (K128) rc = launch_hash<512, true>(h, P, smem, grid);
+    else if (nt == 1024) rc = launch_hash<1024, false>(h, P, smem, grid);
+    else if (nt == 256) rc = launch_hash<256, false>(h, P, smem, grid);
+    else rc = launch_hash<512, false>(h, P, smem, grid);
     if (rc) return rc;
+    if (kst) {
+      unsigned long long hk[16];
+      PMB_CUDA(h, cudaMemcpyAsync(hk, kst, 128, cudaMemcpyDeviceToHost, h->stream));
+      PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+      fprintf(stderr, "kstats: grid=%d nt=%d hot=%d S=%d tile=%d stages=%d tiles=%llu wait_cyc/tile=%.0f proc_cyc/tile=%.0f "
+              "flush_cyc/cta=%.0f smem_rows=%llu global_rows=%llu\n", grid, nt, P.hot_cap, P.smem_slots, P.tile_rows, P.stages,
+              hk[3], (double)hk[0] / (double)(hk[3] ? hk[3] : 1), (double)hk[1] / (double)(hk[3] ? hk[3] : 1),
+              (double)hk[2] / grid, hk[4], hk[5]);
+      double rows = (double)q.n_rows;
+      fprintf(stderr, "  per-row cycles (thread-summed): pred+key %.0f, hot-warp %.0f | per smem row %.0f | per global row: "
+              "sfind %.0f gfind %.0f apply %.0f\n", hk[6] / rows, hk[7] / rows, hk[8] / (double)(hk[4] ? hk[4] : 1),
+              hk[9] / (double)(hk[5] ? hk[5] : 1), hk[10] / (double)(hk[5] ? hk[5] : 1),
+              hk[11] / (double)(hk[5] ? hk[5] : 1));
+    }
     F.gkeys = gkeys;
     F.grecs = grecs;
     F.gcap = cap;
@@ -679,16 +948,18 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
   } else {
     int strategy = q->strategy;
     int64_t est = q->capacity_hint;
+    static thread_local SketchOut sk;  // large (histogram); one per host thread
+    bool have_sk = false;
     if (est <= 0 || strategy == PMB_STRATEGY_AUTO) {
-      SketchOut sk;
       rc = pmb_groupby_sketch(h, cq, &sk);
       if (rc) return bail(rc);
+      have_sk = true;
       int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
       if (est <= 0) est = e;
       if (strategy == PMB_STRATEGY_AUTO) strategy = pmb_choose_strategy(h, cq, sk, est);
     }
     if (strategy == PMB_STRATEGY_SORT) strategy = PMB_STRATEGY_GLOBAL_HASH;  // sort path: see pmb_sort.cu
-    rc = pmb_groupby_hash(h, cq, q, strategy, est, r);
+    rc = pmb_groupby_hash(h, cq, q, strategy, est, have_sk ? &sk : nullptr, r);
     if (rc) return bail(rc);
   }
   rc = pmb_finish_outputs(h, r, q->output_on_device == 0);

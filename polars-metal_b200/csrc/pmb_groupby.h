@@ -31,6 +31,17 @@ struct HashParams {
   uint64_t gcap;
   int32_t gprobe;
   unsigned int* status;       // [0] status bits, [1] EMPTY-key slot used
+  unsigned long long* kstats; // optional phase counters (PMB_KSTATS=1), else nullptr
+  // hot keys (heaviest keys of the sketch sample): per-warp private records, no atomics
+  const unsigned long long* hot_keys;
+  const unsigned int* hot_n;  // device count (<= hot_cap)
+  int32_t hot_cap;
+  int32_t hot_lut_slots;      // power of two >= 2 * hot_cap
+  int32_t hot_lut_off;        // shared: u64 keys[hot_lut_slots] then int idx[hot_lut_slots]
+  int32_t hot_recs_off;       // shared: warps * hot_cap records
+  // warm keys (next heaviest): preloaded into the CTA-shared table
+  const unsigned long long* warm_keys;
+  const unsigned int* warm_n;
 };
 
 #define PMB_MAX_OUT (PMB_MAX_KEYS + PMB_MAX_AGGS)
@@ -48,18 +59,24 @@ struct FinParams {
   uint8_t* out_valid[PMB_MAX_OUT];
 };
 
+#define SK_HIST 1024
+
 struct SketchOut {
   int64_t samples;
   int64_t distinct;
   int64_t singletons;
   int64_t doubletons;
+  unsigned int hist[SK_HIST];  // keys of the sample by occurrence count (last bin: >= SK_HIST - 1)
+  // device-resident sample set (valid until the next workspace reset)
+  const unsigned long long* set_keys;
+  const unsigned int* set_cnt;
 };
 
 int pmb_groupby_sketch(pmb_handle* h, const CompiledQuery& cq, SketchOut* out);
 int64_t pmb_estimate_groups(const SketchOut& s, int64_t n_rows);
 int pmb_choose_strategy(pmb_handle* h, const CompiledQuery& cq, const SketchOut& sk, int64_t est);
 int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
-                     pmb_result* r);
+                     const SketchOut* sk, pmb_result* r);
 
 // Sets bit p of a bitmap for every lane whose `bit` is true. The warp's positions are
 // consecutive from p_first, so they touch at most two 32-bit words: one atomicOr each.

@@ -176,7 +176,7 @@ struct pmb_handle {
     size_t top;
   };
   std::vector<Block> ws;
-  // small pinned host staging for status words / counts
+  // pinned host staging (64 KiB) for status words, counts and the sketch histogram
   uint8_t* pinned = nullptr;
   std::string err;
   int sm_count = 148;

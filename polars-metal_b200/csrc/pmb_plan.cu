@@ -255,6 +255,8 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
     fields.push_back(f);
     return (int)fields.size() - 1;
   };
+  // every record carries a row count: it tells a touched group from an untouched slot
+  field(F_LEN, 0);
   for (int a = 0; a < q->n_aggs; a++) {
     const pmb_agg& A = q->aggs[a];
     DAggOut& o = d.agg[a];
@@ -323,8 +325,12 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
   int rc = pmb_compile_predicate(h, q->predicate, &cq->map, cols, n_cols, &d.prog);
   if (rc) return rc;
 
-  // columns and row count
+  // columns and row count (pointers are filled in when the columns are staged)
   d.n_cols = (int)cq->map.user.size();
+  for (int c = 0; c < d.n_cols; c++) {
+    d.col[c].dtype = cols[cq->map.user[c]].dtype;
+    d.col[c].elem = pmb_dtype_bytes(d.col[c].dtype);
+  }
   int64_t n = cols[cq->map.user[0]].length;
   for (int u : cq->map.user) {
     if (cols[u].length != n)

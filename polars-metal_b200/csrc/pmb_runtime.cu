@@ -310,7 +310,7 @@ int pmb_open(pmb_handle** out, int32_t device, uint64_t workspace_bytes) {
   h->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&h->call_start) != cudaSuccess || cudaEventCreate(&h->call_stop) != cudaSuccess ||
-      cudaMallocHost((void**)&h->pinned, 4096) != cudaSuccess) {
+      cudaMallocHost((void**)&h->pinned, 65536) != cudaSuccess) {
     pmb_close(h);
     return PMB_E_CUDA;
   }
