@@ -1,0 +1,164 @@
+// pmb_device.cuh — device helpers shared by the prebuilt kernels and the kernels compiled at
+// run time (NVRTC). Only built-in types and intrinsics: no host headers, so NVRTC can compile it.
+#pragma once
+
+#ifdef __CUDACC_RTC__
+typedef unsigned long long uint64_t;
+typedef long long int64_t;
+typedef unsigned int uint32_t;
+typedef int int32_t;
+typedef unsigned short uint16_t;
+typedef short int16_t;
+typedef unsigned char uint8_t;
+typedef signed char int8_t;
+#else
+#include <stdint.h>
+#endif
+
+#define PMB_EMPTY64 0xFFFFFFFFFFFFFFFFULL
+
+// status bits written by kernels into the call's device status word
+#define PMB_ST_OVERFLOW 1u  // a hash table ran out of probes / capacity: rehash
+#define PMB_ST_TIMEOUT 2u   // a bounded wait gave up
+#define PMB_ST_BADARG 4u    // a device-side argument check failed
+
+// bounded spins: iterations before a wait gives up and reports PMB_ST_TIMEOUT
+#define PMB_SPIN_LIMIT (1u << 24)
+
+// ----------------------------------------------------------------------------- device helpers
+__device__ __forceinline__ uint32_t pmb_smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(pmb_smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(pmb_smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// 1-D bulk copy global -> shared (TMA engine), completion counted on `bar`.
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          pmb_smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(pmb_smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(pmb_smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; returns false on timeout
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < PMB_SPIN_LIMIT; it++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// MurmurHash3 64-bit finalizer (Appleby, public domain)
+__host__ __device__ __forceinline__ uint64_t pmb_fmix64(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+// total-order key of a double: monotone in IEEE order for non-NaN values (-0.0 < +0.0)
+__device__ __forceinline__ long long pmb_f64_key(double x) {
+  long long b = __double_as_longlong(x);
+  return b ^ ((b >> 63) & 0x7FFFFFFFFFFFFFFFLL);
+}
+__device__ __forceinline__ double pmb_f64_from_key(long long k) {
+  long long b = k ^ ((k >> 63) & 0x7FFFFFFFFFFFFFFFLL);
+  return __longlong_as_double(b);
+}
+
+// Exact-to-double-double accumulation: atomicAdd returns the old partial sum, so the rounding
+// error of that very addition is recovered with TwoSum (Knuth) and added into the low word.
+__device__ __forceinline__ void dd_atomic_add(double* hi, double* lo, double x) {
+  double old = atomicAdd(hi, x);
+  double s = old + x;
+  if (!isfinite(s)) return;
+  double bp = s - old;
+  double err = (old - (s - bp)) + (x - bp);
+  if (err != 0.0) atomicAdd(lo, err);
+}
+
+// TwoSum accumulation when one thread owns the record (no atomics)
+__device__ __forceinline__ void dd_plain_add(double* hi, double* lo, double x) {
+  double old = *hi;
+  double s = old + x;
+  *hi = s;
+  if (!isfinite(s)) return;
+  double bp = s - old;
+  *lo += (old - (s - bp)) + (x - bp);
+}
+
+
+// ----------------------------------------------------------------------------- exact float sums
+// A finite double x is summed as the integer X = trunc(x * 2^F), a 96-bit two's complement value
+// split into three 32-bit limbs that are added into three 64-bit words (limb 0 and 1 unsigned,
+// limb 2 signed). 64-bit words leave 31 bits of headroom, so up to 2^31 additions are exact and
+// the order of additions does not matter. F is chosen per column so that |x| < 2^(94 - F); a
+// value outside that range is reported (status bit + its exponent) and the call is re-run with a
+// wider range. NaN / +inf / -inf are tracked as flag bits beside the limbs.
+#define PMB_ST_FXRANGE 8u  // a float-sum value exceeded its column's fixed-point range
+#define PMB_FX_NAN 1u
+#define PMB_FX_PINF 2u
+#define PMB_FX_NINF 4u
+
+// biased exponent field of x (0 for zero / subnormal, 2047 for inf / NaN)
+__device__ __forceinline__ int pmb_fx_expo(double x) { return (int)((__double_as_longlong(x) >> 52) & 0x7FF); }
+
+// non-finite flag of x (0 for finite values)
+__device__ __forceinline__ unsigned pmb_fx_flag(double x) {
+  long long b = __double_as_longlong(x);
+  if (((b >> 52) & 0x7FF) != 0x7FF) return 0u;
+  if (b & 0xFFFFFFFFFFFFFLL) return PMB_FX_NAN;
+  return b < 0 ? PMB_FX_NINF : PMB_FX_PINF;
+}
+
+// true when the finite x fits the range of fraction bits F (|x| < 2^(94 - F))
+__device__ __forceinline__ bool pmb_fx_fits(double x, int F) { return pmb_fx_expo(x) < 94 - F + 1023; }
+
+// limbs of trunc(x * 2^F) for a finite x that fits
+__device__ __forceinline__ void pmb_fx_split(double x, int F, unsigned long long& l0, unsigned long long& l1,
+                                             unsigned long long& l2) {
+  long long b = __double_as_longlong(x);
+  int ex = (int)((b >> 52) & 0x7FF);
+  unsigned long long m = (unsigned long long)b & 0xFFFFFFFFFFFFFULL;
+  if (ex) m |= 1ULL << 52;
+  else ex = 1;
+  int sh = ex - 1075 + F;  // X = m * 2^sh, sh <= 41 when x fits
+  unsigned long long lo, hi;
+  if (sh >= 0) {
+    lo = m << sh;
+    hi = sh ? (m >> (64 - sh)) : 0ULL;
+  } else {
+    lo = sh > -64 ? (m >> (-sh)) : 0ULL;
+    hi = 0ULL;
+  }
+  if (b < 0) {  // two's complement negation of the 128-bit (hi, lo)
+    lo = ~lo + 1ULL;
+    hi = ~hi + (lo == 0ULL ? 1ULL : 0ULL);
+  }
+  l0 = lo & 0xFFFFFFFFULL;
+  l1 = lo >> 32;
+  l2 = (unsigned long long)(long long)(int)(unsigned)hi;
+}

@@ -240,7 +240,6 @@ __device__ __forceinline__ void eval_pred_tf(const DQuery& q, const TileCtx& t, 
 }
 
 // ------------------------------------------------------------------ keys
-#define PMB_EMPTY64 0xFFFFFFFFFFFFFFFFULL
 
 __device__ __forceinline__ uint64_t pack_key64(const DQuery& q, const TileCtx& t, int64_t lr) {
   uint64_t k = 0;
@@ -303,17 +302,6 @@ __device__ __forceinline__ bool unpack_field(const DKey& K, uint64_t lo, uint64_
 }
 
 // ------------------------------------------------------------------ aggregation state
-// Exact-to-double-double accumulation: atomicAdd returns the old partial sum, so the rounding
-// error of that very addition is recovered with TwoSum (Knuth) and added into the low word.
-__device__ __forceinline__ void dd_atomic_add(double* hi, double* lo, double x) {
-  double old = atomicAdd(hi, x);
-  double s = old + x;
-  if (!isfinite(s)) return;
-  double bp = s - old;
-  double err = (old - (s - bp)) + (x - bp);
-  if (err != 0.0) atomicAdd(lo, err);
-}
-
 // identity value word(s) of a field, written at record init
 __host__ __device__ inline void field_identity(int kind, uint64_t* w0, uint64_t* w1, int* nwords, int* bytes) {
   *w1 = 0;
@@ -321,6 +309,7 @@ __host__ __device__ inline void field_identity(int kind, uint64_t* w0, uint64_t*
   switch (kind) {
     case F_LEN: case F_CNT: *w0 = 0; *bytes = 4; break;
     case F_SUM_DD: *w0 = 0; *nwords = 2; *bytes = 16; break;
+    case F_SUM_FX: *w0 = 0; *nwords = 4; *bytes = 32; break;
     case F_SUM_I: *w0 = 0; *bytes = 8; break;
     case F_MIN_I: case F_MIN_F: *w0 = 0x7FFFFFFFFFFFFFFFULL; *bytes = 8; break;
     case F_MAX_I: case F_MAX_F: *w0 = 0x8000000000000000ULL; *bytes = 8; break;
@@ -337,15 +326,6 @@ __host__ __device__ inline void field_identity(int kind, uint64_t* w0, uint64_t*
 //   apply_row_global  — the global table (native L2 atomics, fire-and-forget where possible:
 //                       adjacent 32-bit counters share one 64-bit add, min/max are issued only
 //                       when the row improves on a possibly stale read).
-__device__ __forceinline__ void dd_plain_add(double* hi, double* lo, double x) {
-  double old = *hi;
-  double s = old + x;
-  *hi = s;
-  if (!isfinite(s)) return;
-  double bp = s - old;
-  *lo += (old - (s - bp)) + (x - bp);
-}
-
 __device__ __forceinline__ long long minmax_key(const DField& F, uint64_t b, int dt, bool is_min) {
   double x = pmb_bits_to_f64(b, dt);
   if (isnan(x)) return is_min ? (long long)0x8000000000000000LL : 0x7FFFFFFFFFFFFFFFLL;
@@ -369,6 +349,20 @@ __device__ __forceinline__ void apply_row_private(const DQuery& q, const TileCtx
     int dt = q.col[F.col].dtype;
     switch (F.kind) {
       case F_SUM_DD: dd_plain_add((double*)p, (double*)(p + 8), pmb_bits_to_f64(b, dt)); break;
+      case F_SUM_FX: {
+        double x = pmb_bits_to_f64(b, dt);
+        unsigned fl = pmb_fx_flag(x);
+        if (fl) {
+          *(unsigned int*)(p + 24) |= fl;
+        } else if (pmb_fx_fits(x, F.fx)) {
+          unsigned long long l0, l1, l2;
+          pmb_fx_split(x, F.fx, l0, l1, l2);
+          ((unsigned long long*)p)[0] += l0;
+          ((unsigned long long*)p)[1] += l1;
+          ((unsigned long long*)p)[2] += l2;
+        }
+        break;
+      }
       case F_SUM_I: *(unsigned long long*)p += (unsigned long long)pmb_bits_to_i64(b, dt); break;
       case F_MIN_I: {
         long long v = (long long)pmb_bits_to_i64(b, dt);
@@ -417,6 +411,20 @@ __device__ __forceinline__ void apply_row_shared(const DQuery& q, const TileCtx&
     int dt = q.col[F.col].dtype;
     switch (F.kind) {
       case F_SUM_DD: dd_atomic_add((double*)p, (double*)(p + 8), pmb_bits_to_f64(b, dt)); break;
+      case F_SUM_FX: {
+        double x = pmb_bits_to_f64(b, dt);
+        unsigned fl = pmb_fx_flag(x);
+        if (fl) {
+          atomicOr((unsigned int*)(p + 24), fl);
+        } else if (pmb_fx_fits(x, F.fx)) {
+          unsigned long long l0, l1, l2;
+          pmb_fx_split(x, F.fx, l0, l1, l2);
+          if (l0) atomicAdd((unsigned long long*)p, l0);
+          if (l1) atomicAdd((unsigned long long*)p + 1, l1);
+          if (l2) atomicAdd((unsigned long long*)p + 2, l2);
+        }
+        break;
+      }
       case F_SUM_I: atomicAdd((unsigned long long*)p, (unsigned long long)pmb_bits_to_i64(b, dt)); break;
       case F_MIN_I: {
         long long v = (long long)pmb_bits_to_i64(b, dt);
@@ -470,6 +478,20 @@ __device__ __forceinline__ void apply_row_global(const DQuery& q, const TileCtx&
     int dt = q.col[F.col].dtype;
     switch (F.kind) {
       case F_SUM_DD: dd_atomic_add((double*)p, (double*)(p + 8), pmb_bits_to_f64(b, dt)); break;
+      case F_SUM_FX: {
+        double x = pmb_bits_to_f64(b, dt);
+        unsigned fl = pmb_fx_flag(x);
+        if (fl) {
+          atomicOr((unsigned int*)(p + 24), fl);
+        } else if (pmb_fx_fits(x, F.fx)) {
+          unsigned long long l0, l1, l2;
+          pmb_fx_split(x, F.fx, l0, l1, l2);
+          if (l0) atomicAdd((unsigned long long*)p, l0);
+          if (l1) atomicAdd((unsigned long long*)p + 1, l1);
+          if (l2) atomicAdd((unsigned long long*)p + 2, l2);
+        }
+        break;
+      }
       case F_SUM_I: atomicAdd((unsigned long long*)p, (unsigned long long)pmb_bits_to_i64(b, dt)); break;
       // a stale read can only be weaker than the stored extreme, so skipping is safe
       case F_MIN_I: {
@@ -522,6 +544,14 @@ __device__ __forceinline__ void merge_record(const DQuery& q, uint8_t* dst, cons
         if (lo != 0.0) atomicAdd((double*)(d + 8), lo);
         break;
       }
+      case F_SUM_FX: {
+        const unsigned long long* l = (const unsigned long long*)s;
+        for (int w = 0; w < 3; w++)
+          if (l[w]) atomicAdd((unsigned long long*)d + w, l[w]);
+        unsigned fl = *(const unsigned int*)(s + 24);
+        if (fl) atomicOr((unsigned int*)(d + 24), fl);
+        break;
+      }
       case F_SUM_I: {
         unsigned long long v = *(const unsigned long long*)s;
         if (v) atomicAdd((unsigned long long*)d, v);
@@ -568,6 +598,12 @@ __device__ __forceinline__ void merge_private(const DQuery& q, uint8_t* dst, con
         *(double*)(d + 8) += lo;
         break;
       }
+      case F_SUM_FX: {
+        const unsigned long long* l = (const unsigned long long*)s;
+        for (int w = 0; w < 3; w++) ((unsigned long long*)d)[w] += l[w];
+        *(unsigned int*)(d + 24) |= *(const unsigned int*)(s + 24);
+        break;
+      }
       case F_SUM_I: *(unsigned long long*)d += *(const unsigned long long*)s; break;
       case F_MIN_I:
       case F_MIN_F: {
@@ -591,6 +627,20 @@ __device__ __forceinline__ void merge_private(const DQuery& q, uint8_t* dst, con
         if (v > *(unsigned long long*)d) *(unsigned long long*)d = v;
         break;
       }
+    }
+  }
+}
+
+// Reports float-sum values outside their column's fixed-point range (the call is then re-run
+// with a wider range); called once per surviving row.
+__device__ __forceinline__ void fx_range_check(const DQuery& q, const TileCtx& t, int64_t lr, unsigned int* status) {
+  for (int i = 0; i < q.n_fields; i++) {
+    const DField F = q.field[i];
+    if (F.kind != F_SUM_FX || !tc_isvalid(q, t, F.col, lr)) continue;
+    double x = pmb_bits_to_f64(tc_bits(q, t, F.col, lr), q.col[F.col].dtype);
+    if (!pmb_fx_flag(x) && !pmb_fx_fits(x, F.fx)) {
+      atomicOr(status, PMB_ST_FXRANGE);
+      atomicMax(&status[4 + F.fx_slot], (unsigned)pmb_fx_expo(x));
     }
   }
 }

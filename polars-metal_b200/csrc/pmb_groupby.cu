@@ -30,19 +30,33 @@
 #include <vector>
 
 #include "pmb_groupby.h"
+#include "pmb_jit.h"
 
 // ============================================================================ sketch
 #define SK_SAMPLES 65536
 #define SK_SLOTS (1 << 18)
 
+struct FxCols {
+  int n;
+  int col[PMB_MAX_FX];
+};
+
 template <bool K128>
 __global__ void k_sketch(const __grid_constant__ DQuery q, int64_t m, unsigned long long* __restrict__ set_keys,
-                         unsigned int* __restrict__ set_cnt) {
+                         unsigned int* __restrict__ set_cnt, const __grid_constant__ FxCols fxc,
+                         unsigned int* __restrict__ fx_expo) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   int64_t row = (m == q.n_rows) ? i : (int64_t)((double)i * (double)q.n_rows / (double)m);
   if (row >= q.n_rows) row = q.n_rows - 1;
   TileCtx t{nullptr, nullptr, nullptr, 0};
+  // largest exponent of the finite values of each float-sum column (fixed-point range)
+  for (int f = 0; f < fxc.n; f++) {
+    int c = fxc.col[f];
+    if (!tc_isvalid(q, t, c, row)) continue;
+    double x = pmb_bits_to_f64(tc_bits(q, t, c, row), q.col[c].dtype);
+    if (!pmb_fx_flag(x)) atomicMax(&fx_expo[f], (unsigned)pmb_fx_expo(x));
+  }
   uint64_t k;
   if (K128) {
     Key128 kk = pack_key128(q, t, row);
@@ -217,6 +231,7 @@ __device__ __forceinline__ int process_rows(const HashParams& P, const DQuery& q
   const bool ks = P.kstats != nullptr;
   long long ck0 = ks ? clock64() : 0;
   bool keep = in_range && eval_keep(q, t, lr);
+  if (keep) fx_range_check(q, t, lr, P.status);
   if (K128) {
     if (!keep) return 0;
     Key128 key = pack_key128(q, t, lr);
@@ -636,6 +651,7 @@ int pmb_groupby_sketch(pmb_handle* h, const CompiledQuery& cq, SketchOut* out) {
   out->samples = m;
   out->distinct = out->singletons = out->doubletons = 0;
   memset(out->hist, 0, sizeof(out->hist));
+  memset(out->fx_expo, 0, sizeof(out->fx_expo));
   out->set_keys = nullptr;
   out->set_cnt = nullptr;
   if (m == 0) return PMB_OK;
@@ -644,12 +660,19 @@ int pmb_groupby_sketch(pmb_handle* h, const CompiledQuery& cq, SketchOut* out) {
   unsigned long long* res = (unsigned long long*)pmb_ws_alloc(h, 64 + 4 * SK_HIST);
   if (!keys || !cnt || !res) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sketch)");
   unsigned int* hist = (unsigned int*)(res + 8);
+  unsigned int* fx_expo = (unsigned int*)(res + 4);  // res[4..7]: 8 x u32
+  FxCols fxc;
+  memset(&fxc, 0, sizeof(fxc));
+  fxc.n = (int)cq.fx_cols.size();
+  for (int f = 0; f < fxc.n; f++) fxc.col[f] = cq.fx_cols[f];
   PMB_CUDA(h, cudaMemsetAsync(keys, 0xFF, sizeof(unsigned long long) * SK_SLOTS, h->stream));
   PMB_CUDA(h, cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * SK_SLOTS, h->stream));
   PMB_CUDA(h, cudaMemsetAsync(res, 0, 64 + 4 * SK_HIST, h->stream));
   pmb_kernel_begin(h, "sketch");
-  if (q.key_bits > 64) k_sketch<true><<<(unsigned)((m + 255) / 256), 256, 0, h->stream>>>(q, m, keys, cnt);
-  else k_sketch<false><<<(unsigned)((m + 255) / 256), 256, 0, h->stream>>>(q, m, keys, cnt);
+  if (q.key_bits > 64)
+    k_sketch<true><<<(unsigned)((m + 255) / 256), 256, 0, h->stream>>>(q, m, keys, cnt, fxc, fx_expo);
+  else
+    k_sketch<false><<<(unsigned)((m + 255) / 256), 256, 0, h->stream>>>(q, m, keys, cnt, fxc, fx_expo);
   pmb_kernel_end(h);
   PMB_CUDA(h, cudaGetLastError());
   pmb_kernel_begin(h, "sketch_reduce");
@@ -662,6 +685,7 @@ int pmb_groupby_sketch(pmb_handle* h, const CompiledQuery& cq, SketchOut* out) {
   out->distinct = (int64_t)r[0];
   out->singletons = (int64_t)r[1];
   out->doubletons = (int64_t)r[2];
+  memcpy(out->fx_expo, h->pinned + 32, 4 * PMB_MAX_FX);
   memcpy(out->hist, h->pinned + 64, 4 * SK_HIST);
   out->set_keys = keys;
   out->set_cnt = cnt;
@@ -689,46 +713,45 @@ static void build_output_columns(const CompiledQuery& cq, pmb_result* r, const p
   (void)cols;
 }
 
-int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
-                     const SketchOut* sk, pmb_result* r) {
+// Shared-memory layout and launch shape of the hash kernel for one query (host-only, no device
+// calls): stage ring, hot-key tier, CTA-shared table. Used by the launch and by the JIT check.
+int pmb_plan_hash(pmb_handle* h, int max_smem_optin, CompiledQuery& cq, int strategy, int64_t est, bool have_sketch,
+                  HashParams& P, int& nt, int& smem) {
   DQuery& q = cq.dq;
   const bool K128 = q.key_bits > 64;
   const int rec = q.rec_bytes;
-  Plan pl;
-  pl.strategy = strategy;
+  int tile = 1024;
   if (const char* e = getenv("PMB_TILE")) {
     int v = atoi(e);
-    if (v >= 256 && v <= 8192 && v % 128 == 0) pl.tile = v;
+    if (v >= 256 && v <= 8192 && v % 128 == 0) tile = v;
   }
-  if (K128 && strategy == PMB_STRATEGY_SMEM_HASH) pl.strategy = PMB_STRATEGY_GLOBAL_HASH;
-  HashParams P;
   memset(&P, 0, sizeof(P));
   P.q = q;
-  P.tile_rows = pl.tile;
-  layout_stage(cq, pl.tile, P);
-  // shared memory budget: mbarriers, stages, table
-  const int budget = h->max_smem_optin - 4096;  // static shared memory (descriptor copy) comes on top
+  P.tile_rows = tile;
+  layout_stage(cq, tile, P);
+  const int budget = max_smem_optin - 4096;  // static shared memory (descriptor copy) comes on top
   int stages = 2;
   if (const char* e = getenv("PMB_STAGES")) stages = std::max(1, std::min(atoi(e), 4));
   while (stages > 1 && 128 + stages * P.stage_bytes > budget / 2) stages--;
   int smem_fixed = 128 + stages * P.stage_bytes;
-  if (smem_fixed > budget) {
+  if (smem_fixed > budget / 2) {
     // very wide queries: smaller tiles
-    pl.tile = 512;
-    P.tile_rows = pl.tile;
-    layout_stage(cq, pl.tile, P);
-    stages = 2;
+    tile = 512;
+    P.tile_rows = tile;
+    layout_stage(cq, tile, P);
+    stages = 1;
     smem_fixed = 128 + stages * P.stage_bytes;
     if (smem_fixed > budget) return pmb_fail(h, PMB_E_UNSUPPORTED, "query touches too many columns for one tile");
   }
-  // hot tier: per-warp private records for the heaviest sample keys
-  int nt = 1024;
+  // hot tier: per-warp private records for the heaviest sample keys (at most 64 KB)
+  nt = 1024;
   if (const char* e = getenv("PMB_NT")) nt = atoi(e);
   if (nt != 256 && nt != 512 && nt != 1024) nt = 1024;
   if (K128) nt = 512;
-  int hot_cap = (K128 || !sk || !sk->set_keys) ? 0 : 32;
+  int hot_cap = (K128 || !have_sketch) ? 0 : 32;
   if (const char* e = getenv("PMB_HOT")) hot_cap = std::max(0, std::min(atoi(e), 128));
-  while (hot_cap > 0 && smem_fixed + (nt / 32) * hot_cap * rec + 16 * 2 * hot_cap > budget / 2) hot_cap /= 2;
+  while (hot_cap > 0 && ((nt / 32) * hot_cap * rec > (64 << 10) || smem_fixed + (nt / 32) * hot_cap * rec > budget))
+    hot_cap /= 2;
   int hot_lut = hot_cap ? (int)next_pow2((uint64_t)(2 * hot_cap)) : 0;
   P.hot_cap = hot_cap;
   P.hot_lut_slots = hot_lut;
@@ -758,7 +781,37 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
   P.stage_region_off = 128;
   P.smem_keys_off = (int)pmb_align((size_t)smem_fixed, 16);
   P.smem_recs_off = P.smem_keys_off + S * 8;
-  int smem = P.smem_recs_off + S * rec;
+  smem = P.smem_recs_off + S * rec;
+  const int64_t n = q.n_rows;
+  P.n_full_tiles = n / tile;
+  P.tail_rows = (int32_t)(n % tile);
+  if (cq.rec_words > (int)(sizeof(P.rec_init.w) / 8)) return pmb_fail(h, PMB_E_UNSUPPORTED, "record too large");
+  for (int w = 0; w < cq.rec_words; w++) P.rec_init.w[w] = cq.rec_init[w];
+  return PMB_OK;
+}
+
+int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
+                     const SketchOut* sk, pmb_result* r) {
+  DQuery& q = cq.dq;
+  const bool K128 = q.key_bits > 64;
+  HashParams P;
+  int nt = 1024, smem = 0;
+  int prc = pmb_plan_hash(h, h->max_smem_optin, cq, strategy, est, sk && sk->set_keys, P, nt, smem);
+  if (prc) return prc;
+  // run-time compiled kernel (warp-independent units) when enabled; its own tier sizes
+  JitPlan J;
+  cudaKernel_t jk = nullptr;
+  if (!K128 && pmb_jit_enabled(q.n_rows) && pmb_plan_jit(h, cq, sk && sk->set_keys, h->max_smem_optin, &J) == PMB_OK) {
+    std::string keep_err = h->err;
+    if (pmb_jit_hash_kernel(h, cq, J, &jk) != PMB_OK) jk = nullptr;  // prebuilt generic kernel: same results
+    h->err = keep_err;
+  }
+  const int hot_cap = jk ? J.hot_cap : P.hot_cap;
+  const int S = jk ? J.S : P.smem_slots;
+  const int rec = q.rec_bytes;
+  Plan pl;
+  pl.strategy = (K128 && strategy == PMB_STRATEGY_SMEM_HASH) ? PMB_STRATEGY_GLOBAL_HASH : strategy;
+  pl.tile = P.tile_rows;
   // hot / warm key lists from the sample histogram
   if (hot_cap || S) {
     if (sk && sk->set_keys) {
@@ -799,10 +852,6 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     P.hot_lut_slots = 0;
   }
   const int64_t n = q.n_rows;
-  P.n_full_tiles = n / pl.tile;
-  P.tail_rows = (int32_t)(n % pl.tile);
-  if (cq.rec_words > (int)(sizeof(P.rec_init.w) / 8)) return pmb_fail(h, PMB_E_UNSUPPORTED, "record too large");
-  for (int w = 0; w < cq.rec_words; w++) P.rec_init.w[w] = cq.rec_init[w];
 
   uint64_t cap = next_pow2((uint64_t)std::max<int64_t>(2 * est, 1024));
   if (uq->capacity_hint > 0) cap = next_pow2((uint64_t)std::max<int64_t>(2 * uq->capacity_hint, 1024));
@@ -815,6 +864,7 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
   cap = std::min(cap, cap_max);
 
   const int n_out = q.n_keys + q.n_aggs;
+  int fx_reruns = 0;
   for (int attempt = 0;; attempt++) {
     const int key_words = K128 ? 2 : 1;
     size_t keys_bytes = (size_t)(cap + 1) * 8 * key_words;
@@ -864,7 +914,8 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     }
     P.kstats = kst;
     int rc;
-    if (K128) rc = launch_hash<512, true>(h, P, smem, grid);
+    if (jk) rc = pmb_jit_launch(h, jk, cq, J, P, h->sm_count);
+    else if (K128) rc = launch_hash<512, true>(h, P, smem, grid);
     else if (nt == 1024) rc = launch_hash<1024, false>(h, P, smem, grid);
     else if (nt == 256) rc = launch_hash<256, false>(h, P, smem, grid);
     else rc = launch_hash<512, false>(h, P, smem, grid);
@@ -897,6 +948,20 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     PMB_CUDA(h, cudaStreamSynchronize(h->stream));
     unsigned int st = *(unsigned int*)h->pinned;
     if (st & PMB_ST_TIMEOUT) return pmb_fail(h, PMB_E_TIMEOUT, "a bounded device wait timed out");
+    if (st & PMB_ST_FXRANGE) {
+      // a float sum left its fixed-point range: widen to the largest exponent seen, run again
+      unsigned expo[PMB_MAX_FX];
+      PMB_CUDA(h, cudaMemcpy(expo, status + 4, sizeof(expo), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < q.n_fields; i++) {
+        DField& f = q.field[i];
+        if (f.kind != F_SUM_FX || expo[f.fx_slot] == 0) continue;
+        int nf = pmb_fx_bits(expo[f.fx_slot], 1);
+        if (nf < f.fx) f.fx = (int16_t)nf;
+        P.q.field[i].fx = f.fx;
+      }
+      if (++fx_reruns > 4) return pmb_fail(h, PMB_E_CUDA, "float-sum range did not converge");
+      continue;
+    }
     if (st & PMB_ST_OVERFLOW) {
       if (cap >= cap_max) return pmb_fail(h, PMB_E_OOM, "hash table overflow at maximum capacity");
       cap = std::min(cap * 4, cap_max);
@@ -949,15 +1014,14 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     int strategy = q->strategy;
     int64_t est = q->capacity_hint;
     static thread_local SketchOut sk;  // large (histogram); one per host thread
-    bool have_sk = false;
-    if (est <= 0 || strategy == PMB_STRATEGY_AUTO) {
-      rc = pmb_groupby_sketch(h, cq, &sk);
-      if (rc) return bail(rc);
-      have_sk = true;
-      int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
-      if (est <= 0) est = e;
-      if (strategy == PMB_STRATEGY_AUTO) strategy = pmb_choose_strategy(h, cq, sk, est);
-    }
+    bool have_sk = true;
+    rc = pmb_groupby_sketch(h, cq, &sk);
+    if (rc) return bail(rc);
+    // fixed-point range of the float sums: sample maximum with 8x headroom
+    pmb_set_fx(cq.dq, sk.fx_expo, 3);
+    int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
+    if (est <= 0) est = e;
+    if (strategy == PMB_STRATEGY_AUTO) strategy = pmb_choose_strategy(h, cq, sk, est);
     if (strategy == PMB_STRATEGY_SORT) strategy = PMB_STRATEGY_GLOBAL_HASH;  // sort path: see pmb_sort.cu
     rc = pmb_groupby_hash(h, cq, q, strategy, est, have_sk ? &sk : nullptr, r);
     if (rc) return bail(rc);

@@ -67,6 +67,7 @@ struct SketchOut {
   int64_t singletons;
   int64_t doubletons;
   unsigned int hist[SK_HIST];  // keys of the sample by occurrence count (last bin: >= SK_HIST - 1)
+  unsigned int fx_expo[PMB_MAX_FX];  // largest biased exponent of each float-sum column in the sample
   // device-resident sample set (valid until the next workspace reset)
   const unsigned long long* set_keys;
   const unsigned int* set_cnt;
@@ -75,6 +76,8 @@ struct SketchOut {
 int pmb_groupby_sketch(pmb_handle* h, const CompiledQuery& cq, SketchOut* out);
 int64_t pmb_estimate_groups(const SketchOut& s, int64_t n_rows);
 int pmb_choose_strategy(pmb_handle* h, const CompiledQuery& cq, const SketchOut& sk, int64_t est);
+int pmb_plan_hash(pmb_handle* h, int max_smem_optin, CompiledQuery& cq, int strategy, int64_t est, bool have_sketch,
+                  HashParams& P, int& nt, int& smem);
 int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
                      const SketchOut* sk, pmb_result* r);
 
@@ -90,6 +93,33 @@ __device__ __forceinline__ void warp_set_bits(unsigned int* words, int64_t p, in
   }
 }
 
+// Correctly rounded double of the exact fixed-point sum (limbs l, fraction bits F, flags).
+__device__ __forceinline__ double fx_value(const unsigned long long* l, int F, unsigned flags) {
+  if ((flags & PMB_FX_NAN) || ((flags & PMB_FX_PINF) && (flags & PMB_FX_NINF)))
+    return __longlong_as_double(0x7FF8000000000000LL);
+  if (flags & PMB_FX_PINF) return __longlong_as_double(0x7FF0000000000000LL);
+  if (flags & PMB_FX_NINF) return __longlong_as_double((long long)0xFFF0000000000000ULL);
+  __int128 S = ((__int128)(long long)l[2] << 64) + ((__int128)l[1] << 32) + (__int128)l[0];
+  bool neg = S < 0;
+  unsigned __int128 M = neg ? (unsigned __int128)(-S) : (unsigned __int128)S;
+  unsigned long long hi = (unsigned long long)(M >> 64), lo = (unsigned long long)M;
+  double v;
+  int sc = 0;
+  if (hi == 0) {
+    v = __ull2double_rn(lo);
+  } else {
+    int lz = __clzll(hi);
+    int sh = 64 - lz;  // bits to drop so that the value fits 64 bits
+    unsigned long long top = lz ? ((hi << lz) | (lo >> sh)) : hi;
+    unsigned long long dropped = sh == 64 ? lo : (lo & ((1ULL << sh) - 1ULL));
+    top |= dropped ? 1ULL : 0ULL;  // sticky bit below the rounding position
+    v = __ull2double_rn(top);
+    sc = sh;
+  }
+  v = ldexp(v, sc - F);
+  return neg ? -v : v;
+}
+
 // Final value of aggregation A from a group record (Polars rules: all-null sum = 0, mean /
 // min / max of no valid value = null, NaN poisons float min / max, ints wrap).
 __device__ __forceinline__ void finalize_agg(const DQuery& q, const DAggOut& A, const uint8_t* rec, bool& valid,
@@ -99,7 +129,12 @@ __device__ __forceinline__ void finalize_agg(const DQuery& q, const DAggOut& A, 
   auto u32 = [&](int f) { return *reinterpret_cast<const unsigned int*>(rec + q.field[f].off); };
   auto u64 = [&](int f) { return *reinterpret_cast<const unsigned long long*>(rec + q.field[f].off); };
   auto ddv = [&](int f) {
-    const double* p = reinterpret_cast<const double*>(rec + q.field[f].off);
+    const DField& F = q.field[f];
+    if (F.kind == F_SUM_FX) {
+      const unsigned long long* l = reinterpret_cast<const unsigned long long*>(rec + F.off);
+      return fx_value(l, F.fx, *reinterpret_cast<const unsigned int*>(rec + F.off + 24));
+    }
+    const double* p = reinterpret_cast<const double*>(rec + F.off);
     return p[0] + p[1];
   };
   const bool fl = pmb_is_float(A.in_dtype);

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/pmb.h"
+#include "pmb_device.cuh"
 
 // ----------------------------------------------------------------------------- limits
 #define PMB_MAX_COLS 16    // distinct columns one query may touch
@@ -17,14 +18,6 @@
 #define PMB_MAX_AGGS 24
 #define PMB_MAX_TERMS 12   // predicate leaf terms
 #define PMB_MAX_OPS 32     // predicate circuit ops
-
-// status bits written by kernels into the call's device status word
-#define PMB_ST_OVERFLOW 1u  // a hash table ran out of probes / capacity: rehash
-#define PMB_ST_TIMEOUT 2u   // a bounded wait gave up
-#define PMB_ST_BADARG 4u    // a device-side argument check failed
-
-// bounded spins: iterations before a wait gives up and reports PMB_ST_TIMEOUT
-#define PMB_SPIN_LIMIT (1u << 24)
 
 // ----------------------------------------------------------------------------- dtype helpers
 __host__ __device__ inline int pmb_dtype_bytes(int dt) {
@@ -121,14 +114,15 @@ enum {
   F_MIN_U = 6,   // u64 min of an unsigned column
   F_MAX_U = 7,
   F_MIN_F = 8,   // ordered-i64 key min of a float column (NaN poisons)
-  F_MAX_F = 9
+  F_MAX_F = 9,
+  F_SUM_FX = 10  // exact fixed-point sum of a float column: 3 x u64 limb sums + u32 non-finite flags
 };
 struct DField {
   int8_t kind;
-  int8_t pad;
+  int8_t fx_slot;  // F_SUM_FX: index of this column's range report in the status words
   int16_t col;
-  int16_t off;  // byte offset inside the group record
-  int16_t pad2;
+  int16_t off;     // byte offset inside the group record
+  int16_t fx;      // F_SUM_FX: fraction bits F (values are summed as integers x * 2^F)
 };
 
 // output column recipe for an aggregation
@@ -225,69 +219,6 @@ int pmb_stage_column(pmb_handle* h, const pmb_column& c, int64_t n_rows, DCol* o
 int pmb_finish_outputs(pmb_handle* h, pmb_result* r, bool to_host);
 
 // ----------------------------------------------------------------------------- device helpers
-__device__ __forceinline__ uint32_t pmb_smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(pmb_smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(pmb_smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-// 1-D bulk copy global -> shared (TMA engine), completion counted on `bar`.
-// dst, src 16-byte aligned; bytes a multiple of 16.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          pmb_smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(pmb_smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(pmb_smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait; returns false on timeout
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (uint32_t it = 0; it < PMB_SPIN_LIMIT; it++)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
-// MurmurHash3 64-bit finalizer (Appleby, public domain)
-__host__ __device__ __forceinline__ uint64_t pmb_fmix64(uint64_t k) {
-  k ^= k >> 33;
-  k *= 0xff51afd7ed558ccdULL;
-  k ^= k >> 33;
-  k *= 0xc4ceb9fe1a85ec53ULL;
-  k ^= k >> 33;
-  return k;
-}
-
-// total-order key of a double: monotone in IEEE order for non-NaN values (-0.0 < +0.0)
-__device__ __forceinline__ long long pmb_f64_key(double x) {
-  long long b = __double_as_longlong(x);
-  return b ^ ((b >> 63) & 0x7FFFFFFFFFFFFFFFLL);
-}
-__device__ __forceinline__ double pmb_f64_from_key(long long k) {
-  long long b = k ^ ((k >> 63) & 0x7FFFFFFFFFFFFFFFLL);
-  return __longlong_as_double(b);
-}
-
 // read the raw bits (zero-extended) of element r of a column chunk
 __device__ __forceinline__ uint64_t pmb_load_bits(const uint8_t* d, int elem, int64_t r) {
   switch (elem) {

@@ -280,10 +280,10 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
     switch (A.op) {
       case PMB_AGG_COUNT: o.f_cnt = (int16_t)cnt; break;
       case PMB_AGG_SUM:
-        o.f_main = (int16_t)field(pmb_is_float(dt) ? F_SUM_DD : F_SUM_I, c);
+        o.f_main = (int16_t)field(pmb_is_float(dt) ? F_SUM_FX : F_SUM_I, c);
         break;
       case PMB_AGG_MEAN:
-        o.f_main = (int16_t)field(pmb_is_float(dt) ? F_SUM_DD : F_SUM_I, c);
+        o.f_main = (int16_t)field(pmb_is_float(dt) ? F_SUM_FX : F_SUM_I, c);
         o.f_cnt = (int16_t)cnt;
         break;
       default: {  // min / max
@@ -302,10 +302,10 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
     }
   }
   if (fields.size() > PMB_MAX_FIELDS) return pmb_fail(h, PMB_E_UNSUPPORTED, "too many aggregation state fields");
-  // record layout: 16-byte fields, then 8-byte, then 4-byte
+  // record layout: 32-byte fields, then 16-, 8- and 4-byte ones
   int rec = 0;
-  for (int pass = 0; pass < 3; pass++) {
-    int want = pass == 0 ? 16 : (pass == 1 ? 8 : 4);
+  for (int pass = 0; pass < 4; pass++) {
+    int want = 32 >> pass;
     for (DField& f : fields) {
       uint64_t w0, w1;
       int nw, bytes;
@@ -316,6 +316,15 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
     }
   }
   rec = (int)pmb_align((size_t)std::max(rec, 8), 8);
+  // exact float sums: one range slot per column (fraction bits are set from the data sample)
+  cq->fx_cols.clear();
+  for (DField& f : fields) {
+    if (f.kind != F_SUM_FX) continue;
+    if (cq->fx_cols.size() >= PMB_MAX_FX) return pmb_fail(h, PMB_E_UNSUPPORTED, "at most 8 float-sum columns");
+    f.fx_slot = (int8_t)cq->fx_cols.size();
+    f.fx = 60;
+    cq->fx_cols.push_back(f.col);
+  }
   d.n_fields = (int)fields.size();
   for (size_t i = 0; i < fields.size(); i++) d.field[i] = fields[i];
   d.rec_bytes = rec;

@@ -26,7 +26,24 @@ SOURCES = [
     "pmb_sort.cu",
     "pmb_batched.cu",
     "pmb_learned.cu",
+    "pmb_jit.cu",
 ]
+
+# device sources compiled at run time by NVRTC, embedded into the library as string literals
+JIT_EMBED = [("kDeviceHeader", "pmb_device.cuh"), ("kSkeleton", "pmb_jit_skeleton.cuh")]
+
+
+def write_jit_sources() -> Path:
+    out = CSRC / "pmb_jit_sources.inc"
+    parts = ["// generated by polars_b200/build.py from the .cuh files it names; do not edit\n"]
+    for name, fname in JIT_EMBED:
+        text = (CSRC / fname).read_text()
+        assert ")PMBSRC" not in text
+        parts.append(f'static const char {name}[] = R"PMBSRC({text})PMBSRC";\n')
+    content = "".join(parts)
+    if not out.exists() or out.read_text() != content:
+        out.write_text(content)
+    return out
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -47,6 +64,7 @@ def _stale(out: Path, deps: list[Path]) -> bool:
 
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
     """Compiles every CUDA source into libpmb.so; a no-op when it is up to date."""
+    write_jit_sources()
     srcs = [CSRC / s for s in SOURCES if (CSRC / s).exists()]
     deps = srcs + sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "pmb.h", Path(__file__)]
     if not force and not _stale(LIB_PATH, deps):
@@ -77,7 +95,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         subprocess.run(cmd, check=True)
         objs.append(o)
     tmp = LIB_PATH.with_suffix(".so.tmp")
-    cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
+    cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart", "-ldl"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
