@@ -134,10 +134,10 @@ __device__ __forceinline__ unsigned pmb_fx_flag(double x) {
   return b < 0 ? PMB_FX_NINF : PMB_FX_PINF;
 }
 
-// true when the finite x fits the range of fraction bits F (|x| < 2^(94 - F))
-__device__ __forceinline__ bool pmb_fx_fits(double x, int F) { return pmb_fx_expo(x) < 94 - F + 1023; }
+// true when the finite x satisfies |x| < 2^E
+__device__ __forceinline__ bool pmb_fx_in_range(double x, int E) { return pmb_fx_expo(x) < E + 1023; }
 
-// limbs of trunc(x * 2^F) for a finite x that fits
+// limbs of trunc(x * 2^F) for a finite x with |x * 2^F| < 2^94
 __device__ __forceinline__ void pmb_fx_split(double x, int F, unsigned long long& l0, unsigned long long& l1,
                                              unsigned long long& l2) {
   long long b = __double_as_longlong(x);

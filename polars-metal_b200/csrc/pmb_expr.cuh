@@ -354,7 +354,7 @@ __device__ __forceinline__ void apply_row_private(const DQuery& q, const TileCtx
         unsigned fl = pmb_fx_flag(x);
         if (fl) {
           *(unsigned int*)(p + 24) |= fl;
-        } else if (pmb_fx_fits(x, F.fx)) {
+        } else if (pmb_fx_in_range(x, q.fx_e[F.fx_slot])) {
           unsigned long long l0, l1, l2;
           pmb_fx_split(x, F.fx, l0, l1, l2);
           ((unsigned long long*)p)[0] += l0;
@@ -416,7 +416,7 @@ __device__ __forceinline__ void apply_row_shared(const DQuery& q, const TileCtx&
         unsigned fl = pmb_fx_flag(x);
         if (fl) {
           atomicOr((unsigned int*)(p + 24), fl);
-        } else if (pmb_fx_fits(x, F.fx)) {
+        } else if (pmb_fx_in_range(x, q.fx_e[F.fx_slot])) {
           unsigned long long l0, l1, l2;
           pmb_fx_split(x, F.fx, l0, l1, l2);
           if (l0) atomicAdd((unsigned long long*)p, l0);
@@ -483,7 +483,7 @@ __device__ __forceinline__ void apply_row_global(const DQuery& q, const TileCtx&
         unsigned fl = pmb_fx_flag(x);
         if (fl) {
           atomicOr((unsigned int*)(p + 24), fl);
-        } else if (pmb_fx_fits(x, F.fx)) {
+        } else if (pmb_fx_in_range(x, q.fx_e[F.fx_slot])) {
           unsigned long long l0, l1, l2;
           pmb_fx_split(x, F.fx, l0, l1, l2);
           if (l0) atomicAdd((unsigned long long*)p, l0);
@@ -638,7 +638,7 @@ __device__ __forceinline__ void fx_range_check(const DQuery& q, const TileCtx& t
     const DField F = q.field[i];
     if (F.kind != F_SUM_FX || !tc_isvalid(q, t, F.col, lr)) continue;
     double x = pmb_bits_to_f64(tc_bits(q, t, F.col, lr), q.col[F.col].dtype);
-    if (!pmb_fx_flag(x) && !pmb_fx_fits(x, F.fx)) {
+    if (!pmb_fx_flag(x) && !pmb_fx_in_range(x, q.fx_e[F.fx_slot])) {
       atomicOr(status, PMB_ST_FXRANGE);
       atomicMax(&status[4 + F.fx_slot], (unsigned)pmb_fx_expo(x));
     }

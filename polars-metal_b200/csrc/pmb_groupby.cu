@@ -920,7 +920,15 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     else if (nt == 256) rc = launch_hash<256, false>(h, P, smem, grid);
     else rc = launch_hash<512, false>(h, P, smem, grid);
     if (rc) return rc;
-    if (kst) {
+    if (kst && jk) {
+      unsigned long long hk[16];
+      PMB_CUDA(h, cudaMemcpyAsync(hk, kst, 128, cudaMemcpyDeviceToHost, h->stream));
+      PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+      double warps = (double)(hk[7] ? hk[7] : 1);
+      fprintf(stderr, "jit kstats: nt=%d hot=%d S=%d buf=%d smem=%d | per warp (Mcycles): wait %.2f filter+hot %.2f warm %.2f "
+              "cold %.2f | rows hot %llu warm %llu cold %llu\n", J.nt, J.hot_cap, J.S, J.buf_bytes, J.smem,
+              hk[0] / warps / 1e6, hk[1] / warps / 1e6, hk[2] / warps / 1e6, hk[3] / warps / 1e6, hk[4], hk[5], hk[6]);
+    } else if (kst) {
       unsigned long long hk[16];
       PMB_CUDA(h, cudaMemcpyAsync(hk, kst, 128, cudaMemcpyDeviceToHost, h->stream));
       PMB_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -955,9 +963,13 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
       for (int i = 0; i < q.n_fields; i++) {
         DField& f = q.field[i];
         if (f.kind != F_SUM_FX || expo[f.fx_slot] == 0) continue;
-        int nf = pmb_fx_bits(expo[f.fx_slot], 1);
-        if (nf < f.fx) f.fx = (int16_t)nf;
+        int e = (int)expo[f.fx_slot] - 1022 + 1;  // the value seen fits with one spare power of two
+        if (e > q.fx_e[f.fx_slot]) {
+          f.fx = (int16_t)(f.fx - (e - q.fx_e[f.fx_slot]));
+          q.fx_e[f.fx_slot] = (int16_t)e;
+        }
         P.q.field[i].fx = f.fx;
+        P.q.fx_e[f.fx_slot] = q.fx_e[f.fx_slot];
       }
       if (++fx_reruns > 4) return pmb_fail(h, PMB_E_CUDA, "float-sum range did not converge");
       continue;
@@ -1017,8 +1029,11 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     bool have_sk = true;
     rc = pmb_groupby_sketch(h, cq, &sk);
     if (rc) return bail(rc);
-    // fixed-point range of the float sums: sample maximum with 8x headroom
-    pmb_set_fx(cq.dq, sk.fx_expo, 3);
+    // fixed-point range of the float sums: sample maximum with 8x headroom; partial sums of a
+    // CTA (at most n / SMs values, with margin) must fit as well
+    int pbits = 2;
+    while ((1LL << pbits) < cq.dq.n_rows / h->sm_count + 1) pbits++;
+    pmb_set_fx(cq.dq, sk.fx_expo, 3, pbits + 1);
     int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
     if (est <= 0) est = e;
     if (strategy == PMB_STRATEGY_AUTO) strategy = pmb_choose_strategy(h, cq, sk, est);

@@ -145,6 +145,7 @@ struct DQuery {
   int32_t key_bits;  // total packed key width
   int32_t rec_bytes; // bytes per group record
   int64_t n_rows;
+  int16_t fx_e[8];   // exact float sums: every value of slot i satisfies |x| < 2^fx_e[i]
   DCol col[PMB_MAX_COLS];
   DKey key[PMB_MAX_KEYS];
   DField field[PMB_MAX_FIELDS];

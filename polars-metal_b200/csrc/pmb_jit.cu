@@ -159,28 +159,18 @@ struct Gen {
       if (need_val[c]) o << "  " << ctype(q.col[c].dtype) << " v" << c << ";\n";
       if (need_valid[c] && q.col[c].valid) o << "  bool ok" << c << ";\n";
     }
-    for (int i = 0; i < q.n_fields; i++)
-      if (q.field[i].kind == F_SUM_FX)
-        o << "  unsigned long long fa" << i << ", fb" << i << ", fc" << i << ";\n  unsigned ff" << i << ";\n";
     o << "};\n";
   }
 
-  // float sums: split each value into fixed-point limbs once per row; `check` reports values
-  // outside the column's range (the call is re-run with a wider range)
-  void fx_loads(std::ostringstream& b, bool check) {
+  // exact float sums: report values outside the slot's range (the call is then re-run wider)
+  void fx_check(std::ostringstream& b) {
     for (int i = 0; i < q.n_fields; i++) {
       const DField& F = q.field[i];
       if (F.kind != F_SUM_FX) continue;
-      std::string s = std::to_string(i), slot = std::to_string(F.fx_slot);
-      b << "  r.fa" << s << " = r.fb" << s << " = r.fc" << s << " = 0ULL; r.ff" << s << " = 0u;\n";
-      b << "  if (" << ok(F.col) << ") {\n    double xv = (double)" << v(F.col) << ";\n    unsigned fl = pmb_fx_flag(xv);\n";
-      b << "    r.ff" << s << " = fl;\n";
-      b << "    if (!fl && pmb_fx_fits(xv, P.fx[" << slot << "])) pmb_fx_split(xv, P.fx[" << slot << "], r.fa" << s
-        << ", r.fb" << s << ", r.fc" << s << ");\n";
-      if (check)
-        b << "    else if (!fl && check) { atomicOr(P.status, PMB_ST_FXRANGE); atomicMax(&P.status[4 + " << slot
-          << "], (unsigned)pmb_fx_expo(xv)); }\n";
-      b << "  }\n";
+      std::string slot = std::to_string(F.fx_slot);
+      b << "  if (check && " << ok(F.col) << ") {\n    double xv = (double)" << v(F.col) << ";\n";
+      b << "    if (!pmb_fx_flag(xv) && !pmb_fx_in_range(xv, P.fx_e[" << slot << "])) { atomicOr(P.status, PMB_ST_FXRANGE); "
+        << "atomicMax(&P.status[4 + " << slot << "], (unsigned)pmb_fx_expo(xv)); }\n  }\n";
     }
   }
 
@@ -349,16 +339,20 @@ struct Gen {
         continue;
       }
       if (F.kind == F_SUM_FX) {
-        std::string i_ = std::to_string(i);
-        const char* lim[3] = {"fa", "fb", "fc"};
-        for (int w = 0; w < 3; w++) {
-          std::string ptr = "reinterpret_cast<unsigned long long*>(rec + " + std::to_string(F.off + 8 * w) + ")";
-          if (mode == 0) b << "  *" << ptr << " += r." << lim[w] << i_ << ";\n";
-          else b << "  if (r." << lim[w] << i_ << ") atomicAdd(" << ptr << ", r." << lim[w] << i_ << ");\n";
+        std::string hi = at(F.off, "double"), lo = at(F.off + 8, "double"), slot = std::to_string(F.fx_slot);
+        b << "  if (" << okc << ") {\n    double xv = (double)" << v(F.col) << ";\n";
+        if (mode == 0) b << "    dd_plain_add(" << hi << ", " << lo << ", xv);\n";
+        else if (mode == 1) b << "    dd_atomic_add(" << hi << ", " << lo << ", xv);\n";
+        else {
+          b << "    unsigned fl = pmb_fx_flag(xv);\n";
+          b << "    if (fl) atomicOr(" << at(F.off + 24, "unsigned int") << ", fl);\n";
+          b << "    else if (pmb_fx_in_range(xv, P.fx_e[" << slot << "])) {\n      unsigned long long a, b_, c;\n";
+          b << "      pmb_fx_split(xv, P.fx[" << slot << "], a, b_, c);\n";
+          b << "      if (a) atomicAdd(" << at(F.off, "unsigned long long") << ", a);\n";
+          b << "      if (b_) atomicAdd(" << at(F.off + 8, "unsigned long long") << ", b_);\n";
+          b << "      if (c) atomicAdd(" << at(F.off + 16, "unsigned long long") << ", c);\n    }\n";
         }
-        std::string fp = "reinterpret_cast<unsigned int*>(rec + " + std::to_string(F.off + 24) + ")";
-        if (mode == 0) b << "  *" << fp << " |= r.ff" << i_ << ";\n";
-        else b << "  if (r.ff" << i_ << ") atomicOr(" << fp << ", r.ff" << i_ << ");\n";
+        b << "  }\n";
         continue;
       }
       std::string x = fval(F);
@@ -412,23 +406,27 @@ struct Gen {
             b << "    dd_plain_add(reinterpret_cast<double*>(d + " << d << "), reinterpret_cast<double*>(d + " << F.off + 8 << "), hi);\n"
               << "    *reinterpret_cast<double*>(d + " << F.off + 8 << ") += lo; }\n";
           break;
-        case F_SUM_FX:
-          for (int w = 0; w < 3; w++) {
-            std::string dw = std::to_string(F.off + 8 * w);
-            if (global)
-              b << "  { unsigned long long x = *reinterpret_cast<const unsigned long long*>(s + " << dw
-                << "); if (x) atomicAdd(reinterpret_cast<unsigned long long*>(d + " << dw << "), x); }\n";
-            else
-              b << "  *reinterpret_cast<unsigned long long*>(d + " << dw << ") += *reinterpret_cast<const unsigned long long*>(s + "
-                << dw << ");\n";
+        case F_SUM_FX: {
+          std::string hs = std::to_string(F.off), ls = std::to_string(F.off + 8), slot = std::to_string(F.fx_slot);
+          b << "  { double hi = *reinterpret_cast<const double*>(s + " << hs << "), lo = *reinterpret_cast<const double*>(s + "
+            << ls << ");\n";
+          if (!global) {
+            b << "    dd_plain_add(reinterpret_cast<double*>(d + " << hs << "), reinterpret_cast<double*>(d + " << ls
+              << "), hi);\n    *reinterpret_cast<double*>(d + " << ls << ") += lo; }\n";
+          } else {
+            // a double-double partial of at most 2^(94 - F - E) values splits exactly into limbs
+            b << "    unsigned fl = pmb_fx_flag(hi);\n";
+            b << "    if (fl) atomicOr(reinterpret_cast<unsigned int*>(d + " << F.off + 24 << "), fl);\n";
+            b << "    else {\n      double parts[2] = {hi, lo};\n      for (int t = 0; t < 2; t++) {\n";
+            b << "        if (parts[t] == 0.0 || !isfinite(parts[t])) continue;\n        unsigned long long a, b_, c;\n";
+            b << "        pmb_fx_split(parts[t], P.fx[" << slot << "], a, b_, c);\n";
+            b << "        if (a) atomicAdd(reinterpret_cast<unsigned long long*>(d + " << F.off << "), a);\n";
+            b << "        if (b_) atomicAdd(reinterpret_cast<unsigned long long*>(d + " << F.off + 8 << "), b_);\n";
+            b << "        if (c) atomicAdd(reinterpret_cast<unsigned long long*>(d + " << F.off + 16 << "), c);\n";
+            b << "      }\n    }\n  }\n";
           }
-          if (global)
-            b << "  { unsigned x = *reinterpret_cast<const unsigned*>(s + " << F.off + 24
-              << "); if (x) atomicOr(reinterpret_cast<unsigned*>(d + " << F.off + 24 << "), x); }\n";
-          else
-            b << "  *reinterpret_cast<unsigned*>(d + " << F.off + 24 << ") |= *reinterpret_cast<const unsigned*>(s + "
-              << F.off + 24 << ");\n";
           break;
+        }
         case F_SUM_I:
           if (global) b << "  { unsigned long long x = *reinterpret_cast<const unsigned long long*>(s + " << d << "); if (x) atomicAdd(reinterpret_cast<unsigned long long*>(d + " << d << "), x); }\n";
           else b << "  *reinterpret_cast<unsigned long long*>(d + " << d << ") += *reinterpret_cast<const unsigned long long*>(s + " << d << ");\n";
@@ -519,12 +517,10 @@ __device__ __forceinline__ long long j_fdiv_i(long long a, long long b, bool& ok
     loads(o, false);
     o << body.str() << "  bool keep = " << keep << ";\n";
     o << "  if (keep) {\n";
-    fx_loads(o, true);
+    fx_check(o);
     o << "  }\n  return keep;\n}\n";
     o << "__device__ __forceinline__ void j_load_vals(const JParams& P, const unsigned char* st, int lr, JRow& r) {\n";
-    o << "  const bool check = false;\n";
     loads(o, true);
-    fx_loads(o, false);
     o << "}\n";
     // key
     o << "__device__ __forceinline__ unsigned long long j_key(const JRow& r) {\n  unsigned long long k = 0ULL;\n";
@@ -541,13 +537,13 @@ __device__ __forceinline__ long long j_fdiv_i(long long a, long long b, bool& ok
     // record updates
     const char* names[] = {"j_private", "j_shared", "j_global"};
     for (int m = 0; m < 3; m++) {
-      o << "__device__ __forceinline__ void " << names[m] << "(unsigned char* rec, const JRow& r) {\n";
+      o << "__device__ __forceinline__ void " << names[m] << "(const JParams& P, unsigned char* rec, const JRow& r) {\n";
       apply(o, m);
       o << "}\n";
     }
     o << "__device__ __forceinline__ void j_merge_private(unsigned char* d, const unsigned char* s) {\n";
     merge(o, false);
-    o << "}\n__device__ __forceinline__ void j_merge_global(unsigned char* d, const unsigned char* s) {\n";
+    o << "}\n__device__ __forceinline__ void j_merge_global(const JParams& P, unsigned char* d, const unsigned char* s) {\n";
     merge(o, true);
     o << "}\n";
     return o.str();
@@ -742,7 +738,10 @@ int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const
   A.warm_n = P.warm_n;
   A.kstats = P.kstats;
   for (int i = 0; i < cq.dq.n_fields; i++)
-    if (cq.dq.field[i].kind == F_SUM_FX) A.fx[cq.dq.field[i].fx_slot] = cq.dq.field[i].fx;
+    if (cq.dq.field[i].kind == F_SUM_FX) {
+      A.fx[cq.dq.field[i].fx_slot] = cq.dq.field[i].fx;
+      A.fx_e[cq.dq.field[i].fx_slot] = cq.dq.fx_e[cq.dq.field[i].fx_slot];
+    }
   PMB_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, J.smem));
   void* args[] = {&A};
   pmb_kernel_begin(h, "hash_agg");

@@ -21,6 +21,7 @@ struct JitParams {
   const unsigned int* warm_n;
   unsigned long long* kstats;
   int fx[8];
+  int fx_e[8];
 };
 
 // shared-memory layout of the run-time kernel (per-warp 128-row unit buffers, hot and warm tiers)

@@ -3,12 +3,14 @@
 // defines, for that signature, the J_* constants and the row functions:
 //   j_issue_unit   one warp's bulk copies (TMA, cp.async.bulk) of a 128-row unit into its buffer
 //   j_copy_unit    plain copy of a partial last unit
-//   JRow, j_load   the values of one row of the buffer, the filter verdict, float sums split into
-//                  fixed-point limbs (with the range report when `check`)
+//   JRow, j_load   the values of one row of the buffer and the filter verdict (with the range
+//                  report of exact float sums when `check`)
 //   j_load_vals    the aggregated values only
 //   j_key          the packed 64-bit group key
 //   j_private / j_shared / j_global      one row into a warp-private / CTA-shared / global record
-//   j_merge_private / j_merge_global     a finished record into another
+//                  (float sums: double-double in the private and shared tiers, fixed-point limbs in
+//                  the global table)
+//   j_merge_private / j_merge_global     a finished private / shared record into another / the table
 //   J_IDENT        the identity record (u64 words)
 //
 // Execution: persistent CTAs, every warp independent (no CTA barrier in the main loop). A warp
@@ -39,7 +41,8 @@ struct JParams {
   const unsigned long long* warm_keys;
   const unsigned int* warm_n;
   unsigned long long* kstats;
-  int fx[8];  // fraction bits of each exact float-sum slot
+  int fx[8];    // fraction bits F of each exact float-sum slot (global limbs hold x * 2^F)
+  int fx_e[8];  // every value of the slot satisfies |x| < 2^fx_e
 };
 
 #define J_UNIT 128
@@ -150,9 +153,14 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
   const long long gw = (long long)blockIdx.x * W + warp, n_warps = (long long)gridDim.x * W;
   unsigned phase = 0;
   bool aborted = false;
+  // optional phase counters (P.kstats): cycles in copy wait / filter+hot / warm / cold, rows per tier
+  const bool ks = P.kstats != nullptr;
+  long long c_wait = 0, c_p1 = 0, c_p2 = 0, c_p3 = 0, c0 = 0;
+  unsigned n_hot_rows = 0, n_warm_rows = 0, n_cold_rows = 0;
   for (long long u = gw; u < P.n_units; u += n_warps) {
     const long long row0 = u * J_UNIT;
     const int rows = (int)min((long long)J_UNIT, P.n_rows - row0);
+    if (ks) c0 = clock64();
     if (rows == J_UNIT) {
       if (lane == 0) {
         fence_proxy_async();  // the warp's reads of the previous unit come before the copy's writes
@@ -172,6 +180,11 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
       j_copy_unit(P, buf, row0, rows);
     }
     __syncwarp();
+    if (ks) {
+      long long c1 = clock64();
+      c_wait += c1 - c0;
+      c0 = c1;
+    }
 
     // 1. filter, key, hot tier; remember cold rows for the batched probe
     unsigned long long ck[4], ch[4];
@@ -192,15 +205,16 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
           unsigned peers = __match_any_sync(0xffffffffu, hot) & hm;
           if (hot >= 0 && lane == __ffs(peers) - 1) {
             unsigned char* rec = my_hot + hot * J_REC;
-            j_private(rec, r);
+            j_private(P, rec, r);
             for (unsigned m = peers & (peers - 1); m; m &= m - 1) {
               JRow rp;
               j_load_vals(P, buf, (__ffs(m) - 1) + 32 * j, rp);
-              j_private(rec, rp);
+              j_private(P, rec, rp);
             }
           }
         }
       }
+      if (ks && hot >= 0) n_hot_rows++;
       ck[j] = key;
       ch[j] = h;
       wslot[j] = -1;
@@ -214,14 +228,26 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
         }
       }
     }
+    if (ks) {
+      long long c1 = clock64();
+      c_p1 += c1 - c0;
+      c0 = c1;
+      n_warm_rows += __popc(warm);
+      n_cold_rows += __popc(cold);
+    }
     // 2. warm rows
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       if (warm & (1u << j)) {
         JRow r;
         j_load_vals(P, buf, lane + 32 * j, r);
-        j_shared(srecs + wslot[j] * J_REC, r);
+        j_shared(P, srecs + wslot[j] * J_REC, r);
       }
+    }
+    if (ks) {
+      long long c1 = clock64();
+      c_p2 += c1 - c0;
+      c0 = c1;
     }
     // 3. cold rows: probe loads first, then resolve and apply
     unsigned long long first[4];
@@ -235,11 +261,32 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
         if (gi >= 0) {
           JRow r;
           j_load_vals(P, buf, lane + 32 * j, r);
-          j_global(P.grecs + (unsigned long long)gi * J_REC, r);
+          j_global(P, P.grecs + (unsigned long long)gi * J_REC, r);
         }
       }
     }
     __syncwarp();
+    if (ks) c_p3 += clock64() - c0;
+  }
+  if (ks) {
+    if (lane == 0) {
+      atomicAdd(&P.kstats[0], (unsigned long long)c_wait);
+      atomicAdd(&P.kstats[1], (unsigned long long)c_p1);
+      atomicAdd(&P.kstats[2], (unsigned long long)c_p2);
+      atomicAdd(&P.kstats[3], (unsigned long long)c_p3);
+    }
+    unsigned a = n_hot_rows, b = n_warm_rows, c = n_cold_rows;
+    for (int o = 16; o; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&P.kstats[4], (unsigned long long)a);
+      atomicAdd(&P.kstats[5], (unsigned long long)b);
+      atomicAdd(&P.kstats[6], (unsigned long long)c);
+      atomicAdd(&P.kstats[7], 1ULL);
+    }
   }
   if (aborted && lane == 0) atomicOr(P.status, PMB_ST_TIMEOUT);
   __syncthreads();
@@ -250,7 +297,7 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
     if (*reinterpret_cast<const unsigned int*>(r0 + J_LEN_OFF) == 0) continue;
     unsigned long long key = P.hot_keys[i];
     long long gi = j_gfind(P, key, pmb_fmix64(key));
-    if (gi >= 0) j_merge_global(P.grecs + (unsigned long long)gi * J_REC, r0);
+    if (gi >= 0) j_merge_global(P, P.grecs + (unsigned long long)gi * J_REC, r0);
   }
   // the warm table (preloaded keys may have seen no rows)
   for (int i = tid; i < J_S; i += J_NT) {
@@ -259,6 +306,6 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
     const unsigned char* r = srecs + i * J_REC;
     if (*reinterpret_cast<const unsigned int*>(r + J_LEN_OFF) == 0) continue;
     long long gi = j_gfind(P, key, pmb_fmix64(key));
-    if (gi >= 0) j_merge_global(P.grecs + (unsigned long long)gi * J_REC, r);
+    if (gi >= 0) j_merge_global(P, P.grecs + (unsigned long long)gi * J_REC, r);
   }
 }

@@ -23,16 +23,18 @@ struct CompiledQuery {
   std::vector<int> fx_cols;        // compact column of each exact float-sum slot
 };
 
-// fraction bits of the fixed-point float sums: |x| < 2^(94 - F); `max_expo` is the largest
-// biased exponent seen, `headroom` extra powers of two on top
-inline int pmb_fx_bits(unsigned max_expo, int headroom) {
-  int e = (int)max_expo - 1022 + headroom;  // |x| < 2^e
-  return 94 - e;
-}
-// set every float-sum field's fraction bits from per-slot exponents
-inline void pmb_set_fx(DQuery& q, const unsigned* max_expo, int headroom) {
-  for (int i = 0; i < q.n_fields; i++)
-    if (q.field[i].kind == F_SUM_FX) q.field[i].fx = (int16_t)pmb_fx_bits(max_expo[q.field[i].fx_slot], headroom);
+// Fixed-point range of the exact float sums. Every value of a slot satisfies |x| < 2^E, E taken
+// from the largest biased exponent seen plus `headroom` powers of two; partial sums of up to
+// 2^partial_bits values must still split into limbs, so the fraction bits are
+// F = 94 - E - partial_bits (|x * 2^F| < 2^94).
+inline void pmb_set_fx(DQuery& q, const unsigned* max_expo, int headroom, int partial_bits) {
+  for (int i = 0; i < q.n_fields; i++) {
+    DField& f = q.field[i];
+    if (f.kind != F_SUM_FX) continue;
+    int e = (int)max_expo[f.fx_slot] - 1022 + headroom;
+    q.fx_e[f.fx_slot] = (int16_t)e;
+    f.fx = (int16_t)(94 - e - partial_bits);
+  }
 }
 
 int pmb_compile_predicate(pmb_handle* h, const pmb_expr* e, ColMap* map, const pmb_column* cols,
