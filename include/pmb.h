@@ -239,6 +239,19 @@ int pmb_filter_compact_expr(pmb_handle* h, const pmb_expr* predicate, const pmb_
 int pmb_cumsum_u8_to_u32(pmb_handle* h, const uint8_t* in, uint32_t* out, int64_t n,
                          int32_t on_device);
 
+/* The same prefix sum for callers that must not allocate device memory (a host framework that
+ * already reserved the device's memory for its own pool, or a latency-critical loop in which
+ * cudaMalloc/cudaFree would synchronise the device). No counterpart in the reference.
+ * `in` and `out` are device pointers of n elements on the current device; `cuda_stream` may be
+ * NULL. The call allocates nothing: its scratch is a fixed array of about 256 KB that every GPU
+ * loading this library holds until the process exits, so n may be at most PMB_NOALLOC_MAX_ROWS
+ * (larger n returns PMB_E_INVALID without touching the GPU). The first call on a device looks up
+ * that array's device address, so make it before capturing work on that device. All calls share
+ * the array: calls that overlap on the GPU (other streams or host threads) race. The call waits
+ * for its stream before returning. Returns PMB_OK, PMB_E_INVALID, PMB_E_TIMEOUT or PMB_E_CUDA. */
+#define PMB_NOALLOC_MAX_ROWS (1LL << 27)
+int pmb_cumsum_u8_to_u32_noalloc(const uint8_t* in, uint32_t* out, int64_t n, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -176,7 +176,11 @@ SIGNATURES = {
     "pmb_filter_compact_expr": (C.c_int, [_H, C.POINTER(Expr), C.POINTER(Column), C.c_int32, C.c_int32,
                                           C.POINTER(C.POINTER(Result))]),
     "pmb_cumsum_u8_to_u32": (C.c_int, [_H, _P, _P, C.c_int64, C.c_int32]),
+    "pmb_cumsum_u8_to_u32_noalloc": (C.c_int, [_P, _P, C.c_int64, _P]),
 }
+
+# largest n of pmb_cumsum_u8_to_u32_noalloc (its fixed scratch array)
+NOALLOC_MAX_ROWS = 1 << 27
 
 _LIB: C.CDLL | None = None
 

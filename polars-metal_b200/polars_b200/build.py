@@ -27,6 +27,7 @@ SOURCES = [
     "pmb_batched.cu",
     "pmb_learned.cu",
     "pmb_jit.cu",
+    "pmb_noalloc.cu",
 ]
 
 # device sources compiled at run time by NVRTC, embedded into the library as string literals
