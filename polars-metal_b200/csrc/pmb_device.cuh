@@ -53,6 +53,22 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       "l"(src), "r"(bytes), "r"(pmb_smem_u32(bar))
       : "memory");
 }
+// L2 eviction policy for inputs that are read once: evict them first, so that the hash tables the
+// same kernel updates stay resident in L2
+__device__ __forceinline__ uint64_t pmb_policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// bulk_g2s with an L2 cache policy
+__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                                              uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          pmb_smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(pmb_smem_u32(bar)), "l"(policy)
+      : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -77,6 +93,52 @@ __host__ __device__ __forceinline__ uint64_t pmb_fmix64(uint64_t k) {
   k *= 0xc4ceb9fe1a85ec53ULL;
   k ^= k >> 33;
   return k;
+}
+
+// slot of hash h in a table of `cap` slots, any cap: the high word of h * cap (Lemire's
+// multiply-shift range reduction), so capacities need not be powers of two
+__device__ __forceinline__ uint64_t pmb_slot(uint64_t h, uint64_t cap) { return __umul64hi(h, cap); }
+
+// Two's complement accumulators of 32-bit words in shared memory, updated with native 32-bit
+// atomics (64-bit adds on shared memory are compare-and-swap loops on this GPU). The thread whose
+// addition wraps a word adds the carry into the next word, so the words always hold the exact
+// total modulo 2^96 (2^64) once all additions are done, in any interleaving.
+__device__ __forceinline__ void pmb_s_add96(unsigned* w, unsigned l0, unsigned l1, unsigned l2) {
+  unsigned c = 0;
+  if (l0) {
+    unsigned o = atomicAdd(&w[0], l0);
+    c = (o + l0) < o;
+  }
+  unsigned t1 = l1 + c;
+  unsigned c1 = t1 < c;  // l1 = 0xFFFFFFFF with an incoming carry
+  if (t1) {
+    unsigned o = atomicAdd(&w[1], t1);
+    c1 |= (o + t1) < o;
+  }
+  unsigned t2 = l2 + c1;
+  if (t2) atomicAdd(&w[2], t2);
+}
+__device__ __forceinline__ void pmb_s_add64(unsigned* w, unsigned lo, unsigned hi) {
+  unsigned c = 0;
+  if (lo) {
+    unsigned o = atomicAdd(&w[0], lo);
+    c = (o + lo) < o;
+  }
+  unsigned t = hi + c;
+  if (t) atomicAdd(&w[1], t);
+}
+// d += s for accumulators owned by one thread
+__device__ __forceinline__ void pmb_s_fold96(unsigned* d, const unsigned* s) {
+  unsigned long long a = (unsigned long long)d[0] + s[0];
+  unsigned long long b = (unsigned long long)d[1] + s[1] + (a >> 32);
+  d[0] = (unsigned)a;
+  d[1] = (unsigned)b;
+  d[2] = d[2] + s[2] + (unsigned)(b >> 32);
+}
+__device__ __forceinline__ void pmb_s_fold64(unsigned* d, const unsigned* s) {
+  unsigned long long a = (unsigned long long)d[0] + s[0];
+  d[0] = (unsigned)a;
+  d[1] = d[1] + s[1] + (unsigned)(a >> 32);
 }
 
 // total-order key of a double: monotone in IEEE order for non-NaN values (-0.0 < +0.0)

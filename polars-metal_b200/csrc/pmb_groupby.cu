@@ -142,7 +142,7 @@ __device__ __forceinline__ int64_t gfind64(const HashParams& P, uint64_t key, ui
     if (*(volatile unsigned int*)&P.status[1] == 0) atomicOr(&P.status[1], 1u);
     return (int64_t)P.gcap;
   }
-  uint64_t mask = P.gcap - 1, i = h & mask;
+  uint64_t i = pmb_slot(h, P.gcap);
   unsigned long long* keys = P.gkeys;
   for (int p = 0; p < P.gprobe; p++) {
     unsigned long long k = keys[i];
@@ -151,7 +151,7 @@ __device__ __forceinline__ int64_t gfind64(const HashParams& P, uint64_t key, ui
       unsigned long long old = atomicCAS(&keys[i], PMB_EMPTY64, key);
       if (old == PMB_EMPTY64 || old == key) return (int64_t)i;
     }
-    i = (i + 1) & mask;
+    i = (i + 1 == P.gcap) ? 0 : i + 1;
   }
   atomicOr(P.status, PMB_ST_OVERFLOW);
   return -1;
@@ -166,7 +166,7 @@ __device__ __forceinline__ int64_t gfind128(const HashParams& P, Key128 key, uin
     if (*(volatile unsigned int*)&P.status[1] == 0) atomicOr(&P.status[1], 1u);
     return (int64_t)P.gcap;
   }
-  uint64_t mask = P.gcap - 1, i = h & mask;
+  uint64_t i = pmb_slot(h, P.gcap);
   K128Slot* keys = reinterpret_cast<K128Slot*>(P.gkeys);
   for (int p = 0; p < P.gprobe; p++) {
     K128Slot cur = keys[i];
@@ -178,7 +178,7 @@ __device__ __forceinline__ int64_t gfind128(const HashParams& P, Key128 key, uin
       if ((old.lo == PMB_EMPTY64 && old.hi == PMB_EMPTY64) || (old.lo == key.lo && old.hi == key.hi))
         return (int64_t)i;
     }
-    i = (i + 1) & mask;
+    i = (i + 1 == P.gcap) ? 0 : i + 1;
   }
   atomicOr(P.status, PMB_ST_OVERFLOW);
   return -1;
@@ -807,7 +807,7 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     h->err = keep_err;
   }
   const int hot_cap = jk ? J.hot_cap : P.hot_cap;
-  const int S = jk ? J.S : P.smem_slots;
+  const int S = jk ? 2 * J.warm_cap : P.smem_slots;
   const int rec = q.rec_bytes;
   Plan pl;
   pl.strategy = (K128 && strategy == PMB_STRATEGY_SMEM_HASH) ? PMB_STRATEGY_GLOBAL_HASH : strategy;
@@ -853,15 +853,18 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
   }
   const int64_t n = q.n_rows;
 
-  uint64_t cap = next_pow2((uint64_t)std::max<int64_t>(2 * est, 1024));
-  if (uq->capacity_hint > 0) cap = next_pow2((uint64_t)std::max<int64_t>(2 * uq->capacity_hint, 1024));
-  const uint64_t cap_max = next_pow2((uint64_t)std::max<int64_t>(2 * n, 1024));
+  // Capacity: 4 slots per estimated group (any size: slots come from a multiply-shift, not a
+  // mask; sample estimates of skewed keys run low), 2 per group of a caller's hint. A table that
+  // fills up is rebuilt 3x larger; the estimate only sets how often that happens, never the result.
+  uint64_t cap = (uint64_t)std::max<int64_t>(4 * est, 1024);
+  if (uq->capacity_hint > 0) cap = (uint64_t)std::max<int64_t>(2 * uq->capacity_hint, 1024);
+  const uint64_t cap_max = (uint64_t)std::max<int64_t>(2 * n, 1024);
   // tuning override: PMB_GCAP_MULT=<k> multiplies the global table capacity
   if (const char* e = getenv("PMB_GCAP_MULT")) {
-    int k = atoi(e);
-    if (k > 1) cap = next_pow2(cap * (uint64_t)k);
+    double k = atof(e);
+    if (k > 0) cap = (uint64_t)std::max(1024.0, (double)cap * k);
   }
-  cap = std::min(cap, cap_max);
+  cap = (std::min(cap, cap_max) + 3) & ~3ULL;  // whole 4-slot buckets
 
   const int n_out = q.n_keys + q.n_aggs;
   int fx_reruns = 0;
@@ -903,7 +906,7 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     P.gkeys = gkeys;
     P.grecs = grecs;
     P.gcap = cap;
-    P.gprobe = (int)std::min<uint64_t>(cap, 1u << 14);
+    P.gprobe = (int)std::min<uint64_t>(cap, 1024);
     P.status = status;
     int grid = (int)std::max<int64_t>(1, std::min<int64_t>(P.n_full_tiles, (int64_t)h->sm_count));
     unsigned long long* kst = nullptr;
@@ -925,9 +928,10 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
       PMB_CUDA(h, cudaMemcpyAsync(hk, kst, 128, cudaMemcpyDeviceToHost, h->stream));
       PMB_CUDA(h, cudaStreamSynchronize(h->stream));
       double warps = (double)(hk[7] ? hk[7] : 1);
-      fprintf(stderr, "jit kstats: nt=%d hot=%d S=%d buf=%d smem=%d | per warp (Mcycles): wait %.2f filter+hot %.2f warm %.2f "
-              "cold %.2f | rows hot %llu warm %llu cold %llu\n", J.nt, J.hot_cap, J.S, J.buf_bytes, J.smem,
-              hk[0] / warps / 1e6, hk[1] / warps / 1e6, hk[2] / warps / 1e6, hk[3] / warps / 1e6, hk[4], hk[5], hk[6]);
+      fprintf(stderr, "jit kstats: nt=%d nbuf=%d hot=%d warm=%d T=%d srec=%d smem=%d cap=%llu | per warp (Mcycles): wait %.2f "
+              "classify %.2f shared %.2f cold %.2f | rows shared %llu cold %llu\n", J.nt, J.nbuf, J.hot_cap, J.warm_cap, J.T,
+              J.srec, J.smem, (unsigned long long)cap, hk[0] / warps / 1e6, hk[1] / warps / 1e6, hk[2] / warps / 1e6,
+              hk[3] / warps / 1e6, hk[4], hk[5]);
     } else if (kst) {
       unsigned long long hk[16];
       PMB_CUDA(h, cudaMemcpyAsync(hk, kst, 128, cudaMemcpyDeviceToHost, h->stream));
@@ -976,7 +980,7 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     }
     if (st & PMB_ST_OVERFLOW) {
       if (cap >= cap_max) return pmb_fail(h, PMB_E_OOM, "hash table overflow at maximum capacity");
-      cap = std::min(cap * 4, cap_max);
+      cap = (std::min(cap * 3, cap_max) + 3) & ~3ULL;
       r->rehash_count++;
       continue;
     }

@@ -105,10 +105,14 @@ struct Gen {
   const DQuery& q;
   const JitPlan& P;
   std::ostringstream o;
-  std::vector<bool> need_val, need_bits, need_valid, field_col;
+  std::vector<bool> need_val, need_bits, need_valid, field_col, pred_col, key_col;
+  JitSLayout S;
   int tmp = 0;
 
   Gen(const DQuery& q_, const JitPlan& p_) : q(q_), P(p_) {
+    pmb_jit_slayout(q, &S);
+    pred_col.assign(q.n_cols, false);
+    key_col.assign(q.n_cols, false);
     need_val.assign(q.n_cols, false);
     need_bits.assign(q.n_cols, false);
     need_valid.assign(q.n_cols, false);
@@ -119,7 +123,7 @@ struct Gen {
   std::string ok(int c) { return q.col[c].valid ? "r.ok" + std::to_string(c) : std::string("true"); }
 
   void mark_leaf(const DLeaf& L) {
-    if (L.col >= 0) need_val[L.col] = need_valid[L.col] = true;
+    if (L.col >= 0) need_val[L.col] = need_valid[L.col] = pred_col[L.col] = true;
   }
   void mark() {
     for (int i = 0; i < q.prog.n_terms; i++) {
@@ -132,7 +136,7 @@ struct Gen {
       }
     }
     for (int k = 0; k < q.n_keys; k++) {
-      need_bits[q.key[k].col] = need_valid[q.key[k].col] = true;
+      need_bits[q.key[k].col] = need_valid[q.key[k].col] = key_col[q.key[k].col] = true;
       need_val[q.key[k].col] = true;
     }
     for (int f = 0; f < q.n_fields; f++) {
@@ -160,18 +164,6 @@ struct Gen {
       if (need_valid[c] && q.col[c].valid) o << "  bool ok" << c << ";\n";
     }
     o << "};\n";
-  }
-
-  // exact float sums: report values outside the slot's range (the call is then re-run wider)
-  void fx_check(std::ostringstream& b) {
-    for (int i = 0; i < q.n_fields; i++) {
-      const DField& F = q.field[i];
-      if (F.kind != F_SUM_FX) continue;
-      std::string slot = std::to_string(F.fx_slot);
-      b << "  if (check && " << ok(F.col) << ") {\n    double xv = (double)" << v(F.col) << ";\n";
-      b << "    if (!pmb_fx_flag(xv) && !pmb_fx_in_range(xv, P.fx_e[" << slot << "])) { atomicOr(P.status, PMB_ST_FXRANGE); "
-        << "atomicMax(&P.status[4 + " << slot << "], (unsigned)pmb_fx_expo(xv)); }\n  }\n";
-    }
   }
 
   // leaf value in compare dtype dt: returns (value expr, valid expr)
@@ -273,14 +265,6 @@ struct Gen {
     return stack.back().first;
   }
 
-  void loads(std::ostringstream& b, bool fields_only) {
-    for (int c = 0; c < q.n_cols; c++) {
-      if (fields_only ? !field_col[c] : !need_val[c]) continue;
-      b << "  r.v" << c << " = " << load_val(c) << ";\n";
-      if (q.col[c].valid) b << "  r.ok" << c << " = " << load_valid(c) << ";\n";
-    }
-  }
-
   std::string raw_bits(int c) {
     switch (q.col[c].dtype) {
       case PMB_BOOL: return "(unsigned long long)(" + v(c) + " ? 1u : 0u)";
@@ -315,70 +299,48 @@ struct Gen {
 
   std::string at(int off, const char* T) { return "reinterpret_cast<" + std::string(T) + "*>(rec + " + std::to_string(off) + ")"; }
 
-  void apply(std::ostringstream& b, int mode) {  // 0 private, 1 shared, 2 global
-    // global: pack 32-bit counters sharing a 64-bit word into one add
+  // ---- global-table record (layout of the plan: u64 words, shared with the prebuilt kernels)
+  void apply_global(std::ostringstream& b) {
+    // pack 32-bit counters sharing a 64-bit word into one add
     std::vector<std::pair<int, std::string>> words;  // (word offset, increment expression)
     for (int i = 0; i < q.n_fields; i++) {
       const DField& F = q.field[i];
       std::string okc = F.kind == F_LEN ? std::string("true") : ok(F.col);
       if (F.kind == F_LEN || F.kind == F_CNT) {
         std::string inc = F.kind == F_LEN ? "1ULL" : "(" + okc + " ? 1ULL : 0ULL)";
-        if (mode == 0) b << "  *" << at(F.off, "unsigned int") << " += (unsigned int)" << inc << ";\n";
-        else if (mode == 1) b << "  if (" << inc << ") atomicAdd(" << at(F.off, "unsigned int") << ", 1u);\n";
-        else {
-          int w = F.off & ~7;
-          std::string sh = (F.off & 4) ? " << 32" : "";
-          bool found = false;
-          for (auto& p : words)
-            if (p.first == w) {
-              p.second += " + (" + inc + sh + ")";
-              found = true;
-            }
-          if (!found) words.push_back({w, "(" + inc + sh + ")"});
-        }
+        int w = F.off & ~7;
+        std::string sh = (F.off & 4) ? " << 32" : "";
+        bool found = false;
+        for (auto& p : words)
+          if (p.first == w) {
+            p.second += " + (" + inc + sh + ")";
+            found = true;
+          }
+        if (!found) words.push_back({w, "(" + inc + sh + ")"});
         continue;
       }
-      if (F.kind == F_SUM_FX) {
-        std::string hi = at(F.off, "double"), lo = at(F.off + 8, "double"), slot = std::to_string(F.fx_slot);
-        b << "  if (" << okc << ") {\n    double xv = (double)" << v(F.col) << ";\n";
-        if (mode == 0) b << "    dd_plain_add(" << hi << ", " << lo << ", xv);\n";
-        else if (mode == 1) b << "    dd_atomic_add(" << hi << ", " << lo << ", xv);\n";
-        else {
-          b << "    unsigned fl = pmb_fx_flag(xv);\n";
+      b << "  if (" << okc << ") {\n";
+      switch (F.kind) {
+        case F_SUM_FX: {
+          std::string slot = std::to_string(F.fx_slot);
+          b << "    double xv = (double)" << v(F.col) << ";\n    unsigned fl = pmb_fx_flag(xv);\n";
           b << "    if (fl) atomicOr(" << at(F.off + 24, "unsigned int") << ", fl);\n";
           b << "    else if (pmb_fx_in_range(xv, P.fx_e[" << slot << "])) {\n      unsigned long long a, b_, c;\n";
           b << "      pmb_fx_split(xv, P.fx[" << slot << "], a, b_, c);\n";
           b << "      if (a) atomicAdd(" << at(F.off, "unsigned long long") << ", a);\n";
           b << "      if (b_) atomicAdd(" << at(F.off + 8, "unsigned long long") << ", b_);\n";
           b << "      if (c) atomicAdd(" << at(F.off + 16, "unsigned long long") << ", c);\n    }\n";
+          break;
         }
-        b << "  }\n";
-        continue;
-      }
-      std::string x = fval(F);
-      b << "  if (" << okc << ") {\n";
-      switch (F.kind) {
         case F_SUM_DD:
-          if (mode == 0) b << "    dd_plain_add(" << at(F.off, "double") << ", " << at(F.off + 8, "double") << ", " << x << ");\n";
-          else b << "    dd_atomic_add(" << at(F.off, "double") << ", " << at(F.off + 8, "double") << ", " << x << ");\n";
+          b << "    dd_atomic_add(" << at(F.off, "double") << ", " << at(F.off + 8, "double") << ", " << fval(F) << ");\n";
           break;
-        case F_SUM_I:
-          if (mode == 0) b << "    *" << at(F.off, "unsigned long long") << " += " << x << ";\n";
-          else b << "    atomicAdd(" << at(F.off, "unsigned long long") << ", " << x << ");\n";
-          break;
+        case F_SUM_I: b << "    atomicAdd(" << at(F.off, "unsigned long long") << ", " << fval(F) << ");\n"; break;
         default: {
           bool mn = F.kind == F_MIN_I || F.kind == F_MIN_U || F.kind == F_MIN_F;
           const char* T = (F.kind == F_MIN_U || F.kind == F_MAX_U) ? "unsigned long long" : "long long";
-          const char* cmp = mn ? "<" : ">";
-          b << "    " << T << " val = " << x << ";\n";
-          if (mode == 0) {
-            b << "    if (val " << cmp << " *" << at(F.off, T) << ") *" << at(F.off, T) << " = val;\n";
-          } else {
-            std::string rd = mode == 1 ? "*reinterpret_cast<volatile " + std::string(T) + "*>(rec + " + std::to_string(F.off) + ")"
-                                       : "*" + at(F.off, T);
-            b << "    if (val " << cmp << " " << rd << ") " << (mn ? "atomicMin(" : "atomicMax(") << at(F.off, T)
-              << ", val);\n";
-          }
+          // no read first: cold keys rarely skip an update, and a fire-and-forget atomic does not wait
+          b << "    " << (mn ? "atomicMin(" : "atomicMax(") << at(F.off, T) << ", (" << T << ")(" << fval(F) << "));\n";
         }
       }
       b << "  }\n";
@@ -387,49 +349,111 @@ struct Gen {
       b << "  atomicAdd(reinterpret_cast<unsigned long long*>(rec + " << p.first << "), " << p.second << ");\n";
   }
 
-  void merge(std::ostringstream& b, bool global) {
+  // ---- shared-memory record: native 32-bit atomics and 64-bit min/max only
+  void apply_shared(std::ostringstream& b) {
     for (int i = 0; i < q.n_fields; i++) {
       const DField& F = q.field[i];
-      std::string d = std::to_string(F.off);
+      const int so = S.off[i];
+      if (F.kind == F_LEN) {
+        b << "  atomicAdd(" << at(so, "unsigned int") << ", 1u);\n";
+        continue;
+      }
+      b << "  if (" << ok(F.col) << ") {\n";
       switch (F.kind) {
-        case F_LEN:
-        case F_CNT:
-          if (global) b << "  { unsigned int x = *reinterpret_cast<const unsigned int*>(s + " << d << "); if (x) atomicAdd(reinterpret_cast<unsigned int*>(d + " << d << "), x); }\n";
-          else b << "  *reinterpret_cast<unsigned int*>(d + " << d << ") += *reinterpret_cast<const unsigned int*>(s + " << d << ");\n";
-          break;
-        case F_SUM_DD:
-          b << "  { double hi = *reinterpret_cast<const double*>(s + " << d << "), lo = *reinterpret_cast<const double*>(s + " << F.off + 8 << ");\n";
-          if (global)
-            b << "    if (hi != 0.0) dd_atomic_add(reinterpret_cast<double*>(d + " << d << "), reinterpret_cast<double*>(d + " << F.off + 8 << "), hi);\n"
-              << "    if (lo != 0.0) atomicAdd(reinterpret_cast<double*>(d + " << F.off + 8 << "), lo); }\n";
-          else
-            b << "    dd_plain_add(reinterpret_cast<double*>(d + " << d << "), reinterpret_cast<double*>(d + " << F.off + 8 << "), hi);\n"
-              << "    *reinterpret_cast<double*>(d + " << F.off + 8 << ") += lo; }\n";
-          break;
+        case F_CNT: b << "    atomicAdd(" << at(so, "unsigned int") << ", 1u);\n"; break;
         case F_SUM_FX: {
-          std::string hs = std::to_string(F.off), ls = std::to_string(F.off + 8), slot = std::to_string(F.fx_slot);
-          b << "  { double hi = *reinterpret_cast<const double*>(s + " << hs << "), lo = *reinterpret_cast<const double*>(s + "
-            << ls << ");\n";
-          if (!global) {
-            b << "    dd_plain_add(reinterpret_cast<double*>(d + " << hs << "), reinterpret_cast<double*>(d + " << ls
-              << "), hi);\n    *reinterpret_cast<double*>(d + " << ls << ") += lo; }\n";
-          } else {
-            // a double-double partial of at most 2^(94 - F - E) values splits exactly into limbs
-            b << "    unsigned fl = pmb_fx_flag(hi);\n";
-            b << "    if (fl) atomicOr(reinterpret_cast<unsigned int*>(d + " << F.off + 24 << "), fl);\n";
-            b << "    else {\n      double parts[2] = {hi, lo};\n      for (int t = 0; t < 2; t++) {\n";
-            b << "        if (parts[t] == 0.0 || !isfinite(parts[t])) continue;\n        unsigned long long a, b_, c;\n";
-            b << "        pmb_fx_split(parts[t], P.fx[" << slot << "], a, b_, c);\n";
-            b << "        if (a) atomicAdd(reinterpret_cast<unsigned long long*>(d + " << F.off << "), a);\n";
-            b << "        if (b_) atomicAdd(reinterpret_cast<unsigned long long*>(d + " << F.off + 8 << "), b_);\n";
-            b << "        if (c) atomicAdd(reinterpret_cast<unsigned long long*>(d + " << F.off + 16 << "), c);\n";
-            b << "      }\n    }\n  }\n";
-          }
+          std::string slot = std::to_string(F.fx_slot);
+          b << "    double xv = (double)" << v(F.col) << ";\n    unsigned fl = pmb_fx_flag(xv);\n";
+          b << "    if (fl) { if ((*reinterpret_cast<volatile unsigned int*>(rec + " << so + 12 << ") & fl) != fl) atomicOr("
+            << at(so + 12, "unsigned int") << ", fl); }\n";
+          b << "    else if (pmb_fx_in_range(xv, P.fx_e[" << slot << "])) {\n      unsigned long long a, b_, c;\n";
+          b << "      pmb_fx_split(xv, P.fx[" << slot << "], a, b_, c);\n";
+          b << "      pmb_s_add96(" << at(so, "unsigned int") << ", (unsigned)a, (unsigned)b_, (unsigned)c);\n    }\n";
           break;
         }
         case F_SUM_I:
-          if (global) b << "  { unsigned long long x = *reinterpret_cast<const unsigned long long*>(s + " << d << "); if (x) atomicAdd(reinterpret_cast<unsigned long long*>(d + " << d << "), x); }\n";
-          else b << "  *reinterpret_cast<unsigned long long*>(d + " << d << ") += *reinterpret_cast<const unsigned long long*>(s + " << d << ");\n";
+          b << "    unsigned long long x = " << fval(F) << ";\n    pmb_s_add64(" << at(so, "unsigned int")
+            << ", (unsigned)x, (unsigned)(x >> 32));\n";
+          break;
+        case F_SUM_DD:
+          b << "    dd_atomic_add(" << at(so, "double") << ", " << at(so + 8, "double") << ", " << fval(F) << ");\n";
+          break;
+        default: {
+          bool mn = F.kind == F_MIN_I || F.kind == F_MIN_U || F.kind == F_MIN_F;
+          const char* T = (F.kind == F_MIN_U || F.kind == F_MAX_U) ? "unsigned long long" : "long long";
+          b << "    " << T << " val = " << fval(F) << ";\n";
+          b << "    if (val " << (mn ? "<" : ">") << " *reinterpret_cast<volatile " << T << "*>(rec + " << so << ")) "
+            << (mn ? "atomicMin(" : "atomicMax(") << at(so, T) << ", val);\n";
+        }
+      }
+      b << "  }\n";
+    }
+  }
+
+  // d += s for shared-memory records with one owner
+  void sfold(std::ostringstream& b) {
+    for (int i = 0; i < q.n_fields; i++) {
+      const DField& F = q.field[i];
+      std::string d = std::to_string(S.off[i]);
+      auto U = [&](int off) { return "reinterpret_cast<unsigned int*>(d + " + std::to_string(off) + ")"; };
+      auto CU = [&](int off) { return "reinterpret_cast<const unsigned int*>(s + " + std::to_string(off) + ")"; };
+      switch (F.kind) {
+        case F_LEN:
+        case F_CNT: b << "  *" << U(S.off[i]) << " += *" << CU(S.off[i]) << ";\n"; break;
+        case F_SUM_FX:
+          b << "  pmb_s_fold96(" << U(S.off[i]) << ", " << CU(S.off[i]) << ");\n";
+          b << "  *" << U(S.off[i] + 12) << " |= *" << CU(S.off[i] + 12) << ";\n";
+          break;
+        case F_SUM_I: b << "  pmb_s_fold64(" << U(S.off[i]) << ", " << CU(S.off[i]) << ");\n"; break;
+        case F_SUM_DD:
+          b << "  dd_plain_add(reinterpret_cast<double*>(d + " << d << "), reinterpret_cast<double*>(d + " << S.off[i] + 8
+            << "), *reinterpret_cast<const double*>(s + " << d << "));\n";
+          b << "  *reinterpret_cast<double*>(d + " << S.off[i] + 8 << ") += *reinterpret_cast<const double*>(s + "
+            << S.off[i] + 8 << ");\n";
+          break;
+        default: {
+          bool mn = F.kind == F_MIN_I || F.kind == F_MIN_U || F.kind == F_MIN_F;
+          const char* T = (F.kind == F_MIN_U || F.kind == F_MAX_U) ? "unsigned long long" : "long long";
+          b << "  { " << T << " x = *reinterpret_cast<const " << T << "*>(s + " << d << ");\n";
+          b << "    if (x " << (mn ? "<" : ">") << " *reinterpret_cast<" << T << "*>(d + " << d << ")) *reinterpret_cast<"
+            << T << "*>(d + " << d << ") = x; }\n";
+        }
+      }
+    }
+  }
+
+  // shared-memory record s into global-table record d
+  void merge_sg(std::ostringstream& b) {
+    for (int i = 0; i < q.n_fields; i++) {
+      const DField& F = q.field[i];
+      const int so = S.off[i];
+      std::string gd = std::to_string(F.off);
+      auto CU = [&](int off) { return "*reinterpret_cast<const unsigned int*>(s + " + std::to_string(off) + ")"; };
+      auto GU64 = [&](int off) { return "reinterpret_cast<unsigned long long*>(d + " + std::to_string(off) + ")"; };
+      switch (F.kind) {
+        case F_LEN:
+        case F_CNT:
+          b << "  { unsigned int x = " << CU(so) << "; if (x) atomicAdd(reinterpret_cast<unsigned int*>(d + " << gd
+            << "), x); }\n";
+          break;
+        case F_SUM_FX:
+          b << "  { unsigned fl = " << CU(so + 12) << "; if (fl) atomicOr(reinterpret_cast<unsigned int*>(d + "
+            << F.off + 24 << "), fl);\n";
+          b << "    unsigned w0 = " << CU(so) << ", w1 = " << CU(so + 4) << ", w2 = " << CU(so + 8) << ";\n";
+          b << "    if (w0) atomicAdd(" << GU64(F.off) << ", (unsigned long long)w0);\n";
+          b << "    if (w1) atomicAdd(" << GU64(F.off + 8) << ", (unsigned long long)w1);\n";
+          b << "    if (w2) atomicAdd(" << GU64(F.off + 16) << ", (unsigned long long)(long long)(int)w2); }\n";
+          break;
+        case F_SUM_I:
+          b << "  { unsigned long long x = ((unsigned long long)" << CU(so + 4) << " << 32) | " << CU(so)
+            << "; if (x) atomicAdd(" << GU64(F.off) << ", x); }\n";
+          break;
+        case F_SUM_DD:
+          b << "  { double hi = *reinterpret_cast<const double*>(s + " << so << "), lo = *reinterpret_cast<const double*>(s + "
+            << so + 8 << ");\n";
+          b << "    if (hi != 0.0) dd_atomic_add(reinterpret_cast<double*>(d + " << gd << "), reinterpret_cast<double*>(d + "
+            << F.off + 8 << "), hi);\n";
+          b << "    if (lo != 0.0) atomicAdd(reinterpret_cast<double*>(d + " << F.off + 8 << "), lo); }\n";
           break;
         default: {
           bool mn = F.kind == F_MIN_I || F.kind == F_MIN_U || F.kind == F_MIN_F;
@@ -437,26 +461,51 @@ struct Gen {
           const char* T = uns ? "unsigned long long" : "long long";
           std::string ident = uns ? (mn ? "0xFFFFFFFFFFFFFFFFULL" : "0ULL")
                                   : (mn ? "0x7FFFFFFFFFFFFFFFLL" : "(long long)0x8000000000000000ULL");
-          b << "  { " << T << " x = *reinterpret_cast<const " << T << "*>(s + " << d << ");\n";
-          if (global)
-            b << "    if (x != " << ident << ") " << (mn ? "atomicMin" : "atomicMax") << "(reinterpret_cast<" << T << "*>(d + " << d << "), x); }\n";
-          else
-            b << "    if (x " << (mn ? "<" : ">") << " *reinterpret_cast<" << T << "*>(d + " << d << ")) *reinterpret_cast<" << T << "*>(d + " << d << ") = x; }\n";
+          b << "  { " << T << " x = *reinterpret_cast<const " << T << "*>(s + " << so << ");\n";
+          b << "    if (x != " << ident << ") " << (mn ? "atomicMin" : "atomicMax") << "(reinterpret_cast<" << T
+            << "*>(d + " << gd << "), x); }\n";
         }
       }
     }
   }
 
-  std::string build(const std::vector<uint64_t>& ident) {
+  // range report of the exact float sums: status bit and the largest exponent seen
+  void fxcheck(std::ostringstream& b) {
+    for (int i = 0; i < q.n_fields; i++) {
+      const DField& F = q.field[i];
+      if (F.kind != F_SUM_FX) continue;
+      std::string slot = std::to_string(F.fx_slot);
+      b << "  if (" << ok(F.col) << ") {\n    double xv = (double)" << v(F.col) << ";\n";
+      b << "    if (!pmb_fx_flag(xv) && !pmb_fx_in_range(xv, P.fx_e[" << slot << "])) {\n";
+      b << "      unsigned ex = (unsigned)pmb_fx_expo(xv);\n";
+      b << "      if (ex > *(volatile unsigned int*)&P.status[4 + " << slot << "]) atomicMax(&P.status[4 + " << slot
+        << "], ex);\n";
+      b << "      if (!(*(volatile unsigned int*)P.status & PMB_ST_FXRANGE)) atomicOr(P.status, PMB_ST_FXRANGE);\n    }\n  }\n";
+    }
+  }
+
+  void loads_of(std::ostringstream& b, const std::vector<bool>& want) {
+    for (int c = 0; c < q.n_cols; c++) {
+      if (!want[c]) continue;
+      b << "  r.v" << c << " = " << load_val(c) << ";\n";
+      if (q.col[c].valid) b << "  r.ok" << c << " = " << load_valid(c) << ";\n";
+    }
+  }
+
+  std::string build() {
     mark();
-    o << "#define J_NT " << P.nt << "\n#define J_OFF_BUF " << P.off_buf << "\n#define J_BUF_BYTES " << P.buf_bytes
-      << "\n#define J_OFF_SKEYS " << P.off_skeys << "\n#define J_OFF_SRECS " << P.off_srecs << "\n#define J_S " << P.S
-      << "\n#define J_HOT_CAP " << P.hot_cap << "\n#define J_HOT_LUT " << std::max(P.hot_lut, 1)
-      << "\n#define J_OFF_HOT_LUT " << P.off_hot_lut << "\n#define J_OFF_HOT_RECS " << P.off_hot_recs
-      << "\n#define J_REC " << q.rec_bytes << "\n#define J_REC_WORDS " << q.rec_bytes / 8 << "\n#define J_LEN_OFF "
-      << q.field[0].off << "\n";
-    o << "__constant__ unsigned long long J_IDENT[" << ident.size() << "] = {";
-    for (size_t i = 0; i < ident.size(); i++) o << (i ? ", " : "") << ident[i] << "ULL";
+    // columns of the predicate and keys (classification) and of the keys alone
+    std::vector<bool> pk(q.n_cols, false), kc(q.n_cols, false);
+    for (int c = 0; c < q.n_cols; c++) pk[c] = pred_col[c] || key_col[c];
+    for (int k = 0; k < q.n_keys; k++) kc[q.key[k].col] = true;
+    o << "#define J_NT " << P.nt << "\n#define J_NBUF " << P.nbuf << "\n#define J_OFF_BARS " << P.off_bars
+      << "\n#define J_OFF_BUF " << P.off_buf << "\n#define J_BUF_BYTES " << P.buf_bytes << "\n#define J_OFF_Q " << P.off_q
+      << "\n#define J_OFF_TKEYS " << P.off_tkeys << "\n#define J_OFF_TVAL " << P.off_tval << "\n#define J_T " << P.T
+      << "\n#define J_OFF_SRECS " << P.off_srecs << "\n#define J_H " << P.hot_cap << "\n#define J_SW " << P.warm_cap
+      << "\n#define J_SREC " << S.bytes << "\n#define J_SREC_WORDS " << S.bytes / 4 << "\n#define J_LEN_SOFF " << S.off[0]
+      << "\n#define J_REC " << q.rec_bytes << "\n";
+    o << "__constant__ unsigned int J_SIDENT[" << S.ident.size() << "] = {";
+    for (size_t i = 0; i < S.ident.size(); i++) o << (i ? ", " : "") << S.ident[i] << "u";
     o << "};\n";
     o << R"(
 __device__ __forceinline__ long long j_minkey(double x) {
@@ -484,14 +533,16 @@ __device__ __forceinline__ long long j_fdiv_i(long long a, long long b, bool& ok
 }
 )";
     row_struct();
-    // bulk copies of one 128-row unit into a warp's buffer
-    o << "__device__ __forceinline__ void j_issue_unit(const JParams& P, unsigned char* st, long long u, unsigned long long* bar) {\n";
+    // bulk copies of one 128-row unit into a warp buffer (inputs are read once: evict-first in L2)
+    o << "__device__ __forceinline__ void j_issue_unit(const JParams& P, unsigned char* st, long long u, "
+         "unsigned long long* bar, unsigned long long pol) {\n";
     o << "  mbar_arrive_expect_tx(bar, " << P.tx_bytes << "u);\n";
     for (int c = 0; c < q.n_cols; c++) {
       const DCol& C = q.col[c];
       int db = C.elem ? 128 * C.elem : 16;
-      o << "  bulk_g2s(st + " << P.doff[c] << ", P.col_data[" << c << "] + u * " << db << "LL, " << db << "u, bar);\n";
-      if (C.valid) o << "  bulk_g2s(st + " << P.voff[c] << ", P.col_valid[" << c << "] + u * 16LL, 16u, bar);\n";
+      o << "  bulk_g2s_hint(st + " << P.doff[c] << ", P.col_data[" << c << "] + u * " << db << "LL, " << db
+        << "u, bar, pol);\n";
+      if (C.valid) o << "  bulk_g2s_hint(st + " << P.voff[c] << ", P.col_valid[" << c << "] + u * 16LL, 16u, bar, pol);\n";
     }
     o << "}\n";
     // plain copy of the partial last unit (lanes of one warp)
@@ -510,17 +561,20 @@ __device__ __forceinline__ long long j_fdiv_i(long long a, long long b, bool& ok
           << "][row0 / 8 + i];\n";
     }
     o << "}\n";
-    // row loads + predicate
+    // predicate + key columns and the filter verdict
     std::ostringstream body;
     std::string keep = predicate(body);
-    o << "__device__ __forceinline__ bool j_load(const JParams& P, const unsigned char* st, int lr, JRow& r, bool check) {\n";
-    loads(o, false);
-    o << body.str() << "  bool keep = " << keep << ";\n";
-    o << "  if (keep) {\n";
-    fx_check(o);
-    o << "  }\n  return keep;\n}\n";
+    o << "__device__ __forceinline__ bool j_load_pk(const JParams& P, const unsigned char* st, int lr, JRow& r) {\n";
+    loads_of(o, pk);
+    o << body.str() << "  return " << keep << ";\n}\n";
+    o << "__device__ __forceinline__ void j_load_key(const JParams& P, const unsigned char* st, int lr, JRow& r) {\n";
+    loads_of(o, kc);
+    o << "}\n";
     o << "__device__ __forceinline__ void j_load_vals(const JParams& P, const unsigned char* st, int lr, JRow& r) {\n";
-    loads(o, true);
+    loads_of(o, field_col);
+    o << "}\n";
+    o << "__device__ __forceinline__ void j_fxcheck(const JParams& P, const JRow& r) {\n";
+    fxcheck(o);
     o << "}\n";
     // key
     o << "__device__ __forceinline__ unsigned long long j_key(const JRow& r) {\n  unsigned long long k = 0ULL;\n";
@@ -534,23 +588,58 @@ __device__ __forceinline__ long long j_fdiv_i(long long a, long long b, bool& ok
         o << "  " << put << "\n";
     }
     o << "  return k;\n}\n";
-    // record updates
-    const char* names[] = {"j_private", "j_shared", "j_global"};
-    for (int m = 0; m < 3; m++) {
-      o << "__device__ __forceinline__ void " << names[m] << "(const JParams& P, unsigned char* rec, const JRow& r) {\n";
-      apply(o, m);
-      o << "}\n";
-    }
-    o << "__device__ __forceinline__ void j_merge_private(unsigned char* d, const unsigned char* s) {\n";
-    merge(o, false);
-    o << "}\n__device__ __forceinline__ void j_merge_global(const JParams& P, unsigned char* d, const unsigned char* s) {\n";
-    merge(o, true);
+    // hash of a packed key: MurmurHash3's 32-bit finalizer for keys of at most 32 bits (its word
+    // repeated, so that the high and the low bits both vary), the 64-bit finalizer otherwise
+    if (q.key_bits <= 32)
+      o << "__device__ __forceinline__ unsigned long long j_hash(unsigned long long k) {\n"
+           "  unsigned x = (unsigned)k;\n  x ^= x >> 16;\n  x *= 0x85ebca6bu;\n  x ^= x >> 13;\n  x *= 0xc2b2ae35u;\n"
+           "  x ^= x >> 16;\n  return ((unsigned long long)x << 32) | x;\n}\n";
+    else
+      o << "__device__ __forceinline__ unsigned long long j_hash(unsigned long long k) { return pmb_fmix64(k); }\n";
+    o << "__device__ __forceinline__ void j_shared(const JParams& P, unsigned char* rec, const JRow& r) {\n";
+    apply_shared(o);
+    o << "}\n__device__ __forceinline__ void j_global(const JParams& P, unsigned char* rec, const JRow& r) {\n";
+    apply_global(o);
+    o << "}\n__device__ __forceinline__ void j_sfold(unsigned char* d, const unsigned char* s) {\n";
+    sfold(o);
+    o << "}\n__device__ __forceinline__ void j_merge_sg(const JParams& P, unsigned char* d, const unsigned char* s) {\n";
+    merge_sg(o);
     o << "}\n";
     return o.str();
   }
 };
 
 }  // namespace
+
+// Shared-memory record layout of the run-time kernel: 8-byte fields (min/max, double-double sums)
+// first, then 32-bit words (counters; exact float sums as three carry-chained words and a flag
+// word; integer sums as two carry-chained words).
+void pmb_jit_slayout(const DQuery& q, JitSLayout* S) {
+  S->off.assign(q.n_fields, 0);
+  int off = 0;
+  for (int pass = 0; pass < 2; pass++)
+    for (int i = 0; i < q.n_fields; i++) {
+      int k = q.field[i].kind;
+      bool eight = k == F_SUM_DD || k == F_MIN_I || k == F_MAX_I || k == F_MIN_U || k == F_MAX_U || k == F_MIN_F ||
+                   k == F_MAX_F;
+      if (eight != (pass == 0)) continue;
+      S->off[i] = off;
+      off += k == F_SUM_DD || k == F_SUM_FX ? 16 : (eight || k == F_SUM_I ? 8 : 4);
+    }
+  S->bytes = (off + 7) & ~7;
+  S->ident.assign(S->bytes / 4, 0u);
+  for (int i = 0; i < q.n_fields; i++) {
+    int k = q.field[i].kind, w = S->off[i] / 4;
+    if (k == F_MIN_I || k == F_MIN_F) {
+      S->ident[w] = 0xFFFFFFFFu;
+      S->ident[w + 1] = 0x7FFFFFFFu;
+    } else if (k == F_MAX_I || k == F_MAX_F) {
+      S->ident[w + 1] = 0x80000000u;
+    } else if (k == F_MIN_U) {
+      S->ident[w] = S->ident[w + 1] = 0xFFFFFFFFu;
+    }
+  }
+}
 
 bool pmb_jit_enabled(int64_t n_rows) {
   const char* e = getenv("PMB_JIT");
@@ -564,18 +653,23 @@ std::string pmb_jit_source(const CompiledQuery& cq, const JitPlan& J) {
   // order: device helpers, the skeleton's parameter block, the generated row program, the kernel
   std::string skel(kSkeleton);
   size_t cut = skel.find("__device__ __forceinline__ long long j_gresolve");
-  return std::string(kDeviceHeader) + "\n" + skel.substr(0, cut) + "\n" + g.build(cq.rec_init) + "\n" + skel.substr(cut);
+  return std::string(kDeviceHeader) + "\n" + skel.substr(0, cut) + "\n" + g.build() + "\n" + skel.substr(cut);
 }
 
 int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int max_smem_optin, JitPlan* J) {
   const DQuery& q = cq.dq;
   memset(J, 0, sizeof(*J));
   J->nt = 1024;
+  J->nbuf = 1;
   if (const char* e = getenv("PMB_NT")) {
     int v = atoi(e);
     if (v == 256 || v == 512 || v == 1024) J->nt = v;
   }
-  const int W = J->nt / 32, rec = q.rec_bytes;
+  if (const char* e = getenv("PMB_NBUF")) {
+    int v = atoi(e);
+    if (v == 1 || v == 2) J->nbuf = v;
+  }
+  const int W = J->nt / 32;
   int off = 0, tx = 0;
   for (int c = 0; c < q.n_cols; c++) {
     int db = q.col[c].elem ? 128 * q.col[c].elem : 16;
@@ -591,34 +685,46 @@ int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int m
   }
   J->buf_bytes = (int)pmb_align((size_t)off, 128);
   J->tx_bytes = tx;
+  JitSLayout S;
+  pmb_jit_slayout(q, &S);
+  J->srec = S.bytes;
   const int budget = max_smem_optin - 1024;
-  J->off_buf = (int)pmb_align((size_t)(8 * W), 128);
-  int used = J->off_buf + W * J->buf_bytes;
-  if (used > budget) return pmb_fail(h, PMB_E_UNSUPPORTED, "query touches too many columns for the unit buffers");
-  // hot tier: per-warp records of the heaviest sample keys (up to 32 KB), then the warm table
-  int hot = have_sketch ? 32 : 0;
-  if (const char* e = getenv("PMB_HOT")) hot = std::max(0, std::min(atoi(e), 128));
-  while (hot > 0 && (W * hot * rec > (32 << 10) || used + W * hot * rec + 16 * hot > budget)) hot /= 2;
-  J->hot_cap = hot;
-  J->hot_lut = hot ? (int)next_pow2_u64((uint64_t)(2 * hot)) : 0;
-  J->off_hot_lut = (int)pmb_align((size_t)used, 16);
-  J->off_hot_recs = (int)pmb_align((size_t)(J->off_hot_lut + 12 * J->hot_lut), 16);
-  used = J->off_hot_recs + W * hot * rec;
-  int S = 0;
+  int used = 0;
+  for (;;) {
+    J->off_bars = 0;
+    J->off_buf = (int)pmb_align((size_t)(8 * W * J->nbuf), 128);
+    J->off_q = J->off_buf + W * J->nbuf * J->buf_bytes;
+    used = J->off_q + W * 128 * 4;
+    if (used <= budget) break;
+    if (J->nbuf == 1) return pmb_fail(h, PMB_E_UNSUPPORTED, "query touches too many columns for the unit buffers");
+    J->nbuf = 1;
+  }
+  // hot keys: one record per warp each; warm keys: the largest count whose table and records fit
+  int hot = have_sketch ? 8 : 0;
+  if (const char* e = getenv("PMB_HOT")) hot = std::max(0, std::min(atoi(e), 64));
+  while (hot > 0 && (int)pmb_align((size_t)used, 16) + 24 * 2 * hot + W * hot * J->srec > budget) hot /= 2;
+  int warm = 0;
   if (have_sketch) {
-    S = 1;
-    while (used + (2 * S) * (8 + rec) + 16 <= budget && 2 * S <= 4096) S *= 2;
-    if (S < 64) S = 0;
+    for (int sw = 8192; sw >= 32; sw -= 32) {
+      int T = (int)next_pow2_u64((uint64_t)(2 * (hot + sw)));
+      int need = (int)pmb_align((size_t)used, 16) + 12 * T + 16 + (W * hot + sw) * J->srec;
+      if (need <= budget) {
+        warm = sw;
+        break;
+      }
+    }
   }
   if (const char* e = getenv("PMB_SMEM_SLOTS")) {
     int v = atoi(e);
-    if (v == 0) S = 0;
-    else if (v > 0 && v < S) S = (int)next_pow2_u64((uint64_t)v);
+    if (v >= 0 && v < warm) warm = v;
   }
-  J->S = S;
-  J->off_skeys = (int)pmb_align((size_t)used, 16);
-  J->off_srecs = J->off_skeys + 8 * S;
-  J->smem = J->off_srecs + S * rec;
+  J->hot_cap = hot;
+  J->warm_cap = warm;
+  J->T = (hot + warm) ? (int)next_pow2_u64((uint64_t)(2 * (hot + warm))) : 0;
+  J->off_tkeys = (int)pmb_align((size_t)used, 16);
+  J->off_tval = J->off_tkeys + 8 * J->T;
+  J->off_srecs = (int)pmb_align((size_t)(J->off_tval + 4 * J->T), 16);
+  J->smem = J->off_srecs + (W * hot + warm) * J->srec;
   return PMB_OK;
 }
 
@@ -727,7 +833,8 @@ int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const
   }
   A.n_rows = cq.dq.n_rows;
   A.n_units = (cq.dq.n_rows + 127) / 128;
-  A.gprobe = P.gprobe;
+  A.gprobe = (int)std::min<unsigned long long>(P.gcap / 4, 256);     // buckets of 4 slots
+  A.occ_limit = (unsigned)std::min<unsigned long long>(P.gcap - P.gcap / 5, 0xFFFFFFFFull);  // 80% full
   A.gkeys = P.gkeys;
   A.grecs = P.grecs;
   A.gcap = P.gcap;

@@ -10,7 +10,7 @@ struct JitParams {
   long long n_rows;
   long long n_units;
   int gprobe;
-  int pad;
+  unsigned int occ_limit;
   unsigned long long* gkeys;
   uint8_t* grecs;
   unsigned long long gcap;
@@ -24,16 +24,29 @@ struct JitParams {
   int fx_e[8];
 };
 
-// shared-memory layout of the run-time kernel (per-warp 128-row unit buffers, hot and warm tiers)
+// shared-memory layout of the run-time kernel: per-warp 128-row unit buffers and queues, the
+// table of sampled keys, hot records (one per warp and key) and warm records (one per key)
 struct JitPlan {
-  int nt;
-  int buf_bytes;      // one warp's unit buffer
+  int nt, nbuf;       // threads per CTA; unit buffers per warp (2: the next unit is in flight)
+  int buf_bytes;      // one unit buffer
   int tx_bytes;       // bytes the bulk copies of one unit deliver
   int doff[16];       // column data offset inside a unit buffer
   int voff[16];       // column validity offset (-1: no bitmap)
-  int hot_cap, hot_lut, S;
-  int off_buf, off_hot_lut, off_hot_recs, off_skeys, off_srecs, smem;
+  int hot_cap;        // hot keys
+  int warm_cap;       // warm keys
+  int T;              // slots of the sampled-key table (power of two, 0 without sampled keys)
+  int srec;           // bytes of a shared-memory record
+  int off_bars, off_buf, off_q, off_tkeys, off_tval, off_srecs, smem;
 };
+
+// field offsets, size and identity words of the shared-memory record
+#include <vector>
+struct JitSLayout {
+  std::vector<int> off;
+  int bytes = 0;
+  std::vector<unsigned> ident;
+};
+void pmb_jit_slayout(const DQuery& q, JitSLayout* S);
 
 int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int max_smem_optin, JitPlan* J);
 

@@ -1,37 +1,41 @@
 // pmb_jit_skeleton.cuh — the fused filter -> group_by -> aggregate kernel compiled at run time
 // for one query signature (NVRTC). This text follows pmb_device.cuh and a generated section that
-// defines, for that signature, the J_* constants and the row functions:
-//   j_issue_unit   one warp's bulk copies (TMA, cp.async.bulk) of a 128-row unit into its buffer
+// defines, for that signature, the J_* layout constants and the row functions:
+//   j_issue_unit   one warp's bulk copies (TMA, cp.async.bulk) of a 128-row unit into a buffer
 //   j_copy_unit    plain copy of a partial last unit
-//   JRow, j_load   the values of one row of the buffer and the filter verdict (with the range
-//                  report of exact float sums when `check`)
-//   j_load_vals    the aggregated values only
+//   JRow           the values of one row of a unit buffer
+//   j_load_pk      the predicate and key columns of a row, and the filter verdict
+//   j_load_vals    the aggregated columns of a row
 //   j_key          the packed 64-bit group key
-//   j_private / j_shared / j_global      one row into a warp-private / CTA-shared / global record
-//                  (float sums: double-double in the private and shared tiers, fixed-point limbs in
-//                  the global table)
-//   j_merge_private / j_merge_global     a finished private / shared record into another / the table
-//   J_IDENT        the identity record (u64 words)
+//   j_fxcheck      range report of the exact float sums (the call is re-run wider on a report)
+//   j_shared       one row into a shared-memory record (native 32-bit atomics only: counters,
+//                  carry-chained 32-bit words for the exact sums, 64-bit min/max)
+//   j_global       one row into a global-table record (fire-and-forget 64-bit atomics)
+//   j_sfold        a shared-memory record into another (one owner)
+//   j_merge_sg     a shared-memory record into a global-table record
+//   J_SIDENT       the identity shared-memory record (u32 words)
 //
-// Execution: persistent CTAs, every warp independent (no CTA barrier in the main loop). A warp
-// takes 128-row units round-robin over all warps of the grid; lane 0 bulk-copies the unit's
-// column chunks into the warp's shared buffer (one mbarrier per warp, bounded wait), then each
-// lane handles rows lane, lane + 32, lane + 64, lane + 96 of the unit:
-//   1. filter, key, hot lookup for the 4 rows; hot rows: lanes with the same hot key are grouped
-//      (__match_any_sync) and the group's first lane applies the group to the warp's private
-//      record (no atomics);
-//   2. warm rows (keys preloaded into the CTA-shared table): shared-memory atomics;
-//   3. cold rows: the 4 probe loads of the global table are issued back to back, then resolved
-//      and the rows applied with fire-and-forget atomics.
-// At exit the warps' private records and the shared table are merged into the global table.
+// Execution: persistent CTAs whose warps run independently (no CTA barrier in the main loop). A
+// warp takes 128-row units round-robin over all warps of the grid; lane 0 bulk-copies a unit's
+// column chunks into one of the warp's J_NBUF buffers (one mbarrier each, bounded waits), so with
+// two buffers the next unit is in flight while this one is processed. Per unit:
+//   1. classify: each lane evaluates the filter and the key of rows lane, lane+32, lane+64,
+//      lane+96 and looks the key up in the CTA's read-only table of sampled keys. Rows of sampled
+//      keys ("hot": the heaviest, with one record per warp; "warm": one record per CTA) and the
+//      other kept rows ("cold") are compacted with ballots into the warp's queue;
+//   2. the queued shared-tier rows are applied 32 at a time, every lane busy;
+//   3. the queued cold rows are applied to the global table 32 at a time.
+// A table overflow (probe limit) or a failed wait makes every warp stop at its next unit; the
+// host then re-runs with a larger table. At exit the hot records of all warps are folded and, with
+// the warm records, merged into the global table.
 
 struct JParams {
   const unsigned char* col_data[16];
   const unsigned char* col_valid[16];
   long long n_rows;
   long long n_units;  // ceil(n_rows / 128)
-  int gprobe;
-  int pad;
+  int gprobe;              // probe limit, in 4-slot buckets
+  unsigned int occ_limit;  // claimed slots at which the table counts as full (overflow)
   unsigned long long* gkeys;
   unsigned char* grecs;
   unsigned long long gcap;
@@ -41,143 +45,160 @@ struct JParams {
   const unsigned long long* warm_keys;
   const unsigned int* warm_n;
   unsigned long long* kstats;
-  int fx[8];    // fraction bits F of each exact float-sum slot (global limbs hold x * 2^F)
+  int fx[8];    // fraction bits F of each exact float-sum slot (sums hold x * 2^F)
   int fx_e[8];  // every value of the slot satisfies |x| < 2^fx_e
 };
 
 #define J_UNIT 128
+#define J_MISS 0xFFFFFFFFu
+#define J_HOTBIT 0x40000000u
 
-// first probe slot of `key` (shared by the batched probe and the resolve step)
+// Global table: linear probing over 4-slot buckets (one 32-byte sector of keys, read with two
+// 16-byte loads), so a probe sequence costs about one round trip to L2 per 4 slots. Returns the
+// slot of `key` (claiming an empty one with a CAS; `claimed` tells), or -1 and PMB_ST_OVERFLOW at
+// the probe limit. The key whose bits equal the EMPTY marker has the extra slot gcap.
 __device__ __forceinline__ long long j_gresolve(const JParams& P, unsigned long long key, unsigned long long h,
-                                                unsigned long long first) {
+                                                bool& claimed) {
+  claimed = false;
   if (key == PMB_EMPTY64) {
     if (*(volatile unsigned int*)&P.status[1] == 0) atomicOr(&P.status[1], 1u);
     return (long long)P.gcap;
   }
-  unsigned long long mask = P.gcap - 1, i = h & mask;
-  unsigned long long k = first;
+  const unsigned long long nb = P.gcap >> 2;
+  unsigned long long bk = pmb_slot(h, nb);
   for (int p = 0; p < P.gprobe; p++) {
-    if (k == key) return (long long)i;
-    if (k == PMB_EMPTY64) {
-      unsigned long long old = atomicCAS(&P.gkeys[i], PMB_EMPTY64, key);
-      if (old == PMB_EMPTY64 || old == key) return (long long)i;
+    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(P.gkeys + 4 * bk);
+    const ulonglong2 a = src[0], c = src[1];
+    const unsigned long long ks[4] = {a.x, a.y, c.x, c.y};
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      if (ks[s] == key) return (long long)(4 * bk + s);
+      if (ks[s] == PMB_EMPTY64) {
+        unsigned long long old = atomicCAS(&P.gkeys[4 * bk + s], PMB_EMPTY64, key);
+        if (old == PMB_EMPTY64) {
+          claimed = true;
+          return (long long)(4 * bk + s);
+        }
+        if (old == key) return (long long)(4 * bk + s);
+      }
     }
-    i = (i + 1) & mask;
-    k = P.gkeys[i];
+    bk = (bk + 1 == nb) ? 0ULL : bk + 1;
   }
   atomicOr(P.status, PMB_ST_OVERFLOW);
   return -1;
 }
 
 __device__ __forceinline__ long long j_gfind(const JParams& P, unsigned long long key, unsigned long long h) {
-  if (key == PMB_EMPTY64) return j_gresolve(P, key, h, 0ULL);
-  return j_gresolve(P, key, h, P.gkeys[h & (P.gcap - 1)]);
+  bool claimed;
+  return j_gresolve(P, key, h, claimed);
 }
 
-// read-only lookup in the warm table (keys preloaded per CTA); -1 when absent
-__device__ __forceinline__ int j_sfind_ro(const unsigned long long* skeys, unsigned long long key, unsigned long long h) {
-  if (J_S == 0 || key == PMB_EMPTY64) return -1;
-  int i = (int)((h >> 40) & (unsigned long long)(J_S - 1));
-  for (int p = 0; p < J_S; p++) {
-    unsigned long long k = skeys[i];
-    if (k == key) return i;
-    if (k == PMB_EMPTY64) return -1;
-    i = (i + 1) & (J_S - 1);
+// the CTA's table of sampled keys: value of `key`, or J_MISS
+__device__ __forceinline__ unsigned j_tfind(const unsigned long long* tk, const unsigned* tv, unsigned long long key,
+                                            unsigned long long h) {
+  if (J_T == 0 || key == PMB_EMPTY64) return J_MISS;
+  int i = (int)((h >> 40) & (unsigned long long)(J_T - 1));
+  for (int p = 0; p < J_T; p++) {
+    unsigned long long k = tk[i];
+    if (k == key) return tv[i];
+    if (k == PMB_EMPTY64) return J_MISS;
+    i = (i + 1) & (J_T - 1);
   }
-  return -1;
+  return J_MISS;
 }
 
-__device__ __forceinline__ void j_sinsert(unsigned long long* skeys, unsigned long long key) {
-  int i = (int)((pmb_fmix64(key) >> 40) & (unsigned long long)(J_S - 1));
-  for (int p = 0; p < J_S; p++) {
-    unsigned long long old = atomicCAS(&skeys[i], PMB_EMPTY64, key);
-    if (old == PMB_EMPTY64 || old == key) return;
-    i = (i + 1) & (J_S - 1);
+__device__ __forceinline__ void j_tinsert(unsigned long long* tk, unsigned* tv, unsigned long long key,
+                                          unsigned long long h, unsigned v) {
+  int i = (int)((h >> 40) & (unsigned long long)(J_T - 1));
+  for (int p = 0; p < J_T; p++) {
+    unsigned long long old = atomicCAS(&tk[i], PMB_EMPTY64, key);
+    if (old == PMB_EMPTY64) {
+      tv[i] = v;
+      return;
+    }
+    if (old == key) return;
+    i = (i + 1) & (J_T - 1);
   }
 }
 
-__device__ __forceinline__ int j_hot_find(const unsigned long long* lk, const int* li, unsigned long long key,
-                                          unsigned long long h) {
-  int i = (int)((h >> 24) & (unsigned long long)(J_HOT_LUT - 1));
-  for (int p = 0; p < J_HOT_LUT; p++) {
-    unsigned long long k = lk[i];
-    if (k == key) return li[i];
-    if (k == PMB_EMPTY64) return -1;
-    i = (i + 1) & (J_HOT_LUT - 1);
-  }
-  return -1;
+__device__ __forceinline__ bool j_stop(const JParams& P) {
+  return (*(volatile unsigned int*)P.status & (PMB_ST_OVERFLOW | PMB_ST_TIMEOUT)) != 0u;
 }
 
 extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __grid_constant__ JParams P) {
   extern __shared__ __align__(128) unsigned char sm[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int W = J_NT / 32;
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(sm);  // one per warp
-  unsigned char* buf = sm + J_OFF_BUF + warp * J_BUF_BYTES;
-  unsigned long long* skeys = reinterpret_cast<unsigned long long*>(sm + J_OFF_SKEYS);
+  unsigned long long* all_bars = reinterpret_cast<unsigned long long*>(sm + J_OFF_BARS);
+  unsigned long long* bars = all_bars + warp * J_NBUF;
+  unsigned char* bufs = sm + J_OFF_BUF + warp * J_NBUF * J_BUF_BYTES;
+  unsigned* q = reinterpret_cast<unsigned*>(sm + J_OFF_Q) + warp * J_UNIT;
+  unsigned long long* tkeys = reinterpret_cast<unsigned long long*>(sm + J_OFF_TKEYS);
+  unsigned* tval = reinterpret_cast<unsigned*>(sm + J_OFF_TVAL);
   unsigned char* srecs = sm + J_OFF_SRECS;
-  unsigned long long* hlk = reinterpret_cast<unsigned long long*>(sm + J_OFF_HOT_LUT);
-  int* hli = reinterpret_cast<int*>(sm + J_OFF_HOT_LUT + 8 * J_HOT_LUT);
-  unsigned char* hrecs = sm + J_OFF_HOT_RECS;
-  unsigned char* my_hot = hrecs + warp * J_HOT_CAP * J_REC;
-  const int n_hot = (J_HOT_CAP > 0 && P.hot_keys) ? (int)min(*P.hot_n, (unsigned)J_HOT_CAP) : 0;
-  const int n_warm = (J_S > 0 && P.warm_keys) ? (int)min(*P.warm_n, (unsigned)(J_S / 2)) : 0;
+  __shared__ unsigned s_claims;  // slots this CTA claimed in the global table (published per 64)
+  const int n_hot = (J_H > 0 && P.hot_keys) ? (int)min(*P.hot_n, (unsigned)J_H) : 0;
+  const int n_warm = (J_SW > 0 && P.warm_keys) ? (int)min(*P.warm_n, (unsigned)J_SW) : 0;
 
-  for (int i = tid; i < J_S; i += J_NT) skeys[i] = PMB_EMPTY64;
-  for (int w = tid; w < J_S * J_REC_WORDS; w += J_NT)
-    reinterpret_cast<unsigned long long*>(srecs)[w] = J_IDENT[w % J_REC_WORDS];
-  if (J_HOT_CAP > 0) {
-    for (int i = tid; i < J_HOT_LUT; i += J_NT) hlk[i] = PMB_EMPTY64;
-    for (int w = tid; w < W * J_HOT_CAP * J_REC_WORDS; w += J_NT)
-      reinterpret_cast<unsigned long long*>(hrecs)[w] = J_IDENT[w % J_REC_WORDS];
-  }
+  for (int i = tid; i < J_T; i += J_NT) tkeys[i] = PMB_EMPTY64;
+  for (int w = tid; w < (W * J_H + J_SW) * J_SREC_WORDS; w += J_NT)
+    reinterpret_cast<unsigned*>(srecs)[w] = J_SIDENT[w % J_SREC_WORDS];
   if (tid == 0) {
-    for (int w = 0; w < W; w++) mbar_init(&bars[w], 1);
+    s_claims = 0u;
+    for (int b = 0; b < W * J_NBUF; b++) mbar_init(&all_bars[b], 1);
     mbar_fence_init();
   }
   __syncthreads();
-  for (int i = tid; i < n_hot; i += J_NT) {
-    unsigned long long k = P.hot_keys[i];
-    int j = (int)((pmb_fmix64(k) >> 24) & (unsigned long long)(J_HOT_LUT - 1));
-    for (int p = 0; p < J_HOT_LUT; p++) {
-      if (atomicCAS(&hlk[j], PMB_EMPTY64, k) == PMB_EMPTY64) {
-        hli[j] = i;
-        break;
-      }
-      j = (j + 1) & (J_HOT_LUT - 1);
-    }
+  for (int i = tid; i < n_hot + n_warm; i += J_NT) {
+    unsigned long long key = i < n_hot ? P.hot_keys[i] : P.warm_keys[i - n_hot];
+    if (key == PMB_EMPTY64) continue;  // that key always takes the global table's extra slot
+    j_tinsert(tkeys, tval, key, j_hash(key), i < n_hot ? (J_HOTBIT | (unsigned)i) : (unsigned)(i - n_hot));
   }
-  for (int i = tid; i < n_warm; i += J_NT) j_sinsert(skeys, P.warm_keys[i]);
   __syncthreads();
 
+  const long long n_full = P.n_rows / J_UNIT;
   const long long gw = (long long)blockIdx.x * W + warp, n_warps = (long long)gridDim.x * W;
-  unsigned phase = 0;
+  const unsigned long long pol = pmb_policy_evict_first();
+  unsigned parity = 0, pending = 0;  // per buffer: phase to wait for, copy in flight
+  if (lane == 0) {
+    for (int b = 0; b < J_NBUF; b++) {
+      long long uu = gw + b * n_warps;
+      if (uu < n_full) {
+        j_issue_unit(P, bufs + b * J_BUF_BYTES, uu, &bars[b], pol);
+        pending |= 1u << b;
+      }
+    }
+  }
   bool aborted = false;
-  // optional phase counters (P.kstats): cycles in copy wait / filter+hot / warm / cold, rows per tier
   const bool ks = P.kstats != nullptr;
-  long long c_wait = 0, c_p1 = 0, c_p2 = 0, c_p3 = 0, c0 = 0;
-  unsigned n_hot_rows = 0, n_warm_rows = 0, n_cold_rows = 0;
-  for (long long u = gw; u < P.n_units; u += n_warps) {
+  long long c_wait = 0, c_cls = 0, c_sh = 0, c_cold = 0, c0 = 0;
+  unsigned n_sh_rows = 0, n_cold_rows = 0;
+  int b = 0;
+  for (long long u = gw, k = 0; u < P.n_units; u += n_warps, k++) {
+    if ((k & 3) == 3) {
+      bool stop = false;
+      if (lane == 0) stop = j_stop(P);
+      if (__shfl_sync(0xffffffffu, stop, 0)) break;
+    }
     const long long row0 = u * J_UNIT;
     const int rows = (int)min((long long)J_UNIT, P.n_rows - row0);
+    unsigned char* st = bufs + b * J_BUF_BYTES;
     if (ks) c0 = clock64();
     if (rows == J_UNIT) {
-      if (lane == 0) {
-        fence_proxy_async();  // the warp's reads of the previous unit come before the copy's writes
-        j_issue_unit(P, buf, u, &bars[warp]);
-      }
       bool ok = true;
-      if (lane == 0) ok = mbar_wait_bounded(&bars[warp], phase);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!ok) {
-        // give the copy in flight one more bounded wait before leaving its buffer
-        if (lane == 0) mbar_wait_bounded(&bars[warp], phase);
+      if (lane == 0) {
+        ok = mbar_wait_bounded(&bars[b], (parity >> b) & 1u);
+        if (ok) {
+          parity ^= 1u << b;
+          pending &= ~(1u << b);
+        }
+      }
+      if (!__shfl_sync(0xffffffffu, ok, 0)) {
         aborted = true;
         break;
       }
-      phase ^= 1u;
     } else {
-      j_copy_unit(P, buf, row0, rows);
+      j_copy_unit(P, st, row0, rows);
     }
     __syncwarp();
     if (ks) {
@@ -186,126 +207,126 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
       c0 = c1;
     }
 
-    // 1. filter, key, hot tier; remember cold rows for the batched probe
-    unsigned long long ck[4], ch[4];
-    unsigned cold = 0, warm = 0;
-    int wslot[4];
+    // 1. classify and compact: shared-tier entries (record << 7 | row) from the front of the
+    //    queue, cold rows from the back
+    int ns = 0, nc = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned ent[4];  // 0: dropped, J_MISS: cold, else shared-tier entry (record << 7 | row) + 1
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const int lr = lane + 32 * j;
       JRow r;
-      bool keep = lr < rows && j_load(P, buf, lr, r, true);
-      unsigned long long key = keep ? j_key(r) : 0ULL;
-      unsigned long long h = pmb_fmix64(key);
-      int hot = -1;
-      if (J_HOT_CAP > 0 && n_hot && keep && key != PMB_EMPTY64) hot = j_hot_find(hlk, hli, key, h);
-      if (J_HOT_CAP > 0) {
-        unsigned hm = __ballot_sync(0xffffffffu, hot >= 0);
-        if (hm) {
-          unsigned peers = __match_any_sync(0xffffffffu, hot) & hm;
-          if (hot >= 0 && lane == __ffs(peers) - 1) {
-            unsigned char* rec = my_hot + hot * J_REC;
-            j_private(P, rec, r);
-            for (unsigned m = peers & (peers - 1); m; m &= m - 1) {
-              JRow rp;
-              j_load_vals(P, buf, (__ffs(m) - 1) + 32 * j, rp);
-              j_private(P, rec, rp);
-            }
-          }
-        }
-      }
-      if (ks && hot >= 0) n_hot_rows++;
-      ck[j] = key;
-      ch[j] = h;
-      wslot[j] = -1;
-      if (keep && hot < 0) {
-        int si = j_sfind_ro(skeys, key, h);
-        if (si >= 0) {
-          wslot[j] = si;
-          warm |= 1u << j;
+      const bool keep = lr < rows && j_load_pk(P, st, lr, r);
+      ent[j] = 0u;
+      if (keep) {
+        const unsigned long long key = j_key(r);
+        const unsigned v = j_tfind(tkeys, tval, key, j_hash(key));
+        if (v != J_MISS) {
+          const unsigned rec = (v & J_HOTBIT) ? (unsigned)(warp * J_H) + (v & ~J_HOTBIT) : (unsigned)(W * J_H) + v;
+          ent[j] = ((rec << 7) | (unsigned)lr) + 1u;
         } else {
-          cold |= 1u << j;
+          ent[j] = J_MISS;
         }
       }
     }
-    if (ks) {
-      long long c1 = clock64();
-      c_p1 += c1 - c0;
-      c0 = c1;
-      n_warm_rows += __popc(warm);
-      n_cold_rows += __popc(cold);
-    }
-    // 2. warm rows
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      if (warm & (1u << j)) {
+      const bool sh = ent[j] != 0u && ent[j] != J_MISS, cold = ent[j] == J_MISS;
+      const unsigned bs = __ballot_sync(0xffffffffu, sh), bc = __ballot_sync(0xffffffffu, cold);
+      if (sh) q[ns + __popc(bs & lt)] = ent[j] - 1u;
+      if (cold) q[J_UNIT - 1 - (nc + __popc(bc & lt))] = (unsigned)(lane + 32 * j);
+      ns += __popc(bs);
+      nc += __popc(bc);
+    }
+    __syncwarp();
+    if (ks) {
+      long long c1 = clock64();
+      c_cls += c1 - c0;
+      c0 = c1;
+      n_sh_rows += ns;
+      n_cold_rows += nc;
+    }
+    // 2. shared tier
+    for (int base = 0; base < ns; base += 32) {
+      if (base + lane < ns) {
+        const unsigned e = q[base + lane];
         JRow r;
-        j_load_vals(P, buf, lane + 32 * j, r);
-        j_shared(P, srecs + wslot[j] * J_REC, r);
+        j_load_vals(P, st, (int)(e & 127u), r);
+        j_fxcheck(P, r);
+        j_shared(P, srecs + (e >> 7) * J_SREC, r);
       }
     }
     if (ks) {
       long long c1 = clock64();
-      c_p2 += c1 - c0;
+      c_sh += c1 - c0;
       c0 = c1;
     }
-    // 3. cold rows: probe loads first, then resolve and apply
-    unsigned long long first[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-      first[j] = ((cold >> j) & 1u) && ck[j] != PMB_EMPTY64 ? P.gkeys[ch[j] & (P.gcap - 1)] : 0ULL;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      if (cold & (1u << j)) {
-        long long gi = j_gresolve(P, ck[j], ch[j], first[j]);
-        if (gi >= 0) {
-          JRow r;
-          j_load_vals(P, buf, lane + 32 * j, r);
-          j_global(P, P.grecs + (unsigned long long)gi * J_REC, r);
+    // 3. cold tier: the probe load of every lane first, then resolve and apply
+    for (int base = 0; base < nc; base += 32) {
+      if (base + lane < nc) {
+        const int lr = (int)q[J_UNIT - 1 - (base + lane)];
+        JRow r;
+        j_load_key(P, st, lr, r);
+        j_load_vals(P, st, lr, r);
+        const unsigned long long key = j_key(r);
+        j_fxcheck(P, r);
+        bool claimed;
+        const long long gi = j_gresolve(P, key, j_hash(key), claimed);
+        if (gi >= 0) j_global(P, P.grecs + (unsigned long long)gi * J_REC, r);
+        if (claimed && ((atomicAdd(&s_claims, 1u) + 1u) & 63u) == 0u) {
+          // every 64 claims of this CTA: publish them; past the limit the table counts as full
+          if (atomicAdd(&P.status[2], 64u) + 64u > P.occ_limit) atomicOr(P.status, PMB_ST_OVERFLOW);
         }
       }
     }
     __syncwarp();
-    if (ks) c_p3 += clock64() - c0;
+    if (ks) c_cold += clock64() - c0;
+    // this buffer is free again: bring in the warp's unit J_NBUF steps ahead
+    if (lane == 0) {
+      const long long uu = u + (long long)J_NBUF * n_warps;
+      if (uu < n_full) {
+        fence_proxy_async();  // the warp's reads of this unit come before the copy's writes
+        j_issue_unit(P, st, uu, &bars[b], pol);
+        pending |= 1u << b;
+      }
+    }
+    b = (b + 1 == J_NBUF) ? 0 : b + 1;
+  }
+  // copies still in flight land before the buffers are given up
+  if (lane == 0) {
+    for (int bb = 0; bb < J_NBUF; bb++)
+      if ((pending >> bb) & 1u) {
+        if (!mbar_wait_bounded(&bars[bb], (parity >> bb) & 1u)) aborted = true;
+      }
   }
   if (ks) {
     if (lane == 0) {
       atomicAdd(&P.kstats[0], (unsigned long long)c_wait);
-      atomicAdd(&P.kstats[1], (unsigned long long)c_p1);
-      atomicAdd(&P.kstats[2], (unsigned long long)c_p2);
-      atomicAdd(&P.kstats[3], (unsigned long long)c_p3);
-    }
-    unsigned a = n_hot_rows, b = n_warm_rows, c = n_cold_rows;
-    for (int o = 16; o; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      b += __shfl_xor_sync(0xffffffffu, b, o);
-      c += __shfl_xor_sync(0xffffffffu, c, o);
-    }
-    if (lane == 0) {
-      atomicAdd(&P.kstats[4], (unsigned long long)a);
-      atomicAdd(&P.kstats[5], (unsigned long long)b);
-      atomicAdd(&P.kstats[6], (unsigned long long)c);
+      atomicAdd(&P.kstats[1], (unsigned long long)c_cls);
+      atomicAdd(&P.kstats[2], (unsigned long long)c_sh);
+      atomicAdd(&P.kstats[3], (unsigned long long)c_cold);
+      atomicAdd(&P.kstats[4], (unsigned long long)n_sh_rows);
+      atomicAdd(&P.kstats[5], (unsigned long long)n_cold_rows);
       atomicAdd(&P.kstats[7], 1ULL);
     }
   }
   if (aborted && lane == 0) atomicOr(P.status, PMB_ST_TIMEOUT);
   __syncthreads();
-  // hot keys: fold the warps' private records, then one merge per touched key
+  if (j_stop(P)) return;  // the host re-runs this call; the partial records are discarded
+  // hot keys: fold the warps' records into warp 0's, then one merge per touched key
   for (int i = tid; i < n_hot; i += J_NT) {
-    unsigned char* r0 = hrecs + i * J_REC;
-    for (int w = 1; w < W; w++) j_merge_private(r0, hrecs + (w * J_HOT_CAP + i) * J_REC);
-    if (*reinterpret_cast<const unsigned int*>(r0 + J_LEN_OFF) == 0) continue;
-    unsigned long long key = P.hot_keys[i];
-    long long gi = j_gfind(P, key, pmb_fmix64(key));
-    if (gi >= 0) j_merge_global(P, P.grecs + (unsigned long long)gi * J_REC, r0);
+    unsigned char* r0 = srecs + i * J_SREC;
+    for (int w = 1; w < W; w++) j_sfold(r0, srecs + (w * J_H + i) * J_SREC);
+    if (*reinterpret_cast<const unsigned*>(r0 + J_LEN_SOFF) == 0u) continue;
+    const unsigned long long key = P.hot_keys[i];
+    const long long gi = j_gfind(P, key, j_hash(key));
+    if (gi >= 0) j_merge_sg(P, P.grecs + (unsigned long long)gi * J_REC, r0);
   }
-  // the warm table (preloaded keys may have seen no rows)
-  for (int i = tid; i < J_S; i += J_NT) {
-    unsigned long long key = skeys[i];
-    if (key == PMB_EMPTY64) continue;
-    const unsigned char* r = srecs + i * J_REC;
-    if (*reinterpret_cast<const unsigned int*>(r + J_LEN_OFF) == 0) continue;
-    long long gi = j_gfind(P, key, pmb_fmix64(key));
-    if (gi >= 0) j_merge_global(P, P.grecs + (unsigned long long)gi * J_REC, r);
+  for (int i = tid; i < n_warm; i += J_NT) {
+    const unsigned char* r = srecs + (W * J_H + i) * J_SREC;
+    if (*reinterpret_cast<const unsigned*>(r + J_LEN_SOFF) == 0u) continue;
+    const unsigned long long key = P.warm_keys[i];
+    const long long gi = j_gfind(P, key, j_hash(key));
+    if (gi >= 0) j_merge_sg(P, P.grecs + (unsigned long long)gi * J_REC, r);
   }
 }
