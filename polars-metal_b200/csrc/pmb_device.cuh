@@ -95,6 +95,26 @@ __host__ __device__ __forceinline__ uint64_t pmb_fmix64(uint64_t k) {
   return k;
 }
 
+// a second 32-bit mixer, independent of the key hash (C. Wellons' "lowbias32", public domain):
+// the alternative bucket of a cuckoo table
+__host__ __device__ __forceinline__ uint32_t pmb_mix32b(uint32_t a) {
+  a ^= a >> 16;
+  a *= 0x7feb352dU;
+  a ^= a >> 15;
+  a *= 0x846ca68bU;
+  a ^= a >> 16;
+  return a;
+}
+// MurmurHash3 32-bit finalizer (Appleby, public domain)
+__host__ __device__ __forceinline__ uint32_t pmb_fmix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x85ebca6bU;
+  x ^= x >> 13;
+  x *= 0xc2b2ae35U;
+  x ^= x >> 16;
+  return x;
+}
+
 // slot of hash h in a table of `cap` slots, any cap: the high word of h * cap (Lemire's
 // multiply-shift range reduction), so capacities need not be powers of two
 __device__ __forceinline__ uint64_t pmb_slot(uint64_t h, uint64_t cap) { return __umul64hi(h, cap); }
@@ -174,12 +194,11 @@ __device__ __forceinline__ void dd_plain_add(double* hi, double* lo, double x) {
 
 
 // ----------------------------------------------------------------------------- exact float sums
-// A finite double x is summed as the integer X = trunc(x * 2^F), a 96-bit two's complement value
-// split into three 32-bit limbs that are added into three 64-bit words (limb 0 and 1 unsigned,
-// limb 2 signed). 64-bit words leave 31 bits of headroom, so up to 2^31 additions are exact and
-// the order of additions does not matter. F is chosen per column so that |x| < 2^(94 - F); a
-// value outside that range is reported (status bit + its exponent) and the call is re-run with a
-// wider range. NaN / +inf / -inf are tracked as flag bits beside the limbs.
+// A finite double x is summed as the integer X = trunc(x * 2^F), a two's complement value split
+// into 32-bit limbs; integer additions are exact and their order does not matter. F is chosen per
+// column so that |x| < 2^(94 - F) and the sums of all rows stay in range; a value outside that
+// range is reported (status bit + its exponent) and the call is re-run with a wider range. NaN /
+// +inf / -inf are tracked as flag bits beside the sum.
 #define PMB_ST_FXRANGE 8u  // a float-sum value exceeded its column's fixed-point range
 #define PMB_FX_NAN 1u
 #define PMB_FX_PINF 2u
@@ -223,4 +242,14 @@ __device__ __forceinline__ void pmb_fx_split(double x, int F, unsigned long long
   l0 = lo & 0xFFFFFFFFULL;
   l1 = lo >> 32;
   l2 = (unsigned long long)(long long)(int)(unsigned)hi;
+}
+
+// The global table keeps an exact float sum in two 64-bit words: the sum of the values' low 32
+// bits (unsigned; up to 2^32 additions fit) and the sum of the values shifted right by 32
+// (signed), so one value costs two fire-and-forget adds. These are the two words of one value.
+__device__ __forceinline__ void pmb_fx_words(double x, int F, unsigned long long& w0, unsigned long long& w1) {
+  unsigned long long l0, l1, l2;
+  pmb_fx_split(x, F, l0, l1, l2);
+  w0 = l0;
+  w1 = l1 + (l2 << 32);
 }

@@ -309,7 +309,7 @@ __host__ __device__ inline void field_identity(int kind, uint64_t* w0, uint64_t*
   switch (kind) {
     case F_LEN: case F_CNT: *w0 = 0; *bytes = 4; break;
     case F_SUM_DD: *w0 = 0; *nwords = 2; *bytes = 16; break;
-    case F_SUM_FX: *w0 = 0; *nwords = 4; *bytes = 32; break;
+    case F_SUM_FX: *w0 = 0; *nwords = 3; *bytes = 24; break;
     case F_SUM_I: *w0 = 0; *bytes = 8; break;
     case F_MIN_I: case F_MIN_F: *w0 = 0x7FFFFFFFFFFFFFFFULL; *bytes = 8; break;
     case F_MAX_I: case F_MAX_F: *w0 = 0x8000000000000000ULL; *bytes = 8; break;
@@ -353,13 +353,12 @@ __device__ __forceinline__ void apply_row_private(const DQuery& q, const TileCtx
         double x = pmb_bits_to_f64(b, dt);
         unsigned fl = pmb_fx_flag(x);
         if (fl) {
-          *(unsigned int*)(p + 24) |= fl;
+          *(unsigned int*)(p + 16) |= fl;
         } else if (pmb_fx_in_range(x, q.fx_e[F.fx_slot])) {
-          unsigned long long l0, l1, l2;
-          pmb_fx_split(x, F.fx, l0, l1, l2);
-          ((unsigned long long*)p)[0] += l0;
-          ((unsigned long long*)p)[1] += l1;
-          ((unsigned long long*)p)[2] += l2;
+          unsigned long long w0, w1;
+          pmb_fx_words(x, F.fx, w0, w1);
+          ((unsigned long long*)p)[0] += w0;
+          ((unsigned long long*)p)[1] += w1;
         }
         break;
       }
@@ -415,13 +414,12 @@ __device__ __forceinline__ void apply_row_shared(const DQuery& q, const TileCtx&
         double x = pmb_bits_to_f64(b, dt);
         unsigned fl = pmb_fx_flag(x);
         if (fl) {
-          atomicOr((unsigned int*)(p + 24), fl);
+          atomicOr((unsigned int*)(p + 16), fl);
         } else if (pmb_fx_in_range(x, q.fx_e[F.fx_slot])) {
-          unsigned long long l0, l1, l2;
-          pmb_fx_split(x, F.fx, l0, l1, l2);
-          if (l0) atomicAdd((unsigned long long*)p, l0);
-          if (l1) atomicAdd((unsigned long long*)p + 1, l1);
-          if (l2) atomicAdd((unsigned long long*)p + 2, l2);
+          unsigned long long w0, w1;
+          pmb_fx_words(x, F.fx, w0, w1);
+          if (w0) atomicAdd((unsigned long long*)p, w0);
+          if (w1) atomicAdd((unsigned long long*)p + 1, w1);
         }
         break;
       }
@@ -482,13 +480,12 @@ __device__ __forceinline__ void apply_row_global(const DQuery& q, const TileCtx&
         double x = pmb_bits_to_f64(b, dt);
         unsigned fl = pmb_fx_flag(x);
         if (fl) {
-          atomicOr((unsigned int*)(p + 24), fl);
+          atomicOr((unsigned int*)(p + 16), fl);
         } else if (pmb_fx_in_range(x, q.fx_e[F.fx_slot])) {
-          unsigned long long l0, l1, l2;
-          pmb_fx_split(x, F.fx, l0, l1, l2);
-          if (l0) atomicAdd((unsigned long long*)p, l0);
-          if (l1) atomicAdd((unsigned long long*)p + 1, l1);
-          if (l2) atomicAdd((unsigned long long*)p + 2, l2);
+          unsigned long long w0, w1;
+          pmb_fx_words(x, F.fx, w0, w1);
+          if (w0) atomicAdd((unsigned long long*)p, w0);
+          if (w1) atomicAdd((unsigned long long*)p + 1, w1);
         }
         break;
       }
@@ -546,10 +543,10 @@ __device__ __forceinline__ void merge_record(const DQuery& q, uint8_t* dst, cons
       }
       case F_SUM_FX: {
         const unsigned long long* l = (const unsigned long long*)s;
-        for (int w = 0; w < 3; w++)
+        for (int w = 0; w < 2; w++)
           if (l[w]) atomicAdd((unsigned long long*)d + w, l[w]);
-        unsigned fl = *(const unsigned int*)(s + 24);
-        if (fl) atomicOr((unsigned int*)(d + 24), fl);
+        unsigned fl = *(const unsigned int*)(s + 16);
+        if (fl) atomicOr((unsigned int*)(d + 16), fl);
         break;
       }
       case F_SUM_I: {
@@ -600,8 +597,8 @@ __device__ __forceinline__ void merge_private(const DQuery& q, uint8_t* dst, con
       }
       case F_SUM_FX: {
         const unsigned long long* l = (const unsigned long long*)s;
-        for (int w = 0; w < 3; w++) ((unsigned long long*)d)[w] += l[w];
-        *(unsigned int*)(d + 24) |= *(const unsigned int*)(s + 24);
+        for (int w = 0; w < 2; w++) ((unsigned long long*)d)[w] += l[w];
+        *(unsigned int*)(d + 16) |= *(const unsigned int*)(s + 16);
         break;
       }
       case F_SUM_I: *(unsigned long long*)d += *(const unsigned long long*)s; break;

@@ -851,6 +851,26 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     P.hot_cap = 0;
     P.hot_lut_slots = 0;
   }
+  // run-time kernel: its sampled-key table is built here from the selected key lists
+  std::vector<uint8_t> ttab_host;
+  uint8_t* ttab = nullptr;
+  int tnb = 0;
+  if (jk && P.hot_n && (P.hot_keys || P.warm_keys)) {
+    unsigned int cnt[2] = {0, 0};
+    PMB_CUDA(h, cudaMemcpyAsync(cnt, P.hot_n, 8, cudaMemcpyDeviceToHost, h->stream));
+    PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+    const int nh = P.hot_keys ? (int)std::min<unsigned>(cnt[0], (unsigned)hot_cap) : 0;
+    const int nw = P.warm_keys ? (int)std::min<unsigned>(cnt[1], (unsigned)(S / 2)) : 0;
+    std::vector<unsigned long long> hk(nh), wk(nw);
+    if (nh) PMB_CUDA(h, cudaMemcpy(hk.data(), P.hot_keys, 8 * (size_t)nh, cudaMemcpyDeviceToHost));
+    if (nw) PMB_CUDA(h, cudaMemcpy(wk.data(), P.warm_keys, 8 * (size_t)nw, cudaMemcpyDeviceToHost));
+    tnb = pmb_jit_sampled_table(cq, J, hk.data(), nh, wk.data(), nw, &ttab_host);
+    if (tnb > 0) {
+      ttab = (uint8_t*)pmb_ws_alloc(h, ttab_host.size());
+      if (!ttab) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sampled-key table)");
+      PMB_CUDA(h, cudaMemcpyAsync(ttab, ttab_host.data(), ttab_host.size(), cudaMemcpyHostToDevice, h->stream));
+    }
+  }
   const int64_t n = q.n_rows;
 
   // Capacity: 4 slots per estimated group (any size: slots come from a multiply-shift, not a
@@ -917,7 +937,7 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     }
     P.kstats = kst;
     int rc;
-    if (jk) rc = pmb_jit_launch(h, jk, cq, J, P, h->sm_count);
+    if (jk) rc = pmb_jit_launch(h, jk, cq, J, P, h->sm_count, ttab, tnb);
     else if (K128) rc = launch_hash<512, true>(h, P, smem, grid);
     else if (nt == 1024) rc = launch_hash<1024, false>(h, P, smem, grid);
     else if (nt == 256) rc = launch_hash<256, false>(h, P, smem, grid);
@@ -928,8 +948,8 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
       PMB_CUDA(h, cudaMemcpyAsync(hk, kst, 128, cudaMemcpyDeviceToHost, h->stream));
       PMB_CUDA(h, cudaStreamSynchronize(h->stream));
       double warps = (double)(hk[7] ? hk[7] : 1);
-      fprintf(stderr, "jit kstats: nt=%d nbuf=%d hot=%d warm=%d T=%d srec=%d smem=%d cap=%llu | per warp (Mcycles): wait %.2f "
-              "classify %.2f shared %.2f cold %.2f | rows shared %llu cold %llu\n", J.nt, J.nbuf, J.hot_cap, J.warm_cap, J.T,
+      fprintf(stderr, "jit kstats: nt=%d nbuf=%d hot=%d warm=%d tnb=%d srec=%d smem=%d cap=%llu | per warp (Mcycles): wait %.2f "
+              "classify %.2f shared %.2f cold %.2f | rows shared %llu cold %llu\n", J.nt, J.nbuf, J.hot_cap, J.warm_cap, tnb,
               J.srec, J.smem, (unsigned long long)cap, hk[0] / warps / 1e6, hk[1] / warps / 1e6, hk[2] / warps / 1e6,
               hk[3] / warps / 1e6, hk[4], hk[5]);
     } else if (kst) {
@@ -1035,9 +1055,10 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     if (rc) return bail(rc);
     // fixed-point range of the float sums: sample maximum with 8x headroom; partial sums of a
     // CTA (at most n / SMs values, with margin) must fit as well
-    int pbits = 2;
+    int pbits = 2, tbits = 2;
     while ((1LL << pbits) < cq.dq.n_rows / h->sm_count + 1) pbits++;
-    pmb_set_fx(cq.dq, sk.fx_expo, 3, pbits + 1);
+    while ((1LL << tbits) < cq.dq.n_rows + 1) tbits++;
+    pmb_set_fx(cq.dq, sk.fx_expo, 3, pbits + 1, tbits + 1);
     int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
     if (est <= 0) est = e;
     if (strategy == PMB_STRATEGY_AUTO) strategy = pmb_choose_strategy(h, cq, sk, est);

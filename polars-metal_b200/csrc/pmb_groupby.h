@@ -93,13 +93,13 @@ __device__ __forceinline__ void warp_set_bits(unsigned int* words, int64_t p, in
   }
 }
 
-// Correctly rounded double of the exact fixed-point sum (limbs l, fraction bits F, flags).
+// Correctly rounded double of the exact fixed-point sum (its two words l, fraction bits F, flags).
 __device__ __forceinline__ double fx_value(const unsigned long long* l, int F, unsigned flags) {
   if ((flags & PMB_FX_NAN) || ((flags & PMB_FX_PINF) && (flags & PMB_FX_NINF)))
     return __longlong_as_double(0x7FF8000000000000LL);
   if (flags & PMB_FX_PINF) return __longlong_as_double(0x7FF0000000000000LL);
   if (flags & PMB_FX_NINF) return __longlong_as_double((long long)0xFFF0000000000000ULL);
-  __int128 S = ((__int128)(long long)l[2] << 64) + ((__int128)l[1] << 32) + (__int128)l[0];
+  __int128 S = ((__int128)(long long)l[1] << 32) + (__int128)l[0];
   bool neg = S < 0;
   unsigned __int128 M = neg ? (unsigned __int128)(-S) : (unsigned __int128)S;
   unsigned long long hi = (unsigned long long)(M >> 64), lo = (unsigned long long)M;
@@ -132,7 +132,7 @@ __device__ __forceinline__ void finalize_agg(const DQuery& q, const DAggOut& A, 
     const DField& F = q.field[f];
     if (F.kind == F_SUM_FX) {
       const unsigned long long* l = reinterpret_cast<const unsigned long long*>(rec + F.off);
-      return fx_value(l, F.fx, *reinterpret_cast<const unsigned int*>(rec + F.off + 24));
+      return fx_value(l, F.fx, *reinterpret_cast<const unsigned int*>(rec + F.off + 16));
     }
     const double* p = reinterpret_cast<const double*>(rec + F.off);
     return p[0] + p[1];

@@ -25,12 +25,6 @@
 
 namespace {
 
-uint64_t next_pow2_u64(uint64_t x) {
-  uint64_t p = 1;
-  while (p < x) p <<= 1;
-  return p;
-}
-
 #include "pmb_jit_sources.inc"  // kDeviceHeader, kSkeleton (generated from the .cuh files by the build)
 
 // ---------------------------------------------------------------------------- NVRTC via dlopen
@@ -324,12 +318,11 @@ struct Gen {
         case F_SUM_FX: {
           std::string slot = std::to_string(F.fx_slot);
           b << "    double xv = (double)" << v(F.col) << ";\n    unsigned fl = pmb_fx_flag(xv);\n";
-          b << "    if (fl) atomicOr(" << at(F.off + 24, "unsigned int") << ", fl);\n";
-          b << "    else if (pmb_fx_in_range(xv, P.fx_e[" << slot << "])) {\n      unsigned long long a, b_, c;\n";
-          b << "      pmb_fx_split(xv, P.fx[" << slot << "], a, b_, c);\n";
-          b << "      if (a) atomicAdd(" << at(F.off, "unsigned long long") << ", a);\n";
-          b << "      if (b_) atomicAdd(" << at(F.off + 8, "unsigned long long") << ", b_);\n";
-          b << "      if (c) atomicAdd(" << at(F.off + 16, "unsigned long long") << ", c);\n    }\n";
+          b << "    if (fl) atomicOr(" << at(F.off + 16, "unsigned int") << ", fl);\n";
+          b << "    else if (pmb_fx_in_range(xv, P.fx_e[" << slot << "])) {\n      unsigned long long w0, w1;\n";
+          b << "      pmb_fx_words(xv, P.fx[" << slot << "], w0, w1);\n";
+          b << "      if (w0) atomicAdd(" << at(F.off, "unsigned long long") << ", w0);\n";
+          b << "      if (w1) atomicAdd(" << at(F.off + 8, "unsigned long long") << ", w1);\n    }\n";
           break;
         }
         case F_SUM_DD:
@@ -437,12 +430,13 @@ struct Gen {
             << "), x); }\n";
           break;
         case F_SUM_FX:
+          // the 96-bit partial P: its low 32 bits, and P >> 32 as a signed 64-bit word
           b << "  { unsigned fl = " << CU(so + 12) << "; if (fl) atomicOr(reinterpret_cast<unsigned int*>(d + "
-            << F.off + 24 << "), fl);\n";
-          b << "    unsigned w0 = " << CU(so) << ", w1 = " << CU(so + 4) << ", w2 = " << CU(so + 8) << ";\n";
+            << F.off + 16 << "), fl);\n";
+          b << "    unsigned w0 = " << CU(so) << ";\n    unsigned long long hi = ((unsigned long long)" << CU(so + 8)
+            << " << 32) | " << CU(so + 4) << ";\n";
           b << "    if (w0) atomicAdd(" << GU64(F.off) << ", (unsigned long long)w0);\n";
-          b << "    if (w1) atomicAdd(" << GU64(F.off + 8) << ", (unsigned long long)w1);\n";
-          b << "    if (w2) atomicAdd(" << GU64(F.off + 16) << ", (unsigned long long)(long long)(int)w2); }\n";
+          b << "    if (hi) atomicAdd(" << GU64(F.off + 8) << ", hi); }\n";
           break;
         case F_SUM_I:
           b << "  { unsigned long long x = ((unsigned long long)" << CU(so + 4) << " << 32) | " << CU(so)
@@ -500,7 +494,8 @@ struct Gen {
     for (int k = 0; k < q.n_keys; k++) kc[q.key[k].col] = true;
     o << "#define J_NT " << P.nt << "\n#define J_NBUF " << P.nbuf << "\n#define J_OFF_BARS " << P.off_bars
       << "\n#define J_OFF_BUF " << P.off_buf << "\n#define J_BUF_BYTES " << P.buf_bytes << "\n#define J_OFF_Q " << P.off_q
-      << "\n#define J_OFF_TKEYS " << P.off_tkeys << "\n#define J_OFF_TVAL " << P.off_tval << "\n#define J_T " << P.T
+      << "\n#define J_OFF_TKEYS " << P.off_tkeys << "\n#define J_OFF_TVAL " << P.off_tval << "\n#define J_TKEY " << P.tkey
+      << "\n#define J_TNB " << P.tnb
       << "\n#define J_OFF_SRECS " << P.off_srecs << "\n#define J_H " << P.hot_cap << "\n#define J_SW " << P.warm_cap
       << "\n#define J_SREC " << S.bytes << "\n#define J_SREC_WORDS " << S.bytes / 4 << "\n#define J_LEN_SOFF " << S.off[0]
       << "\n#define J_REC " << q.rec_bytes << "\n";
@@ -592,8 +587,7 @@ __device__ __forceinline__ long long j_fdiv_i(long long a, long long b, bool& ok
     // repeated, so that the high and the low bits both vary), the 64-bit finalizer otherwise
     if (q.key_bits <= 32)
       o << "__device__ __forceinline__ unsigned long long j_hash(unsigned long long k) {\n"
-           "  unsigned x = (unsigned)k;\n  x ^= x >> 16;\n  x *= 0x85ebca6bu;\n  x ^= x >> 13;\n  x *= 0xc2b2ae35u;\n"
-           "  x ^= x >> 16;\n  return ((unsigned long long)x << 32) | x;\n}\n";
+           "  const unsigned x = pmb_fmix32((unsigned)k);\n  return ((unsigned long long)x << 32) | x;\n}\n";
     else
       o << "__device__ __forceinline__ unsigned long long j_hash(unsigned long long k) { return pmb_fmix64(k); }\n";
     o << "__device__ __forceinline__ void j_shared(const JParams& P, unsigned char* rec, const JRow& r) {\n";
@@ -699,15 +693,18 @@ int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int m
     if (J->nbuf == 1) return pmb_fail(h, PMB_E_UNSUPPORTED, "query touches too many columns for the unit buffers");
     J->nbuf = 1;
   }
-  // hot keys: one record per warp each; warm keys: the largest count whose table and records fit
+  // hot keys: one record per warp each; warm keys: the largest count whose table and records fit.
+  // The sampled-key table: buckets of 4 keys and 4 16-bit values, filled to at most 80%.
+  J->tkey = q.key_bits <= 32 ? 4 : 8;
+  auto buckets = [](int keys) { return keys ? ((keys * 5 / 16 + 2) + 1) & ~1 : 0; };
+  auto tbytes = [&](int keys) { return buckets(keys) * 4 * (J->tkey + 2); };
   int hot = have_sketch ? 8 : 0;
   if (const char* e = getenv("PMB_HOT")) hot = std::max(0, std::min(atoi(e), 64));
-  while (hot > 0 && (int)pmb_align((size_t)used, 16) + 24 * 2 * hot + W * hot * J->srec > budget) hot /= 2;
+  while (hot > 0 && (int)pmb_align((size_t)used, 16) + tbytes(hot) + 32 + W * hot * J->srec > budget) hot /= 2;
   int warm = 0;
   if (have_sketch) {
-    for (int sw = 8192; sw >= 32; sw -= 32) {
-      int T = (int)next_pow2_u64((uint64_t)(2 * (hot + sw)));
-      int need = (int)pmb_align((size_t)used, 16) + 12 * T + 16 + (W * hot + sw) * J->srec;
+    for (int sw = 16384; sw >= 32; sw -= 32) {
+      int need = (int)pmb_align((size_t)used, 16) + tbytes(hot + sw) + 32 + (W * hot + sw) * J->srec;
       if (need <= budget) {
         warm = sw;
         break;
@@ -720,10 +717,10 @@ int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int m
   }
   J->hot_cap = hot;
   J->warm_cap = warm;
-  J->T = (hot + warm) ? (int)next_pow2_u64((uint64_t)(2 * (hot + warm))) : 0;
+  J->tnb = buckets(hot + warm);
   J->off_tkeys = (int)pmb_align((size_t)used, 16);
-  J->off_tval = J->off_tkeys + 8 * J->T;
-  J->off_srecs = (int)pmb_align((size_t)(J->off_tval + 4 * J->T), 16);
+  J->off_tval = J->off_tkeys + J->tnb * 4 * J->tkey;
+  J->off_srecs = (int)pmb_align((size_t)(J->off_tval + J->tnb * 8), 16);
   J->smem = J->off_srecs + (W * hot + warm) * J->srec;
   return PMB_OK;
 }
@@ -739,8 +736,11 @@ static bool jit_compile(const std::string& src, std::vector<char>& cubin, std::s
     log = "nvrtcCreateProgram failed";
     return false;
   }
-  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-diag-suppress=177"};
-  int rc = g_nv.compile(prog, 4, opts);
+  // PMB_JIT_DEBUG=2 also asks ptxas for its resource report (registers, spills, shared memory)
+  const char* dbg = getenv("PMB_JIT_DEBUG");
+  const bool verbose = dbg && dbg[0] == '2';
+  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-diag-suppress=177", "--ptxas-options=-v"};
+  int rc = g_nv.compile(prog, verbose ? 5 : 4, opts);
   size_t n = 0;
   g_nv.log_size(prog, &n);
   log.assign(n, '\0');
@@ -807,7 +807,11 @@ extern "C" int pmb_debug_jit_compile(const pmb_query* q, const pmb_column* cols,
       rc = pmb_plan_jit(&h, cq, true, 232448, &J);
       if (rc == PMB_OK) {
         std::vector<char> cubin;
-        if (!jit_compile(pmb_jit_source(cq, J), cubin, msg)) rc = PMB_E_UNSUPPORTED;
+        const std::string src = pmb_jit_source(cq, J);
+        if (const char* e = getenv("PMB_JIT_DEBUG"))
+          if (e[0] == '2') fprintf(stderr, "%s\n", src.c_str());  // the generated source, for inspection
+        if (!jit_compile(src, cubin, msg)) rc = PMB_E_UNSUPPORTED;
+        else if (getenv("PMB_JIT_DEBUG") && getenv("PMB_JIT_DEBUG")[0] == '2') fprintf(stderr, "%s\n", msg.c_str());
       } else {
         msg = h.err;
       }
@@ -823,8 +827,92 @@ extern "C" int pmb_debug_jit_compile(const pmb_query* q, const pmb_column* cols,
   return rc;
 }
 
+int pmb_jit_sampled_table(const CompiledQuery& cq, const JitPlan& J, const unsigned long long* hot, int n_hot,
+                          const unsigned long long* warm, int n_warm, std::vector<uint8_t>* out) {
+  out->clear();
+  const int n = n_hot + n_warm;
+  if (n == 0 || J.tnb == 0) return 0;
+  const bool narrow = J.tkey == 4;
+  // the kernel's key hash (j_hash) and the two candidate buckets
+  auto hash = [&](unsigned long long k) -> unsigned long long {
+    if (narrow) {
+      uint32_t x = pmb_fmix32((uint32_t)k);
+      return ((unsigned long long)x << 32) | x;
+    }
+    return pmb_fmix64(k);
+  };
+  std::vector<unsigned long long> keys;
+  std::vector<uint16_t> vals;
+  keys.reserve(n);
+  for (int i = 0; i < n_hot; i++) {
+    keys.push_back(hot[i]);
+    vals.push_back((uint16_t)(0x8000u | (unsigned)i));
+  }
+  for (int i = 0; i < n_warm; i++) {
+    keys.push_back(warm[i]);
+    vals.push_back((uint16_t)i);
+  }
+  // a marker key outside the sampled set for empty slots (its rows miss, as they should)
+  unsigned long long mark = narrow ? 0xFFFFFFFFull : PMB_EMPTY64;
+  {
+    std::vector<unsigned long long> sorted(keys);
+    std::sort(sorted.begin(), sorted.end());
+    while (std::binary_search(sorted.begin(), sorted.end(), mark)) mark--;
+  }
+  int nb = std::min(J.tnb, std::max(2, (((n * 5) / 16 + 2) + 1) & ~1));
+  std::vector<unsigned long long> tk;
+  std::vector<uint16_t> tv;
+  uint32_t rng = 0x9E3779B9u;
+  for (;;) {
+    tk.assign((size_t)nb * 4, mark);
+    tv.assign((size_t)nb * 4, 0xFFFFu);
+    int dropped = 0;
+    for (size_t i = 0; i < keys.size(); i++) {
+      unsigned long long k = keys[i];
+      uint16_t v = vals[i];
+      if (k == PMB_EMPTY64 || (narrow && k > 0xFFFFFFFFull)) continue;  // never looked up in the table
+      bool placed = false;
+      for (int step = 0; step < 512 && !placed; step++) {
+        const unsigned long long hk = hash(k);
+        const uint32_t a = (uint32_t)(hk >> 32), b = pmb_mix32b(a);
+        const uint32_t bk[2] = {(uint32_t)(((uint64_t)a * (uint32_t)nb) >> 32),
+                                (uint32_t)(((uint64_t)b * (uint32_t)nb) >> 32)};
+        for (int c = 0; c < 2 && !placed; c++)
+          for (int sl = 0; sl < 4; sl++)
+            if (tk[(size_t)bk[c] * 4 + sl] == mark) {
+              tk[(size_t)bk[c] * 4 + sl] = k;
+              tv[(size_t)bk[c] * 4 + sl] = v;
+              placed = true;
+              break;
+            }
+        if (placed) break;
+        // both buckets full: displace a random resident and re-insert it
+        rng = rng * 1664525u + 1013904223u;
+        const size_t at = (size_t)bk[(rng >> 16) & 1] * 4 + ((rng >> 20) & 3);
+        std::swap(k, tk[at]);
+        std::swap(v, tv[at]);
+      }
+      if (!placed) dropped++;  // the key left over is served by the global table
+    }
+    if (dropped == 0 || nb >= J.tnb) break;
+    nb = std::min(J.tnb, ((nb + nb / 8 + 2) + 1) & ~1);
+  }
+  const size_t kb = (size_t)nb * 4 * J.tkey, vb = (size_t)nb * 8;
+  out->assign(kb + vb, 0);
+  for (size_t i = 0; i < (size_t)nb * 4; i++) {
+    if (narrow) {
+      uint32_t k32 = (uint32_t)tk[i];
+      memcpy(out->data() + 4 * i, &k32, 4);
+    } else {
+      memcpy(out->data() + 8 * i, &tk[i], 8);
+    }
+  }
+  memcpy(out->data() + kb, tv.data(), vb);
+  return nb;
+}
+
 int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const JitPlan& J, const HashParams& P,
-                   int grid) {
+                   int grid, const uint8_t* ttab, int tnb) {
   JitParams A;
   memset(&A, 0, sizeof(A));
   for (int c = 0; c < cq.dq.n_cols; c++) {
@@ -844,6 +932,8 @@ int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const
   A.warm_keys = P.warm_keys;
   A.warm_n = P.warm_n;
   A.kstats = P.kstats;
+  A.ttab = ttab;
+  A.tnb = ttab ? tnb : 0;
   for (int i = 0; i < cq.dq.n_fields; i++)
     if (cq.dq.field[i].kind == F_SUM_FX) {
       A.fx[cq.dq.field[i].fx_slot] = cq.dq.field[i].fx;

@@ -20,6 +20,9 @@ struct JitParams {
   const unsigned long long* warm_keys;
   const unsigned int* warm_n;
   unsigned long long* kstats;
+  const uint8_t* ttab;
+  int tnb;
+  int tpad;
   int fx[8];
   int fx_e[8];
 };
@@ -34,7 +37,8 @@ struct JitPlan {
   int voff[16];       // column validity offset (-1: no bitmap)
   int hot_cap;        // hot keys
   int warm_cap;       // warm keys
-  int T;              // slots of the sampled-key table (power of two, 0 without sampled keys)
+  int tkey;           // bytes of a key in the sampled-key table (4 for keys of at most 32 bits, else 8)
+  int tnb;            // buckets of the sampled-key table (4 slots each; even), 0 without sampled keys
   int srec;           // bytes of a shared-memory record
   int off_bars, off_buf, off_q, off_tkeys, off_tval, off_srecs, smem;
 };
@@ -50,10 +54,18 @@ void pmb_jit_slayout(const DQuery& q, JitSLayout* S);
 
 int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int max_smem_optin, JitPlan* J);
 
+// Builds the sampled-key table of the run-time kernel on the host: a bucketed cuckoo table (two
+// candidate buckets of 4 slots per key) holding the hot keys (value 0x8000 | index) and the warm
+// keys (value index), laid out as keys of all buckets then 16-bit values. Keys that do not fit
+// are left out (their rows take the global table: slower, same results). Returns the bucket
+// count (even, at most J.tnb) and the bytes in `out`.
+int pmb_jit_sampled_table(const CompiledQuery& cq, const JitPlan& J, const unsigned long long* hot, int n_hot,
+                          const unsigned long long* warm, int n_warm, std::vector<uint8_t>* out);
+
 // JIT policy: PMB_JIT=0 never, PMB_JIT=1 always, otherwise inputs of at least 2M rows
 bool pmb_jit_enabled(int64_t n_rows);
 // compiled kernel for this signature and layout (cached); PMB_E_UNSUPPORTED when unavailable
 int pmb_jit_hash_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out);
 // launches over the global table and key lists set up in P (gkeys, grecs, gcap, status, lists)
 int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const JitPlan& J, const HashParams& P,
-                   int grid);
+                   int grid, const uint8_t* ttab, int tnb);

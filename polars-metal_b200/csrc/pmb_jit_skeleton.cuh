@@ -45,6 +45,9 @@ struct JParams {
   const unsigned long long* warm_keys;
   const unsigned int* warm_n;
   unsigned long long* kstats;
+  const unsigned char* ttab;  // sampled-key table built by the host: keys of all buckets, then values
+  int tnb;                    // its buckets (4 slots each), at most J_TNB
+  int tpad;
   int fx[8];    // fraction bits F of each exact float-sum slot (sums hold x * 2^F)
   int fx_e[8];  // every value of the slot satisfies |x| < 2^fx_e
 };
@@ -93,32 +96,33 @@ __device__ __forceinline__ long long j_gfind(const JParams& P, unsigned long lon
   return j_gresolve(P, key, h, claimed);
 }
 
-// the CTA's table of sampled keys: value of `key`, or J_MISS
-__device__ __forceinline__ unsigned j_tfind(const unsigned long long* tk, const unsigned* tv, unsigned long long key,
-                                            unsigned long long h) {
-  if (J_T == 0 || key == PMB_EMPTY64) return J_MISS;
-  int i = (int)((h >> 40) & (unsigned long long)(J_T - 1));
-  for (int p = 0; p < J_T; p++) {
-    unsigned long long k = tk[i];
-    if (k == key) return tv[i];
-    if (k == PMB_EMPTY64) return J_MISS;
-    i = (i + 1) & (J_T - 1);
-  }
-  return J_MISS;
+// The CTA's table of sampled keys (hot and warm), built by the host as a bucketed cuckoo table:
+// every key sits in one of its two 4-slot buckets, so a lookup is two bucket loads and no loop.
+// Empty slots hold a key outside the sampled set and the value 0xFFFF. Returns the key's value
+// (J_HOTBIT | hot index, or warm index) or J_MISS.
+__device__ __forceinline__ unsigned j_tvalue(unsigned short v) {
+  return v == 0xFFFFu ? J_MISS : ((v & 0x8000u) ? (J_HOTBIT | (v & 0x7FFFu)) : (unsigned)v);
 }
-
-__device__ __forceinline__ void j_tinsert(unsigned long long* tk, unsigned* tv, unsigned long long key,
-                                          unsigned long long h, unsigned v) {
-  int i = (int)((h >> 40) & (unsigned long long)(J_T - 1));
-  for (int p = 0; p < J_T; p++) {
-    unsigned long long old = atomicCAS(&tk[i], PMB_EMPTY64, key);
-    if (old == PMB_EMPTY64) {
-      tv[i] = v;
-      return;
-    }
-    if (old == key) return;
-    i = (i + 1) & (J_T - 1);
-  }
+__device__ __forceinline__ unsigned j_tfind(const unsigned char* tk, const unsigned short* tv, unsigned tnb,
+                                            unsigned long long key, unsigned long long h) {
+  if (tnb == 0u) return J_MISS;
+  const unsigned a = (unsigned)(h >> 32), b = pmb_mix32b(a);
+  const unsigned b1 = __umulhi(a, tnb), b2 = __umulhi(b, tnb);
+#if J_TKEY == 4
+  const unsigned k = (unsigned)key;
+  const uint4 x = reinterpret_cast<const uint4*>(tk)[b1], y = reinterpret_cast<const uint4*>(tk)[b2];
+  int s = x.x == k ? 0 : x.y == k ? 1 : x.z == k ? 2 : x.w == k ? 3 : -1;
+  if (s >= 0) return j_tvalue(tv[4 * b1 + s]);
+  s = y.x == k ? 0 : y.y == k ? 1 : y.z == k ? 2 : y.w == k ? 3 : -1;
+  return s >= 0 ? j_tvalue(tv[4 * b2 + s]) : J_MISS;
+#else
+  const ulonglong2* t = reinterpret_cast<const ulonglong2*>(tk);
+  const ulonglong2 x0 = t[2 * b1], x1 = t[2 * b1 + 1], y0 = t[2 * b2], y1 = t[2 * b2 + 1];
+  int s = x0.x == key ? 0 : x0.y == key ? 1 : x1.x == key ? 2 : x1.y == key ? 3 : -1;
+  if (s >= 0) return j_tvalue(tv[4 * b1 + s]);
+  s = y0.x == key ? 0 : y0.y == key ? 1 : y1.x == key ? 2 : y1.y == key ? 3 : -1;
+  return s >= 0 ? j_tvalue(tv[4 * b2 + s]) : J_MISS;
+#endif
 }
 
 __device__ __forceinline__ bool j_stop(const JParams& P) {
@@ -133,26 +137,27 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
   unsigned long long* bars = all_bars + warp * J_NBUF;
   unsigned char* bufs = sm + J_OFF_BUF + warp * J_NBUF * J_BUF_BYTES;
   unsigned* q = reinterpret_cast<unsigned*>(sm + J_OFF_Q) + warp * J_UNIT;
-  unsigned long long* tkeys = reinterpret_cast<unsigned long long*>(sm + J_OFF_TKEYS);
-  unsigned* tval = reinterpret_cast<unsigned*>(sm + J_OFF_TVAL);
+  unsigned char* tkeys = sm + J_OFF_TKEYS;
+  unsigned short* tval = reinterpret_cast<unsigned short*>(sm + J_OFF_TVAL);
+  const unsigned tnb = (unsigned)min(P.tnb, J_TNB);
   unsigned char* srecs = sm + J_OFF_SRECS;
   __shared__ unsigned s_claims;  // slots this CTA claimed in the global table (published per 64)
   const int n_hot = (J_H > 0 && P.hot_keys) ? (int)min(*P.hot_n, (unsigned)J_H) : 0;
   const int n_warm = (J_SW > 0 && P.warm_keys) ? (int)min(*P.warm_n, (unsigned)J_SW) : 0;
 
-  for (int i = tid; i < J_T; i += J_NT) tkeys[i] = PMB_EMPTY64;
+  // the sampled-key table: keys (tnb * 4 * J_TKEY bytes), then values (tnb * 8 bytes; tnb is even)
+  if (P.ttab) {
+    const uint4* src = reinterpret_cast<const uint4*>(P.ttab);
+    const int kw = (int)(tnb * 4u * J_TKEY / 16u), vw = (int)(tnb * 8u / 16u);
+    for (int i = tid; i < kw; i += J_NT) reinterpret_cast<uint4*>(tkeys)[i] = src[i];
+    for (int i = tid; i < vw; i += J_NT) reinterpret_cast<uint4*>(tval)[i] = src[kw + i];
+  }
   for (int w = tid; w < (W * J_H + J_SW) * J_SREC_WORDS; w += J_NT)
     reinterpret_cast<unsigned*>(srecs)[w] = J_SIDENT[w % J_SREC_WORDS];
   if (tid == 0) {
     s_claims = 0u;
     for (int b = 0; b < W * J_NBUF; b++) mbar_init(&all_bars[b], 1);
     mbar_fence_init();
-  }
-  __syncthreads();
-  for (int i = tid; i < n_hot + n_warm; i += J_NT) {
-    unsigned long long key = i < n_hot ? P.hot_keys[i] : P.warm_keys[i - n_hot];
-    if (key == PMB_EMPTY64) continue;  // that key always takes the global table's extra slot
-    j_tinsert(tkeys, tval, key, j_hash(key), i < n_hot ? (J_HOTBIT | (unsigned)i) : (unsigned)(i - n_hot));
   }
   __syncthreads();
 
@@ -220,7 +225,7 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
       ent[j] = 0u;
       if (keep) {
         const unsigned long long key = j_key(r);
-        const unsigned v = j_tfind(tkeys, tval, key, j_hash(key));
+        const unsigned v = j_tfind(tkeys, tval, P.ttab ? tnb : 0u, key, j_hash(key));
         if (v != J_MISS) {
           const unsigned rec = (v & J_HOTBIT) ? (unsigned)(warp * J_H) + (v & ~J_HOTBIT) : (unsigned)(W * J_H) + v;
           ent[j] = ((rec << 7) | (unsigned)lr) + 1u;

@@ -276,15 +276,17 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
     bool nullable = uc.validity != nullptr;
     o.in_dtype = (int8_t)dt;
     o.out_dtype = (int8_t)pmb_agg_out_dtype(A.op, dt);
-    int cnt = nullable ? field(F_CNT, c) : field(F_LEN, 0);
+    // the column's non-null count, created only for the aggregates that read it (count, mean, and
+    // integer min/max, whose identity value is also a valid value); sums and float min/max need none
+    auto cnt = [&]() { return (int16_t)(nullable ? field(F_CNT, c) : field(F_LEN, 0)); };
     switch (A.op) {
-      case PMB_AGG_COUNT: o.f_cnt = (int16_t)cnt; break;
+      case PMB_AGG_COUNT: o.f_cnt = cnt(); break;
       case PMB_AGG_SUM:
         o.f_main = (int16_t)field(pmb_is_float(dt) ? F_SUM_FX : F_SUM_I, c);
         break;
       case PMB_AGG_MEAN:
         o.f_main = (int16_t)field(pmb_is_float(dt) ? F_SUM_FX : F_SUM_I, c);
-        o.f_cnt = (int16_t)cnt;
+        o.f_cnt = cnt();
         break;
       default: {  // min / max
         bool mn = A.op == PMB_AGG_MIN;
@@ -292,20 +294,23 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
           o.f_main = (int16_t)field(mn ? F_MIN_F : F_MAX_F, c);
         } else if (pmb_is_signed(dt) || dt == PMB_BOOL) {
           o.f_main = (int16_t)field(mn ? F_MIN_I : F_MAX_I, c);
-          o.f_cnt = (int16_t)cnt;
+          o.f_cnt = cnt();
         } else {
           o.f_main = (int16_t)field(mn ? F_MIN_U : F_MAX_U, c);
-          o.f_cnt = (int16_t)cnt;
+          o.f_cnt = cnt();
         }
         break;
       }
     }
   }
   if (fields.size() > PMB_MAX_FIELDS) return pmb_fail(h, PMB_E_UNSUPPORTED, "too many aggregation state fields");
-  // record layout: 32-byte fields, then 16-, 8- and 4-byte ones
+  // record layout: 24-byte fields (exact float sums), then 16-, 8- and 4-byte ones, so every
+  // field stays aligned to its size (at most 8)
   int rec = 0;
+  static const int kSizes[4] = {24, 16, 8, 4};
+  size_t placed = 0;
   for (int pass = 0; pass < 4; pass++) {
-    int want = 32 >> pass;
+    int want = kSizes[pass];
     for (DField& f : fields) {
       uint64_t w0, w1;
       int nw, bytes;
@@ -313,8 +318,10 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
       if (bytes != want) continue;
       f.off = (int16_t)rec;
       rec += bytes;
+      placed++;
     }
   }
+  if (placed != fields.size()) return pmb_fail(h, PMB_E_CUDA, "internal: a record field has no layout slot");
   rec = (int)pmb_align((size_t)std::max(rec, 8), 8);
   // exact float sums: one range slot per column (fraction bits are set from the data sample)
   cq->fx_cols.clear();

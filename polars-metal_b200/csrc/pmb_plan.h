@@ -24,16 +24,19 @@ struct CompiledQuery {
 };
 
 // Fixed-point range of the exact float sums. Every value of a slot satisfies |x| < 2^E, E taken
-// from the largest biased exponent seen plus `headroom` powers of two; partial sums of up to
-// 2^partial_bits values must still split into limbs, so the fraction bits are
-// F = 94 - E - partial_bits (|x * 2^F| < 2^94).
-inline void pmb_set_fx(DQuery& q, const unsigned* max_expo, int headroom, int partial_bits) {
+// from the largest biased exponent seen plus `headroom` powers of two. The fraction bits F keep
+// two sums in range: a partial sum of up to 2^partial_bits values (a CTA's 96-bit shared-memory
+// accumulator: E + F + partial_bits <= 94) and the global table's signed high word, the sum of
+// all 2^total_bits values shifted right by 32 (E + F - 32 + total_bits <= 62).
+inline void pmb_set_fx(DQuery& q, const unsigned* max_expo, int headroom, int partial_bits, int total_bits) {
   for (int i = 0; i < q.n_fields; i++) {
     DField& f = q.field[i];
     if (f.kind != F_SUM_FX) continue;
     int e = (int)max_expo[f.fx_slot] - 1022 + headroom;
     q.fx_e[f.fx_slot] = (int16_t)e;
-    f.fx = (int16_t)(94 - e - partial_bits);
+    int F = 94 - e - partial_bits;
+    if (94 - e - total_bits < F) F = 94 - e - total_bits;
+    f.fx = (int16_t)F;
   }
 }
 
