@@ -58,54 +58,85 @@ def load_peaks() -> tuple[float, str]:
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """Samples SM clocks and throttle reasons while the timed region runs: NVML queries (read only)
+    every 10 ms in a thread, or nvidia-smi every 50 ms when NVML is not importable."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.samples = []
+        self.samples = []  # (sm_mhz, max_mhz, reasons)
         self._stop = threading.Event()
         self._proc = None
+        self._t = None
 
     def __enter__(self):
         try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            dev = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(dev, pynvml.NVML_CLOCK_SM)
+            reasons_of = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def loop():
+                while not self._stop.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(dev, pynvml.NVML_CLOCK_SM)
+                        bits = reasons_of(dev)
+                        self.samples.append((float(sm), float(mx),
+                                             {n for n, m in self.REASONS.items() if bits & m}))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.01)
+
+            self._t = threading.Thread(target=loop, daemon=True)
+            self._t.start()
+            return self
+        except Exception:
+            pass
+        try:
+            fields = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                      "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
             self._proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={fields}", "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+
+            def read():
+                names = ["hw_slowdown", "sw_thermal_slowdown", "hw_thermal_slowdown", "sw_power_cap"]
+                for line in self._proc.stdout:
+                    f = [x.strip() for x in line.split(",")]
+                    try:
+                        self.samples.append((float(f[0]), float(f[1]),
+                                             {n for n, v in zip(names, f[2:6]) if v.lower() == "active"}))
+                    except (ValueError, IndexError):
+                        continue
+
+            self._t = threading.Thread(target=read, daemon=True)
             self._t.start()
         except Exception:
             self._proc = None
         return self
 
-    def _read(self):
-        for line in self._proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
-
     def __exit__(self, *exc):
+        self._stop.set()
         if self._proc:
-            time.sleep(0.25)
+            time.sleep(0.1)
             self._proc.terminate()
             try:
                 self._proc.wait(timeout=5)
             except Exception:
                 self._proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for s in self.samples:
-            try:
-                sm.append(float(s[1]))
-                mx.append(float(s[2]))
-                for n, v in zip(names, s[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(n)
-            except (ValueError, IndexError):
-                continue
+        sm = [x[0] for x in self.samples]
+        mx = [x[1] for x in self.samples]
+        reasons = set()
+        for x in self.samples:
+            reasons |= x[2]
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
 

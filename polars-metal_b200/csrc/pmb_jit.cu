@@ -219,6 +219,20 @@ struct Gen {
         std::string t = "t" + std::to_string(op), f = "f" + std::to_string(op);
         switch (T.kind) {
           case T_CMP: {
+            // `x % c == 0` / `!= 0` with an integer literal c: whether the remainder is zero does
+            // not depend on the sign convention, so C's truncated remainder (a multiply-based
+            // divisibility test for a constant divisor) gives the floor-mod verdict; the divisor
+            // is not zero, so the remainder is valid exactly when x is
+            if (T.dtype != PMB_F64 && (T.op == PMB_CMP_EQ || T.op == PMB_CMP_NE) && T.lhs.arith == PMB_ARITH_MOD &&
+                T.lhs.b.col < 0 && T.lhs.b.i != 0 && T.lhs.b.i != -1 && T.rhs.arith < 0 && T.rhs.a.col < 0 &&
+                T.rhs.a.i == 0) {
+              auto x = leaf(T.lhs.a, T.dtype);
+              b << "    bool " << t << "v = " << x.second << ";\n";
+              b << "    bool " << t << "c = (" << x.first << " % " << lit_i64(T.lhs.b.i) << ") "
+                << (T.op == PMB_CMP_EQ ? "==" : "!=") << " 0LL;\n";
+              b << "    bool " << t << " = " << t << "v && " << t << "c, " << f << " = " << t << "v && !" << t << "c;\n";
+              break;
+            }
             auto l = operand(T.lhs, T.dtype, b);
             auto r = operand(T.rhs, T.dtype, b);
             const char* sym[] = {"==", "!=", "<", "<=", ">", ">="};

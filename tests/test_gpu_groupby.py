@@ -206,6 +206,27 @@ def test_predicates_kleene_not_isnull_arith():
         run_both(cols, ["k"], aggs, p, label=f"pred {i}")
 
 
+@pytest.mark.parametrize("jit", ["0", "1"])
+def test_remainder_zero_tests_on_both_kernels(jit, monkeypatch):
+    """`x % c == 0` / `!= 0` on negative x and divisors of both signs, on the prebuilt and the
+    run-time compiled kernel (the latter emits a divisibility test for these shapes)."""
+    monkeypatch.setenv("PMB_JIT", jit)
+    rng = np.random.default_rng(21)
+    n = 300_000
+    cols = {"k": (rng.integers(0, 500, n).astype(np.int32), None),
+            "y": (rng.integers(-10**12, 10**12, n).astype(np.int64), pack(rng.random(n) > 0.1)),
+            "x": (rng.standard_normal(n), pack(rng.random(n) > 0.05))}
+    cols["y"][0][:4] = [np.iinfo(np.int64).min, np.iinfo(np.int64).max, -7, 0]
+    col = lambda c: {"kind": "Column", "name": c}  # noqa: E731
+    aggs = [("Sum", "x", "s"), ("Count", "y", "c"), ("Min", "y", "lo"), ("Len", None, "n")]
+    for c in (7, -7, 3, 2, -1, 1000003):
+        for op in ("Eq", "Ne"):
+            p = {"kind": "Compare", "op": op, "dtype": "I64",
+                 "lhs": {"kind": "Arith", "op": "Mod", "lhs": col("y"), "rhs": {"kind": "LiteralI64", "value": c}},
+                 "rhs": {"kind": "LiteralI64", "value": 0}}
+            run_both(cols, ["k"], aggs, p, label=f"jit={jit} y % {c} {op} 0")
+
+
 def test_column_offsets_host_and_device():
     import torch
 

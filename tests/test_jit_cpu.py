@@ -103,6 +103,9 @@ def test_predicate_forms_compile():
         {"kind": "Compare", "op": "Eq", "dtype": "I64",
          "lhs": {"kind": "Arith", "op": "FloorDiv", "lhs": col("y"), "rhs": {"kind": "LiteralI64", "value": -(2 ** 63)}},
          "rhs": {"kind": "LiteralI64", "value": 3}},
+        {"kind": "Compare", "op": "Ne", "dtype": "I64",
+         "lhs": {"kind": "Arith", "op": "Mod", "lhs": col("y"), "rhs": {"kind": "LiteralI64", "value": -(2 ** 63)}},
+         "rhs": {"kind": "LiteralI64", "value": 0}},
         {"kind": "LiteralBool", "value": True},
     ]
     for p in preds:
