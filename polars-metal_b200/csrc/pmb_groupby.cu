@@ -1062,8 +1062,8 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
     if (est <= 0) est = e;
     if (strategy == PMB_STRATEGY_AUTO) strategy = pmb_choose_strategy(h, cq, sk, est);
-    if (strategy == PMB_STRATEGY_SORT) strategy = PMB_STRATEGY_GLOBAL_HASH;  // sort path: see pmb_sort.cu
-    rc = pmb_groupby_hash(h, cq, q, strategy, est, have_sk ? &sk : nullptr, r);
+    if (strategy == PMB_STRATEGY_SORT) rc = pmb_groupby_sort(h, cq, r);
+    else rc = pmb_groupby_hash(h, cq, q, strategy, est, have_sk ? &sk : nullptr, r);
     if (rc) return bail(rc);
   }
   rc = pmb_finish_outputs(h, r, q->output_on_device == 0);

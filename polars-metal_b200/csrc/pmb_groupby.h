@@ -80,6 +80,9 @@ int pmb_plan_hash(pmb_handle* h, int max_smem_optin, CompiledQuery& cq, int stra
                   HashParams& P, int& nt, int& smem);
 int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
                      const SketchOut* sk, pmb_result* r);
+// sort strategy (pmb_sort.cu): packed-key LSD radix sort + segmented reduce; groups come out in
+// packed-key order
+int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r);
 
 // Sets bit p of a bitmap for every lane whose `bit` is true. The warp's positions are
 // consecutive from p_first, so they touch at most two 32-bit words: one atomicOr each.

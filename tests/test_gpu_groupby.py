@@ -14,7 +14,7 @@ from polars_b200._native import ColumnData, groupby
 
 pytestmark = pytest.mark.gpu
 GOLD = load_golden()
-STRATEGIES = ["auto", "smem_hash", "global_hash"]
+STRATEGIES = ["auto", "smem_hash", "global_hash", "sort"]
 
 
 def _product_cols(cols: dict) -> dict:
@@ -79,11 +79,37 @@ def test_hash_workload_device_resident_inputs():
     assert_results_match(as_dict(got), want, 1, t.aggs, "device inputs")
 
 
-def test_sort_workload_shape_parity():
-    # two-column key (int64 + int32): 96 data bits -> the 128-bit key table
+@pytest.mark.parametrize("strategy", ["auto", "sort"])
+def test_sort_workload_shape_parity(strategy):
+    # two-column key (int64 + int32): 96 data bits -> the 128-bit key table, or 20 + 6 packed bits
+    # for the sort
     t = datagen.make_sort(2_000_000, seed=7, pool=20_000)
     cols = datagen.to_numpy_columns(t)
-    run_both(cols, t.keys, t.aggs, None, "auto", "two-key")
+    got = run_both(cols, t.keys, t.aggs, None, strategy, f"two-key {strategy}")
+    if strategy == "sort":
+        assert got.strategy == "sort"
+
+
+def test_sort_two_word_keys_big_groups_and_filter():
+    rng = np.random.default_rng(31)
+    n = 400_000
+    # full-range int64 + int32 keys: more than 64 packed bits (two-word sort keys)
+    k1 = rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, 3000, dtype=np.int64)[rng.integers(0, 3000, n)]
+    k2 = rng.integers(-2**31, 2**31 - 1, 50, dtype=np.int64).astype(np.int32)[rng.integers(0, 50, n)]
+    cols = {"a": (k1, pack(rng.random(n) > 0.02)), "b": (k2, None),
+            "v": (rng.standard_normal(n), pack(rng.random(n) > 0.1)),
+            "w": (rng.integers(-10**6, 10**6, n).astype(np.int64), None)}
+    aggs = [("Sum", "v", "s"), ("Mean", "v", "m"), ("Min", "w", "mn"), ("Max", "v", "mx"), ("Count", "v", "c"),
+            ("Len", None, "n")]
+    run_both(cols, ["a", "b"], aggs, None, "sort", "two-word keys")
+    # a few very large groups (one CTA per group beyond 256 rows) mixed with singletons
+    g = np.where(rng.random(n) < 0.5, rng.integers(0, 4, n), rng.integers(1000, 10**9, n)).astype(np.int64)
+    cols2 = {"g": (g, None), "v": (rng.standard_normal(n), pack(rng.random(n) > 0.1)),
+             "w": (rng.integers(-100, 100, n).astype(np.int32), None)}
+    pred = {"kind": "Compare", "op": "Gt", "lhs": {"kind": "Column", "name": "v"},
+            "rhs": {"kind": "LiteralF64", "value": -0.3}}
+    got = run_both(cols2, ["g"], aggs[:1] + [("Min", "w", "mn"), ("Len", None, "n")], pred, "sort", "big groups")
+    assert got.strategy == "sort"
 
 
 def test_empty_input():
@@ -117,8 +143,9 @@ def test_ragged_sizes(n):
 KEY_DTYPES = ["int8", "int16", "int32", "int64", "uint8", "uint16", "uint32", "uint64", "float32", "float64"]
 
 
+@pytest.mark.parametrize("strategy", ["auto", "sort"])
 @pytest.mark.parametrize("kdt", KEY_DTYPES)
-def test_key_dtypes(kdt):
+def test_key_dtypes(kdt, strategy):
     rng = np.random.default_rng(3)
     n = 50_000
     k = rng.integers(0, 100, n).astype(kdt)
@@ -127,14 +154,15 @@ def test_key_dtypes(kdt):
         k[::89] = -0.0
     cols = {"k": (k, pack(rng.random(n) > 0.05)), "v": (rng.standard_normal(n).astype(np.float32), None)}
     run_both(cols, ["k"], [("Sum", "v", "s"), ("Min", "v", "mn"), ("Max", "v", "mx"), ("Len", None, "n")],
-             label=f"key {kdt}")
+             strategy=strategy, label=f"key {kdt} {strategy}")
 
 
 VALUE_DTYPES = ["int8", "int16", "int32", "int64", "uint8", "uint16", "uint32", "uint64", "float32", "float64"]
 
 
+@pytest.mark.parametrize("strategy", ["auto", "sort"])
 @pytest.mark.parametrize("vdt", VALUE_DTYPES)
-def test_value_dtypes(vdt):
+def test_value_dtypes(vdt, strategy):
     rng = np.random.default_rng(4)
     n = 60_000
     if vdt.startswith("float"):
@@ -146,17 +174,19 @@ def test_value_dtypes(vdt):
         v = rng.integers(info.min, info.max, n, dtype=vdt, endpoint=True)
     cols = {"k": (rng.integers(0, 300, n).astype(np.int64), None), "v": (v, pack(rng.random(n) > 0.1))}
     aggs = [("Sum", "v", "s"), ("Mean", "v", "m"), ("Min", "v", "mn"), ("Max", "v", "mx"), ("Count", "v", "c")]
-    run_both(cols, ["k"], aggs, label=f"values {vdt}")
+    run_both(cols, ["k"], aggs, strategy=strategy, label=f"values {vdt} {strategy}")
 
 
-def test_multi_key_with_nulls_and_bool():
+@pytest.mark.parametrize("strategy", ["auto", "sort"])
+def test_multi_key_with_nulls_and_bool(strategy):
     rng = np.random.default_rng(8)
     n = 100_000
     cols = {"a": (rng.integers(0, 5, n).astype(np.int64), pack(rng.random(n) > 0.1)),
             "b": (pack(rng.random(n) > 0.5), pack(rng.random(n) > 0.2), A.BOOL, n),
             "c": (rng.integers(-3, 3, n).astype(np.int16), None),
             "v": (rng.standard_normal(n), None)}
-    run_both(cols, ["a", "b", "c"], [("Sum", "v", "s"), ("Len", None, "n")], label="multi-key")
+    run_both(cols, ["a", "b", "c"], [("Sum", "v", "s"), ("Len", None, "n")], strategy=strategy,
+             label=f"multi-key {strategy}")
 
 
 def test_high_cardinality_rehash():
