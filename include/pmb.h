@@ -201,6 +201,42 @@ int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb_column* co
 
 void pmb_result_free(pmb_result* r);
 
+/* ---- learned strategy selection ----
+ * No counterpart in the reference, whose routing is a row-count threshold and an estimated-
+ * cardinality gate (crates/polars-metal-core/src/router/cost.rs:35-52,
+ * crates/polars-metal-kernels/src/groupby.rs:475-486). A query's features are computed on the
+ * device from a 4096-row sample of its keys (HyperLogLog registers, hash-bucket occupancy, null
+ * and filter fractions, sample frequency profile, key width); an MLP (PMB_SELECTOR_FEATURES ->
+ * 64 -> 64 -> 4, fp32) maps them to three strategy scores (shared-memory hash, global hash, sort)
+ * and log2 of the group count, which sizes the hash table. Without installed parameters, or for
+ * a non-finite output, the plain cardinality heuristic decides. The strategy never changes a
+ * result: every strategy is exact, and an undersized table is rebuilt larger. */
+#define PMB_SELECTOR_FEATURES 24
+#define PMB_SELECTOR_HIDDEN 64
+#define PMB_SELECTOR_OUTPUTS 4
+/* parameter count: W1[64][24] b1[64] W2[64][64] b2[64] W3[4][64] b3[4], in that order */
+#define PMB_SELECTOR_PARAMS                                                                   \
+  (PMB_SELECTOR_HIDDEN * PMB_SELECTOR_FEATURES + PMB_SELECTOR_HIDDEN +                       \
+   PMB_SELECTOR_HIDDEN * PMB_SELECTOR_HIDDEN + PMB_SELECTOR_HIDDEN +                         \
+   PMB_SELECTOR_OUTPUTS * PMB_SELECTOR_HIDDEN + PMB_SELECTOR_OUTPUTS)
+
+/* Features of a group-by query (filter applied) into `out` (host, PMB_SELECTOR_FEATURES floats). */
+int pmb_selector_features(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols, float* out);
+/* Installs selector parameters (host, PMB_SELECTOR_PARAMS floats) on the handle; NULL removes them. */
+int pmb_selector_set(pmb_handle* h, const float* params, int32_t n_params);
+/* The strategy and group count the handle's AUTO strategy would use for this query. */
+int pmb_selector_choose(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols,
+                        int32_t* strategy, int64_t* groups);
+/* MLP kernels on device buffers (params, features x[batch][24], outputs out[batch][4]). */
+int pmb_mlp_forward(pmb_handle* h, const float* params, const float* x, int32_t batch, float* out);
+/* Gradient of the mean loss over the batch, sum_b sw[b] * (CE(softmax(out[b][0:3]), cls[b]) +
+ * wreg * (out[b][3] - y[b])^2) / batch (sw may be NULL for all ones), into grad (overwritten),
+ * and that loss into *loss (device float). */
+int pmb_mlp_gradient(pmb_handle* h, const float* params, const float* x, const int32_t* cls, const float* y,
+                     const float* sw, int32_t batch, float wreg, float* grad, float* loss);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8; `step` counts from 1) on device buffers. */
+int pmb_mlp_adam_step(pmb_handle* h, float* params, const float* grad, float* m, float* v, int32_t step, float lr);
+
 /* ---- the operator surface on the filter side ---- */
 
 /* Null-aware comparison -> bit-packed (data, validity); rhs == NULL compares with the scalar

@@ -1060,8 +1060,21 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     while ((1LL << tbits) < cq.dq.n_rows + 1) tbits++;
     pmb_set_fx(cq.dq, sk.fx_expo, 3, pbits + 1, tbits + 1);
     int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
+    if (strategy == PMB_STRATEGY_AUTO) {
+      // the learned selector when installed, else the plain cardinality heuristic. The predicted
+      // group count can only enlarge the table: an undersized table costs a rebuild, an oversized
+      // one only its initialisation
+      int s = 0;
+      int64_t g = 0;
+      if (pmb_selector_pick(h, cq, &s, &g)) {
+        strategy = s;
+        if (est <= 0) est = std::max<int64_t>(e, std::min<int64_t>(g, cq.dq.n_rows));
+      } else {
+        if (est <= 0) est = e;
+        strategy = pmb_choose_strategy(h, cq, sk, est);
+      }
+    }
     if (est <= 0) est = e;
-    if (strategy == PMB_STRATEGY_AUTO) strategy = pmb_choose_strategy(h, cq, sk, est);
     if (strategy == PMB_STRATEGY_SORT) rc = pmb_groupby_sort(h, cq, r);
     else rc = pmb_groupby_hash(h, cq, q, strategy, est, have_sk ? &sk : nullptr, r);
     if (rc) return bail(rc);

@@ -83,6 +83,9 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
 // sort strategy (pmb_sort.cu): packed-key LSD radix sort + segmented reduce; groups come out in
 // packed-key order
 int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r);
+// learned selector (pmb_learned.cu): strategy and group count for AUTO; false when no selector is
+// installed or its output is unusable
+bool pmb_selector_pick(pmb_handle* h, const CompiledQuery& cq, int* strategy, int64_t* groups);
 
 // Sets bit p of a bitmap for every lane whose `bit` is true. The warp's positions are
 // consecutive from p_first, so they touch at most two 32-bit words: one atomicOr each.

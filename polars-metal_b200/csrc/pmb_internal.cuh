@@ -183,6 +183,8 @@ struct pmb_handle {
   size_t event_next = 0;
   cudaEvent_t call_start = nullptr, call_stop = nullptr;
   pmb_stats last_stats{};
+  // strategy selector: MLP parameters on the device (nullptr: the cardinality heuristic decides)
+  float* selector = nullptr;
   int32_t launches = 0;
   int64_t h2d = 0, d2h = 0;
 };

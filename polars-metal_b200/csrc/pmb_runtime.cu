@@ -334,6 +334,7 @@ void pmb_close(pmb_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   ws_free_all(h);
   if (h->pinned) cudaFreeHost(h->pinned);
+  if (h->selector) cudaFree(h->selector);
   for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
   if (h->call_start) cudaEventDestroy(h->call_start);
   if (h->call_stop) cudaEventDestroy(h->call_stop);

@@ -258,18 +258,17 @@ __global__ void __launch_bounds__(ST_NT) k_sort_pass(const __grid_constant__ Pas
   const long long tile = s_tile;
   const int64_t base = tile * ST_TILE;
   const unsigned lt = (1u << lane) - 1u;
-  // warp-striped items: warp w owns tile elements [w*512, w*512+512), item j of lane l is w*512 + j*32 + l
-  PKey<W> key[ST_PER];
-  unsigned int ix[ST_PER];
+  // warp-striped items: warp w owns tile elements [w*512, w*512+512), item j of lane l is
+  // w*512 + j*32 + l. Only the digit and the rank stay in registers; the keys are read again (from
+  // L2) when the tile is reordered in shared memory.
   unsigned int rank[ST_PER];
   unsigned short dg[ST_PER];
 #pragma unroll
   for (int j = 0; j < ST_PER; j++) {
     const int64_t e = base + warp * (ST_PER * 32) + j * 32 + lane;
-    const bool ok = e < P.n;
-    for (int i = 0; i < W; i++) key[j].w[i] = ok ? P.kin[(uint64_t)i * P.cap + e] : 0ULL;
-    ix[j] = ok ? P.iin[e] : 0u;
-    dg[j] = ok ? (unsigned short)digit_of<W>(key[j], P.shift) : (unsigned short)RADIX;
+    PKey<W> k;
+    for (int i = 0; i < W; i++) k.w[i] = e < P.n ? P.kin[(uint64_t)i * P.cap + e] : 0ULL;
+    dg[j] = e < P.n ? (unsigned short)digit_of<W>(k, P.shift) : (unsigned short)RADIX;
   }
   // ranks within the warp, in item order (stable): lanes with the same digit in one round are
   // ordered by lane; earlier rounds come first
@@ -346,9 +345,10 @@ __global__ void __launch_bounds__(ST_NT) k_sort_pass(const __grid_constant__ Pas
   for (int j = 0; j < ST_PER; j++) {
     const unsigned d = dg[j];
     if (d < RADIX) {
+      const int64_t e = base + warp * (ST_PER * 32) + j * 32 + lane;
       const unsigned lp = s_excl[d] + s_whist[warp][d] + rank[j];
-      for (int i = 0; i < W; i++) s_key[i * ST_TILE + lp] = key[j].w[i];
-      s_idx[lp] = ix[j];
+      for (int i = 0; i < W; i++) s_key[i * ST_TILE + lp] = P.kin[(uint64_t)i * P.cap + e];
+      s_idx[lp] = P.iin[e];
     }
   }
   __syncthreads();
@@ -494,11 +494,11 @@ __device__ __forceinline__ void write_group(const ReduceParams& R, int64_t p, in
   }
 }
 
-template <int W>
+template <int W, int RW>
 __global__ void __launch_bounds__(ST_NT) k_seg_reduce(const __grid_constant__ ReduceParams R) {
   const int64_t ng = (int64_t)*R.n_groups;
   const TileCtx t{nullptr, nullptr, nullptr, 0};
-  uint64_t recw[48];
+  uint64_t recw[RW];  // the group record, RW >= rec_bytes / 8
   uint8_t* rec = reinterpret_cast<uint8_t*>(recw);
   const int rw = R.q.rec_bytes / 8;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -696,7 +696,9 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
     PMB_CUDA(h, cudaMemsetAsync(status, 0, 64, h->stream));
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)ng + ST_NT - 1) / ST_NT, (int64_t)h->sm_count * 16));
     pmb_kernel_begin(h, "seg_reduce");
-    k_seg_reduce<W><<<blocks, ST_NT, 0, h->stream>>>(R);
+    if (q.rec_bytes <= 96) k_seg_reduce<W, 12><<<blocks, ST_NT, 0, h->stream>>>(R);
+    else if (q.rec_bytes <= 192) k_seg_reduce<W, 24><<<blocks, ST_NT, 0, h->stream>>>(R);
+    else k_seg_reduce<W, 48><<<blocks, ST_NT, 0, h->stream>>>(R);
     pmb_kernel_end(h);
     PMB_CUDA(h, cudaGetLastError());
     const size_t big_smem = (size_t)BIG_NT * q.rec_bytes;

@@ -177,7 +177,23 @@ SIGNATURES = {
                                           C.POINTER(C.POINTER(Result))]),
     "pmb_cumsum_u8_to_u32": (C.c_int, [_H, _P, _P, C.c_int64, C.c_int32]),
     "pmb_cumsum_u8_to_u32_noalloc": (C.c_int, [_P, _P, C.c_int64, _P]),
+    "pmb_selector_features": (C.c_int, [_H, C.POINTER(Query), C.POINTER(Column), C.c_int32, _P]),
+    "pmb_selector_set": (C.c_int, [_H, _P, C.c_int32]),
+    "pmb_selector_choose": (C.c_int, [_H, C.POINTER(Query), C.POINTER(Column), C.c_int32, C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_int64)]),
+    "pmb_mlp_forward": (C.c_int, [_H, _P, _P, C.c_int32, _P]),
+    "pmb_mlp_gradient": (C.c_int, [_H, _P, _P, _P, _P, _P, C.c_int32, C.c_float, _P, _P]),
+    "pmb_mlp_adam_step": (C.c_int, [_H, _P, _P, _P, _P, C.c_int32, C.c_float]),
 }
+
+# learned strategy selector (include/pmb.h)
+SELECTOR_FEATURES = 24
+SELECTOR_HIDDEN = 64
+SELECTOR_OUTPUTS = 4
+SELECTOR_PARAMS = (SELECTOR_HIDDEN * SELECTOR_FEATURES + SELECTOR_HIDDEN + SELECTOR_HIDDEN * SELECTOR_HIDDEN
+                   + SELECTOR_HIDDEN + SELECTOR_OUTPUTS * SELECTOR_HIDDEN + SELECTOR_OUTPUTS)
+# strategy index of the selector's scores
+SELECTOR_STRATEGIES = ["smem_hash", "global_hash", "sort"]
 
 # largest n of pmb_cumsum_u8_to_u32_noalloc (its fixed scratch array)
 NOALLOC_MAX_ROWS = 1 << 27

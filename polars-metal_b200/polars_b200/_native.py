@@ -35,15 +35,33 @@ _ERRORS = {
 
 
 class Handle:
-    """One device context: a CUDA stream plus a growable device workspace (libpmb handle)."""
+    """One device context: a CUDA stream plus a growable device workspace (libpmb handle).
 
-    def __init__(self, device: int = 0, workspace_bytes: int = 0):
+    selector: "default" installs the strategy-selector parameters shipped with the package (when
+    present), None leaves the AUTO strategy to the plain cardinality heuristic, or a float array
+    of SELECTOR_PARAMS parameters."""
+
+    def __init__(self, device: int = 0, workspace_bytes: int = 0, selector: Any = "default"):
         self._lib = A.lib()
         self._h = C.c_void_p()
         rc = self._lib.pmb_open(C.byref(self._h), device, workspace_bytes)
         if rc != A.PMB_OK:
             raise _ERRORS.get(rc, RuntimeError)(f"polars_b200: pmb_open failed with status {rc}")
         self.device = device
+        if isinstance(selector, str) and selector == "default":
+            from .selector import default_params
+
+            selector = default_params()
+        if selector is not None:
+            self.set_selector(selector)
+
+    def set_selector(self, params: Any) -> None:
+        """Installs MLP parameters for the AUTO strategy (None: the cardinality heuristic)."""
+        if params is None:
+            self.check(self._lib.pmb_selector_set(self._h, None, 0))
+            return
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float32).ravel())
+        self.check(self._lib.pmb_selector_set(self._h, p.ctypes.data, p.size))
 
     @property
     def raw(self) -> C.c_void_p:
@@ -345,6 +363,90 @@ def groupby(
     finally:
         h._lib.pmb_result_free(res_p)
         del keep, expr_keep
+
+
+def _query(columns, keys, aggs, predicate):
+    names = list(columns)
+    index = {n: i for i, n in enumerate(names)}
+    cols = [c if isinstance(c, ColumnData) else ColumnData(c) for c in columns.values()]
+    for k in keys:
+        if k not in index:
+            raise KeyError(f"polars_b200: key column {k!r} not found in upstream columns")
+    key_arr = (C.c_int32 * max(1, len(keys)))(*[index[k] for k in keys])
+    agg_arr = (A.Agg * max(1, len(aggs)))()
+    for i, (op, col, _alias) in enumerate(aggs):
+        if op not in A.AGG_OPS:
+            raise ValueError(f"polars_b200: unknown aggregation op {op!r}")
+        agg_arr[i].op = A.AGG_OPS[op]
+        if op == "Len":
+            agg_arr[i].column = -1
+        else:
+            if col not in index:
+                raise KeyError(f"polars_b200: agg input column {col!r} not found in upstream columns")
+            agg_arr[i].column = index[col]
+    expr, expr_keep = compile_predicate(predicate, index)
+    q = A.Query()
+    q.key_columns = key_arr
+    q.n_keys = len(keys)
+    q.aggs = agg_arr
+    q.n_aggs = len(aggs)
+    q.predicate = C.pointer(expr) if expr is not None else None
+    abi_cols, keep = _to_abi_columns(cols)
+    return q, abi_cols, len(cols), (keep, expr_keep, key_arr, agg_arr, expr)
+
+
+def selector_features(columns, keys, aggs, predicate=None, handle: Handle | None = None) -> np.ndarray:
+    """The learned selector's features of a query (PMB_SELECTOR_FEATURES floats), computed on the
+    device from a 4096-row sample of its keys."""
+    h = handle or default_handle()
+    q, cols, n, keep = _query(columns, keys, aggs, predicate)
+    out = np.zeros(A.SELECTOR_FEATURES, dtype=np.float32)
+    h.check(h._lib.pmb_selector_features(h.raw, C.byref(q), cols, n, out.ctypes.data))
+    del keep
+    return out
+
+
+def selector_choose(columns, keys, aggs, predicate=None, handle: Handle | None = None) -> tuple[str, int]:
+    """The strategy and group count the AUTO strategy of `handle` would use for this query."""
+    h = handle or default_handle()
+    q, cols, n, keep = _query(columns, keys, aggs, predicate)
+    s, g = C.c_int32(), C.c_int64()
+    h.check(h._lib.pmb_selector_choose(h.raw, C.byref(q), cols, n, C.byref(s), C.byref(g)))
+    del keep
+    return A.STRATEGY_NAMES.get(s.value, str(s.value)), int(g.value)
+
+
+def _dev_ptr(t) -> int:
+    assert t.is_cuda and t.is_contiguous(), "expected a contiguous CUDA tensor"
+    return t.data_ptr()
+
+
+def mlp_forward(params, x, handle: Handle | None = None):
+    """Selector MLP outputs [batch, 4] for features x [batch, 24] (CUDA float32 tensors)."""
+    import torch
+
+    h = handle or default_handle()
+    out = torch.empty((x.shape[0], A.SELECTOR_OUTPUTS), dtype=torch.float32, device=x.device)
+    h.check(h._lib.pmb_mlp_forward(h.raw, _dev_ptr(params), _dev_ptr(x), x.shape[0], _dev_ptr(out)))
+    return out
+
+
+def mlp_gradient(params, x, cls, y, sw=None, wreg: float = 0.25, handle: Handle | None = None):
+    """(gradient, loss) of the selector loss on a batch (CUDA tensors; cls int32, others float32)."""
+    import torch
+
+    h = handle or default_handle()
+    grad = torch.empty_like(params)
+    loss = torch.empty(1, dtype=torch.float32, device=params.device)
+    h.check(h._lib.pmb_mlp_gradient(h.raw, _dev_ptr(params), _dev_ptr(x), _dev_ptr(cls), _dev_ptr(y),
+                                    _dev_ptr(sw) if sw is not None else None, x.shape[0], wreg, _dev_ptr(grad),
+                                    _dev_ptr(loss)))
+    return grad, float(loss.item())
+
+
+def mlp_adam_step(params, grad, m, v, step: int, lr: float, handle: Handle | None = None) -> None:
+    h = handle or default_handle()
+    h.check(h._lib.pmb_mlp_adam_step(h.raw, _dev_ptr(params), _dev_ptr(grad), _dev_ptr(m), _dev_ptr(v), step, lr))
 
 
 # ------------------------------------------------------------------------------- wire format

@@ -1,0 +1,57 @@
+"""The learned strategy selector on the CPU: the numpy statement of the MLP (the oracle of the
+device kernels) against finite differences, and the shipped network's gain over the plain
+cardinality heuristic, replayed on held-out tables whose strategy times the engine measured."""
+
+import numpy as np
+import pytest
+
+from oracle import mlp
+from polars_b200 import _abi as A
+from polars_b200 import selector as S
+
+
+def test_parameter_layout_matches_header():
+    assert mlp.N_PARAMS == A.SELECTOR_PARAMS
+    assert (mlp.NF, mlp.NH, mlp.NO) == (A.SELECTOR_FEATURES, A.SELECTOR_HIDDEN, A.SELECTOR_OUTPUTS)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    p = S.init_params(3).astype(np.float64)
+    X = rng.random((16, mlp.NF))
+    cls = rng.integers(0, 3, 16)
+    y = rng.random(16) * 20
+    sw = rng.random(16) + 0.5
+    loss, g = mlp.loss_and_grad(p, X, cls, y, sw, wreg=0.1)
+    idx = rng.choice(p.size, 200, replace=False)
+    eps = 1e-6
+    for i in idx:
+        d = np.zeros_like(p)
+        d[i] = eps
+        lp, _ = mlp.loss_and_grad(p + d, X, cls, y, sw, wreg=0.1)
+        lm, _ = mlp.loss_and_grad(p - d, X, cls, y, sw, wreg=0.1)
+        num = (lp - lm) / (2 * eps)
+        assert abs(num - g[i]) <= 1e-6 + 1e-5 * abs(num), (i, num, g[i])
+
+
+def test_labels_pick_the_fastest_strategy():
+    T = np.array([[3.0, 1.0, 2.0], [1.0, 5.0, 9.0]])
+    cls, sw, y = S.labels(T, np.array([7, 1]))
+    assert list(cls) == [1, 0] and sw[0] == 3.0 and sw[1] == 9.0 and y[0] == pytest.approx(np.log2(7))
+
+
+@pytest.mark.skipif(not (S.DATASET_FILE.exists() and S.PARAMS_FILE.exists()), reason="no shipped selector")
+def test_shipped_selector_gains_over_the_heuristic_on_held_out_tables():
+    d = np.load(S.DATASET_FILE)
+    p = S.default_params()
+    assert p is not None and p.size == A.SELECTOR_PARAMS
+    tr, te = S.split(d["X"].shape[0])
+    out = mlp.forward(p, d["X"][te])
+    rep = S.evaluate(np.argmax(out[:, :3], axis=1), d["T"][te], d["H"][te])
+    print(rep)
+    # never slower than the heuristic in total, and most of the way to the best pick per table
+    assert rep["gain_vs_heuristic"] >= 1.0
+    assert rep["learned_vs_best"] <= 1.25
+    # the size prediction: log2(groups) within 1.5 on most held-out tables
+    err = np.abs(out[:, 3] - np.log2(np.maximum(d["G"][te], 1)))
+    assert np.median(err) < 1.5
