@@ -194,8 +194,14 @@ int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32
                 pmb_result** out);
 
 /* Many independent queries in one persistent launch over a device work queue.
- * No reference counterpart (new batching layer); each query follows pmb_groupby's
- * semantics. cols[i] holds n_cols[i] columns of query i. */
+ * No reference counterpart (new batching layer); each query follows pmb_groupby's semantics and
+ * results. cols[i] holds n_cols[i] columns of query i; outs[i] receives query i's result.
+ * Two or more queries of one signature (same column dtypes and nullability, keys, aggregates and
+ * filter; keys of at most 64 packed bits; strategy AUTO, no capacity hint) run batched: one
+ * sampling launch, one run-time compiled persistent kernel over all their rows, one finalize,
+ * replayed from a CUDA graph while the launch shape repeats. Otherwise the queries run one by one
+ * through pmb_groupby with host outputs (a device output request then returns PMB_E_UNSUPPORTED).
+ * Device outputs stay valid until the next call on the handle. */
 int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb_column* const* cols,
                         const int32_t* n_cols, int32_t n_queries, pmb_result** outs);
 

@@ -136,6 +136,12 @@ __global__ void k_table_init(unsigned long long* __restrict__ keys, int64_t key_
   for (int64_t w = i; w < total; w += stride) recs[w] = ri.w[w % rec_words];
 }
 
+// launcher of k_table_init for other translation units (batched tables)
+void k_table_init_pub(unsigned long long* keys, int64_t key_words, uint64_t* recs, int64_t n_recs, int rec_words,
+                      const RecInit& ri, int blocks, cudaStream_t s) {
+  k_table_init<<<blocks, 256, 0, s>>>(keys, key_words, recs, n_recs, rec_words, ri);
+}
+
 // ============================================================================ global table
 __device__ __forceinline__ int64_t gfind64(const HashParams& P, uint64_t key, uint64_t h) {
   if (key == PMB_EMPTY64) {
@@ -995,6 +1001,7 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
         P.q.field[i].fx = f.fx;
         P.q.fx_e[f.fx_slot] = q.fx_e[f.fx_slot];
       }
+      if (pmb_fx_to_dd(cq)) return PMB_RETRY_DD;
       if (++fx_reruns > 4) return pmb_fail(h, PMB_E_CUDA, "float-sum range did not converge");
       continue;
     }
@@ -1013,6 +1020,21 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     }
     return PMB_OK;
   }
+}
+
+// compiles the query again (its float-sum columns listed in cq.dd_user_cols in double-double),
+// keeping the staged column pointers: the same columns come in the same order
+int recompile_dd(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols, CompiledQuery& cq) {
+  CompiledQuery nc;
+  nc.dd_user_cols = cq.dd_user_cols;
+  int rc = pmb_compile_groupby(h, q, cols, n_cols, &nc);
+  if (rc) return rc;
+  for (int c = 0; c < nc.dq.n_cols; c++) {
+    nc.dq.col[c].data = cq.dq.col[c].data;
+    nc.dq.col[c].valid = cq.dq.col[c].valid;
+  }
+  cq = nc;
+  return PMB_OK;
 }
 
 extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols,
@@ -1046,7 +1068,7 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
       r->columns[c].data = pmb_ws_alloc(h, 16);
       r->columns[c].validity = (uint8_t*)pmb_ws_alloc(h, 16);
     }
-  } else {
+  } else for (int pass = 0;; pass++) {
     int strategy = q->strategy;
     int64_t est = q->capacity_hint;
     static thread_local SketchOut sk;  // large (histogram); one per host thread
@@ -1059,6 +1081,12 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     while ((1LL << pbits) < cq.dq.n_rows / h->sm_count + 1) pbits++;
     while ((1LL << tbits) < cq.dq.n_rows + 1) tbits++;
     pmb_set_fx(cq.dq, sk.fx_expo, 3, pbits + 1, tbits + 1);
+    if (pass < 3 && pmb_fx_to_dd(cq)) {
+      // a float-sum column's range leaves too few fraction bits: sum it in double-double
+      rc = recompile_dd(h, q, cols, n_cols, cq);
+      if (rc) return bail(rc);
+      continue;
+    }
     int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
     if (strategy == PMB_STRATEGY_AUTO) {
       // the learned selector when installed, else the plain cardinality heuristic. The predicted
@@ -1077,7 +1105,14 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     if (est <= 0) est = e;
     if (strategy == PMB_STRATEGY_SORT) rc = pmb_groupby_sort(h, cq, r);
     else rc = pmb_groupby_hash(h, cq, q, strategy, est, have_sk ? &sk : nullptr, r);
-    if (rc) return bail(rc);
+    if (rc == PMB_RETRY_DD && pass < 3) {
+      // a float sum outgrew the fixed point: its column now sums in double-double
+      rc = recompile_dd(h, q, cols, n_cols, cq);
+      if (rc) return bail(rc);
+      continue;
+    }
+    if (rc) return bail(rc == PMB_RETRY_DD ? pmb_fail(h, PMB_E_CUDA, "float-sum range did not converge") : rc);
+    break;
   }
   rc = pmb_finish_outputs(h, r, q->output_on_device == 0);
   if (rc) return bail(rc);

@@ -80,12 +80,20 @@ int pmb_plan_hash(pmb_handle* h, int max_smem_optin, CompiledQuery& cq, int stra
                   HashParams& P, int& nt, int& smem);
 int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
                      const SketchOut* sk, pmb_result* r);
+// compiles the query again with cq.dd_user_cols, keeping the staged column pointers
+int recompile_dd(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols, CompiledQuery& cq);
+// keys = EMPTY, records = identity (k_table_init) on stream s
+void k_table_init_pub(unsigned long long* keys, int64_t key_words, uint64_t* recs, int64_t n_recs, int rec_words,
+                      const RecInit& ri, int blocks, cudaStream_t s);
 // sort strategy (pmb_sort.cu): packed-key LSD radix sort + segmented reduce; groups come out in
 // packed-key order
 int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r);
 // learned selector (pmb_learned.cu): strategy and group count for AUTO; false when no selector is
 // installed or its output is unusable
 bool pmb_selector_pick(pmb_handle* h, const CompiledQuery& cq, int* strategy, int64_t* groups);
+// group counts the selector predicts for a batch of queries (device DQuery array); false without
+// an installed selector
+bool pmb_selector_predict_batch(pmb_handle* h, const DQuery* d_qs, int nq, int64_t* out_groups, const int64_t* n_rows);
 
 // Sets bit p of a bitmap for every lane whose `bit` is true. The warp's positions are
 // consecutive from p_first, so they touch at most two 32-bit words: one atomicOr each.

@@ -202,6 +202,14 @@ int pmb_cuda_check(pmb_handle* h, cudaError_t e, const char* what);
 // blocks); pmb_ws_alloc bumps 256-byte aligned chunks and adds a block when one is full, so
 // earlier allocations of the same call never move. Returns nullptr when the device is full.
 int pmb_ws_begin(pmb_handle* h);
+// a position in the workspace, and giving back everything allocated after it (only when no device
+// work still uses that memory)
+struct WsMark {
+  size_t blocks;
+  size_t top;
+};
+WsMark pmb_ws_mark(const pmb_handle* h);
+void pmb_ws_release(pmb_handle* h, WsMark m);
 void* pmb_ws_alloc(pmb_handle* h, size_t bytes);
 inline size_t pmb_align(size_t x, size_t a) { return (x + a - 1) / a * a; }
 

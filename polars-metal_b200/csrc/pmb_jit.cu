@@ -771,11 +771,12 @@ static bool jit_compile(const std::string& src, std::vector<char>& cubin, std::s
   return true;
 }
 
-int pmb_jit_hash_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out) {
+// compiled kernel `name` of a source (cached by source text)
+static int jit_kernel(pmb_handle* h, const std::string& src, const char* name, cudaKernel_t* out) {
   *out = nullptr;
-  std::string src = pmb_jit_source(cq, J);
+  const std::string key = std::string(name) + "\n" + src;
   std::lock_guard<std::mutex> lock(g_mu);
-  auto it = g_cache.find(src);
+  auto it = g_cache.find(key);
   if (it != g_cache.end()) {
     *out = it->second;
     return PMB_OK;
@@ -791,18 +792,76 @@ int pmb_jit_hash_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J
   cudaLibrary_t lib;
   PMB_CUDA(h, cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
   cudaKernel_t k;
-  PMB_CUDA(h, cudaLibraryGetKernel(&k, lib, "pmb_jit_hash_agg"));
-  g_cache[src] = k;
+  PMB_CUDA(h, cudaLibraryGetKernel(&k, lib, name));
+  g_cache[key] = k;
   *out = k;
   if (getenv("PMB_JIT_DEBUG")) fprintf(stderr, "pmb jit: compiled a %zu-byte cubin (%zu cached)\n", cubin.size(), g_cache.size());
   return PMB_OK;
 }
 
+int pmb_jit_hash_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out) {
+  return jit_kernel(h, pmb_jit_source(cq, J), "pmb_jit_hash_agg", out);
+}
+
+int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int max_smem_optin, JitPlan* J) {
+  const DQuery& q = cq.dq;
+  memset(J, 0, sizeof(*J));
+  J->nt = nt;
+  J->nbuf = 1;
+  const int W = nt / 32;
+  int off = 0, tx = 0;
+  for (int c = 0; c < q.n_cols; c++) {
+    int db = q.col[c].elem ? 128 * q.col[c].elem : 16;
+    J->doff[c] = off;
+    off += db;
+    tx += db;
+    J->voff[c] = -1;
+    if (q.col[c].valid) {
+      J->voff[c] = off;
+      off += 16;
+      tx += 16;
+    }
+  }
+  J->buf_bytes = (int)pmb_align((size_t)off, 128);
+  J->tx_bytes = tx;
+  JitSLayout S;
+  pmb_jit_slayout(q, &S);
+  J->srec = S.bytes;
+  const int budget = max_smem_optin - 1024;
+  J->off_bars = 0;
+  J->off_buf = (int)pmb_align((size_t)(8 * W), 128);
+  J->off_q = J->off_buf + W * J->buf_bytes;
+  const int used = J->off_q + W * 128 * 4;
+  if (used > budget) return pmb_fail(h, PMB_E_UNSUPPORTED, "query touches too many columns for the unit buffers");
+  // hot keys: 8 per item, one record per warp each; warm: the largest power of two that fits
+  int hot = 8;
+  while (hot > 0 && (int)pmb_align((size_t)used, 16) + 64 + W * hot * J->srec > budget) hot /= 2;
+  int warm = 0;
+  for (int sw = 1 << 14; sw >= 64; sw /= 2)
+    if ((int)pmb_align((size_t)used, 16) + 8 * sw + 64 + (W * hot + sw) * J->srec <= budget) {
+      warm = sw;
+      break;
+    }
+  J->hot_cap = hot;
+  J->warm_cap = warm;
+  J->tkey = 8;
+  J->tnb = 0;
+  J->off_tkeys = (int)pmb_align((size_t)used, 16);
+  J->off_tval = J->off_tkeys + 8 * warm;
+  J->off_srecs = (int)pmb_align((size_t)(J->off_tval + 64), 16);
+  J->smem = J->off_srecs + (W * hot + warm) * J->srec;
+  return PMB_OK;
+}
+
+int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out) {
+  return jit_kernel(h, pmb_jit_source(cq, J) + "\n" + std::string(kBatchSkeleton), "pmb_jit_batch_agg", out);
+}
+
 // Internal check (not part of the C ABI in pmb.h): generates and compiles the run-time kernel of
 // a query with NVRTC, without a GPU. Column pointers are not read, only their dtypes and whether
 // a validity bitmap is present. Returns PMB_OK, or an error with the compiler log in `log`.
-extern "C" int pmb_debug_jit_compile(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,
-                                     int64_t log_cap) {
+static int debug_compile(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log, int64_t log_cap,
+                         bool batch) {
   pmb_handle h;
   CompiledQuery cq;
   int rc = pmb_compile_groupby(&h, q, cols, n_cols, &cq);
@@ -818,10 +877,10 @@ extern "C" int pmb_debug_jit_compile(const pmb_query* q, const pmb_column* cols,
       msg = "128-bit keys use the prebuilt kernel";
     } else {
       JitPlan J;
-      rc = pmb_plan_jit(&h, cq, true, 232448, &J);
+      rc = batch ? pmb_plan_jit_batch(&h, cq, 1024, 232448, &J) : pmb_plan_jit(&h, cq, true, 232448, &J);
       if (rc == PMB_OK) {
         std::vector<char> cubin;
-        const std::string src = pmb_jit_source(cq, J);
+        const std::string src = batch ? pmb_jit_source(cq, J) + "\n" + std::string(kBatchSkeleton) : pmb_jit_source(cq, J);
         if (const char* e = getenv("PMB_JIT_DEBUG"))
           if (e[0] == '2') fprintf(stderr, "%s\n", src.c_str());  // the generated source, for inspection
         if (!jit_compile(src, cubin, msg)) rc = PMB_E_UNSUPPORTED;
@@ -839,6 +898,16 @@ extern "C" int pmb_debug_jit_compile(const pmb_query* q, const pmb_column* cols,
     log[n] = 0;
   }
   return rc;
+}
+
+extern "C" int pmb_debug_jit_compile(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,
+                                     int64_t log_cap) {
+  return debug_compile(q, cols, n_cols, log, log_cap, false);
+}
+// the same for the batched kernel (pmb_jit_batch.cuh)
+extern "C" int pmb_debug_jit_compile_batch(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,
+                                           int64_t log_cap) {
+  return debug_compile(q, cols, n_cols, log, log_cap, true);
 }
 
 int pmb_jit_sampled_table(const CompiledQuery& cq, const JitPlan& J, const unsigned long long* hot, int n_hot,

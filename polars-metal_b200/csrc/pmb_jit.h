@@ -66,6 +66,22 @@ int pmb_jit_sampled_table(const CompiledQuery& cq, const JitPlan& J, const unsig
 bool pmb_jit_enabled(int64_t n_rows);
 // compiled kernel for this signature and layout (cached); PMB_E_UNSUPPORTED when unavailable
 int pmb_jit_hash_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out);
+// host mirrors of JBatchItem / JBatch in pmb_jit_batch.cuh
+struct JBatchItemH {
+  int q;
+  int pad;
+  long long u0, u1;
+};
+struct JBatchH {
+  const JitParams* qp;
+  const JBatchItemH* items;
+  long long n_items;
+  unsigned long long* ticket;
+};
+
+// the batched kernel (pmb_jit_batch.cuh): layout for `nt` threads and its compiled kernel
+int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int max_smem_optin, JitPlan* J);
+int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out);
 // launches over the global table and key lists set up in P (gkeys, grecs, gcap, status, lists)
 int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const JitPlan& J, const HashParams& P,
                    int grid, const uint8_t* ttab, int tnb);

@@ -7,8 +7,10 @@
 // that plain heuristic (pmb_choose_strategy) stays the fallback.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "pmb_groupby.h"
 
@@ -34,12 +36,12 @@ struct FeatParams {
 
 __device__ __forceinline__ float lg2p1(double x) { return (float)log2(x + 1.0); }
 
-__global__ void __launch_bounds__(F_NT) k_features(const __grid_constant__ FeatParams F) {
+// the features of query q into out[NF]; called by one whole CTA of F_NT threads
+__device__ __forceinline__ void features_body(const DQuery& q, float* out) {
   extern __shared__ unsigned long long s_slot[];  // TSLOTS
   __shared__ unsigned int s_hll[HLL];
   __shared__ unsigned int s_bkt[BUCKETS];
   __shared__ unsigned int s_acc[16];
-  const DQuery& q = F.q;
   const int tid = threadIdx.x;
   for (int i = tid; i < TSLOTS; i += F_NT) s_slot[i] = 0ULL;
   for (int i = tid; i < HLL; i += F_NT) s_hll[i] = 0u;
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(F_NT) k_features(const __grid_constant__ FeatP
     const double neff = (double)n * (m > 0 ? kept / m : 0.0);
     const double gee = kept > 0 ? sqrt(neff / mk) * f1 + (d - f1) : 0.0;
     const double chao = d + f1 * f1 / (2.0 * (f2 > 0 ? f2 : 1.0));
-    float* o = F.out;
+    float* o = out;
     o[0] = lg2p1((double)n) / 32.f;
     o[1] = q.key_bits / 128.f;
     o[2] = (float)(s_acc[1] / mk);
@@ -148,6 +150,13 @@ __global__ void __launch_bounds__(F_NT) k_features(const __grid_constant__ FeatP
     o[22] = (kept > 0 && d == kept) ? 1.f : 0.f;
     o[23] = 1.f;
   }
+}
+
+__global__ void __launch_bounds__(F_NT) k_features(const __grid_constant__ FeatParams F) { features_body(F.q, F.out); }
+
+// one CTA per query of a batch
+__global__ void __launch_bounds__(F_NT) k_features_batch(const DQuery* __restrict__ qs, float* __restrict__ out) {
+  features_body(qs[blockIdx.x], out + (size_t)blockIdx.x * NF);
 }
 
 // ---------------------------------------------------------------- MLP (one CTA of 64 threads per sample)
@@ -267,6 +276,35 @@ int stage_query(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32
 }
 
 }  // namespace
+
+// Group counts predicted by the installed selector for the queries of a batch (device DQuery
+// array): out_groups[i] (host) = 2^(output 3), or 0 when unusable; false without a selector.
+bool pmb_selector_predict_batch(pmb_handle* h, const DQuery* d_qs, int nq, int64_t* out_groups, const int64_t* n_rows) {
+  if (!h->selector || nq <= 0) return false;
+  float* feat = (float*)pmb_ws_alloc(h, (size_t)nq * NF * sizeof(float));
+  float* o = (float*)pmb_ws_alloc(h, (size_t)nq * NO * sizeof(float));
+  if (!feat || !o) return false;
+  const int smem = TSLOTS * 8;
+  if (cudaFuncSetAttribute(k_features_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return false;
+  pmb_kernel_begin(h, "features");
+  k_features_batch<<<nq, F_NT, smem, h->stream>>>(d_qs, feat);
+  pmb_kernel_end(h);
+  pmb_kernel_begin(h, "mlp_forward");
+  k_mlp_forward<<<nq, NH, 0, h->stream>>>(h->selector, feat, nq, o);
+  pmb_kernel_end(h);
+  if (cudaGetLastError() != cudaSuccess) return false;
+  std::vector<float> ho((size_t)nq * NO);
+  if (cudaMemcpyAsync(ho.data(), o, ho.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+    return false;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return false;
+  for (int i = 0; i < nq; i++) {
+    const float g = ho[(size_t)i * NO + 3];
+    out_groups[i] = std::isfinite(g) ? (int64_t)std::min<double>(std::exp2(std::min<double>(std::max<double>(g, 0.0), 40.0)),
+                                                                 (double)n_rows[i])
+                                     : 0;
+  }
+  return true;
+}
 
 // AUTO strategy with the installed selector: false when none is installed or its output is not
 // usable (the caller then takes the cardinality heuristic)

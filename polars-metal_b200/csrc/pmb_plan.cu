@@ -279,13 +279,16 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
     // the column's non-null count, created only for the aggregates that read it (count, mean, and
     // integer min/max, whose identity value is also a valid value); sums and float min/max need none
     auto cnt = [&]() { return (int16_t)(nullable ? field(F_CNT, c) : field(F_LEN, 0)); };
+    const int fsum = std::find(cq->dd_user_cols.begin(), cq->dd_user_cols.end(), A.column) != cq->dd_user_cols.end()
+                         ? F_SUM_DD
+                         : F_SUM_FX;
     switch (A.op) {
       case PMB_AGG_COUNT: o.f_cnt = cnt(); break;
       case PMB_AGG_SUM:
-        o.f_main = (int16_t)field(pmb_is_float(dt) ? F_SUM_FX : F_SUM_I, c);
+        o.f_main = (int16_t)field(pmb_is_float(dt) ? fsum : F_SUM_I, c);
         break;
       case PMB_AGG_MEAN:
-        o.f_main = (int16_t)field(pmb_is_float(dt) ? F_SUM_FX : F_SUM_I, c);
+        o.f_main = (int16_t)field(pmb_is_float(dt) ? fsum : F_SUM_I, c);
         o.f_cnt = cnt();
         break;
       default: {  // min / max

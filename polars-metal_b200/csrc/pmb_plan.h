@@ -21,7 +21,31 @@ struct CompiledQuery {
   int rec_words = 0;
   std::vector<uint64_t> rec_init;  // identity record, one u64 per 8 bytes
   std::vector<int> fx_cols;        // compact column of each exact float-sum slot
+  // caller's columns whose float sums use double-double accumulation instead of the exact
+  // fixed point (kept by pmb_compile_groupby; see PMB_FX_MIN_F)
+  std::vector<int> dd_user_cols;
 };
+
+// Fewest fraction bits an exact float sum may have. A column whose range needs more integer bits
+// than that leaves (an outlier far above the other values) would truncate every other group's
+// small values: it is summed in double-double instead (accurate relative to each group's own
+// magnitude), and the call runs again.
+#define PMB_FX_MIN_F 48
+// internal status: a float-sum column moved to double-double, compile the query again and re-run
+#define PMB_RETRY_DD 100
+
+// true (and the caller's columns added to cq.dd_user_cols) when a float-sum field has fewer than
+// PMB_FX_MIN_F fraction bits
+inline bool pmb_fx_to_dd(CompiledQuery& cq) {
+  bool any = false;
+  for (int i = 0; i < cq.dq.n_fields; i++) {
+    const DField& f = cq.dq.field[i];
+    if (f.kind != F_SUM_FX || f.fx >= PMB_FX_MIN_F) continue;
+    cq.dd_user_cols.push_back(cq.map.user[f.col]);
+    any = true;
+  }
+  return any;
+}
 
 // Fixed-point range of the exact float sums. Every value of a slot satisfies |x| < 2^E, E taken
 // from the largest biased exponent seen plus `headroom` powers of two. The fraction bits F keep

@@ -49,6 +49,17 @@ int pmb_ws_begin(pmb_handle* h) {
   return PMB_OK;
 }
 
+WsMark pmb_ws_mark(const pmb_handle* h) { return {h->ws.size(), h->ws.empty() ? 0 : h->ws.back().top}; }
+
+void pmb_ws_release(pmb_handle* h, WsMark m) {
+  if (m.blocks == 0) {
+    for (auto& b : h->ws) b.top = 0;
+    return;
+  }
+  h->ws[m.blocks - 1].top = m.top;
+  for (size_t i = m.blocks; i < h->ws.size(); i++) h->ws[i].top = 0;
+}
+
 void* pmb_ws_alloc(pmb_handle* h, size_t bytes) {
   bytes = pmb_align(bytes ? bytes : 1, 256);
   if (!h->ws.empty()) {

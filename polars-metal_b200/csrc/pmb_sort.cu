@@ -724,6 +724,7 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
         q.fx_e[f.fx_slot] = (int16_t)e;
       }
     }
+    if (pmb_fx_to_dd(cq)) return PMB_RETRY_DD;
     R.q = q;
     for (int c = 0; c < n_out; c++) {
       PMB_CUDA(h, cudaMemsetAsync(R.out_valid[c], 0, vbytes, h->stream));

@@ -395,6 +395,46 @@ def _query(columns, keys, aggs, predicate):
     return q, abi_cols, len(cols), (keep, expr_keep, key_arr, agg_arr, expr)
 
 
+def groupby_batched(queries, output: str = "host", handle: Handle | None = None) -> list:
+    """Many independent group-by queries in one call (pmb_groupby_batched).
+
+    queries: a list of (columns, keys, aggs, predicate) with the meanings of `groupby`. Queries of
+    one signature run in one persistent launch; the results come back in query order."""
+    h = handle or default_handle()
+    n = len(queries)
+    qarr = (A.Query * max(1, n))()
+    col_ptrs = (C.POINTER(A.Column) * max(1, n))()
+    ncols = (C.c_int32 * max(1, n))()
+    keep = []
+    names = []
+    for i, (columns, keys, aggs, predicate) in enumerate(queries):
+        q, cols, nc, kp = _query(columns, keys, aggs, predicate)
+        q.strategy = A.STRATEGIES["auto"]
+        q.output_on_device = 1 if output == "device" else 0
+        q.capacity_hint = 0
+        qarr[i] = q
+        col_ptrs[i] = C.cast(cols, C.POINTER(A.Column))
+        ncols[i] = nc
+        keep.append((q, cols, kp))
+        names.append(list(keys) + [a[2] for a in aggs])
+    outs = (C.POINTER(A.Result) * max(1, n))()
+    h.check(h._lib.pmb_groupby_batched(h.raw, qarr, col_ptrs, ncols, n, outs))
+    results = []
+    try:
+        for i in range(n):
+            res = outs[i].contents
+            data, valid, dts = _read_result(res, names[i], output != "device")
+            results.append(GroupByResult(n_groups=res.n_groups, names=names[i], dtypes=dts, data=data, validity=valid,
+                                         strategy=A.STRATEGY_NAMES.get(res.strategy_used, str(res.strategy_used)),
+                                         rehash_count=res.rehash_count, capacity=res.capacity))
+    finally:
+        for i in range(n):
+            if outs[i]:
+                h._lib.pmb_result_free(outs[i])
+        del keep
+    return results
+
+
 def selector_features(columns, keys, aggs, predicate=None, handle: Handle | None = None) -> np.ndarray:
     """The learned selector's features of a query (PMB_SELECTOR_FEATURES floats), computed on the
     device from a 4096-row sample of its keys."""

@@ -187,6 +187,44 @@ def make_sort(n: int = 200_000_000, seed: int = 3, device="cpu", pool: int = 781
     return Table(cols, ["k1", "k2"], aggs, None, n, "sort")
 
 
+PRED_BATCH = {"kind": "Compare", "op": "Gt", "lhs": {"kind": "Column", "name": "v"},
+              "rhs": {"kind": "LiteralF64", "value": -1.0}}
+AGGS_BATCH = [("Sum", "v", "v_sum"), ("Mean", "v", "v_mean"), ("Min", "v", "v_min"), ("Max", "v", "v_max"),
+              ("Len", None, "count")]
+
+
+def batch_sizes(n_queries: int, seed: int, mu: float = 11.512925464970229, sigma: float = 1.5,
+                lo: int = 1000, hi: int = 10_000_000):
+    """Per-query rows (lognormal(mu = ln 1e5, sigma), clipped), cardinality (log-uniform in
+    [10, 1e6], at most the rows) and Zipf skew (uniform in [0, 1.5]) of the batched workload."""
+    rng = np.random.default_rng(seed)
+    rows = np.clip(np.exp(rng.normal(mu, sigma, n_queries)), lo, hi).astype(np.int64)
+    card = np.exp(rng.uniform(np.log(10), np.log(1e6), n_queries)).astype(np.int64)
+    card = np.minimum(card, rows)
+    s = rng.uniform(0.0, 1.5, n_queries)
+    return rows, card, s
+
+
+def make_batch(n_queries: int = 4096, seed: int = 4, device="cpu", max_total: int | None = None):
+    """Independent filter -> group_by queries: key int32 (Zipf over its cardinality), v float64
+    N(0,1) with 1% nulls; filter v > -1; sum/mean/min/max(v), len. Returns Tables."""
+    torch = _torch()
+    rows, card, s = batch_sizes(n_queries, seed)
+    if max_total is not None and rows.sum() > max_total:
+        rows = np.maximum(1000, (rows * (max_total / rows.sum())).astype(np.int64))
+        card = np.minimum(card, rows)
+    g = _gen(seed, device)
+    out = []
+    for i in range(n_queries):
+        n, d = int(rows[i]), int(max(card[i], 1))
+        k = zipf_keys(n, d, float(s[i]), g, device, torch.int64)
+        k = ((k * 0x9E3779B1 + i) & 0x7FFFFFFF).to(torch.int32)
+        v = torch.randn(n, generator=g, device=device, dtype=torch.float64)
+        cols = {"key": (k, None), "v": (v, _nulls(n, 0.01, g, device))}
+        out.append(Table(cols, ["key"], AGGS_BATCH, PRED_BATCH, n, f"batch{i}"))
+    return out
+
+
 def to_column_data(t: Table) -> dict:
     """Table -> {name: ColumnData} (torch tensors; zero-copy when on the GPU)."""
     from ._native import ColumnData

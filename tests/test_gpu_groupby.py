@@ -282,3 +282,16 @@ def test_device_outputs_report_groups():
     got = groupby(datagen.to_column_data(t), t.keys, t.aggs, t.predicate, output="device")
     assert got.n_groups == 1000
     assert all(isinstance(p, int) and p != 0 for p in got.data)
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+@pytest.mark.parametrize("n", [50_000, 3_000_000])
+def test_float_sum_outlier_beyond_the_fixed_point(strategy, n):
+    # one value far above the rest, on a row the sample skips: the exact fixed point would truncate
+    # every other group's sums, so the column moves to double-double sums and the call runs again
+    rng = np.random.default_rng(41)
+    v = rng.standard_normal(n)
+    v[1] = 3.0e30
+    cols = {"k": (rng.integers(0, 1000, n).astype(np.int32), None), "v": (v, pack(rng.random(n) > 0.05))}
+    aggs = [("Sum", "v", "s"), ("Mean", "v", "m"), ("Len", None, "n")]
+    run_both(cols, ["k"], aggs, None, strategy, f"outlier {strategy} n={n}")

@@ -20,7 +20,7 @@ def _lib():
     return L
 
 
-def jit_compile(cols: dict, keys, aggs, predicate=None) -> tuple[int, str]:
+def jit_compile(cols: dict, keys, aggs, predicate=None, batch: bool = False) -> tuple[int, str]:
     L = _lib()
     names = list(cols)
     cds = [c if isinstance(c, ColumnData) else ColumnData(*c) for c in cols.values()]
@@ -39,7 +39,9 @@ def jit_compile(cols: dict, keys, aggs, predicate=None) -> tuple[int, str]:
     q.n_aggs = len(aggs)
     q.predicate = C.pointer(expr) if expr is not None else None
     buf = C.create_string_buffer(1 << 16)
-    rc = L.pmb_debug_jit_compile(C.byref(q), abi, len(names), buf, 1 << 16)
+    fn = L.pmb_debug_jit_compile_batch if batch else L.pmb_debug_jit_compile
+    fn.argtypes = [C.POINTER(A.Query), C.POINTER(A.Column), C.c_int32, C.c_char_p, C.c_int64]
+    rc = fn(C.byref(q), abi, len(names), buf, 1 << 16)
     return rc, buf.value.decode(errors="replace")
 
 
@@ -111,3 +113,13 @@ def test_predicate_forms_compile():
     for p in preds:
         rc, log = jit_compile(cols, ["k", "f"], [("Sum", "x", "s"), ("Len", None, "n")], p)
         assert rc == 0, log
+
+
+def test_batch_kernel_compiles():
+    n = 256
+    cols = {"key": ColumnData(np.zeros(n, np.int32)), "v": ColumnData(np.zeros(n), np.zeros(32, np.uint8))}
+    rc, log = jit_compile(cols, ["key"], datagen.AGGS_BATCH, datagen.PRED_BATCH, batch=True)
+    assert rc == 0, log
+    t = datagen.make_hash(4096, seed=1)
+    rc, log = jit_compile(datagen.to_column_data(t), t.keys, t.aggs, t.predicate, batch=True)
+    assert rc == 0, log
