@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -524,12 +525,23 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
     }
     return rc;
   };
+  // host phase timing (PMB_BATCH_TIMING=1 prints it)
+  const bool timing = getenv("PMB_BATCH_TIMING") != nullptr;
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto t_prev = now();
+  auto phase = [&](const char* name) {
+    if (!timing) return;
+    const auto t = now();
+    fprintf(stderr, "batch %-12s %8.2f ms\n", name, std::chrono::duration<double, std::milli>(t - t_prev).count());
+    t_prev = t;
+  };
   // compile every query; the batched path takes the queries of query 0's signature
   std::vector<CompiledQuery> cqs(n_queries);
   for (int i = 0; i < n_queries; i++) {
     int rc = pmb_compile_groupby(h, &qs[i], cols[i], n_cols[i], &cqs[i]);
     if (rc) return fail_all(rc);
   }
+  phase("compile");
   const std::string sig0 = signature(cqs[0].dq);
   std::vector<int> batch, single;
   for (int i = 0; i < n_queries; i++) {
@@ -567,6 +579,7 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
       }
     }
     const int nb = (int)batch.size();
+    phase("stage");
     // 1. per-query sample
     DQuery* d_all = (DQuery*)pmb_ws_alloc(h, sizeof(DQuery) * n_queries);
     BatchSketch* d_sk = (BatchSketch*)pmb_ws_alloc(h, sizeof(BatchSketch) * n_queries);
@@ -587,6 +600,7 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
     std::vector<BatchSketch> skb(nb);
     PMB_CUDA(h, cudaMemcpyAsync(skb.data(), d_sk, sizeof(BatchSketch) * nb, cudaMemcpyDeviceToHost, h->stream));
     PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+    phase("sketch");
     // 2. estimates (the selector's prediction can only enlarge them) and float-sum ranges
     std::vector<int64_t> nrows(nb), pred(nb, 0);
     for (int j = 0; j < nb; j++) nrows[j] = cqs[batch[j]].dq.n_rows;
@@ -610,6 +624,7 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
       pmb_set_fx(cqs[i].dq, skb[j].fx_expo, 3, pbits + 1, tbits + 1);
       total_rows += cqs[i].dq.n_rows;
     }
+    phase("estimates");
     // 3. autotune (first batch of a signature and size class), then the round itself
     int size_class = 0;
     while ((1LL << size_class) < total_rows) size_class++;
@@ -654,6 +669,7 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
         if (cq.dq.field[f].kind == F_SUM_FX) cq.dd_user_cols.push_back(cq.map.user[cq.dq.field[f].col]);
       return recompile_dd(h, &qs[i], cols[i], n_cols[i], cq);
     };
+    phase("autotune");
     std::vector<int> again = batch;
     for (int round = 0; !again.empty() && round < 7; round++) {
       std::map<std::string, std::vector<int>> groups;
@@ -670,6 +686,7 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
       }
       again.swap(next);
     }
+    phase("rounds");
     if (!again.empty()) return fail_all(pmb_fail(h, PMB_E_OOM, "batched group-by did not converge"));
     for (int i : batch) {
       rc = pmb_finish_outputs(h, outs[i], qs[i].output_on_device == 0);
@@ -677,6 +694,7 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
     }
     PMB_CUDA(h, cudaStreamSynchronize(h->stream));
     pmb_call_end(h);
+    phase("outputs");
   }
   return PMB_OK;
 }

@@ -407,8 +407,16 @@ def groupby_batched(queries, output: str = "host", handle: Handle | None = None)
     ncols = (C.c_int32 * max(1, n))()
     keep = []
     names = []
+    shapes = {}  # queries usually share keys, aggregates and filter: those are built once
     for i, (columns, keys, aggs, predicate) in enumerate(queries):
-        q, cols, nc, kp = _query(columns, keys, aggs, predicate)
+        shape = (tuple(columns), tuple(keys), tuple(aggs), id(predicate))
+        if shape not in shapes:
+            shapes[shape] = _query_shape(list(columns), keys, aggs, predicate)
+        q, sk = _query_from_shape(shapes[shape])
+        cols_l = [c if isinstance(c, ColumnData) else ColumnData(c) for c in columns.values()]
+        cols, ck = _to_abi_columns(cols_l)
+        nc = len(cols_l)
+        kp = (sk, ck, predicate)
         q.strategy = A.STRATEGIES["auto"]
         q.output_on_device = 1 if output == "device" else 0
         q.capacity_hint = 0
@@ -433,6 +441,39 @@ def groupby_batched(queries, output: str = "host", handle: Handle | None = None)
                 h._lib.pmb_result_free(outs[i])
         del keep
     return results
+
+
+def _query_shape(names, keys, aggs, predicate):
+    """The parts of a query that do not depend on the column buffers."""
+    index = {n: i for i, n in enumerate(names)}
+    for k in keys:
+        if k not in index:
+            raise KeyError(f"polars_b200: key column {k!r} not found in upstream columns")
+    key_arr = (C.c_int32 * max(1, len(keys)))(*[index[k] for k in keys])
+    agg_arr = (A.Agg * max(1, len(aggs)))()
+    for i, (op, col, _alias) in enumerate(aggs):
+        if op not in A.AGG_OPS:
+            raise ValueError(f"polars_b200: unknown aggregation op {op!r}")
+        agg_arr[i].op = A.AGG_OPS[op]
+        if op == "Len":
+            agg_arr[i].column = -1
+        else:
+            if col not in index:
+                raise KeyError(f"polars_b200: agg input column {col!r} not found in upstream columns")
+            agg_arr[i].column = index[col]
+    expr, expr_keep = compile_predicate(predicate, index)
+    return key_arr, len(keys), agg_arr, len(aggs), expr, expr_keep
+
+
+def _query_from_shape(shape):
+    key_arr, nk, agg_arr, na, expr, expr_keep = shape
+    q = A.Query()
+    q.key_columns = key_arr
+    q.n_keys = nk
+    q.aggs = agg_arr
+    q.n_aggs = na
+    q.predicate = C.pointer(expr) if expr is not None else None
+    return q, shape
 
 
 def selector_features(columns, keys, aggs, predicate=None, handle: Handle | None = None) -> np.ndarray:
