@@ -9,7 +9,12 @@ One step = one full pmb_groupby call on device-resident inputs (sketch, table in
 aggregation, finalize, group-count readback). `value` = rows of all ranks / max step time;
 `e2e` = the same call with inputs in pinned host memory and results copied back to the host.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload hash|small|sort]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload hash|small|sort|batch]
+
+Every line of the default workload also carries "batched": the batched workload (4096 independent
+filter -> group_by queries, ~500M rows in total) run through pmb_groupby_batched with the learned
+strategy selector, against the same queries run one by one through pmb_groupby with the plain
+cardinality heuristic (total rows/s of both). --workload batch makes that the headline line.
 
 --impl reference times the CPU restatement of the reference's algorithm (the oracle, all host
 threads) on a bounded sample of the same workload; the reference itself (Rust + Metal) cannot
@@ -47,6 +52,12 @@ WORKLOADS = {
 }
 
 
+BATCH_QUERIES, BATCH_ROWS = 4096, 500_000_000
+BATCH_DESC = ("batch: 4096 independent queries, rows lognormal(ln 1e5, 1.5) clipped to [1K, 10M] and scaled to 500M "
+              "in total; key int32, cardinality log-uniform [10, 1e6] (at most the rows), Zipf s ~ U[0, 1.5]; "
+              "v f64 N(0,1) with 1% nulls; filter v > -1; sum/mean/min/max(v), len")
+
+
 def load_peaks() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -59,7 +70,8 @@ def load_peaks() -> tuple[float, str]:
 
 class ClockSampler:
     """Samples SM clocks and throttle reasons while the timed region runs: NVML queries (read only)
-    every 10 ms in a thread, or nvidia-smi every 50 ms when NVML is not importable."""
+    when the region starts, every 2 ms in a thread, and when it ends; or nvidia-smi every 50 ms when
+    NVML is not importable."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
@@ -80,17 +92,20 @@ class ClockSampler:
             reasons_of = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
                 pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
 
-            def loop():
-                while not self._stop.is_set():
-                    try:
-                        sm = pynvml.nvmlDeviceGetClockInfo(dev, pynvml.NVML_CLOCK_SM)
-                        bits = reasons_of(dev)
-                        self.samples.append((float(sm), float(mx),
-                                             {n for n, m in self.REASONS.items() if bits & m}))
-                    except Exception:
-                        pass
-                    self._stop.wait(0.01)
+            def sample():
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(dev, pynvml.NVML_CLOCK_SM)
+                    bits = reasons_of(dev)
+                    self.samples.append((float(sm), float(mx), {n for n, m in self.REASONS.items() if bits & m}))
+                except Exception:
+                    pass
 
+            def loop():
+                while not self._stop.wait(0.002):
+                    sample()
+                sample()
+
+            sample()
             self._t = threading.Thread(target=loop, daemon=True)
             self._t.start()
             return self
@@ -174,6 +189,69 @@ def cpu_baseline(workload: str, threads: int, sample_rows: int, reps: int = 3) -
             "sample": f"first {sample_rows:,} rows of the same generator (seed 99), median of {reps} after 1 warm-up"}
 
 
+def batch_queries(device, seed: int, stop_rows: int | None = None):
+    """The batched workload's tables and their (columns, keys, aggs, predicate) tuples."""
+    from polars_b200 import datagen
+
+    tables = datagen.make_batch(BATCH_QUERIES, seed=seed, device=device, max_total=BATCH_ROWS, stop_rows=stop_rows)
+    return tables, [(datagen.to_column_data(t), t.keys, t.aggs, t.predicate) for t in tables]
+
+
+def time_calls(fn, stream, steps: int, warmup: int) -> float:
+    """ms per call of fn(), CUDA events on `stream`. The library calls synchronise before they
+    return, so the events bracket their host work too."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def batch_vs_plain(qs, rows: int, stream, h_learned, h_plain, steps: int = 3, plain_steps: int = 2) -> dict:
+    """Batched + learned selector against the plain loop (one pmb_groupby per query, heuristic)."""
+    from polars_b200._native import groupby, groupby_batched
+
+    def plain():
+        for c, k, a, p in qs:
+            groupby(c, k, a, p, output="device", handle=h_plain)
+
+    ms_b = time_calls(lambda: groupby_batched(qs, output="device", handle=h_learned), stream, steps, 3)
+    ms_p = time_calls(plain, stream, plain_steps, 1)
+    return {"workload": BATCH_DESC, "queries": len(qs), "rows": rows,
+            "batched_learned": {"rows_per_s": rows / (ms_b / 1e3), "ms_per_step": ms_b, "steps": steps},
+            "plain_heuristic": {"rows_per_s": rows / (ms_p / 1e3), "ms_per_step": ms_p, "steps": plain_steps},
+            "speedup": ms_p / ms_b}
+
+
+def batch_cpu_sample(threads: int, stop_rows: int, reps: int = 3) -> tuple[float, int, int]:
+    """The oracle over the batched workload's leading queries (CPU-generated, same generator):
+    (seconds per pass, rows, queries), median of `reps` after one warm-up."""
+    from oracle import pyoracle
+    from polars_b200 import datagen
+
+    tables = datagen.make_batch(BATCH_QUERIES, seed=4, device="cpu", max_total=BATCH_ROWS, stop_rows=stop_rows)
+    cols = [datagen.to_numpy_columns(t) for t in tables]
+
+    def one():
+        for t, c in zip(tables, cols):
+            pyoracle.groupby(c, t.keys, t.aggs, t.predicate, n_threads=threads)
+
+    one()
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times), sum(t.n_rows for t in tables), len(tables)
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -182,6 +260,22 @@ def run_reference(args) -> None:
     from oracle import pyoracle
     from polars_b200 import datagen
 
+    if args.workload == "batch":
+        sec, rows, nq = batch_cpu_sample(threads, 10_000_000, reps=max(1, args.steps))
+        value = rows / sec
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": BATCH_DESC, "rows_per_step": rows,
+                       "note": "CPU restatement of the reference algorithm (oracle/oracle.cpp), one call per query; "
+                               "the reference is Rust+Metal and cannot run here"},
+            "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
+                             "sample": f"the leading {nq} queries ({rows:,} rows) of the batch, CPU-generated, median"},
+            "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     sample = {"hash": 20_000_000, "small": 1_000_000, "sort": 20_000_000}[args.workload]
     maker = getattr(datagen, WORKLOADS[args.workload][0])
     t = maker(sample, seed=99, device="cpu")
@@ -215,7 +309,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hash", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="hash", choices=sorted(WORKLOADS) + ["batch"])
+    ap.add_argument("--no-batched", action="store_true", help="leave out the batched-vs-plain comparison")
     ap.add_argument("--rows", type=int, default=0, help="override the workload's row count")
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -241,6 +336,9 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
     device = torch.device("cuda", local_rank)
     torch.cuda.set_device(device)
+    if args.workload == "batch":
+        run_batch(args, device, rank, local_rank, world)
+        return
 
     maker_name, default_rows, desc = WORKLOADS[args.workload]
     n = args.rows or default_rows
@@ -326,6 +424,16 @@ def main():
         sample = {"hash": 10_000_000, "small": 1_000_000, "sort": 10_000_000}[args.workload]
         cpu = cpu_baseline(args.workload, threads, sample)
 
+    batched = None
+    if not args.no_batched:
+        tables_b, qs_b = batch_queries(device, seed=4 + rank)
+        torch.cuda.synchronize()
+        h_plain = Handle(local_rank, selector=None)
+        h_plain.set_stream(stream.cuda_stream)
+        batched = batch_vs_plain(qs_b, sum(tb.n_rows for tb in tables_b), stream, h, h_plain)
+        h_plain.close()
+        del tables_b, qs_b
+
     if rank == 0:
         clocks = clk.summary()
         line = {
@@ -355,6 +463,111 @@ def main():
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clocks,
+            "batched": batched,
+        }
+        print(json.dumps(line), flush=True)
+    h.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def run_batch(args, device, rank: int, local_rank: int, world: int) -> None:
+    """--workload batch: the headline is pmb_groupby_batched with the learned selector."""
+    import torch
+
+    from polars_b200._native import ColumnData, Handle, groupby_batched
+    from polars_b200.replicas import barrier, reduce_step_stats
+
+    tables, qs = batch_queries(device, seed=4 + rank)
+    torch.cuda.synchronize()
+    rows = sum(t.n_rows for t in tables)
+    bytes_per_row = tables[0].bytes_per_row()
+    alg_bytes = bytes_per_row * rows
+    stream = torch.cuda.current_stream(device)
+    h = Handle(local_rank)
+    h.set_stream(stream.cuda_stream)
+
+    def step():
+        return groupby_batched(qs, output="device", handle=h)
+
+    for _ in range(args.warmup):
+        res = step()
+    barrier(device)
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        ms = time_calls(step, stream, args.steps, 0)
+    launches = h.last_stats()["kernel_launches"] * args.steps
+    barrier(device)
+    ms_max, rows_all = reduce_step_stats(ms, rows, device)
+    value = rows_all / (ms_max / 1e3)
+    # one profiled call (the same launches run eagerly, an event pair around each kernel)
+    h.set_profiling(True)
+    step()
+    st = h.last_stats()
+    h.set_profiling(False)
+    kern = {k: v["ms"] for k, v in st["kernels"].items()}
+    agg_ms = st["kernels"]["batch_agg"]["ms"] / max(1, st["kernels"]["batch_agg"]["launches"])
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (agg_ms / 1e3) / 1e9
+    groups = sum(r.n_groups for r in res)
+
+    # end to end: every query's columns in pinned host memory, results copied back
+    host_qs = []
+    for c, k, a, p in qs:
+        hc = {}
+        for name, col in c.items():
+            hd = torch.empty(col.data.shape, dtype=col.data.dtype, pin_memory=True)
+            hd.copy_(col.data)
+            hv = None
+            if col.validity is not None:
+                hv = torch.empty(col.validity.shape, dtype=col.validity.dtype, pin_memory=True)
+                hv.copy_(col.validity)
+            hc[name] = ColumnData(hd, hv, dtype=col.dtype, length=col.length)
+        host_qs.append((hc, k, a, p))
+    groupby_batched(host_qs, output="host", handle=h)
+    h.set_profiling(True)
+    groupby_batched(host_qs, output="host", handle=h)
+    io = h.last_stats()
+    h.set_profiling(False)
+    e2e_steps = args.e2e_steps or 3
+    e2e_ms = time_calls(lambda: groupby_batched(host_qs, output="host", handle=h), stream, e2e_steps, 0)
+    e2e_ms_max, rows_e2e = reduce_step_stats(e2e_ms, rows, device)
+    del host_qs
+
+    h_plain = Handle(local_rank, selector=None)
+    h_plain.set_stream(stream.cuda_stream)
+    cmp = batch_vs_plain(qs, rows, stream, h, h_plain, steps=args.steps)
+    h_plain.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = len(os.sched_getaffinity(0))
+        sec, srows, snq = batch_cpu_sample(threads, 10_000_000)
+        cpu = {"value": srows / sec, "unit": "rows/s", "cores": threads, "kind": "port",
+               "sample": f"the leading {snq} queries ({srows:,} rows) of the batch, CPU-generated, oracle one call per "
+                         f"query, median of 3 after 1 warm-up"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": BATCH_DESC, "queries": len(qs), "rows_per_gpu": rows, "groups": groups,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": f"inputs {alg_bytes / 1e9:.2f} GB per GPU > 126 MB L2, no flush needed",
+                       "bytes_per_row": bytes_per_row, "selector": "learned (shipped parameters)"},
+            "roofline": {"bound": "hbm", "kernel": "batch_agg", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": ncu_traffic("batch_agg"),
+                         "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": agg_ms,
+                         "pipeline_frac": (alg_bytes / (ms / 1e3) / 1e9) / peak},
+            "kernels_ms_per_step": kern,
+            "cpu_baseline": cpu,
+            "e2e": {"value": rows_e2e / (e2e_ms_max / 1e3), "unit": "rows/s", "h2d_bytes_per_step": int(io["h2d_bytes"]),
+                    "d2h_bytes_per_step": int(io["d2h_bytes"]), "ms_per_step": e2e_ms_max, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "vs_plain": cmp,
         }
         print(json.dumps(line), flush=True)
     h.close()

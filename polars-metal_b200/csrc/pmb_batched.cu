@@ -410,25 +410,32 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
   const int init_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)total * std::max(1, rec / 8) + 255) / 256,
                                                                       (int64_t)h->sm_count * 16));
   const int fin_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)total + 255) / 256, (int64_t)h->sm_count * 16));
-  // the device work of the round: one graph, replayed while the launch shape is the same
-  auto enqueue = [&](cudaStream_t s, cudaEvent_t a0, cudaEvent_t a1) -> cudaError_t {
+  // the device work of the round: one graph, replayed while the launch shape is the same; with
+  // profiling on it runs eagerly with an event pair around each kernel
+  auto enqueue = [&](cudaStream_t s, bool prof, cudaEvent_t a0, cudaEvent_t a1) -> cudaError_t {
     cudaError_t e;
     if ((e = cudaMemsetAsync(status, 0, (size_t)nq * 64, s))) return e;
     if ((e = cudaMemsetAsync(ctr, 0, 8 * ((size_t)nq + 1), s))) return e;
     if ((e = cudaMemsetAsync(out_base + bits_start, 0, (size_t)(ob - bits_start), s))) return e;
+    if (prof) pmb_kernel_begin(h, "batch_table_init");
     k_table_init_pub(keys, (int64_t)total, (uint64_t*)recs, (int64_t)total, rec / 8, ri, init_blocks, s);
+    if (prof) pmb_kernel_end(h);
     if (a0 && (e = cudaEventRecord(a0, s))) return e;
+    if (prof) pmb_kernel_begin(h, "batch_agg");
     void* args[] = {&B};
     if ((e = cudaLaunchKernel((const void*)k, dim3(h->sm_count), dim3(J.nt), args, (size_t)J.smem, s))) return e;
+    if (prof) pmb_kernel_end(h);
     if (a1 && (e = cudaEventRecord(a1, s))) return e;
+    if (prof) pmb_kernel_begin(h, "batch_finalize");
     k_batch_finalize<<<fin_blocks, 256, 0, s>>>(F);
+    if (prof) pmb_kernel_end(h);
     return cudaGetLastError();
   };
   if (tuning) {
     cudaEvent_t a0, a1;
     PMB_CUDA(h, cudaEventCreate(&a0));
     PMB_CUDA(h, cudaEventCreate(&a1));
-    cudaError_t e = enqueue(h->stream, a0, a1);
+    cudaError_t e = enqueue(h->stream, false, a0, a1);
     if (e == cudaSuccess) e = cudaEventSynchronize(a1);
     float ms = 0;
     if (e == cudaSuccess) cudaEventElapsedTime(&ms, a0, a1);
@@ -436,6 +443,8 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
     cudaEventDestroy(a1);
     PMB_CUDA(h, e);
     if (agg_ms) *agg_ms = ms;
+  } else if (h->profiling) {
+    PMB_CUDA(h, enqueue(h->stream, true, nullptr, nullptr));
   } else {
     // graph key: everything the captured launches read
     std::string key;
@@ -456,7 +465,7 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
       gc.key.clear();
       cudaGraph_t g;
       PMB_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-      cudaError_t e = enqueue(h->stream, nullptr, nullptr);
+      cudaError_t e = enqueue(h->stream, false, nullptr, nullptr);
       cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
       PMB_CUDA(h, e);
       PMB_CUDA(h, e2);
@@ -465,10 +474,8 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
       PMB_CUDA(h, e);
       gc.key = key;
     }
-    pmb_kernel_begin(h, "batch_graph");
-    cudaError_t e = cudaGraphLaunch(gc.exec, h->stream);
-    pmb_kernel_end(h);
-    PMB_CUDA(h, e);
+    h->launches += 3;  // table init, aggregation, finalize
+    PMB_CUDA(h, cudaGraphLaunch(gc.exec, h->stream));
   }
   // group counts and status words of every query
   std::vector<unsigned long long> cnt(nq + 1);

@@ -205,9 +205,12 @@ def batch_sizes(n_queries: int, seed: int, mu: float = 11.512925464970229, sigma
     return rows, card, s
 
 
-def make_batch(n_queries: int = 4096, seed: int = 4, device="cpu", max_total: int | None = None):
+def make_batch(n_queries: int = 4096, seed: int = 4, device="cpu", max_total: int | None = None,
+               stop_rows: int | None = None):
     """Independent filter -> group_by queries: key int32 (Zipf over its cardinality), v float64
-    N(0,1) with 1% nulls; filter v > -1; sum/mean/min/max(v), len. Returns Tables."""
+    N(0,1) with 1% nulls; filter v > -1; sum/mean/min/max(v), len. Returns Tables. With
+    `stop_rows`, only the leading queries up to that many rows are made (the same ones as in
+    the full batch on the same device)."""
     torch = _torch()
     rows, card, s = batch_sizes(n_queries, seed)
     if max_total is not None and rows.sum() > max_total:
@@ -215,7 +218,11 @@ def make_batch(n_queries: int = 4096, seed: int = 4, device="cpu", max_total: in
         card = np.minimum(card, rows)
     g = _gen(seed, device)
     out = []
+    made = 0
     for i in range(n_queries):
+        if stop_rows is not None and made >= stop_rows:
+            break
+        made += int(rows[i])
         n, d = int(rows[i]), int(max(card[i], 1))
         k = zipf_keys(n, d, float(s[i]), g, device, torch.int64)
         k = ((k * 0x9E3779B1 + i) & 0x7FFFFFFF).to(torch.int32)
