@@ -7,7 +7,7 @@
 //      singletons (the group estimate), the heaviest keys (the hot keys of the query) and the
 //      float-sum ranges; with an installed strategy selector its predicted group count can only
 //      enlarge the estimate;
-//   2. the host sizes every query's global table (4 slots per estimated group) inside one arena,
+//   2. the host sizes every query's global table (2.5 slots per estimated group) inside one arena,
 //      cuts the queries into work items (query, range of 128-row units) and uploads them;
 //   3. one init kernel, the persistent run-time compiled kernel pmb_jit_batch_agg over the work
 //      queue, and k_batch_finalize (every query's occupied slots into its output columns, in slot
@@ -152,7 +152,11 @@ struct BatchFin {
   uint8_t* out_base;
   const unsigned long long* out_off;   // per query x output column x {data, validity}
   unsigned long long total_slots;
+  const unsigned long long* chunk_off;  // nq + 1: first finalize chunk of each query
 };
+
+constexpr int FIN_NT = 256, FIN_PER = 8, FIN_CH = FIN_NT * FIN_PER;  // a finalize CTA's slots
+constexpr int FIN_W = FIN_CH / 32 + 2;  // bitmap words a CTA's output rows can touch
 
 __device__ __forceinline__ int find_query(const unsigned long long* off, int nq, unsigned long long g) {
   int lo = 0, hi = nq - 1;
@@ -174,52 +178,102 @@ __device__ __forceinline__ void store_out(uint8_t* d, int bytes, unsigned long l
   }
 }
 
-__global__ void __launch_bounds__(256) k_batch_finalize(const __grid_constant__ BatchFin F) {
-  const int lane = threadIdx.x & 31;
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  const unsigned long long span = (F.total_slots + stride - 1) / stride * stride;
-  for (unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; g < span; g += stride) {
-    int qi = -1;
-    bool occ = false;
-    if (g < F.total_slots) {
-      qi = find_query(F.slot_off, F.nq, g);
-      const unsigned long long s = g - F.slot_off[qi];
-      const uint64_t cap = F.gcap[qi];
-      if (s < cap) occ = F.keys[g] != PMB_EMPTY64;
-      else if (s == cap) occ = F.status[qi][1] != 0u;
-    }
-    // one atomic per query and warp for the output positions
-    const unsigned peers = __match_any_sync(0xffffffffu, occ ? qi : -1);
-    unsigned long long base = 0;
-    if (occ && lane == __ffs(peers) - 1) base = atomicAdd(&F.count[qi], (unsigned long long)__popc(peers));
-    base = __shfl_sync(0xffffffffu, base, __ffs(peers) - 1);
-    if (!occ) continue;
-    const unsigned long long p = base + __popc(peers & ((1u << lane) - 1u));
-    const DQuery& q = F.qs[qi];
+// One CTA per chunk of FIN_CH consecutive slots of one query (the extra slot of the EMPTY-bit key
+// included). The occupied slots are compacted into a shared list in slot order (coalesced key
+// reads, one ballot per 32 slots); after one atomic per CTA on the query's row count, every
+// thread finalises list entries i, i + FIN_NT, ... into output rows base + i, so all lanes work
+// and the output writes are coalesced. The validity bits (and Bool key data) are built in shared
+// memory and merged into the output bitmaps with one atomic OR per word.
+__global__ void __launch_bounds__(FIN_NT) k_batch_finalize(const __grid_constant__ BatchFin F) {
+  __shared__ unsigned s_vb[PMB_MAX_OUT][FIN_W];
+  __shared__ unsigned s_db[PMB_MAX_KEYS][FIN_W];
+  __shared__ unsigned s_off[FIN_PER][FIN_NT / 32];
+  __shared__ unsigned short s_list[FIN_CH];
+  __shared__ unsigned long long s_base;
+  __shared__ unsigned s_total;
+  __shared__ __align__(16) unsigned char s_q[sizeof(DQuery)];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned long long c = blockIdx.x;
+  const int qi = find_query(F.chunk_off, F.nq, c);
+  // the query descriptor in shared memory: the per-row decoding reads it many times
+  static_assert(sizeof(DQuery) % 4 == 0, "DQuery is copied in 4-byte words");
+  for (int i = tid; i < (int)(sizeof(DQuery) / 4); i += FIN_NT)
+    reinterpret_cast<unsigned*>(s_q)[i] = reinterpret_cast<const unsigned*>(F.qs + qi)[i];
+  const DQuery& q = *reinterpret_cast<const DQuery*>(s_q);
+  const uint64_t cap = F.gcap[qi];
+  const unsigned long long g0 = F.slot_off[qi];
+  const unsigned long long s0 = (c - F.chunk_off[qi]) * FIN_CH;
+  const bool extra = F.status[qi][1] != 0u;  // a row had the key whose bits equal EMPTY
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned bal[FIN_PER];
+#pragma unroll
+  for (int j = 0; j < FIN_PER; j++) {
+    const unsigned long long s = s0 + (unsigned long long)j * FIN_NT + tid;
+    bool o = false;
+    if (s < cap) o = F.keys[g0 + s] != PMB_EMPTY64;
+    else if (s == cap) o = extra;
+    bal[j] = __ballot_sync(0xffffffffu, o);
+    if (lane == 0) s_off[j][warp] = __popc(bal[j]);
+  }
+  for (int i = tid; i < PMB_MAX_OUT * FIN_W; i += FIN_NT) (&s_vb[0][0])[i] = 0u;
+  for (int i = tid; i < PMB_MAX_KEYS * FIN_W; i += FIN_NT) (&s_db[0][0])[i] = 0u;
+  __syncthreads();
+  if (tid == 0) {
+    unsigned acc = 0;
+    for (int j = 0; j < FIN_PER; j++)
+      for (int w = 0; w < FIN_NT / 32; w++) {
+        const unsigned v = s_off[j][w];
+        s_off[j][w] = acc;
+        acc += v;
+      }
+    s_total = acc;
+    s_base = acc ? atomicAdd(&F.count[qi], (unsigned long long)acc) : 0ULL;
+  }
+  __syncthreads();
+  const unsigned total = s_total;
+  if (total == 0) return;  // the whole CTA leaves together
+#pragma unroll
+  for (int j = 0; j < FIN_PER; j++)
+    if ((bal[j] >> lane) & 1u) s_list[s_off[j][warp] + __popc(bal[j] & lt)] = (unsigned short)(j * FIN_NT + tid);
+  __syncthreads();
+  const unsigned long long base = s_base, a = base & ~31ULL;
+  const unsigned long long* oo = F.out_off + (size_t)qi * F.n_out * 2;
+  for (unsigned i = tid; i < total; i += FIN_NT) {
+    const unsigned long long p = base + i;
+    const unsigned long long g = g0 + s0 + s_list[i];
+    const unsigned r = (unsigned)(p - a);  // bit of this row in the CTA's bitmaps
     const unsigned long long klo = F.keys[g];
     const uint8_t* rec = F.recs + g * (unsigned long long)F.rec_bytes;
-    const unsigned long long* oo = F.out_off + (size_t)qi * F.n_out * 2;
     int oc = 0;
     for (int k = 0; k < q.n_keys; k++, oc++) {
       uint64_t v = 0;
       const bool valid = unpack_field(q.key[k], klo, 0ULL, v);
       const int dt = q.col[q.key[k].col].dtype;
-      uint8_t* d = F.out_base + oo[2 * oc];
-      unsigned int* vw = reinterpret_cast<unsigned int*>(F.out_base + oo[2 * oc + 1]);
       if (dt == PMB_BOOL) {
-        if (valid && v) atomicOr(reinterpret_cast<unsigned int*>(d) + (p >> 5), 1u << (p & 31));
+        if (valid && v) atomicOr(&s_db[k][r >> 5], 1u << (r & 31));
       } else {
-        store_out(d, pmb_dtype_bytes(dt), p, v);
+        store_out(F.out_base + oo[2 * oc], pmb_dtype_bytes(dt), p, v);
       }
-      if (valid) atomicOr(vw + (p >> 5), 1u << (p & 31));
+      if (valid) atomicOr(&s_vb[oc][r >> 5], 1u << (r & 31));
     }
-    for (int a = 0; a < q.n_aggs; a++, oc++) {
-      const DAggOut& A = q.agg[a];
+    for (int ag = 0; ag < q.n_aggs; ag++, oc++) {
+      const DAggOut& A = q.agg[ag];
       bool valid = true;
       uint64_t bits = 0;
       finalize_agg(q, A, rec, valid, bits);
       store_out(F.out_base + oo[2 * oc], pmb_dtype_bytes(A.out_dtype), p, bits);
-      if (valid) atomicOr(reinterpret_cast<unsigned int*>(F.out_base + oo[2 * oc + 1]) + (p >> 5), 1u << (p & 31));
+      if (valid) atomicOr(&s_vb[oc][r >> 5], 1u << (r & 31));
+    }
+  }
+  __syncthreads();
+  const int nw = (int)((base - a + total + 31) / 32);
+  for (int i = tid; i < F.n_out * nw; i += FIN_NT) {
+    const int oc = i / nw, w = i % nw;
+    const unsigned v = s_vb[oc][w];
+    if (v) atomicOr(reinterpret_cast<unsigned*>(F.out_base + oo[2 * oc + 1]) + (a >> 5) + w, v);
+    if (oc < q.n_keys && q.col[q.key[oc].col].dtype == PMB_BOOL) {
+      const unsigned d = s_db[oc][w];
+      if (d) atomicOr(reinterpret_cast<unsigned*>(F.out_base + oo[2 * oc]) + (a >> 5) + w, d);
     }
   }
 }
@@ -253,6 +307,9 @@ std::string signature(const DQuery& q) {
 struct TuneChoice {
   int nt = 1024;
   int item_units = 256;
+  int nbuf = 2;       // unit buffers per warp
+  int warm_rule = 1;  // 0: every query fills a warm table; 1: only queries whose groups fit it, or
+                      // whose items hold at least as many rows as the query has groups
 };
 std::mutex g_tune_mu;
 std::map<std::string, TuneChoice> g_tuned;  // signature + size class -> choice
@@ -275,7 +332,7 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
   const CompiledQuery& c0 = cqs[qidx[0]];
   const int rec = c0.dq.rec_bytes;
   JitPlan J;
-  int rc = pmb_plan_jit_batch(h, c0, tc.nt, h->max_smem_optin, &J);
+  int rc = pmb_plan_jit_batch(h, c0, tc.nt, tc.nbuf, h->max_smem_optin, &J);
   if (rc) return rc;
   cudaKernel_t k = nullptr;
   rc = pmb_jit_batch_kernel(h, c0, J, &k);
@@ -333,6 +390,8 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
         A.fx[cq.dq.field[f].fx_slot] = cq.dq.field[f].fx;
         A.fx_e[cq.dq.field[f].fx_slot] = cq.dq.fx_e[cq.dq.field[f].fx_slot];
       }
+    const int64_t g = std::max<int64_t>(est[qidx[i]], 1);
+    A.flags = (tc.warm_rule == 0 || g <= 2LL * J.warm_cap || (int64_t)tc.item_units * 128 >= g) ? 1 : 0;
     for (long long u0 = 0; u0 < A.n_units; u0 += tc.item_units)
       items.push_back({i, 0, u0, std::min<long long>(A.n_units, u0 + tc.item_units)});
   }
@@ -343,7 +402,8 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
   unsigned long long* d_soff = (unsigned long long*)pmb_ws_alloc(h, 8 * ((size_t)nq + 1));
   uint64_t* d_cap = (uint64_t*)pmb_ws_alloc(h, 8 * (size_t)nq);
   unsigned int** d_st = (unsigned int**)pmb_ws_alloc(h, sizeof(void*) * nq);
-  if (!d_jp || !d_items || !ctr || !d_qs || !d_soff || !d_cap || !d_st)
+  unsigned long long* d_coff = (unsigned long long*)pmb_ws_alloc(h, 8 * ((size_t)nq + 1));
+  if (!d_jp || !d_items || !ctr || !d_qs || !d_soff || !d_cap || !d_st || !d_coff)
     return pmb_fail(h, PMB_E_OOM, "workspace exhausted (batch plan)");
   // outputs: per query and output column a data block and a validity bitmap (sized by capacity)
   const int n_out = c0.dq.n_keys + c0.dq.n_aggs;
@@ -387,6 +447,9 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
   PMB_CUDA(h, cudaMemcpyAsync(d_cap, cap.data(), 8 * cap.size(), cudaMemcpyHostToDevice, h->stream));
   PMB_CUDA(h, cudaMemcpyAsync(d_st, hst.data(), sizeof(void*) * nq, cudaMemcpyHostToDevice, h->stream));
   PMB_CUDA(h, cudaMemcpyAsync(d_ooff, out_off.data(), 8 * out_off.size(), cudaMemcpyHostToDevice, h->stream));
+  std::vector<unsigned long long> chunk_off(nq + 1, 0);
+  for (int i = 0; i < nq; i++) chunk_off[i + 1] = chunk_off[i] + (cap[i] + 1 + FIN_CH - 1) / FIN_CH;
+  PMB_CUDA(h, cudaMemcpyAsync(d_coff, chunk_off.data(), 8 * chunk_off.size(), cudaMemcpyHostToDevice, h->stream));
   // record identity (every query of the round has the same record layout)
   RecInit ri;
   memset(&ri, 0, sizeof(ri));
@@ -406,10 +469,11 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
   F.out_base = out_base;
   F.out_off = d_ooff;
   F.total_slots = total;
+  F.chunk_off = d_coff;
   PMB_CUDA(h, cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, J.smem));
   const int init_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)total * std::max(1, rec / 8) + 255) / 256,
                                                                       (int64_t)h->sm_count * 16));
-  const int fin_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)total + 255) / 256, (int64_t)h->sm_count * 16));
+  const int fin_blocks = (int)chunk_off[nq];
   // the device work of the round: one graph, replayed while the launch shape is the same; with
   // profiling on it runs eagerly with an event pair around each kernel
   auto enqueue = [&](cudaStream_t s, bool prof, cudaEvent_t a0, cudaEvent_t a1) -> cudaError_t {
@@ -427,7 +491,7 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
     if (prof) pmb_kernel_end(h);
     if (a1 && (e = cudaEventRecord(a1, s))) return e;
     if (prof) pmb_kernel_begin(h, "batch_finalize");
-    k_batch_finalize<<<fin_blocks, 256, 0, s>>>(F);
+    k_batch_finalize<<<fin_blocks, FIN_NT, 0, s>>>(F);
     if (prof) pmb_kernel_end(h);
     return cudaGetLastError();
   };
@@ -631,6 +695,12 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
       pmb_set_fx(cqs[i].dq, skb[j].fx_expo, 3, pbits + 1, tbits + 1);
       total_rows += cqs[i].dq.n_rows;
     }
+    if (timing) {
+      int64_t e_sum = 0, p_sum = 0;
+      for (int j = 0; j < nb; j++) e_sum += est[batch[j]], p_sum += pred[j];
+      fprintf(stderr, "batch estimates: %lld groups in total (selector predictions %lld)\n", (long long)e_sum,
+              (long long)p_sum);
+    }
     phase("estimates");
     // 3. autotune (first batch of a signature and size class), then the round itself
     int size_class = 0;
@@ -647,7 +717,8 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
       }
     }
     if (!have && !getenv("PMB_NO_AUTOTUNE")) {
-      static const TuneChoice cands[] = {{1024, 64}, {1024, 256}, {1024, 1024}, {512, 256}};
+      static const TuneChoice cands[] = {{1024, 256, 1, 0}, {1024, 256, 2, 0}, {1024, 256, 2, 1}, {1024, 64, 2, 1},
+                                         {1024, 1024, 2, 1}, {512, 256, 2, 1},  {512, 1024, 2, 1}};
       float best = 1e30f;
       for (const TuneChoice& c : cands) {
         float ms = 0;
@@ -655,6 +726,9 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
         rc = batch_round(h, cqs, batch, est, sk, c, true, outs, nullptr, &ms);
         if (rc) return fail_all(rc);
         pmb_ws_release(h, mark);
+        if (timing)
+          fprintf(stderr, "batch tuning candidate %d threads / %d units / %d buffers / warm rule %d: %.3f ms\n", c.nt,
+                  c.item_units, c.nbuf, c.warm_rule, ms);
         if (ms < best) {
           best = ms;
           tc = c;
@@ -663,6 +737,9 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
       std::lock_guard<std::mutex> lock(g_tune_mu);
       g_tuned[tkey] = tc;
     }
+    if (timing)
+      fprintf(stderr, "batch tuning: %d threads, %d units per item, %d buffers, warm rule %d\n", tc.nt, tc.item_units,
+              tc.nbuf, tc.warm_rule);
     // 4. the rounds: queries grouped by record layout (a query whose float sums would have too few
     //    fraction bits sums them in double-double: another layout); queries that overflowed (3x
     //    table) or left their float-sum range (already widened) run again
@@ -690,6 +767,12 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
       for (auto& g : groups) {
         rc = batch_round(h, cqs, g.second, est, sk, tc, false, outs, &next, nullptr);
         if (rc) return fail_all(rc);
+        if (timing) {
+          int64_t rows = 0, e = 0;
+          for (int i : g.second) rows += cqs[i].dq.n_rows, e += est[i];
+          fprintf(stderr, "batch round %d: %zu queries, %lld rows, %lld estimated groups, %zu to run again\n", round,
+                  g.second.size(), (long long)rows, (long long)e, next.size());
+        }
       }
       again.swap(next);
     }

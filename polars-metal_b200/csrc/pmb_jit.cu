@@ -803,11 +803,11 @@ int pmb_jit_hash_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J
   return jit_kernel(h, pmb_jit_source(cq, J), "pmb_jit_hash_agg", out);
 }
 
-int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int max_smem_optin, JitPlan* J) {
+int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf, int max_smem_optin, JitPlan* J) {
   const DQuery& q = cq.dq;
   memset(J, 0, sizeof(*J));
   J->nt = nt;
-  J->nbuf = 1;
+  J->nbuf = nbuf;
   const int W = nt / 32;
   int off = 0, tx = 0;
   for (int c = 0; c < q.n_cols; c++) {
@@ -828,9 +828,14 @@ int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int max_s
   pmb_jit_slayout(q, &S);
   J->srec = S.bytes;
   const int budget = max_smem_optin - 1024;
+  // fewer buffers per warp when wide rows do not leave room for them
+  while (nbuf > 1 && (int)pmb_align((size_t)(8 * W * nbuf), 128) + W * nbuf * J->buf_bytes + W * 128 * 4 +
+                             64 + W * J->srec > budget)
+    nbuf--;
+  J->nbuf = nbuf;
   J->off_bars = 0;
-  J->off_buf = (int)pmb_align((size_t)(8 * W), 128);
-  J->off_q = J->off_buf + W * J->buf_bytes;
+  J->off_buf = (int)pmb_align((size_t)(8 * W * nbuf), 128);
+  J->off_q = J->off_buf + W * nbuf * J->buf_bytes;
   const int used = J->off_q + W * 128 * 4;
   if (used > budget) return pmb_fail(h, PMB_E_UNSUPPORTED, "query touches too many columns for the unit buffers");
   // hot keys: 8 per item, one record per warp each; warm: the largest power of two that fits
@@ -877,7 +882,7 @@ static int debug_compile(const pmb_query* q, const pmb_column* cols, int32_t n_c
       msg = "128-bit keys use the prebuilt kernel";
     } else {
       JitPlan J;
-      rc = batch ? pmb_plan_jit_batch(&h, cq, 1024, 232448, &J) : pmb_plan_jit(&h, cq, true, 232448, &J);
+      rc = batch ? pmb_plan_jit_batch(&h, cq, 1024, 2, 232448, &J) : pmb_plan_jit(&h, cq, true, 232448, &J);
       if (rc == PMB_OK) {
         std::vector<char> cubin;
         const std::string src = batch ? pmb_jit_source(cq, J) + "\n" + std::string(kBatchSkeleton) : pmb_jit_source(cq, J);

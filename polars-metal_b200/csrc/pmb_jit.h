@@ -22,7 +22,7 @@ struct JitParams {
   unsigned long long* kstats;
   const uint8_t* ttab;
   int tnb;
-  int tpad;
+  int flags;  // batched kernel: bit 0 = fill the CTA's warm table
   int fx[8];
   int fx_e[8];
 };
@@ -79,8 +79,9 @@ struct JBatchH {
   unsigned long long* ticket;
 };
 
-// the batched kernel (pmb_jit_batch.cuh): layout for `nt` threads and its compiled kernel
-int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int max_smem_optin, JitPlan* J);
+// the batched kernel (pmb_jit_batch.cuh): layout for `nt` threads with `nbuf` unit buffers per
+// warp, and its compiled kernel
+int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf, int max_smem_optin, JitPlan* J);
 int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out);
 // launches over the global table and key lists set up in P (gkeys, grecs, gcap, status, lists)
 int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const JitPlan& J, const HashParams& P,

@@ -7,9 +7,12 @@
 //   1. the CTA's tables are reset: the query's hot keys (one record per warp each) and a warm
 //      table filled on the fly (find-or-insert with a short probe; a full table sends the row to
 //      the global table instead);
-//   2. warps stream the item's 128-row units through their buffers (1-D TMA copies, a bounded
-//      wait), classify rows (filter, key, hot / warm / cold) into the warp queue and apply them:
-//      shared-memory records with native 32-bit atomics, cold rows to the query's global table;
+//   2. warps stream the item's 128-row units through their J_NBUF buffers (1-D TMA copies, the
+//      warp's next units in flight while it works on one; bounded waits), classify rows (filter,
+//      key, hot / warm / cold) into the warp queue and apply them: shared-memory records with
+//      native 32-bit atomics, cold rows to the query's global table. The warm table is used only
+//      for queries whose flags bit 0 the host set (few groups, or many rows per group in an item);
+//      otherwise a key's rows would rarely meet in one item and the table would only add work;
 //   3. after a CTA barrier the hot records of all warps are folded and, with the warm records,
 //      merged into the query's global table.
 // A failed wait stops the warp for the rest of the launch and reports PMB_ST_TIMEOUT in the
@@ -49,19 +52,23 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_batch_agg(const __
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int W = J_NT / 32;
   unsigned long long* all_bars = reinterpret_cast<unsigned long long*>(sm + J_OFF_BARS);
-  unsigned long long* bar = all_bars + warp * J_NBUF;
-  unsigned char* st = sm + J_OFF_BUF + warp * J_NBUF * J_BUF_BYTES;
+  unsigned long long* bars = all_bars + warp * J_NBUF;
+  unsigned char* bufs = sm + J_OFF_BUF + warp * J_NBUF * J_BUF_BYTES;
   unsigned* q = reinterpret_cast<unsigned*>(sm + J_OFF_Q) + warp * J_UNIT;
   unsigned long long* wk = reinterpret_cast<unsigned long long*>(sm + J_OFF_TKEYS);  // J_SW warm keys
   unsigned long long* hk = reinterpret_cast<unsigned long long*>(sm + J_OFF_TVAL);   // J_H hot keys
   unsigned char* srecs = sm + J_OFF_SRECS;  // W * J_H hot records, then J_SW warm records
   __shared__ long long s_item;
   __shared__ int s_nhot;
+  // the item's query parameters live in shared memory: the unit loop reads them for every row,
+  // and the small L1 left beside the tables would keep evicting them
+  __shared__ __align__(16) unsigned char s_par[sizeof(JParams)];
+  const JParams& P = *reinterpret_cast<const JParams*>(s_par);
   if (tid == 0) {
     for (int b = 0; b < W * J_NBUF; b++) mbar_init(&all_bars[b], 1);
     mbar_fence_init();
   }
-  unsigned parity = 0;
+  unsigned parity = 0, pending = 0;  // per buffer: phase to wait for, copy in flight
   bool dead = false;  // a wait of this warp gave up: it does no more work in this launch
   const unsigned long long pol = pmb_policy_evict_first();
   const unsigned lt = (1u << lane) - 1u;
@@ -72,9 +79,25 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_batch_agg(const __
     const long long it = s_item;
     if (it >= B.n_items) break;
     const JBatchItem I = B.items[it];
-    const JParams& P = B.qp[I.q];
-    for (int i = tid; i < J_SW; i += J_NT) wk[i] = PMB_EMPTY64;
-    for (int w = tid; w < (W * J_H + J_SW) * J_SREC_WORDS; w += J_NT)
+    for (int i = tid; i < (int)(sizeof(JParams) / 4); i += J_NT)
+      reinterpret_cast<unsigned*>(s_par)[i] = reinterpret_cast<const unsigned*>(B.qp + I.q)[i];
+    __syncthreads();
+    const bool warm = J_SW > 0 && (P.flags & 1);
+    const long long n_full = P.n_rows / J_UNIT;
+    // the warp's first units of the item go in flight while the tables are reset
+    if (lane == 0 && !dead) {
+      for (int b = 0; b < J_NBUF; b++) {
+        const long long uu = I.u0 + warp + (long long)b * W;
+        if (uu < I.u1 && uu < n_full) {
+          fence_proxy_async();  // the warp's reads of the buffer's previous unit come before the copy's writes
+          j_issue_unit(P, bufs + b * J_BUF_BYTES, uu, &bars[b], pol);
+          pending |= 1u << b;
+        }
+      }
+    }
+    if (warm)
+      for (int i = tid; i < J_SW; i += J_NT) wk[i] = PMB_EMPTY64;
+    for (int w = tid; w < (W * J_H + (warm ? J_SW : 0)) * J_SREC_WORDS; w += J_NT)
       reinterpret_cast<unsigned*>(srecs)[w] = J_SIDENT[w % J_SREC_WORDS];
     if (tid == 0) {
       const int nh = (J_H > 0 && P.hot_keys) ? (int)min(*P.hot_n, (unsigned)J_H) : 0;
@@ -83,20 +106,18 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_batch_agg(const __
     }
     __syncthreads();
     const int nhot = s_nhot;
+    int b = 0;
     for (long long u = I.u0 + warp; u < I.u1 && !dead; u += W) {
       const long long row0 = u * J_UNIT;
       const int rows = (int)min((long long)J_UNIT, P.n_rows - row0);
+      unsigned char* st = bufs + b * J_BUF_BYTES;
       if (rows == J_UNIT) {
         bool ok = true;
         if (lane == 0) {
-          fence_proxy_async();  // the warp's reads of its previous unit come before the copy's writes
-          j_issue_unit(P, st, u, bar, pol);
-          ok = mbar_wait_bounded(bar, parity & 1u);
+          ok = mbar_wait_bounded(&bars[b], (parity >> b) & 1u);
           if (ok) {
-            parity ^= 1u;
-          } else {
-            mbar_wait_bounded(bar, parity & 1u);  // one more bounded wait for the copy in flight
-            atomicOr(P.status, PMB_ST_TIMEOUT);
+            parity ^= 1u << b;
+            pending &= ~(1u << b);
           }
         }
         if (!__shfl_sync(0xffffffffu, ok, 0)) {
@@ -104,7 +125,7 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_batch_agg(const __
           break;
         }
       } else {
-        j_copy_unit(P, st, row0, rows);
+        j_copy_unit(P, st, row0, rows);  // the query's last, partial unit: no copy was issued into this buffer
       }
       __syncwarp();
       int ns = 0, nc = 0;
@@ -120,7 +141,7 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_batch_agg(const __
           unsigned rec = J_MISS;
           for (int i = 0; i < nhot; i++)
             if (hk[i] == key) rec = (unsigned)(warp * J_H + i);
-          if (rec == J_MISS) {
+          if (rec == J_MISS && warm) {
             const unsigned s = j_wfind(wk, key, j_hash(key));
             if (s != J_MISS) rec = (unsigned)(W * J_H) + s;
           }
@@ -160,6 +181,23 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_batch_agg(const __
         }
       }
       __syncwarp();
+      // this buffer is free again: bring in the warp's unit J_NBUF steps ahead (inside the item)
+      if (lane == 0) {
+        const long long uu = u + (long long)J_NBUF * W;
+        if (uu < I.u1 && uu < n_full) {
+          fence_proxy_async();
+          j_issue_unit(P, st, uu, &bars[b], pol);
+          pending |= 1u << b;
+        }
+      }
+      b = (b + 1 == J_NBUF) ? 0 : b + 1;
+    }
+    if (dead && lane == 0 && pending) {
+      // copies still in flight land (bounded) before the warp gives up its buffers
+      for (int bb = 0; bb < J_NBUF; bb++)
+        if ((pending >> bb) & 1u) mbar_wait_bounded(&bars[bb], (parity >> bb) & 1u);
+      pending = 0;
+      atomicOr(P.status, PMB_ST_TIMEOUT);
     }
     __syncthreads();
     // merge the item's CTA records into the query's global table
@@ -171,13 +209,14 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_batch_agg(const __
       const long long gi = j_gfind(P, key, j_hash(key));
       if (gi >= 0) j_merge_sg(P, P.grecs + (unsigned long long)gi * J_REC, r0);
     }
-    for (int i = tid; i < J_SW; i += J_NT) {
-      const unsigned long long key = wk[i];
-      if (key == PMB_EMPTY64) continue;
-      const unsigned char* r = srecs + (W * J_H + i) * J_SREC;
-      if (*reinterpret_cast<const unsigned*>(r + J_LEN_SOFF) == 0u) continue;
-      const long long gi = j_gfind(P, key, j_hash(key));
-      if (gi >= 0) j_merge_sg(P, P.grecs + (unsigned long long)gi * J_REC, r);
-    }
+    if (warm)
+      for (int i = tid; i < J_SW; i += J_NT) {
+        const unsigned long long key = wk[i];
+        if (key == PMB_EMPTY64) continue;
+        const unsigned char* r = srecs + (W * J_H + i) * J_SREC;
+        if (*reinterpret_cast<const unsigned*>(r + J_LEN_SOFF) == 0u) continue;
+        const long long gi = j_gfind(P, key, j_hash(key));
+        if (gi >= 0) j_merge_sg(P, P.grecs + (unsigned long long)gi * J_REC, r);
+      }
   }
 }

@@ -47,7 +47,7 @@ struct JParams {
   unsigned long long* kstats;
   const unsigned char* ttab;  // sampled-key table built by the host: keys of all buckets, then values
   int tnb;                    // its buckets (4 slots each), at most J_TNB
-  int tpad;
+  int flags;                  // batched kernel: bit 0 = fill the CTA's warm table
   int fx[8];    // fraction bits F of each exact float-sum slot (sums hold x * 2^F)
   int fx_e[8];  // every value of the slot satisfies |x| < 2^fx_e
 };
