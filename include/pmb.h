@@ -120,7 +120,9 @@ enum {
   PMB_STRATEGY_AUTO = 0,        /* sketch + learned selector, heuristic fallback   */
   PMB_STRATEGY_SMEM_HASH = 1,   /* per-CTA shared-memory tables + small global merge */
   PMB_STRATEGY_GLOBAL_HASH = 2, /* global open addressing with a shared-memory hot cache */
-  PMB_STRATEGY_SORT = 3         /* packed-key LSD radix sort + segmented reduce   */
+  PMB_STRATEGY_SORT = 3,        /* packed-key LSD radix sort + segmented reduce   */
+  PMB_STRATEGY_PARTITIONED = 4  /* rows scattered by key-hash partition, then one
+                                   shared-memory table per partition            */
 };
 
 typedef struct pmb_query {

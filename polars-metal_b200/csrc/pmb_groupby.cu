@@ -1042,6 +1042,8 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
   if (!h) return PMB_E_INVALID;
   if (!out) return pmb_fail(h, PMB_E_INVALID, "out is NULL");
   *out = nullptr;
+  if (q && (q->strategy < PMB_STRATEGY_AUTO || q->strategy > PMB_STRATEGY_PARTITIONED))
+    return pmb_fail(h, PMB_E_INVALID, "unknown strategy");
   PMB_CUDA(h, cudaSetDevice(h->device));
   CompiledQuery cq;
   int rc = pmb_compile_groupby(h, q, cols, n_cols, &cq);
@@ -1103,7 +1105,8 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
       }
     }
     if (est <= 0) est = e;
-    if (strategy == PMB_STRATEGY_SORT) rc = pmb_groupby_sort(h, cq, r);
+    if (strategy == PMB_STRATEGY_SORT) rc = pmb_groupby_sort(h, cq, r, 0);
+    else if (strategy == PMB_STRATEGY_PARTITIONED) rc = pmb_groupby_sort(h, cq, r, std::max<int64_t>(est, 1));
     else rc = pmb_groupby_hash(h, cq, q, strategy, est, have_sk ? &sk : nullptr, r);
     if (rc == PMB_RETRY_DD && pass < 3) {
       // a float sum outgrew the fixed point: its column now sums in double-double

@@ -87,7 +87,8 @@ void k_table_init_pub(unsigned long long* keys, int64_t key_words, uint64_t* rec
                       const RecInit& ri, int blocks, cudaStream_t s);
 // sort strategy (pmb_sort.cu): packed-key LSD radix sort + segmented reduce; groups come out in
 // packed-key order
-int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r);
+// the sort strategy (part_groups == 0), or the partitioned strategy sized for part_groups groups
+int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r, int64_t part_groups);
 // learned selector (pmb_learned.cu): strategy and group count for AUTO; false when no selector is
 // installed or its output is unusable
 bool pmb_selector_pick(pmb_handle* h, const CompiledQuery& cq, int* strategy, int64_t* groups);

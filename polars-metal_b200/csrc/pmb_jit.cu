@@ -477,6 +477,53 @@ struct Gen {
     }
   }
 
+  // shared-memory record s written as a global-table record d (plain stores: d is not shared)
+  void store_sg(std::ostringstream& b) {
+    for (int i = 0; i < q.n_fields; i++) {
+      const DField& F = q.field[i];
+      const int so = S.off[i];
+      auto CU = [&](int off) { return "(*reinterpret_cast<const unsigned int*>(s + " + std::to_string(off) + "))"; };
+      auto D = [&](const char* T, int off) {
+        return "*reinterpret_cast<" + std::string(T) + "*>(d + " + std::to_string(off) + ")";
+      };
+      switch (F.kind) {
+        case F_LEN:
+        case F_CNT: b << "  " << D("unsigned int", F.off) << " = " << CU(so) << ";\n"; break;
+        case F_SUM_FX:
+          b << "  " << D("unsigned long long", F.off) << " = (unsigned long long)" << CU(so) << ";\n";
+          b << "  " << D("unsigned long long", F.off + 8) << " = ((unsigned long long)" << CU(so + 8) << " << 32) | "
+            << CU(so + 4) << ";\n";
+          b << "  " << D("unsigned int", F.off + 16) << " = " << CU(so + 12) << ";\n";
+          break;
+        case F_SUM_I:
+          b << "  " << D("unsigned long long", F.off) << " = ((unsigned long long)" << CU(so + 4) << " << 32) | " << CU(so)
+            << ";\n";
+          break;
+        case F_SUM_DD:
+          b << "  " << D("double", F.off) << " = *reinterpret_cast<const double*>(s + " << so << ");\n";
+          b << "  " << D("double", F.off + 8) << " = *reinterpret_cast<const double*>(s + " << so + 8 << ");\n";
+          break;
+        default:
+          b << "  " << D("unsigned long long", F.off) << " = *reinterpret_cast<const unsigned long long*>(s + " << so
+            << ");\n";
+      }
+    }
+  }
+
+  // the aggregated columns of row `row`, read straight from the columns (a gather)
+  void gather(std::ostringstream& b) {
+    for (int c = 0; c < q.n_cols; c++) {
+      if (!field_col[c]) continue;
+      const DCol& C = q.col[c];
+      const std::string cs = std::to_string(c);
+      if (C.dtype == PMB_BOOL)
+        b << "  r.v" << cs << " = ((P.col_data[" << cs << "][row >> 3] >> (row & 7)) & 1) != 0;\n";
+      else
+        b << "  r.v" << cs << " = reinterpret_cast<const " << ctype(C.dtype) << "*>(P.col_data[" << cs << "])[row];\n";
+      if (C.valid) b << "  r.ok" << cs << " = ((P.col_valid[" << cs << "][row >> 3] >> (row & 7)) & 1) != 0;\n";
+    }
+  }
+
   // range report of the exact float sums: status bit and the largest exponent seen
   void fxcheck(std::ostringstream& b) {
     for (int i = 0; i < q.n_fields; i++) {
@@ -587,7 +634,8 @@ __device__ __forceinline__ long long j_fdiv_i(long long a, long long b, bool& ok
     o << "}\n";
     // key
     o << "__device__ __forceinline__ unsigned long long j_key(const JRow& r) {\n  unsigned long long k = 0ULL;\n";
-    for (int i = 0; i < q.n_keys; i++) {
+    // (keys wider than 64 bits never use it: the partitioned kernel reads packed sort keys)
+    for (int i = 0; i < q.n_keys && q.key_bits <= 64; i++) {
       const DKey& K = q.key[i];
       std::string mask = K.bits < 64 ? std::to_string((1ULL << K.bits) - 1ULL) + "ULL" : "0xFFFFFFFFFFFFFFFFULL";
       std::string put = "k |= (" + raw_bits(K.col) + " & " + mask + ") << " + std::to_string(K.data_off) + ";";
@@ -612,6 +660,10 @@ __device__ __forceinline__ long long j_fdiv_i(long long a, long long b, bool& ok
     sfold(o);
     o << "}\n__device__ __forceinline__ void j_merge_sg(const JParams& P, unsigned char* d, const unsigned char* s) {\n";
     merge_sg(o);
+    o << "}\n__device__ __forceinline__ void j_store_sg(unsigned char* d, const unsigned char* s) {\n";
+    store_sg(o);
+    o << "}\n__device__ __forceinline__ void j_gather(const JParams& P, long long row, JRow& r) {\n";
+    gather(o);
     o << "}\n";
     return o.str();
   }
@@ -634,7 +686,10 @@ void pmb_jit_slayout(const DQuery& q, JitSLayout* S) {
       S->off[i] = off;
       off += k == F_SUM_DD || k == F_SUM_FX ? 16 : (eight || k == F_SUM_I ? 8 : 4);
     }
+  // records sit at random slots: a stride of 2 mod 4 words spreads them over 16 bank pairs (a
+  // multiple of 16 words would put every record's field in the same two banks)
   S->bytes = (off + 7) & ~7;
+  if (S->bytes % 16 == 0) S->bytes += 8;
   S->ident.assign(S->bytes / 4, 0u);
   for (int i = 0; i < q.n_fields; i++) {
     int k = q.field[i].kind, w = S->off[i] / 4;
@@ -858,6 +913,22 @@ int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf,
   return PMB_OK;
 }
 
+// source of the partitioned aggregation: device helpers, the parameter block, the generated row
+// functions and pmb_jit_part.cuh (not the hash kernel)
+static std::string part_source(const CompiledQuery& cq, const JitPlan& J, int key_words) {
+  Gen g(cq.dq, J);
+  std::string skel(kSkeleton);
+  size_t cut = skel.find("__device__ __forceinline__ long long j_gresolve");
+  return "#define JP_W " + std::to_string(key_words) + "\n" + std::string(kDeviceHeader) + "\n" + skel.substr(0, cut) +
+         "\n" + g.build() + "\n" + std::string(kPartSkeleton);
+}
+
+int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, JitPlan* J, cudaKernel_t* out) {
+  int rc = pmb_plan_jit_batch(h, cq, 1024, 1, h->max_smem_optin, J);
+  if (rc) return rc;
+  return jit_kernel(h, part_source(cq, *J, key_words), "pmb_jit_part_agg", out);
+}
+
 int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out) {
   return jit_kernel(h, pmb_jit_source(cq, J) + "\n" + std::string(kBatchSkeleton), "pmb_jit_batch_agg", out);
 }
@@ -865,8 +936,11 @@ int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& 
 // Internal check (not part of the C ABI in pmb.h): generates and compiles the run-time kernel of
 // a query with NVRTC, without a GPU. Column pointers are not read, only their dtypes and whether
 // a validity bitmap is present. Returns PMB_OK, or an error with the compiler log in `log`.
+// mode 0: the hash kernel, 1: the batched kernel, 2: the partitioned aggregation (one- and
+// two-word packed keys)
 static int debug_compile(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log, int64_t log_cap,
-                         bool batch) {
+                         int mode) {
+  const bool batch = mode == 1;
   pmb_handle h;
   CompiledQuery cq;
   int rc = pmb_compile_groupby(&h, q, cols, n_cols, &cq);
@@ -877,7 +951,16 @@ static int debug_compile(const pmb_query* q, const pmb_column* cols, int32_t n_c
       cq.dq.col[c].data = dummy;
       cq.dq.col[c].valid = cols[cq.map.user[c]].validity ? dummy : nullptr;
     }
-    if (cq.dq.key_bits > 64) {
+    if (mode == 2) {
+      JitPlan J;
+      rc = pmb_plan_jit_batch(&h, cq, 1024, 1, 232448, &J);
+      if (rc != PMB_OK) msg = h.err;
+      for (int w = 1; w <= 2 && rc == PMB_OK; w++) {
+        std::vector<char> cubin;
+        if (!jit_compile(part_source(cq, J, w), cubin, msg)) rc = PMB_E_UNSUPPORTED;
+        else if (getenv("PMB_JIT_DEBUG") && getenv("PMB_JIT_DEBUG")[0] == '2') fprintf(stderr, "%s\n", msg.c_str());
+      }
+    } else if (cq.dq.key_bits > 64) {
       rc = PMB_E_UNSUPPORTED;
       msg = "128-bit keys use the prebuilt kernel";
     } else {
@@ -907,12 +990,17 @@ static int debug_compile(const pmb_query* q, const pmb_column* cols, int32_t n_c
 
 extern "C" int pmb_debug_jit_compile(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,
                                      int64_t log_cap) {
-  return debug_compile(q, cols, n_cols, log, log_cap, false);
+  return debug_compile(q, cols, n_cols, log, log_cap, 0);
 }
 // the same for the batched kernel (pmb_jit_batch.cuh)
 extern "C" int pmb_debug_jit_compile_batch(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,
                                            int64_t log_cap) {
-  return debug_compile(q, cols, n_cols, log, log_cap, true);
+  return debug_compile(q, cols, n_cols, log, log_cap, 1);
+}
+// the same for the partitioned strategy's aggregation kernel (pmb_jit_part.cuh)
+extern "C" int pmb_debug_jit_compile_part(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,
+                                          int64_t log_cap) {
+  return debug_compile(q, cols, n_cols, log, log_cap, 2);
 }
 
 int pmb_jit_sampled_table(const CompiledQuery& cq, const JitPlan& J, const unsigned long long* hot, int n_hot,

@@ -79,6 +79,27 @@ struct JBatchH {
   unsigned long long* ticket;
 };
 
+// host mirror of JPart in pmb_jit_part.cuh (same member order and types)
+struct JPartH {
+  JitParams qp;
+  const unsigned long long* keys;
+  unsigned long long kcap;
+  const unsigned int* idx;
+  const unsigned long long* pstart;
+  const unsigned int* items;
+  long long n_items;
+  int slots;
+  int pad;
+  unsigned long long* ticket;
+  unsigned long long* gkeys;
+  unsigned char* grecs;
+  unsigned long long gcap;
+  unsigned long long* n_groups;
+};
+// the partitioned strategy's aggregation kernel (pmb_jit_part.cuh) for packed keys of
+// `key_words` words; J receives the plan (threads, shared-memory record bytes)
+int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, JitPlan* J, cudaKernel_t* out);
+
 // the batched kernel (pmb_jit_batch.cuh): layout for `nt` threads with `nbuf` unit buffers per
 // warp, and its compiled kernel
 int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf, int max_smem_optin, JitPlan* J);

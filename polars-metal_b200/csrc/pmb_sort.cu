@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "pmb_groupby.h"
+#include "pmb_jit.h"
 
 namespace {
 
@@ -157,6 +158,21 @@ __device__ __forceinline__ unsigned digit_of(const PKey<W>& k, int shift) {
   return (unsigned)(v & 0xFF);
 }
 
+// hash of a packed key for the partitioned strategy: its top bits are the partition, its low 32
+// bits the slot in the partition's shared-memory table
+template <int W>
+__device__ __forceinline__ unsigned long long part_hash(const PKey<W>& k) {
+  unsigned long long h = pmb_fmix64(k.w[0]);
+  if (W > 1) h = pmb_fmix64(h ^ (k.w[W - 1] + 0x9E3779B97F4A7C15ULL));
+  return h;
+}
+
+// digit of a pass: key bits (sort strategy) or hash bits (partitioned strategy)
+template <int W>
+__device__ __forceinline__ unsigned pass_digit(const PKey<W>& k, int shift, bool hashed) {
+  return hashed ? (unsigned)((part_hash<W>(k) >> shift) & 0xFFu) : digit_of<W>(k, shift);
+}
+
 struct EncodeParams {
   DQuery q;
   SortKeyLayout L;
@@ -170,6 +186,10 @@ struct EncodeParams {
   unsigned long long* kept;    // rows that passed the filter
   unsigned int* hist;          // passes x 256
   unsigned int* status;
+  int hashed;                  // digits of the key hash (partitioned strategy)
+  int shift0;                  // bit of pass 0's digit; pass p uses shift0 + 8p
+  unsigned int* phist;         // partitioned strategy: rows per partition (2^pb counters), or null
+  int pb;
 };
 
 // filter, pack and compact in row order (4096-row tiles, decoupled look-back), with the digit
@@ -213,7 +233,8 @@ __global__ void __launch_bounds__(ST_NT) k_sort_encode(const __grid_constant__ E
     if (!keep[j]) continue;
     const int64_t r = tile * ST_TILE + (int64_t)j * ST_NT + tid;
     const PKey<W> k = pack_sort_key<W>(E.L, r);
-    for (int p = 0; p < E.passes; p++) atomicAdd(&s_hist[p][digit_of<W>(k, 8 * p)], 1u);
+    for (int p = 0; p < E.passes; p++) atomicAdd(&s_hist[p][pass_digit<W>(k, E.shift0 + 8 * p, E.hashed)], 1u);
+    if (E.phist) atomicAdd(&E.phist[part_hash<W>(k) >> (64 - E.pb)], 1u);
     const uint64_t pos = s_base + s_cnt[j][warp] + __popc(b & ((1u << lane) - 1u));
     for (int i = 0; i < W; i++) E.keys[(uint64_t)i * E.cap + pos] = k.w[i];
     E.idx[pos] = (unsigned)r;
@@ -238,6 +259,7 @@ struct PassParams {
   int64_t n_tiles;
   unsigned long long* ticket;
   unsigned int* status;
+  int hashed;  // digits of the key hash (partitioned strategy)
 };
 
 // One stable LSD pass over 8 bits at `shift`.
@@ -268,7 +290,7 @@ __global__ void __launch_bounds__(ST_NT) k_sort_pass(const __grid_constant__ Pas
     const int64_t e = base + warp * (ST_PER * 32) + j * 32 + lane;
     PKey<W> k;
     for (int i = 0; i < W; i++) k.w[i] = e < P.n ? P.kin[(uint64_t)i * P.cap + e] : 0ULL;
-    dg[j] = e < P.n ? (unsigned short)digit_of<W>(k, P.shift) : (unsigned short)RADIX;
+    dg[j] = e < P.n ? (unsigned short)pass_digit<W>(k, P.shift, P.hashed) : (unsigned short)RADIX;
   }
   // ranks within the warp, in item order (stable): lanes with the same digit in one round are
   // ordered by lane; earlier rounds come first
@@ -356,7 +378,7 @@ __global__ void __launch_bounds__(ST_NT) k_sort_pass(const __grid_constant__ Pas
   for (int i = tid; i < valid; i += ST_NT) {
     PKey<W> k;
     for (int w = 0; w < W; w++) k.w[w] = s_key[w * ST_TILE + i];
-    const unsigned d = digit_of<W>(k, P.shift);
+    const unsigned d = pass_digit<W>(k, P.shift, P.hashed);
     const uint64_t g = s_gbase[d] + (uint64_t)(i - (int)s_excl[d]);
     for (int w = 0; w < W; w++) P.kout[(uint64_t)w * P.cap + g] = k.w[w];
     P.iout[g] = s_idx[i];
@@ -557,17 +579,548 @@ __global__ void __launch_bounds__(BIG_NT) k_seg_reduce_big(const __grid_constant
   }
 }
 
+// ---------------------------------------------------------------- partitioned strategy
+// After the hash-digit passes the kept rows are ordered by partition (the top `pb` bits of the key
+// hash), so every group's rows lie inside one partition; the encode pass counted the rows of every
+// partition, so their offsets are exact. k_part_agg: persistent CTAs take work items (runs of
+// consecutive partitions) and aggregate one partition at a time in a shared-memory table (slot claim by a tag word, records in the global-record layout updated by
+// apply_row_shared, values gathered by row index). At the end of each partition the occupied
+// slots are compacted and written straight to the output columns (one atomic per partition for
+// the output rows; validity words built in shared memory). No global hash table is involved.
+constexpr int PA_NT = 1024;
+constexpr int PA_R = 2;   // rows per thread and step
+constexpr int PA_UC = 4;  // aggregated columns whose loads are issued together
+
+struct PartParams {
+  DQuery q;
+  RecInit ri;
+  SortKeyLayout L;
+  const unsigned long long* keys;  // sorted packed keys, word-major (stride cap)
+  uint64_t cap;
+  const unsigned int* idx;         // their row indices
+  int64_t m;                       // kept rows
+  int pb;                          // partition bits
+  const unsigned long long* pstart;  // 2^pb + 1: first row of every partition
+  const unsigned int* items;       // n_items + 1: first partition of every work item (whole partitions
+                                   // whose rows, an upper bound of their groups, fit the table)
+  int64_t n_items;
+  int slots;                       // shared table slots
+  int n_out;
+  int stage_bytes;                 // one row's aggregated columns, staged per thread
+  unsigned int used;               // columns the aggregates read (bit per column)
+  int n_used;
+  int32_t ucol[PMB_MAX_COLS];      // those columns, in order
+  int32_t sdoff[PMB_MAX_COLS];     // a column's value in the stage
+  int32_t svoff[PMB_MAX_COLS];     // its validity byte in the stage
+  unsigned long long* ticket;
+  unsigned long long* n_groups;    // output rows claimed
+  int64_t out_cap;
+  unsigned int* status;
+  uint8_t* out_data[PMB_MAX_OUT];
+  uint8_t* out_valid[PMB_MAX_OUT];
+};
+
 template <int W>
-int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_result* r) {
+__device__ __forceinline__ PKey<W> pa_key(const PartParams& A, int64_t i) {
+  PKey<W> k;
+#pragma unroll
+  for (int w = 0; w < W; w++) k.w[w] = A.keys[(uint64_t)w * A.cap + i];
+  return k;
+}
+// shared-memory layout of k_part_agg for `slots` slots
+struct PaLayout {
+  size_t tag, key, rec, list, vb, db, stage, bytes;
+};
+__host__ __device__ inline PaLayout pa_layout(int slots, int W, int rec_bytes, int n_out, int stage_bytes) {
+  PaLayout o;
+  const size_t words = (size_t)slots / 32 + 2;
+  o.tag = 0;
+  o.key = ((size_t)slots * 4 + 15) & ~(size_t)15;
+  o.rec = o.key + (size_t)slots * 8 * W;
+  o.list = o.rec + (size_t)slots * rec_bytes;
+  o.vb = (o.list + (size_t)slots * 2 + 15) & ~(size_t)15;
+  o.db = o.vb + (size_t)n_out * words * 4;
+  o.stage = (o.db + (size_t)PMB_MAX_KEYS * words * 4 + 15) & ~(size_t)15;
+  o.bytes = o.stage + (size_t)PA_NT * stage_bytes;
+  return o;
+}
+
+template <int W>
+__global__ void __launch_bounds__(PA_NT, 1) k_part_agg(const __grid_constant__ PartParams A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int S = A.slots, rb = A.q.rec_bytes, rw = rb / 8;
+  const PaLayout Ly = pa_layout(S, W, rb, A.n_out, A.stage_bytes);
+  unsigned int* tag = reinterpret_cast<unsigned int*>(smem + Ly.tag);  // 0 empty, 1 claimed, 2 key published
+  unsigned long long* tkey = reinterpret_cast<unsigned long long*>(smem + Ly.key);  // W x S
+  uint8_t* trec = smem + Ly.rec;
+  unsigned short* list = reinterpret_cast<unsigned short*>(smem + Ly.list);
+  const int nwords = S / 32 + 2;
+  unsigned int* vb = reinterpret_cast<unsigned int*>(smem + Ly.vb);  // n_out x nwords
+  unsigned int* db = reinterpret_cast<unsigned int*>(smem + Ly.db);  // n_keys x nwords (Bool keys)
+  uint8_t* stage = smem + Ly.stage + (size_t)threadIdx.x * A.stage_bytes;
+  __shared__ long long s_item;
+  __shared__ unsigned long long s_base;
+  __shared__ unsigned s_total;  // claimed slots of the current partition
+  const int tid = threadIdx.x;
+  bool has_fx = false;
+  for (int f = 0; f < A.q.n_fields; f++) has_fx |= A.q.field[f].kind == F_SUM_FX;
+  for (int i = tid; i < S; i += PA_NT) {
+    tag[i] = 0u;
+    for (int w = 0; w < rw; w++) reinterpret_cast<uint64_t*>(trec + (size_t)i * rb)[w] = A.ri.w[w];
+  }
+  for (int i = tid; i < (A.n_out + PMB_MAX_KEYS) * nwords; i += PA_NT) vb[i] = 0u;  // vb and db are adjacent
+  if (tid == 0) s_total = 0u;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_item = (long long)atomicAdd(A.ticket, 1ULL);
+    __syncthreads();
+    const long long it = s_item;
+    if (it >= A.n_items) break;
+    {
+      // the item's partitions: rows [ps, pe)
+      const int64_t ps = (int64_t)A.pstart[A.items[it]], pe = (int64_t)A.pstart[A.items[it + 1]];
+      for (int64_t b = ps; b < pe; b += (int64_t)PA_NT * PA_R) {
+        // PA_R rows per thread; their key and row-index loads go out together
+        PKey<W> k[PA_R];
+        unsigned slot[PA_R], row[PA_R], probes[PA_R];
+        bool pending[PA_R];
+        int found[PA_R];
+#pragma unroll
+        for (int r = 0; r < PA_R; r++) {
+          const int64_t i = b + (int64_t)r * PA_NT + tid;
+          pending[r] = i < pe;
+          found[r] = -1;
+          probes[r] = 0;
+          slot[r] = 0;
+          row[r] = 0;
+          if (pending[r]) {
+            k[r] = pa_key<W>(A, i);
+            row[r] = A.idx[i];
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < PA_R; r++)
+          if (pending[r]) slot[r] = (unsigned)(((part_hash<W>(k[r]) & 0xFFFFFFFFULL) * (unsigned long long)S) >> 32);
+        // find or claim the keys' slots. A claimer publishes its key before the next barrier, so a
+        // row that meets a slot being claimed tries that slot again after the barrier instead of
+        // waiting for it (a wait could stall on a claimer in its own warp)
+        for (int round = 0; round < 64; round++) {
+          bool any = false;
+#pragma unroll
+          for (int r = 0; r < PA_R; r++) {
+            while (pending[r]) {
+              const unsigned sl = slot[r];
+              unsigned tg = *reinterpret_cast<volatile unsigned int*>(&tag[sl]);
+              if (tg == 0u) {
+                if (atomicCAS(&tag[sl], 0u, 1u) == 0u) {
+#pragma unroll
+                  for (int w = 0; w < W; w++) tkey[(size_t)w * S + sl] = k[r].w[w];
+                  __threadfence_block();
+                  *reinterpret_cast<volatile unsigned int*>(&tag[sl]) = 2u;
+                  list[atomicAdd(&s_total, 1u)] = (unsigned short)sl;  // the item's groups, in claim order
+                  found[r] = (int)sl;
+                  pending[r] = false;
+                  break;
+                }
+                tg = *reinterpret_cast<volatile unsigned int*>(&tag[sl]);
+              }
+              if (tg != 2u) break;  // being claimed: this slot again after the barrier
+              __threadfence_block();
+              bool eq = true;
+#pragma unroll
+              for (int w = 0; w < W; w++) eq &= reinterpret_cast<volatile unsigned long long*>(tkey)[(size_t)w * S + sl] == k[r].w[w];
+              if (eq) {
+                found[r] = (int)sl;
+                pending[r] = false;
+                break;
+              }
+              slot[r] = sl + 1 == (unsigned)S ? 0u : sl + 1;
+              if (++probes[r] >= (unsigned)S) {
+                atomicOr(A.status, PMB_ST_OVERFLOW);  // the item has more groups than the table
+                pending[r] = false;
+              }
+            }
+            any |= pending[r];
+          }
+          if (!__syncthreads_or(any)) break;
+        }
+        // the rows' aggregated columns: the first PA_UC columns of both rows are loaded together,
+        // then every row is staged (one copy of each value) and applied to its record
+        uint64_t vals[PA_R][PA_UC];
+        unsigned vmask[PA_R];
+#pragma unroll
+        for (int r = 0; r < PA_R; r++) {
+          vmask[r] = 0u;
+          if (pending[r]) atomicOr(A.status, PMB_ST_OVERFLOW);
+#pragma unroll
+          for (int u = 0; u < PA_UC; u++) {
+            vals[r][u] = 0;
+            if (found[r] >= 0 && u < A.n_used) {
+              const DCol& C = A.q.col[A.ucol[u]];
+              vals[r][u] = pmb_load_bits(C.data, C.elem, row[r]);
+              if (C.valid && pmb_valid_bit(C.valid, row[r])) vmask[r] |= 1u << u;
+            }
+          }
+        }
+        auto put = [&](int c, uint64_t v, bool ok) {
+          const DCol& C = A.q.col[c];
+          uint8_t* d = stage + A.sdoff[c];
+          switch (C.elem) {
+            case 8: *reinterpret_cast<uint64_t*>(d) = v; break;
+            case 4: *reinterpret_cast<uint32_t*>(d) = (uint32_t)v; break;
+            case 2: *reinterpret_cast<uint16_t*>(d) = (uint16_t)v; break;
+            default: *d = (uint8_t)v; break;
+          }
+          if (C.valid) stage[A.svoff[c]] = ok ? 1 : 0;
+        };
+#pragma unroll
+        for (int r = 0; r < PA_R; r++) {
+          if (found[r] < 0) continue;
+#pragma unroll
+          for (int u = 0; u < PA_UC; u++)
+            if (u < A.n_used) put(A.ucol[u], vals[r][u], (vmask[r] >> u) & 1u);
+          for (int u = PA_UC; u < A.n_used; u++) {
+            const DCol& C = A.q.col[A.ucol[u]];
+            put(A.ucol[u], pmb_load_bits(C.data, C.elem, row[r]), C.valid && pmb_valid_bit(C.valid, row[r]));
+          }
+          const TileCtx ts{stage, A.sdoff, A.svoff, 0};
+          if (has_fx) fx_range_check(A.q, ts, 0, A.status);
+          apply_row_shared(A.q, ts, trec + (size_t)found[r] * rb, 0);
+        }
+      }
+      // the partition is complete: its groups (the claimed slots) go to the output
+      __syncthreads();
+      const unsigned total = s_total;
+      if (tid == 0) s_base = total ? atomicAdd(A.n_groups, (unsigned long long)total) : 0ULL;
+      __syncthreads();
+      const unsigned long long base = s_base, a0 = base & ~31ULL;
+      for (unsigned li = tid; li < total; li += PA_NT) {
+        const unsigned long long p = base + li;
+        if ((int64_t)p >= A.out_cap) {
+          atomicOr(A.status, PMB_ST_OVERFLOW);
+          continue;
+        }
+        const int sl = list[li];
+        const unsigned rbit = (unsigned)(p - a0);
+        PKey<W> k;
+#pragma unroll
+        for (int w = 0; w < W; w++) k.w[w] = tkey[(size_t)w * S + sl];
+        const uint8_t* rec = trec + (size_t)sl * rb;
+        int oc = 0;
+        for (int c = 0; c < A.q.n_keys; c++, oc++) {
+          uint64_t v = 0;
+          const bool valid = unpack_sort_key<W>(A.L, k, c, v);
+          const int dt = A.L.dtype[c];
+          if (dt == PMB_BOOL) {
+            if (valid && v) atomicOr(&db[c * nwords + (rbit >> 5)], 1u << (rbit & 31));
+          } else {
+            store_bits(A.out_data[oc], pmb_dtype_bytes(dt), (int64_t)p, v);
+          }
+          if (valid) atomicOr(&vb[oc * nwords + (rbit >> 5)], 1u << (rbit & 31));
+        }
+        for (int ag = 0; ag < A.q.n_aggs; ag++, oc++) {
+          const DAggOut& Ag = A.q.agg[ag];
+          bool valid = true;
+          uint64_t bits = 0;
+          finalize_agg(A.q, Ag, rec, valid, bits);
+          store_bits(A.out_data[oc], pmb_dtype_bytes(Ag.out_dtype), (int64_t)p, bits);
+          if (valid) atomicOr(&vb[oc * nwords + (rbit >> 5)], 1u << (rbit & 31));
+        }
+      }
+      __syncthreads();
+      // bitmap words into the outputs, then the table and the bitmaps are reset
+      const int nw = total ? (int)((base - a0 + total + 31) / 32) : 0;
+      for (int i = tid; i < A.n_out * nw; i += PA_NT) {
+        const int oc = i / nw, w = i % nw;
+        if ((int64_t)((a0 >> 5) + w) * 32 >= A.out_cap + 32) continue;
+        const unsigned v = vb[oc * nwords + w];
+        if (v) atomicOr(reinterpret_cast<unsigned int*>(A.out_valid[oc]) + (a0 >> 5) + w, v);
+        vb[oc * nwords + w] = 0u;
+        if (oc < A.q.n_keys && A.L.dtype[oc] == PMB_BOOL) {
+          const unsigned d = db[oc * nwords + w];
+          if (d) atomicOr(reinterpret_cast<unsigned int*>(A.out_data[oc]) + (a0 >> 5) + w, d);
+          db[oc * nwords + w] = 0u;
+        }
+      }
+      for (unsigned li = tid; li < total; li += PA_NT) {
+        const int sl = list[li];
+        tag[sl] = 0u;
+        for (int w = 0; w < rw; w++) reinterpret_cast<uint64_t*>(trec + (size_t)sl * rb)[w] = A.ri.w[w];
+      }
+      if (tid == 0) s_total = 0u;  // every thread read it before the s_base barrier
+      __syncthreads();
+    }
+  }
+}
+
+// dense groups of the run-time compiled partitioned aggregation (packed keys, global-layout
+// records) into the output columns, group g into output row g
+struct PartFinParams {
+  ReduceParams R;
+  const unsigned long long* gkeys;  // word-major, stride gcap
+  const uint8_t* grecs;
+  uint64_t gcap;
+};
+
+template <int W>
+__global__ void __launch_bounds__(ST_NT) k_part_finalize(const __grid_constant__ PartFinParams F) {
+  const int64_t ng = (int64_t)*F.R.n_groups;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  // every lane of a warp runs the same number of iterations (warp-wide bit setting)
+  const int64_t span = (ng + stride - 1) / stride * stride;
+  for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < span; g0 += stride) {
+    const int64_t g = g0 + threadIdx.x;
+    const int64_t p_first = g0 + (threadIdx.x & ~31);
+    const bool have = g < ng;
+    PKey<W> k{};
+    if (have)
+      for (int w = 0; w < W; w++) k.w[w] = F.gkeys[(uint64_t)w * F.gcap + g];
+    write_group<W, true>(F.R, g, p_first, have, k, have ? F.grecs + (uint64_t)g * F.R.q.rec_bytes : nullptr);
+  }
+}
+
+// the per-thread stage of k_part_agg: the aggregated columns' values (widest first, each aligned
+// to its size), then one validity byte per nullable column; returns its bytes (a multiple of 8)
+static int pa_stage(const DQuery& q, unsigned* used, int32_t* sdoff, int32_t* svoff) {
+  *used = 0;
+  for (int f = 0; f < q.n_fields; f++)
+    if (q.field[f].kind != F_LEN) *used |= 1u << q.field[f].col;
+  int off = 0;
+  for (int e = 8; e >= 1; e /= 2)
+    for (int c = 0; c < q.n_cols; c++)
+      if (((*used >> c) & 1u) && std::max<int>(q.col[c].elem, 1) == e) {
+        sdoff[c] = off;
+        off += e;
+      }
+  for (int c = 0; c < q.n_cols; c++)
+    if (((*used >> c) & 1u) && q.col[c].valid) svoff[c] = off++;
+  return (off + 7) & ~7;
+}
+
+// float sums that left their fixed-point range: widen to the largest exponent seen (the sorted
+// order does not depend on it); true when a column must switch to double-double instead
+static bool widen_fx(CompiledQuery& cq, const unsigned int* st) {
+  DQuery& q = cq.dq;
+  for (int i = 0; i < q.n_fields; i++) {
+    DField& f = q.field[i];
+    if (f.kind != F_SUM_FX || st[4 + f.fx_slot] == 0) continue;
+    const int e = (int)st[4 + f.fx_slot] - 1022 + 1;
+    if (e > q.fx_e[f.fx_slot]) {
+      f.fx = (int16_t)(f.fx - (e - q.fx_e[f.fx_slot]));
+      q.fx_e[f.fx_slot] = (int16_t)e;
+    }
+  }
+  return pmb_fx_to_dd(cq);
+}
+
+template <int W>
+int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_result* r, int64_t part_groups);
+
+// the aggregation of the partitioned strategy over keys / row indices sorted by partition
+template <int W>
+int run_part_agg(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_result* r, const unsigned long long* keys,
+                 const unsigned int* idx, uint64_t cap, int64_t m, int pb, const std::vector<unsigned int>& counts,
+                 int slots, int64_t groups,
+                 unsigned long long* ctr, unsigned int* status) {
+  DQuery& q = cq.dq;
+  const int n_out = q.n_keys + q.n_aggs;
+  PartParams A;
+  memset(&A, 0, sizeof(A));
+  for (size_t w = 0; w < cq.rec_init.size() && w < 48; w++) A.ri.w[w] = cq.rec_init[w];
+  A.L = L;
+  A.keys = keys;
+  A.cap = cap;
+  A.idx = idx;
+  A.m = m;
+  A.pb = pb;
+  // partition offsets, and work items: runs of whole partitions whose rows (an upper bound of
+  // their groups) stay within 70% of the table, at least one partition each
+  const unsigned long long lim = (unsigned long long)(0.7 * slots);
+  std::vector<unsigned long long> pstart(counts.size() + 1, 0);
+  std::vector<unsigned int> items(1, 0);
+  unsigned long long run = 0;
+  for (size_t p = 0; p < counts.size(); p++) {
+    pstart[p + 1] = pstart[p] + counts[p];
+    if (run > 0 && run + counts[p] > lim) {
+      items.push_back((unsigned)p);
+      run = 0;
+    }
+    run += counts[p];
+  }
+  if (run > 0 || items.size() == 1) items.push_back((unsigned)counts.size());
+  if ((int64_t)pstart.back() != m) return pmb_fail(h, PMB_E_CUDA, "partition counts do not add up");
+  unsigned long long* d_pstart = (unsigned long long*)pmb_ws_alloc(h, pstart.size() * 8);
+  unsigned int* d_items = (unsigned int*)pmb_ws_alloc(h, items.size() * 4);
+  if (!d_pstart || !d_items) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (partition offsets)");
+  PMB_CUDA(h, cudaMemcpyAsync(d_pstart, pstart.data(), pstart.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  PMB_CUDA(h, cudaMemcpyAsync(d_items, items.data(), items.size() * 4, cudaMemcpyHostToDevice, h->stream));
+  A.pstart = d_pstart;
+  A.items = d_items;
+  A.n_items = (int64_t)items.size() - 1;
+  A.slots = slots;
+  A.n_out = n_out;
+  A.stage_bytes = pa_stage(q, &A.used, A.sdoff, A.svoff);
+  for (int c = 0; c < q.n_cols; c++)
+    if ((A.used >> c) & 1u) A.ucol[A.n_used++] = c;
+  A.ticket = ctr + 1;
+  A.n_groups = ctr + 2;
+  A.status = status;
+  const size_t smem = pa_layout(slots, W, q.rec_bytes, n_out, A.stage_bytes).bytes;
+  PMB_CUDA(h, cudaFuncSetAttribute(k_part_agg<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int64_t out_cap = std::min<int64_t>(std::max<int64_t>(m, 1), 2 * groups + 65536);
+  for (int attempt = 0;; attempt++) {
+    if (attempt >= 6) return pmb_fail(h, PMB_E_CUDA, "partitioned strategy did not converge");
+    const WsMark mark = pmb_ws_mark(h);
+    const size_t vbytes = (size_t)((out_cap + 31) / 32 * 4) + 16;
+    for (int c = 0; c < n_out; c++) {
+      const int dt = r->columns[c].dtype;
+      const size_t dbytes = dt == PMB_BOOL ? vbytes : (size_t)out_cap * pmb_dtype_bytes(dt) + 16;
+      A.out_data[c] = (uint8_t*)pmb_ws_alloc(h, dbytes);
+      A.out_valid[c] = (uint8_t*)pmb_ws_alloc(h, vbytes);
+      if (!A.out_data[c] || !A.out_valid[c]) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (outputs)");
+      PMB_CUDA(h, cudaMemsetAsync(A.out_valid[c], 0, vbytes, h->stream));
+      if (dt == PMB_BOOL) PMB_CUDA(h, cudaMemsetAsync(A.out_data[c], 0, vbytes, h->stream));
+    }
+    A.q = q;
+    A.out_cap = out_cap;
+    PMB_CUDA(h, cudaMemsetAsync(ctr + 1, 0, 16, h->stream));
+    PMB_CUDA(h, cudaMemsetAsync(status, 0, 64, h->stream));
+    unsigned long long ng = 0;
+    unsigned int st[12] = {0};
+    // the run-time compiled aggregation writes dense groups that a prebuilt kernel finalises;
+    // without NVRTC (or for a signature it cannot take) the prebuilt kernel does both
+    JitPlan J;
+    cudaKernel_t jk = nullptr;
+    if (m > 0 && pmb_jit_enabled(1LL << 40) && pmb_jit_part_kernel(h, cq, W, &J, &jk) != PMB_OK) {
+      jk = nullptr;  // the prebuilt kernel instead (the compile error stays readable in pmb_last_error)
+    }
+    unsigned long long* gkeys = nullptr;
+    uint8_t* grecs = nullptr;
+    if (jk) {
+      gkeys = (unsigned long long*)pmb_ws_alloc(h, (size_t)W * out_cap * 8 + 16);
+      grecs = (uint8_t*)pmb_ws_alloc(h, (size_t)out_cap * q.rec_bytes + 16);
+      if (!gkeys || !grecs) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (groups)");
+    }
+    if (m > 0) {
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(A.n_items, h->sm_count));
+      if (jk) {
+        JPartH JA;
+        memset(&JA, 0, sizeof(JA));
+        for (int c = 0; c < q.n_cols; c++) {
+          JA.qp.col_data[c] = q.col[c].data;
+          JA.qp.col_valid[c] = q.col[c].valid;
+        }
+        JA.qp.n_rows = q.n_rows;
+        JA.qp.status = status;
+        for (int f = 0; f < q.n_fields; f++)
+          if (q.field[f].kind == F_SUM_FX) {
+            JA.qp.fx[q.field[f].fx_slot] = q.field[f].fx;
+            JA.qp.fx_e[q.field[f].fx_slot] = q.fx_e[q.field[f].fx_slot];
+          }
+        JA.keys = keys;
+        JA.kcap = cap;
+        JA.idx = idx;
+        JA.pstart = A.pstart;
+        JA.items = A.items;
+        JA.n_items = A.n_items;
+        JA.slots = slots;
+        JA.ticket = A.ticket;
+        JA.gkeys = gkeys;
+        JA.grecs = grecs;
+        JA.gcap = (unsigned long long)out_cap;
+        JA.n_groups = A.n_groups;
+        const size_t jsmem = (((size_t)slots * 4 + 15) & ~(size_t)15) + (size_t)slots * (8 * W + J.srec + 2);
+        PMB_CUDA(h, cudaFuncSetAttribute((const void*)jk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)jsmem));
+        void* args[] = {&JA};
+        pmb_kernel_begin(h, "part_agg");
+        PMB_CUDA(h, cudaLaunchKernel((const void*)jk, dim3(grid), dim3(J.nt), args, jsmem, h->stream));
+        pmb_kernel_end(h);
+      } else {
+        pmb_kernel_begin(h, "part_agg");
+        k_part_agg<W><<<grid, PA_NT, smem, h->stream>>>(A);
+        pmb_kernel_end(h);
+        PMB_CUDA(h, cudaGetLastError());
+      }
+      PMB_CUDA(h, cudaMemcpyAsync(&ng, ctr + 2, 8, cudaMemcpyDeviceToHost, h->stream));
+      PMB_CUDA(h, cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+      PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+      if (jk && !(st[0] & (PMB_ST_TIMEOUT | PMB_ST_FXRANGE | PMB_ST_OVERFLOW)) && ng > 0) {
+        PartFinParams F;
+        memset(&F, 0, sizeof(F));
+        F.R.q = q;
+        F.R.L = L;
+        F.R.n_groups = A.n_groups;
+        for (int c = 0; c < n_out; c++) {
+          F.R.out_data[c] = A.out_data[c];
+          F.R.out_valid[c] = A.out_valid[c];
+        }
+        F.gkeys = gkeys;
+        F.grecs = grecs;
+        F.gcap = (uint64_t)out_cap;
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)ng + ST_NT - 1) / ST_NT, (int64_t)h->sm_count * 16));
+        pmb_kernel_begin(h, "part_finalize");
+        k_part_finalize<W><<<blocks, ST_NT, 0, h->stream>>>(F);
+        pmb_kernel_end(h);
+        PMB_CUDA(h, cudaGetLastError());
+      }
+    }
+    if (st[0] & PMB_ST_TIMEOUT) return pmb_fail(h, PMB_E_TIMEOUT, "a bounded device wait timed out (partitioned)");
+    if (st[0] & PMB_ST_FXRANGE) {
+      if (widen_fx(cq, st)) return PMB_RETRY_DD;
+      pmb_ws_release(h, mark);
+      continue;
+    }
+    if (st[0] & PMB_ST_OVERFLOW) {
+      pmb_ws_release(h, mark);
+      if ((int64_t)ng > out_cap) {  // more groups than output rows: the exact upper bound next
+        out_cap = std::max<int64_t>(m, 1);
+        continue;
+      }
+      // a partition had more groups than its table: the sort strategy instead
+      PMB_CUDA(h, cudaMemsetAsync(ctr, 0, 64, h->stream));
+      return run_sort<W>(h, cq, L, r, 0);
+    }
+    r->n_groups = (int64_t)ng;
+    r->capacity = out_cap;
+    r->strategy_used = PMB_STRATEGY_PARTITIONED;
+    for (int c = 0; c < n_out; c++) {
+      r->columns[c].data = A.out_data[c];
+      r->columns[c].validity = A.out_valid[c];
+    }
+    return PMB_OK;
+  }
+}
+
+template <int W>
+int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_result* r, int64_t part_groups) {
   DQuery& q = cq.dq;
   const int64_t n = q.n_rows;
-  const int passes = std::max(0, (L.bits + 7) / 8);
+  const int n_out = q.n_keys + q.n_aggs;
+  // partitioned strategy: the largest shared table that fits, and 2^8 or 2^16 partitions so that
+  // a partition holds about a third of a table
+  int pb = 0, slots = 0;
+  if (part_groups > 0) {
+    unsigned used;
+    int32_t sd[PMB_MAX_COLS], sv[PMB_MAX_COLS];
+    const int stage = pa_stage(q, &used, sd, sv);
+    for (slots = 4096; slots >= 256; slots /= 2)
+      if (pa_layout(slots, W, q.rec_bytes, n_out, stage).bytes + 2048 <= (size_t)h->max_smem_optin) break;
+    if (slots < 256) return pmb_fail(h, PMB_E_UNSUPPORTED, "partitioned strategy: group record too large");
+    // twice the estimate: an undersized partition count overflows tables (and falls back to the
+    // sort), an oversized one costs one more pass
+    pb = 2 * part_groups * 3 / slots + 1 <= 256 ? 8 : 16;
+  }
+  const int passes = part_groups > 0 ? pb / 8 : std::max(0, (L.bits + 7) / 8);
   const uint64_t cap = (uint64_t)n;
   unsigned long long* k0 = (unsigned long long*)pmb_ws_alloc(h, (size_t)W * cap * 8 + 16);
   unsigned long long* k1 = (unsigned long long*)pmb_ws_alloc(h, (size_t)W * cap * 8 + 16);
   unsigned int* i0 = (unsigned int*)pmb_ws_alloc(h, (size_t)cap * 4 + 16);
   unsigned int* i1 = (unsigned int*)pmb_ws_alloc(h, (size_t)cap * 4 + 16);
   unsigned int* hist = (unsigned int*)pmb_ws_alloc(h, (size_t)MAX_PASSES * RADIX * 4);
+  const size_t n_parts = part_groups > 0 ? (size_t)1 << pb : 0;
+  unsigned int* phist = n_parts ? (unsigned int*)pmb_ws_alloc(h, n_parts * 4) : nullptr;
+  if (n_parts && !phist) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (partition counts)");
+  if (n_parts) PMB_CUDA(h, cudaMemsetAsync(phist, 0, n_parts * 4, h->stream));
   unsigned long long* ctr = (unsigned long long*)pmb_ws_alloc(h, 64);  // kept, ticket, n_groups, big_n
   unsigned int* status = (unsigned int*)pmb_ws_alloc(h, 64);
   const int64_t max_tiles = (n + ST_TILE - 1) / ST_TILE;
@@ -592,6 +1145,10 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
     E.kept = ctr;
     E.hist = hist;
     E.status = status;
+    E.hashed = part_groups > 0;
+    E.shift0 = part_groups > 0 ? 64 - pb : 0;
+    E.phist = phist;
+    E.pb = pb;
     PMB_CUDA(h, cudaMemsetAsync(lb, 0, (size_t)std::max<int64_t>(max_tiles, 1) * 8, h->stream));
     pmb_kernel_begin(h, "sort_encode");
     k_sort_encode<W><<<(unsigned)std::max<int64_t>(max_tiles, 1), ST_NT, 0, h->stream>>>(E);
@@ -604,6 +1161,8 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
   PMB_CUDA(h, cudaMemcpyAsync(&kept, ctr, 8, cudaMemcpyDeviceToHost, h->stream));
   PMB_CUDA(h, cudaMemcpyAsync(&st0, status, 4, cudaMemcpyDeviceToHost, h->stream));
   if (passes) PMB_CUDA(h, cudaMemcpyAsync(hh.data(), hist, (size_t)passes * RADIX * 4, cudaMemcpyDeviceToHost, h->stream));
+  std::vector<unsigned int> ph(n_parts);
+  if (n_parts) PMB_CUDA(h, cudaMemcpyAsync(ph.data(), phist, n_parts * 4, cudaMemcpyDeviceToHost, h->stream));
   PMB_CUDA(h, cudaStreamSynchronize(h->stream));
   if (st0 & PMB_ST_TIMEOUT) return pmb_fail(h, PMB_E_TIMEOUT, "a bounded device wait timed out (sort)");
   const int64_t m = (int64_t)kept;
@@ -623,7 +1182,8 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
     P.iout = i1;
     P.cap = cap;
     P.n = m;
-    P.shift = 8 * p;
+    P.shift = (part_groups > 0 ? 64 - pb : 0) + 8 * p;
+    P.hashed = part_groups > 0;
     P.hist = hist + (size_t)p * RADIX;
     P.lb = lb;
     P.n_tiles = tiles;
@@ -639,6 +1199,7 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
     std::swap(i0, i1);
     done++;
   }
+  if (part_groups > 0) return run_part_agg<W>(h, cq, L, r, k0, i0, cap, m, pb, ph, slots, part_groups, ctr, status);
   // segment starts
   unsigned int* starts = (unsigned int*)pmb_ws_alloc(h, (size_t)(m + 2) * 4);
   if (!starts) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (segment starts)");
@@ -666,7 +1227,6 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
     if (st & PMB_ST_TIMEOUT) return pmb_fail(h, PMB_E_TIMEOUT, "a bounded device wait timed out (sort)");
   }
   // outputs
-  const int n_out = q.n_keys + q.n_aggs;
   ReduceParams R;
   memset(&R, 0, sizeof(R));
   R.q = q;
@@ -715,16 +1275,7 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
     // a float sum left its fixed-point range: widen to the largest exponent seen; the sorted
     // order does not depend on it, so only the reduction runs again
     if (attempt >= 4) return pmb_fail(h, PMB_E_CUDA, "float-sum range did not converge");
-    for (int i = 0; i < q.n_fields; i++) {
-      DField& f = q.field[i];
-      if (f.kind != F_SUM_FX || st[4 + f.fx_slot] == 0) continue;
-      const int e = (int)st[4 + f.fx_slot] - 1022 + 1;
-      if (e > q.fx_e[f.fx_slot]) {
-        f.fx = (int16_t)(f.fx - (e - q.fx_e[f.fx_slot]));
-        q.fx_e[f.fx_slot] = (int16_t)e;
-      }
-    }
-    if (pmb_fx_to_dd(cq)) return PMB_RETRY_DD;
+    if (widen_fx(cq, st)) return PMB_RETRY_DD;
     R.q = q;
     for (int c = 0; c < n_out; c++) {
       PMB_CUDA(h, cudaMemsetAsync(R.out_valid[c], 0, vbytes, h->stream));
@@ -744,7 +1295,7 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
 
 }  // namespace
 
-int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r) {
+int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r, int64_t part_groups) {
   DQuery& q = cq.dq;
   if (q.n_rows > 0xFFFFFFF0LL) return pmb_fail(h, PMB_E_UNSUPPORTED, "sort strategy: more than 2^32 rows");
   if (q.rec_bytes > 384) return pmb_fail(h, PMB_E_UNSUPPORTED, "sort strategy: group record above 384 bytes");
@@ -793,5 +1344,5 @@ int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r) {
   L.bits = off;
   L.words = off > 64 ? 2 : 1;
   if (off > 128) return pmb_fail(h, PMB_E_UNSUPPORTED, "sort strategy: packed key above 128 bits");
-  return L.words == 1 ? run_sort<1>(h, cq, L, r) : run_sort<2>(h, cq, L, r);
+  return L.words == 1 ? run_sort<1>(h, cq, L, r, part_groups) : run_sort<2>(h, cq, L, r, part_groups);
 }

@@ -63,7 +63,7 @@ AGG_OPS = {"Sum": 0, "Mean": 1, "Count": 2, "Min": 3, "Max": 4, "Len": 5}
 AGG_LEN = 5
 
 # ---- strategies
-STRATEGIES = {"auto": 0, "smem_hash": 1, "global_hash": 2, "sort": 3}
+STRATEGIES = {"auto": 0, "smem_hash": 1, "global_hash": 2, "sort": 3, "partitioned": 4}
 STRATEGY_NAMES = {v: k for k, v in STRATEGIES.items()}
 
 

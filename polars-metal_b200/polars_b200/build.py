@@ -32,7 +32,7 @@ SOURCES = [
 
 # device sources compiled at run time by NVRTC, embedded into the library as string literals
 JIT_EMBED = [("kDeviceHeader", "pmb_device.cuh"), ("kSkeleton", "pmb_jit_skeleton.cuh"),
-             ("kBatchSkeleton", "pmb_jit_batch.cuh")]
+             ("kBatchSkeleton", "pmb_jit_batch.cuh"), ("kPartSkeleton", "pmb_jit_part.cuh")]
 
 
 def write_jit_sources() -> Path:

@@ -14,7 +14,7 @@ from polars_b200._native import ColumnData, groupby
 
 pytestmark = pytest.mark.gpu
 GOLD = load_golden()
-STRATEGIES = ["auto", "smem_hash", "global_hash", "sort"]
+STRATEGIES = ["auto", "smem_hash", "global_hash", "sort", "partitioned"]
 
 
 def _product_cols(cols: dict) -> dict:
@@ -66,7 +66,7 @@ def test_hash_workload_parity(n):
     t = datagen.make_hash(n, seed=5)
     cols = datagen.to_numpy_columns(t)
     got = run_both(cols, t.keys, t.aggs, t.predicate, "auto", f"hash n={n}")
-    assert got.strategy in ("global_hash", "smem_hash", "sort")
+    assert got.strategy in ("global_hash", "smem_hash", "sort", "partitioned")
 
 
 def test_hash_workload_device_resident_inputs():
@@ -79,7 +79,7 @@ def test_hash_workload_device_resident_inputs():
     assert_results_match(as_dict(got), want, 1, t.aggs, "device inputs")
 
 
-@pytest.mark.parametrize("strategy", ["auto", "sort"])
+@pytest.mark.parametrize("strategy", ["auto", "sort", "partitioned"])
 def test_sort_workload_shape_parity(strategy):
     # two-column key (int64 + int32): 96 data bits -> the 128-bit key table, or 20 + 6 packed bits
     # for the sort
@@ -110,6 +110,39 @@ def test_sort_two_word_keys_big_groups_and_filter():
             "rhs": {"kind": "LiteralF64", "value": -0.3}}
     got = run_both(cols2, ["g"], aggs[:1] + [("Min", "w", "mn"), ("Len", None, "n")], pred, "sort", "big groups")
     assert got.strategy == "sort"
+
+
+@pytest.mark.parametrize("hint", [0, 50_000_000, 1])
+def test_partitioned_partitions_and_fallbacks(hint):
+    # hint 0: partitions sized from the sample; 50M: 2^16 partitions of a few rows each (two hash
+    # passes, work items spanning many partitions); 1: too few output rows and partitions far
+    # larger than their tables (the output is re-sized, then the sort strategy takes over)
+    t = datagen.make_sort(1_500_000, seed=17, pool=60_000)
+    cols = datagen.to_numpy_columns(t)
+    got = groupby(_product_cols(cols), t.keys, t.aggs, None, strategy="partitioned", capacity_hint=hint)
+    want = pyoracle.groupby(cols, t.keys, t.aggs, None)
+    assert_results_match(as_dict(got), want, len(t.keys), t.aggs, f"partitioned hint={hint}")
+    assert got.strategy == ("sort" if hint == 1 else "partitioned")
+
+
+def test_partitioned_heavy_keys_two_words_and_filter():
+    rng = np.random.default_rng(37)
+    n = 600_000
+    # a handful of keys holding half the rows (partitions much longer than a work item) among
+    # full-range two-column keys (two-word packed keys)
+    hot = rng.random(n) < 0.5
+    k1 = np.where(hot, rng.integers(0, 3, n), rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n,
+                                                             dtype=np.int64)).astype(np.int64)
+    k2 = np.where(hot, 7, rng.integers(-2**31, 2**31 - 1, n)).astype(np.int32)
+    cols = {"a": (k1, pack(rng.random(n) > 0.02)), "b": (k2, None),
+            "v": (rng.standard_normal(n), pack(rng.random(n) > 0.1)),
+            "w": (rng.integers(-10**6, 10**6, n).astype(np.int64), None), "f": (rng.random(n).astype(np.float32), None)}
+    aggs = [("Sum", "v", "s"), ("Mean", "v", "m"), ("Min", "w", "mn"), ("Max", "v", "mx"), ("Count", "v", "c"),
+            ("Len", None, "n"), ("Sum", "f", "sf"), ("Max", "f", "mf")]
+    pred = {"kind": "Compare", "op": "Gt", "lhs": {"kind": "Column", "name": "v"},
+            "rhs": {"kind": "LiteralF64", "value": -0.8}}
+    got = run_both(cols, ["a", "b"], aggs, pred, "partitioned", "partitioned heavy keys")
+    assert got.strategy == "partitioned"
 
 
 def test_empty_input():
@@ -143,7 +176,7 @@ def test_ragged_sizes(n):
 KEY_DTYPES = ["int8", "int16", "int32", "int64", "uint8", "uint16", "uint32", "uint64", "float32", "float64"]
 
 
-@pytest.mark.parametrize("strategy", ["auto", "sort"])
+@pytest.mark.parametrize("strategy", ["auto", "sort", "partitioned"])
 @pytest.mark.parametrize("kdt", KEY_DTYPES)
 def test_key_dtypes(kdt, strategy):
     rng = np.random.default_rng(3)
@@ -160,7 +193,7 @@ def test_key_dtypes(kdt, strategy):
 VALUE_DTYPES = ["int8", "int16", "int32", "int64", "uint8", "uint16", "uint32", "uint64", "float32", "float64"]
 
 
-@pytest.mark.parametrize("strategy", ["auto", "sort"])
+@pytest.mark.parametrize("strategy", ["auto", "sort", "partitioned"])
 @pytest.mark.parametrize("vdt", VALUE_DTYPES)
 def test_value_dtypes(vdt, strategy):
     rng = np.random.default_rng(4)
@@ -177,7 +210,7 @@ def test_value_dtypes(vdt, strategy):
     run_both(cols, ["k"], aggs, strategy=strategy, label=f"values {vdt} {strategy}")
 
 
-@pytest.mark.parametrize("strategy", ["auto", "sort"])
+@pytest.mark.parametrize("strategy", ["auto", "sort", "partitioned"])
 def test_multi_key_with_nulls_and_bool(strategy):
     rng = np.random.default_rng(8)
     n = 100_000

@@ -20,7 +20,7 @@ def _lib():
     return L
 
 
-def jit_compile(cols: dict, keys, aggs, predicate=None, batch: bool = False) -> tuple[int, str]:
+def jit_compile(cols: dict, keys, aggs, predicate=None, batch: bool = False, part: bool = False) -> tuple[int, str]:
     L = _lib()
     names = list(cols)
     cds = [c if isinstance(c, ColumnData) else ColumnData(*c) for c in cols.values()]
@@ -39,7 +39,7 @@ def jit_compile(cols: dict, keys, aggs, predicate=None, batch: bool = False) -> 
     q.n_aggs = len(aggs)
     q.predicate = C.pointer(expr) if expr is not None else None
     buf = C.create_string_buffer(1 << 16)
-    fn = L.pmb_debug_jit_compile_batch if batch else L.pmb_debug_jit_compile
+    fn = L.pmb_debug_jit_compile_part if part else L.pmb_debug_jit_compile_batch if batch else L.pmb_debug_jit_compile
     fn.argtypes = [C.POINTER(A.Query), C.POINTER(A.Column), C.c_int32, C.c_char_p, C.c_int64]
     rc = fn(C.byref(q), abi, len(names), buf, 1 << 16)
     return rc, buf.value.decode(errors="replace")
@@ -122,4 +122,24 @@ def test_batch_kernel_compiles():
     assert rc == 0, log
     t = datagen.make_hash(4096, seed=1)
     rc, log = jit_compile(datagen.to_column_data(t), t.keys, t.aggs, t.predicate, batch=True)
+    assert rc == 0, log
+
+
+@pytest.mark.parametrize("maker", ["make_sort", "make_hash", "make_small"])
+def test_partitioned_kernel_compiles(maker):
+    # packed sort keys of one and two words; 96-bit table keys (the sort workload) included
+    t = getattr(datagen, maker)(4096, seed=1)
+    rc, log = jit_compile(datagen.to_column_data(t), t.keys, t.aggs, t.predicate, part=True)
+    assert rc == 0, log
+
+
+def test_partitioned_kernel_value_dtypes_compile():
+    n = 64
+    cols = {"k": ColumnData(np.zeros(n, np.int64), np.zeros(8, np.uint8)),
+            "f": ColumnData(np.zeros(n, np.float32), np.zeros(8, np.uint8)),
+            "u": ColumnData(np.zeros(n, np.uint16)),
+            "b": ColumnData(np.zeros(8, np.uint8), np.zeros(8, np.uint8), dtype=A.BOOL, length=n)}
+    aggs = [("Sum", "f", "s"), ("Mean", "u", "m"), ("Min", "f", "mn"), ("Max", "u", "mx"), ("Count", "b", "c"),
+            ("Sum", "b", "sb"), ("Len", None, "n")]
+    rc, log = jit_compile(cols, ["k"], aggs, part=True)
     assert rc == 0, log
