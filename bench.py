@@ -311,6 +311,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hash", choices=sorted(WORKLOADS) + ["batch"])
     ap.add_argument("--no-batched", action="store_true", help="leave out the batched-vs-plain comparison")
+    ap.add_argument("--strategy", default="auto", help="group-by strategy of the timed calls (default: auto)")
     ap.add_argument("--rows", type=int, default=0, help="override the workload's row count")
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -352,7 +353,7 @@ def main():
     h.set_stream(stream.cuda_stream)
 
     def step(profile: bool):
-        return groupby(cols, t.keys, t.aggs, t.predicate, output="device", handle=h)
+        return groupby(cols, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="device", handle=h)
 
     for _ in range(args.warmup):
         r = step(False)
@@ -403,15 +404,15 @@ def main():
                 hv.copy_(c.validity)
             host[name] = ColumnData(hd, hv, dtype=c.dtype, length=c.length)
         e2e_steps = args.e2e_steps or max(3, min(args.steps, 5))
-        groupby(host, t.keys, t.aggs, t.predicate, output="host", handle=h)
+        groupby(host, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="host", handle=h)
         h.set_profiling(True)
-        groupby(host, t.keys, t.aggs, t.predicate, output="host", handle=h)
+        groupby(host, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="host", handle=h)
         io = h.last_stats()
         h.set_profiling(False)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
-            groupby(host, t.keys, t.aggs, t.predicate, output="host", handle=h)
+            groupby(host, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="host", handle=h)
         torch.cuda.synchronize()
         e2e_ms = 1e3 * (time.perf_counter() - t0) / e2e_steps
         e2e_ms_max, rows_e2e = reduce_step_stats(e2e_ms, n, device)
@@ -424,8 +425,15 @@ def main():
         sample = {"hash": 10_000_000, "small": 1_000_000, "sort": 10_000_000}[args.workload]
         cpu = cpu_baseline(args.workload, threads, sample)
 
+    # the sort workload also reports the LSD radix sort + segmented reduce strategy itself
+    sort_strategy = None
+    if args.workload == "sort" and r.strategy != "sort":
+        ms_sort = time_calls(lambda: groupby(cols, t.keys, t.aggs, t.predicate, strategy="sort", output="device",
+                                             handle=h), stream, 3, 1)
+        sort_strategy = {"strategy": "sort", "ms_per_step": ms_sort, "rows_per_s": n / (ms_sort / 1e3)}
+
     batched = None
-    if not args.no_batched:
+    if not args.no_batched and args.workload == "hash":
         tables_b, qs_b = batch_queries(device, seed=4 + rank)
         torch.cuda.synchronize()
         h_plain = Handle(local_rank, selector=None)
@@ -464,6 +472,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks,
             "batched": batched,
+            "sort_strategy": sort_strategy,
         }
         print(json.dumps(line), flush=True)
     h.close()

@@ -76,6 +76,8 @@ struct SketchOut {
 int pmb_groupby_sketch(pmb_handle* h, const CompiledQuery& cq, SketchOut* out);
 int64_t pmb_estimate_groups(const SketchOut& s, int64_t n_rows);
 int pmb_choose_strategy(pmb_handle* h, const CompiledQuery& cq, const SketchOut& sk, int64_t est);
+// AUTO's switch from a chosen global-table or sort strategy to the partitioned strategy
+bool pmb_prefer_partitioned(const CompiledQuery& cq, const SketchOut& sk, int strategy, int64_t est);
 int pmb_plan_hash(pmb_handle* h, int max_smem_optin, CompiledQuery& cq, int strategy, int64_t est, bool have_sketch,
                   HashParams& P, int& nt, int& smem);
 int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,

@@ -380,13 +380,19 @@ extern "C" int pmb_selector_choose(pmb_handle* h, const pmb_query* q, const pmb_
   if (rc) return rc;
   int s = 0;
   int64_t g = 0;
-  if (!pmb_selector_pick(h, cq, &s, &g)) {
-    static thread_local SketchOut sk;
-    rc = pmb_groupby_sketch(h, cq, &sk);
-    if (rc) return rc;
-    g = pmb_estimate_groups(sk, cq.dq.n_rows);
+  // the same decisions as pmb_groupby's AUTO: sample estimate, selector (which can only enlarge
+  // the estimate) or heuristic, then the switch to the partitioned strategy
+  static thread_local SketchOut sk;
+  rc = pmb_groupby_sketch(h, cq, &sk);
+  if (rc) return rc;
+  const int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
+  if (pmb_selector_pick(h, cq, &s, &g)) {
+    g = std::max<int64_t>(e, std::min<int64_t>(g, cq.dq.n_rows));
+  } else {
+    g = e;
     s = pmb_choose_strategy(h, cq, sk, g);
   }
+  if (pmb_prefer_partitioned(cq, sk, s, g)) s = PMB_STRATEGY_PARTITIONED;
   *strategy = s;
   *groups = g;
   return PMB_OK;
