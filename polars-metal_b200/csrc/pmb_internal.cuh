@@ -298,3 +298,34 @@ __device__ __forceinline__ unsigned long long pmb_lookback(unsigned long long* s
   atomicExch(&status[tile], (2ULL << 62) | (excl + count));
   return excl;
 }
+
+// the same over states spaced `stride` apart (state of tile t at status[t * stride])
+__device__ __forceinline__ unsigned long long pmb_lookback_strided(unsigned long long* status, long long tile,
+                                                                   long long stride, unsigned long long count,
+                                                                   unsigned int* st) {
+  const unsigned long long VAL = (1ULL << 62) - 1;
+  if (tile == 0) {
+    atomicExch(&status[0], (2ULL << 62) | count);
+    return 0;
+  }
+  atomicExch(&status[tile * stride], (1ULL << 62) | count);
+  unsigned long long excl = 0;
+  long long t = tile - 1;
+  uint32_t spins = 0;
+  while (t >= 0) {
+    unsigned long long s = *((volatile unsigned long long*)&status[t * stride]);
+    unsigned long long flag = s >> 62;
+    if (flag == 0) {
+      if (++spins > PMB_SPIN_LIMIT) {
+        atomicOr(st, PMB_ST_TIMEOUT);
+        return 0;
+      }
+      continue;
+    }
+    excl += s & VAL;
+    if (flag == 2) break;
+    t--;
+  }
+  atomicExch(&status[tile * stride], (2ULL << 62) | (excl + count));
+  return excl;
+}

@@ -915,18 +915,19 @@ int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf,
 
 // source of the partitioned aggregation: device helpers, the parameter block, the generated row
 // functions and pmb_jit_part.cuh (not the hash kernel)
-static std::string part_source(const CompiledQuery& cq, const JitPlan& J, int key_words) {
+static std::string part_source(const CompiledQuery& cq, const JitPlan& J, int key_words, bool cas64) {
   Gen g(cq.dq, J);
   std::string skel(kSkeleton);
   size_t cut = skel.find("__device__ __forceinline__ long long j_gresolve");
-  return "#define JP_W " + std::to_string(key_words) + "\n" + std::string(kDeviceHeader) + "\n" + skel.substr(0, cut) +
-         "\n" + g.build() + "\n" + std::string(kPartSkeleton);
+  return "#define JP_W " + std::to_string(key_words) + "\n#define JP_CAS64 " + (cas64 ? "1" : "0") + "\n" +
+         std::string(kDeviceHeader) + "\n" + skel.substr(0, cut) + "\n" + g.build() + "\n" + std::string(kPartSkeleton);
 }
 
-int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, JitPlan* J, cudaKernel_t* out) {
+int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, bool cas64, JitPlan* J,
+                        cudaKernel_t* out) {
   int rc = pmb_plan_jit_batch(h, cq, 1024, 1, h->max_smem_optin, J);
   if (rc) return rc;
-  return jit_kernel(h, part_source(cq, *J, key_words), "pmb_jit_part_agg", out);
+  return jit_kernel(h, part_source(cq, *J, key_words, cas64 && key_words == 1), "pmb_jit_part_agg", out);
 }
 
 int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out) {
@@ -955,9 +956,9 @@ static int debug_compile(const pmb_query* q, const pmb_column* cols, int32_t n_c
       JitPlan J;
       rc = pmb_plan_jit_batch(&h, cq, 1024, 1, 232448, &J);
       if (rc != PMB_OK) msg = h.err;
-      for (int w = 1; w <= 2 && rc == PMB_OK; w++) {
+      for (int v = 0; v < 3 && rc == PMB_OK; v++) {
         std::vector<char> cubin;
-        if (!jit_compile(part_source(cq, J, w), cubin, msg)) rc = PMB_E_UNSUPPORTED;
+        if (!jit_compile(part_source(cq, J, v == 2 ? 2 : 1, v == 1), cubin, msg)) rc = PMB_E_UNSUPPORTED;
         else if (getenv("PMB_JIT_DEBUG") && getenv("PMB_JIT_DEBUG")[0] == '2') fprintf(stderr, "%s\n", msg.c_str());
       }
     } else if (cq.dq.key_bits > 64) {

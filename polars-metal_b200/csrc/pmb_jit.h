@@ -97,8 +97,10 @@ struct JPartH {
   unsigned long long* n_groups;
 };
 // the partitioned strategy's aggregation kernel (pmb_jit_part.cuh) for packed keys of
-// `key_words` words; J receives the plan (threads, shared-memory record bytes)
-int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, JitPlan* J, cudaKernel_t* out);
+// `key_words` words (cas64: one-word keys that never equal all ones, claimed by a CAS on the key);
+// J receives the plan (threads, shared-memory record bytes)
+int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, bool cas64, JitPlan* J,
+                        cudaKernel_t* out);
 
 // the batched kernel (pmb_jit_batch.cuh): layout for `nt` threads with `nbuf` unit buffers per
 // warp, and its compiled kernel

@@ -1,13 +1,16 @@
 // pmb_jit_part.cuh — the aggregation step of the partitioned strategy, compiled at run time for
 // one query signature (follows pmb_jit_skeleton.cuh's parameter block and the generated row
-// functions in the same NVRTC source; JP_W, the words of a packed key, is defined before it).
+// functions in the same NVRTC source; JP_W, the words of a packed key, and JP_CAS64 are defined
+// before it).
 //
 // Input: the kept rows as packed keys and row indices, ordered by partition (the top bits of the
 // key hash), with the first row of every partition; work items are runs of whole partitions whose
 // rows fit the shared-memory table. Persistent CTAs take items through a ticket. Per item:
-//   1. rows are taken PA_R per thread: the key and row-index loads go out together, the key is
-//      found or claimed in the table (a slot is claimed with a CAS on its tag word; a row that
-//      meets a slot being claimed retries it after the next barrier instead of waiting), the
+//   1. rows are taken JP_R per thread: the key and row-index loads go out together, the key is
+//      found or claimed in the table (one-word keys that cannot equal the all-ones EMPTY marker,
+//      JP_CAS64: a CAS on the key word claims and publishes at once, no barrier; otherwise a CAS
+//      on the slot's tag word claims, and a row that meets a slot being claimed retries it after
+//      the next barrier instead of waiting), the
 //      row's aggregated columns are gathered by row index (j_gather) and applied to the slot's
 //      record with native 32-bit shared atomics (j_shared);
 //   2. the claimed slots (listed in claim order) are written as dense groups: the packed key and
@@ -51,7 +54,10 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_part_agg(const __g
   __shared__ long long s_item;
   __shared__ unsigned long long s_base;
   __shared__ unsigned int s_total;  // claimed slots of the current item
-  for (int i = tid; i < S; i += J_NT) tag[i] = 0u;
+  for (int i = tid; i < S; i += J_NT) {
+    tag[i] = 0u;
+    if (JP_CAS64) tkey[i] = 0xFFFFFFFFFFFFFFFFULL;
+  }
   for (int w = tid; w < S * J_SREC_WORDS; w += J_NT) reinterpret_cast<unsigned int*>(srec)[w] = J_SIDENT[w % J_SREC_WORDS];
   if (tid == 0) s_total = 0u;
   for (;;) {
@@ -81,6 +87,35 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_part_agg(const __g
 #pragma unroll
       for (int r = 0; r < JP_R; r++)
         if (pending[r]) slot[r] = (unsigned)(((jp_hash(k[r]) & 0xFFFFFFFFULL) * (unsigned long long)S) >> 32);
+#if JP_CAS64
+      // the key word is the claim: no tag, no barrier
+#pragma unroll
+      for (int r = 0; r < JP_R; r++) {
+        while (pending[r]) {
+          const unsigned sl = slot[r];
+          unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&tkey[sl]);
+          if (cur == 0xFFFFFFFFFFFFFFFFULL) {
+            cur = atomicCAS(&tkey[sl], 0xFFFFFFFFFFFFFFFFULL, k[r][0]);
+            if (cur == 0xFFFFFFFFFFFFFFFFULL) {
+              list[atomicAdd(&s_total, 1u)] = (unsigned short)sl;
+              found[r] = (int)sl;
+              pending[r] = false;
+              break;
+            }
+          }
+          if (cur == k[r][0]) {
+            found[r] = (int)sl;
+            pending[r] = false;
+            break;
+          }
+          slot[r] = sl + 1 == (unsigned)S ? 0u : sl + 1;
+          if (++probes[r] >= (unsigned)S) {
+            atomicOr(P.status, PMB_ST_OVERFLOW);  // the item has more groups than the table
+            pending[r] = false;
+          }
+        }
+      }
+#else
       for (int round = 0; round < 64; round++) {
         bool any = false;
 #pragma unroll
@@ -121,6 +156,7 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_part_agg(const __g
         }
         if (!__syncthreads_or(any)) break;
       }
+#endif
       JRow rw[JP_R];
 #pragma unroll
       for (int r = 0; r < JP_R; r++) {
@@ -151,6 +187,7 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_part_agg(const __g
         atomicOr(P.status, PMB_ST_OVERFLOW);
       }
       tag[sl] = 0u;
+      if (JP_CAS64) tkey[sl] = 0xFFFFFFFFFFFFFFFFULL;
       for (int w = 0; w < J_SREC_WORDS; w++) reinterpret_cast<unsigned int*>(srec + (size_t)sl * J_SREC)[w] = J_SIDENT[w];
     }
     if (tid == 0) s_total = 0u;  // every thread read it before the s_base barrier

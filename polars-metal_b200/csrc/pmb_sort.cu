@@ -262,13 +262,16 @@ struct PassParams {
   int hashed;  // digits of the key hash (partitioned strategy)
 };
 
-// One stable LSD pass over 8 bits at `shift`.
+// One stable LSD pass over 8 bits at `shift`. Look-back states are tile-major (tile * 256 + digit),
+// so the 32 digits of a warp read one predecessor's states in one coalesced access. Per-warp digit
+// counts are 16-bit (at most 512 keys per warp), which with 4 CTAs per SM keeps the shared memory
+// of a CTA under a quarter of the SM's.
 template <int W>
-__global__ void __launch_bounds__(ST_NT) k_sort_pass(const __grid_constant__ PassParams P) {
+__global__ void __launch_bounds__(ST_NT, 4) k_sort_pass(const __grid_constant__ PassParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned long long* s_key = reinterpret_cast<unsigned long long*>(smem);       // W x ST_TILE
   unsigned int* s_idx = reinterpret_cast<unsigned int*>(s_key + W * ST_TILE);   // ST_TILE
-  __shared__ unsigned int s_whist[ST_NT / 32][RADIX];
+  __shared__ unsigned short s_whist[ST_NT / 32][RADIX];
   __shared__ unsigned int s_excl[RADIX];      // tile-local exclusive offset of each digit
   __shared__ unsigned long long s_gbase[RADIX];
   __shared__ unsigned int s_scan[ST_NT / 32];
@@ -302,7 +305,7 @@ __global__ void __launch_bounds__(ST_NT) k_sort_pass(const __grid_constant__ Pas
     unsigned old = 0;
     if (d < RADIX && lane == leader) {
       old = s_whist[warp][d];
-      s_whist[warp][d] = old + __popc(peers);
+      s_whist[warp][d] = (unsigned short)(old + __popc(peers));
     }
     old = __shfl_sync(0xffffffffu, old, leader);
     rank[j] = old + __popc(peers & lt);
@@ -315,7 +318,7 @@ __global__ void __launch_bounds__(ST_NT) k_sort_pass(const __grid_constant__ Pas
     unsigned acc = 0;
     for (int w = 0; w < ST_NT / 32; w++) {
       unsigned c = s_whist[w][d];
-      s_whist[w][d] = acc;
+      s_whist[w][d] = (unsigned short)acc;
       acc += c;
     }
     // tile-local exclusive scan over digits (block scan of one value per thread)
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(ST_NT) k_sort_pass(const __grid_constant__ Pas
     }
     __syncthreads();
     const unsigned long long gstart = (unsigned long long)(y - hd + s_scan[warp]);
-    const unsigned long long pre = pmb_lookback(P.lb + (int64_t)d * P.n_tiles, tile, acc, P.status);
+    const unsigned long long pre = pmb_lookback_strided(P.lb + d, tile, RADIX, acc, P.status);
     s_gbase[d] = gstart + pre;
   }
   __syncthreads();
@@ -991,7 +994,7 @@ int run_part_agg(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_r
     // without NVRTC (or for a signature it cannot take) the prebuilt kernel does both
     JitPlan J;
     cudaKernel_t jk = nullptr;
-    if (m > 0 && pmb_jit_enabled(1LL << 40) && pmb_jit_part_kernel(h, cq, W, &J, &jk) != PMB_OK) {
+    if (m > 0 && pmb_jit_enabled(1LL << 40) && pmb_jit_part_kernel(h, cq, W, L.bits < 64, &J, &jk) != PMB_OK) {
       jk = nullptr;  // the prebuilt kernel instead (the compile error stays readable in pmb_last_error)
     }
     unsigned long long* gkeys = nullptr;
