@@ -70,12 +70,13 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_part_agg(const __g
     for (long long b = ps; b < pe; b += (long long)J_NT * JP_R) {
       unsigned long long k[JP_R][JP_W];
       unsigned slot[JP_R], row[JP_R], probes[JP_R];
-      bool pending[JP_R];
+      bool pending[JP_R], claimed[JP_R];
       int found[JP_R];
 #pragma unroll
       for (int r = 0; r < JP_R; r++) {
         const long long i = b + (long long)r * J_NT + tid;
         pending[r] = i < pe;
+        claimed[r] = false;
         found[r] = -1;
         probes[r] = 0;
         slot[r] = 0;
@@ -97,7 +98,7 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_part_agg(const __g
           if (cur == 0xFFFFFFFFFFFFFFFFULL) {
             cur = atomicCAS(&tkey[sl], 0xFFFFFFFFFFFFFFFFULL, k[r][0]);
             if (cur == 0xFFFFFFFFFFFFFFFFULL) {
-              list[atomicAdd(&s_total, 1u)] = (unsigned short)sl;
+              claimed[r] = true;
               found[r] = (int)sl;
               pending[r] = false;
               break;
@@ -129,7 +130,7 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_part_agg(const __g
                 for (int w = 0; w < JP_W; w++) tkey[(size_t)w * S + sl] = k[r][w];
                 __threadfence_block();
                 *reinterpret_cast<volatile unsigned int*>(&tag[sl]) = 2u;
-                list[atomicAdd(&s_total, 1u)] = (unsigned short)sl;
+                claimed[r] = true;
                 found[r] = (int)sl;
                 pending[r] = false;
                 break;
@@ -157,6 +158,18 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_part_agg(const __g
         if (!__syncthreads_or(any)) break;
       }
 #endif
+      // the new groups join the item's list: one shared atomic per warp and row
+      {
+        const int lane = tid & 31;
+#pragma unroll
+        for (int r = 0; r < JP_R; r++) {
+          const unsigned bl = __ballot_sync(0xffffffffu, claimed[r]);
+          unsigned at = 0;
+          if (bl && lane == __ffs(bl) - 1) at = atomicAdd(&s_total, (unsigned)__popc(bl));
+          at = __shfl_sync(0xffffffffu, at, bl ? __ffs(bl) - 1 : 0);
+          if (claimed[r]) list[at + __popc(bl & ((1u << lane) - 1u))] = (unsigned short)found[r];
+        }
+      }
       JRow rw[JP_R];
 #pragma unroll
       for (int r = 0; r < JP_R; r++) {

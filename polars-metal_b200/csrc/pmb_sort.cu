@@ -92,17 +92,27 @@ __global__ void __launch_bounds__(ST_NT) k_key_range(const __grid_constant__ Sor
     hi[k] = 0;
     nul[k] = any[k] = 0;
   }
+  // four rows per step, their loads issued together
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+  for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r0 < n; r0 += 4 * stride) {
     for (int k = 0; k < L.n_keys; k++) {
-      if (!pmb_valid_bit(L.valid[k], r)) {
-        nul[k] = 1;
-        continue;
+      uint64_t b[4];
+      bool v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int64_t r = r0 + u * stride;
+        v[u] = r < n && pmb_valid_bit(L.valid[k], r);
+        b[u] = r < n ? pmb_load_bits(L.data[k], L.elem[k], r) : 0;
+        nul[k] |= (r < n && !v[u]) ? 1u : 0u;
       }
-      unsigned long long o = ordered_bits(pmb_load_bits(L.data[k], L.elem[k], r), L.dtype[k]);
-      lo[k] = o < lo[k] ? o : lo[k];
-      hi[k] = o > hi[k] ? o : hi[k];
-      any[k] = 1;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (!v[u]) continue;
+        const unsigned long long o = ordered_bits(b[u], L.dtype[k]);
+        lo[k] = o < lo[k] ? o : lo[k];
+        hi[k] = o > hi[k] ? o : hi[k];
+        any[k] = 1;
+      }
     }
   }
   for (int k = 0; k < L.n_keys; k++) {
