@@ -189,11 +189,11 @@ def cpu_baseline(workload: str, threads: int, sample_rows: int, reps: int = 3) -
             "sample": f"first {sample_rows:,} rows of the same generator (seed 99), median of {reps} after 1 warm-up"}
 
 
-def batch_queries(device, seed: int, stop_rows: int | None = None):
+def batch_queries(device, seed: int, stop_rows: int | None = None, max_total: int = BATCH_ROWS):
     """The batched workload's tables and their (columns, keys, aggs, predicate) tuples."""
     from polars_b200 import datagen
 
-    tables = datagen.make_batch(BATCH_QUERIES, seed=seed, device=device, max_total=BATCH_ROWS, stop_rows=stop_rows)
+    tables = datagen.make_batch(BATCH_QUERIES, seed=seed, device=device, max_total=max_total, stop_rows=stop_rows)
     return tables, [(datagen.to_column_data(t), t.keys, t.aggs, t.predicate) for t in tables]
 
 
@@ -312,7 +312,8 @@ def main():
     ap.add_argument("--workload", default="hash", choices=sorted(WORKLOADS) + ["batch"])
     ap.add_argument("--no-batched", action="store_true", help="leave out the batched-vs-plain comparison")
     ap.add_argument("--strategy", default="auto", help="group-by strategy of the timed calls (default: auto)")
-    ap.add_argument("--rows", type=int, default=0, help="override the workload's row count")
+    ap.add_argument("--rows", type=int, default=0,
+                    help="override the workload's row count (batch: the total over its 4096 queries)")
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -489,7 +490,7 @@ def run_batch(args, device, rank: int, local_rank: int, world: int) -> None:
     from polars_b200._native import ColumnData, Handle, groupby_batched
     from polars_b200.replicas import barrier, reduce_step_stats
 
-    tables, qs = batch_queries(device, seed=4 + rank)
+    tables, qs = batch_queries(device, seed=4 + rank, max_total=args.rows or BATCH_ROWS)
     torch.cuda.synchronize()
     rows = sum(t.n_rows for t in tables)
     bytes_per_row = tables[0].bytes_per_row()

@@ -433,16 +433,29 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
   uint8_t* out_base = (uint8_t*)pmb_ws_alloc(h, (size_t)ob + 16);
   unsigned long long* d_ooff = (unsigned long long*)pmb_ws_alloc(h, 8 * out_off.size());
   if (!out_base || !d_ooff) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (batch outputs)");
-  std::vector<DQuery> hq(nq);
+  // the round's descriptors go up from the pinned staging area when it has room
+  std::vector<DQuery> hq_own;
+  DQuery* hq = (DQuery*)pmb_host_stage(h, sizeof(DQuery) * nq);
+  if (!hq) {
+    hq_own.resize(nq);
+    hq = hq_own.data();
+  }
   std::vector<unsigned int*> hst(nq);
   for (int i = 0; i < nq; i++) {
     hq[i] = cqs[qidx[i]].dq;
     hst[i] = status + 16 * i;
   }
-  PMB_CUDA(h, cudaMemcpyAsync(d_jp, jp.data(), sizeof(JitParams) * nq, cudaMemcpyHostToDevice, h->stream));
-  PMB_CUDA(h, cudaMemcpyAsync(d_items, items.data(), sizeof(JBatchItemH) * items.size(), cudaMemcpyHostToDevice, h->stream));
-  PMB_CUDA(h, cudaMemcpyAsync(hot, hot_h.data(), 8 * hot_h.size(), cudaMemcpyHostToDevice, h->stream));
-  PMB_CUDA(h, cudaMemcpyAsync(d_qs, hq.data(), sizeof(DQuery) * nq, cudaMemcpyHostToDevice, h->stream));
+  auto upload = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+    if (void* st = pmb_host_stage(h, bytes)) {
+      memcpy(st, src, bytes);
+      src = st;
+    }
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+  };
+  PMB_CUDA(h, upload(d_jp, jp.data(), sizeof(JitParams) * nq));
+  PMB_CUDA(h, upload(d_items, items.data(), sizeof(JBatchItemH) * items.size()));
+  PMB_CUDA(h, upload(hot, hot_h.data(), 8 * hot_h.size()));
+  PMB_CUDA(h, cudaMemcpyAsync(d_qs, hq, sizeof(DQuery) * nq, cudaMemcpyHostToDevice, h->stream));
   PMB_CUDA(h, cudaMemcpyAsync(d_soff, slot_off.data(), 8 * slot_off.size(), cudaMemcpyHostToDevice, h->stream));
   PMB_CUDA(h, cudaMemcpyAsync(d_cap, cap.data(), 8 * cap.size(), cudaMemcpyHostToDevice, h->stream));
   PMB_CUDA(h, cudaMemcpyAsync(d_st, hst.data(), sizeof(void*) * nq, cudaMemcpyHostToDevice, h->stream));
@@ -655,9 +668,14 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
     DQuery* d_all = (DQuery*)pmb_ws_alloc(h, sizeof(DQuery) * n_queries);
     BatchSketch* d_sk = (BatchSketch*)pmb_ws_alloc(h, sizeof(BatchSketch) * n_queries);
     if (!d_all || !d_sk) return fail_all(pmb_fail(h, PMB_E_OOM, "workspace exhausted (batch sketch)"));
-    std::vector<DQuery> hb(nb);
+    std::vector<DQuery> hb_own;
+    DQuery* hb = (DQuery*)pmb_host_stage(h, sizeof(DQuery) * nb);
+    if (!hb) {
+      hb_own.resize(nb);
+      hb = hb_own.data();
+    }
     for (int j = 0; j < nb; j++) hb[j] = cqs[batch[j]].dq;
-    PMB_CUDA(h, cudaMemcpyAsync(d_all, hb.data(), sizeof(DQuery) * nb, cudaMemcpyHostToDevice, h->stream));
+    PMB_CUDA(h, cudaMemcpyAsync(d_all, hb, sizeof(DQuery) * nb, cudaMemcpyHostToDevice, h->stream));
     FxColsB fxc;
     memset(&fxc, 0, sizeof(fxc));
     fxc.n = (int)cqs[batch[0]].fx_cols.size();

@@ -176,6 +176,9 @@ struct pmb_handle {
   std::string err;
   int sm_count = 148;
   int max_smem_optin = 227 * 1024;
+  // pinned host staging (pmb_host_stage)
+  uint8_t* hstage = nullptr;
+  size_t hstage_cap = 0, hstage_used = 0, hstage_want = 0;
   // profiling
   bool profiling = false;
   std::vector<KernelTiming> timings;
@@ -211,6 +214,10 @@ struct WsMark {
 WsMark pmb_ws_mark(const pmb_handle* h);
 void pmb_ws_release(pmb_handle* h, WsMark m);
 void* pmb_ws_alloc(pmb_handle* h, size_t bytes);
+// pinned host staging for bulk uploads of a call: bump-allocated, reset by pmb_ws_begin, and sized
+// to what the previous call asked for; nullptr when the current area is full (the caller then
+// uploads from its own memory)
+void* pmb_host_stage(pmb_handle* h, size_t bytes);
 inline size_t pmb_align(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // profiling around launches (pmb_runtime.cu)

@@ -46,7 +46,28 @@ int pmb_ws_begin(pmb_handle* h) {
     h->ws.push_back({p, total, 0});
   }
   for (auto& b : h->ws) b.top = 0;
+  // the staging area grows between calls (the previous call's copies have completed by now)
+  if (h->hstage_want > h->hstage_cap) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return pmb_cuda_check(h, e, "cudaStreamSynchronize");
+    if (h->hstage) cudaFreeHost(h->hstage);
+    h->hstage = nullptr;
+    h->hstage_cap = 0;
+    if (cudaMallocHost((void**)&h->hstage, h->hstage_want) == cudaSuccess) h->hstage_cap = h->hstage_want;
+    else cudaGetLastError();
+  }
+  h->hstage_used = 0;
+  h->hstage_want = 0;
   return PMB_OK;
+}
+
+void* pmb_host_stage(pmb_handle* h, size_t bytes) {
+  const size_t b = (bytes + 255) & ~(size_t)255;
+  h->hstage_want += b;
+  if (!h->hstage || h->hstage_used + b > h->hstage_cap) return nullptr;
+  void* p = h->hstage + h->hstage_used;
+  h->hstage_used += b;
+  return p;
 }
 
 WsMark pmb_ws_mark(const pmb_handle* h) { return {h->ws.size(), h->ws.empty() ? 0 : h->ws.back().top}; }
@@ -345,6 +366,7 @@ void pmb_close(pmb_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   ws_free_all(h);
   if (h->pinned) cudaFreeHost(h->pinned);
+  if (h->hstage) cudaFreeHost(h->hstage);
   if (h->selector) cudaFree(h->selector);
   for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
   if (h->call_start) cudaEventDestroy(h->call_start);

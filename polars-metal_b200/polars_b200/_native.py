@@ -138,8 +138,15 @@ class ColumnData:
             self.length = int(_nelem(self.data)) - self.offset
 
 
+_TORCH_TYPES: dict[type, bool] = {}
+
+
 def _is_torch(x) -> bool:
-    return type(x).__module__.startswith("torch")
+    t = type(x)
+    r = _TORCH_TYPES.get(t)
+    if r is None:
+        r = _TORCH_TYPES[t] = t.__module__.startswith("torch")
+    return r
 
 
 def _nelem(x) -> int:
@@ -274,6 +281,11 @@ def _bitmap_bytes(n: int) -> int:
     return max(b, 4)
 
 
+def _host_copy(addr: int, nbytes: int, dtype) -> np.ndarray:
+    """A numpy copy of `nbytes` of host memory at `addr` (one copy)."""
+    return np.frombuffer((C.c_char * nbytes).from_address(addr), dtype=dtype).copy()
+
+
 def _read_result(res: A.Result, names, to_host: bool) -> tuple[list, list, list]:
     n = res.n_groups
     data, valid, dts = [], [], []
@@ -285,13 +297,12 @@ def _read_result(res: A.Result, names, to_host: bool) -> tuple[list, list, list]
             valid.append(int(oc.validity or 0))
             continue
         vb = _bitmap_bytes(n)
-        v = np.frombuffer(C.string_at(oc.validity, vb), dtype=np.uint8).copy() if oc.validity else np.zeros(vb, np.uint8)
+        v = _host_copy(oc.validity, vb, np.uint8) if oc.validity else np.zeros(vb, np.uint8)
         if oc.dtype == A.BOOL:
-            d = np.frombuffer(C.string_at(oc.data, vb), dtype=np.uint8).copy() if oc.data else np.zeros(vb, np.uint8)
+            d = _host_copy(oc.data, vb, np.uint8) if oc.data else np.zeros(vb, np.uint8)
         else:
             nb = n * A.DTYPE_BYTES[oc.dtype]
-            raw = C.string_at(oc.data, nb) if (oc.data and nb) else b""
-            d = np.frombuffer(raw, dtype=A.NUMPY_NAME[oc.dtype]).copy()
+            d = _host_copy(oc.data, nb, A.NUMPY_NAME[oc.dtype]) if (oc.data and nb) else np.zeros(0, A.NUMPY_NAME[oc.dtype])
         data.append(d)
         valid.append(v)
     return data, valid, dts
@@ -395,6 +406,74 @@ def _query(columns, keys, aggs, predicate):
     return q, abi_cols, len(cols), (keep, expr_keep, key_arr, agg_arr, expr)
 
 
+def _np_struct(S) -> np.dtype:
+    """numpy dtype with the layout of a ctypes structure (pointers as 64-bit addresses)."""
+    names, formats, offsets = [], [], []
+    for name, t in S._fields_:
+        names.append(name)
+        offsets.append(getattr(S, name).offset)
+        is_ptr = t is C.c_void_p or (isinstance(t, type) and issubclass(t, C._Pointer))
+        formats.append("<u8" if is_ptr else np.dtype(t).str)
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": C.sizeof(S)})
+
+
+_COLUMN_NP = _np_struct(A.Column)
+_QUERY_NP = _np_struct(A.Query)
+# groupby_batched reads results as 64-bit words: n_groups | n_columns | columns | strategy_used,
+# rehash_count | capacity, and every output column as data | validity | length | dtype, on_device
+assert [A.Result.n_groups.offset, A.Result.n_columns.offset, A.Result.columns.offset, A.Result.strategy_used.offset,
+        A.Result.rehash_count.offset, A.Result.capacity.offset, C.sizeof(A.Result)] == [0, 8, 16, 24, 28, 32, 40]
+assert [A.OutColumn.data.offset, A.OutColumn.validity.offset, A.OutColumn.dtype.offset, C.sizeof(A.OutColumn)] == \
+    [0, 8, 24, 32]
+
+
+def _batch_args(queries, output: str):
+    """The C arguments of pmb_groupby_batched: query structs, one pointer per query to its column
+    structs, the column counts, plus what must stay alive during the call and the output names.
+    Queries usually share keys, aggregates and filter: those parts are built once per shape, and
+    the per-query structs are filled as numpy records."""
+    n = len(queries)
+    shapes = {}
+    qrec = np.zeros(max(1, n), dtype=_QUERY_NP)
+    ncols = np.zeros(max(1, n), dtype=np.int32)
+    counts = [len(q[0]) for q in queries]
+    crec = np.zeros(max(1, sum(counts)), dtype=_COLUMN_NP)
+    first = np.zeros(max(1, n), dtype=np.uint64)
+    keep, names, fields, qrows = [], [], [], []
+    on_dev = 1 if output == "device" else 0
+    ci = 0
+    for i, (columns, keys, aggs, predicate) in enumerate(queries):
+        key = (tuple(columns), tuple(keys), tuple(aggs), id(predicate))
+        sh = shapes.get(key)
+        if sh is None:
+            parts = _query_shape(list(columns), keys, aggs, predicate)
+            key_arr, nk, agg_arr, na, expr, _ek = parts
+            sh = ((C.addressof(key_arr), nk, C.addressof(agg_arr), na, C.addressof(expr) if expr is not None else 0,
+                   A.STRATEGIES["auto"], on_dev, 0), list(keys) + [a[2] for a in aggs], parts, predicate)
+            shapes[key] = sh
+            keep.append(sh)
+        qrows.append(sh[0])
+        names.append(sh[1])
+        first[i] = ci
+        for c in columns.values():
+            cd = c if isinstance(c, ColumnData) else ColumnData(c)
+            dp, dd, k1 = _ptr(cd.data)
+            vp, vd, k2 = _ptr(cd.validity)
+            if cd.validity is not None and vd != dd:
+                raise ValueError("data and validity of a column must live in the same memory space")
+            fields.append((dp, vp, cd.length, cd.offset, cd.dtype, dd))
+            keep.append((k1, k2))
+            ci += 1
+    if qrows:
+        qrec[:n] = qrows
+        ncols[:n] = counts
+    if fields:
+        crec[: len(fields)] = fields
+    ptrs = (first * np.uint64(_COLUMN_NP.itemsize) + np.uint64(crec.ctypes.data)).astype(np.uint64)
+    keep += [qrec, crec, ptrs, ncols]
+    return qrec, ptrs, ncols, keep, names
+
+
 def groupby_batched(queries, output: str = "host", handle: Handle | None = None) -> list:
     """Many independent group-by queries in one call (pmb_groupby_batched).
 
@@ -402,39 +481,32 @@ def groupby_batched(queries, output: str = "host", handle: Handle | None = None)
     one signature run in one persistent launch; the results come back in query order."""
     h = handle or default_handle()
     n = len(queries)
-    qarr = (A.Query * max(1, n))()
-    col_ptrs = (C.POINTER(A.Column) * max(1, n))()
-    ncols = (C.c_int32 * max(1, n))()
-    keep = []
-    names = []
-    shapes = {}  # queries usually share keys, aggregates and filter: those are built once
-    for i, (columns, keys, aggs, predicate) in enumerate(queries):
-        shape = (tuple(columns), tuple(keys), tuple(aggs), id(predicate))
-        if shape not in shapes:
-            shapes[shape] = _query_shape(list(columns), keys, aggs, predicate)
-        q, sk = _query_from_shape(shapes[shape])
-        cols_l = [c if isinstance(c, ColumnData) else ColumnData(c) for c in columns.values()]
-        cols, ck = _to_abi_columns(cols_l)
-        nc = len(cols_l)
-        kp = (sk, ck, predicate)
-        q.strategy = A.STRATEGIES["auto"]
-        q.output_on_device = 1 if output == "device" else 0
-        q.capacity_hint = 0
-        qarr[i] = q
-        col_ptrs[i] = C.cast(cols, C.POINTER(A.Column))
-        ncols[i] = nc
-        keep.append((q, cols, kp))
-        names.append(list(keys) + [a[2] for a in aggs])
+    qrec, ptrs, ncols, keep, names = _batch_args(queries, output)
     outs = (C.POINTER(A.Result) * max(1, n))()
-    h.check(h._lib.pmb_groupby_batched(h.raw, qarr, col_ptrs, ncols, n, outs))
+    h.check(h._lib.pmb_groupby_batched(h.raw, qrec.ctypes.data_as(C.POINTER(A.Query)),
+                                       ptrs.ctypes.data_as(C.POINTER(C.POINTER(A.Column))),
+                                       ncols.ctypes.data_as(C.POINTER(C.c_int32)), n, outs))
+    addrs = list(C.cast(outs, C.POINTER(C.c_uint64 * max(1, n))).contents)[:n]
     results = []
     try:
+        to_host = output != "device"
+        head_at = (C.c_uint64 * 5).from_address  # a pmb_result read as 64-bit words (layout checked at import)
+        cols_at = {}
         for i in range(n):
-            res = outs[i].contents
-            data, valid, dts = _read_result(res, names[i], output != "device")
-            results.append(GroupByResult(n_groups=res.n_groups, names=names[i], dtypes=dts, data=data, validity=valid,
-                                         strategy=A.STRATEGY_NAMES.get(res.strategy_used, str(res.strategy_used)),
-                                         rehash_count=res.rehash_count, capacity=res.capacity))
+            hw = head_at(addrs[i])[:]
+            nc = hw[1] & 0xFFFFFFFF
+            su = hw[3] & 0xFFFFFFFF
+            if to_host:
+                data, valid, dts = _read_result(A.Result.from_address(addrs[i]), names[i], True)
+            else:
+                at = cols_at.get(nc)
+                if at is None:
+                    at = cols_at[nc] = (C.c_uint64 * (4 * nc)).from_address
+                cw = at(hw[2])[:]  # per column: data, validity, length, dtype
+                data, valid, dts = cw[0::4], cw[1::4], [x & 0xFFFFFFFF for x in cw[3::4]]
+            results.append(GroupByResult(n_groups=hw[0], names=names[i], dtypes=dts, data=data, validity=valid,
+                                         strategy=A.STRATEGY_NAMES.get(su, str(su)), rehash_count=hw[3] >> 32,
+                                         capacity=hw[4]))
     finally:
         for i in range(n):
             if outs[i]:

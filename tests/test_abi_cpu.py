@@ -108,3 +108,26 @@ def test_pack_bits_matches_numpy():
     got = datagen.pack_bits(m).numpy()
     want = np.packbits(m.numpy(), bitorder="little")
     assert np.array_equal(got, want)
+
+
+def test_batched_arguments_are_the_c_structs():
+    # the numpy records handed to pmb_groupby_batched read back as the C structs they stand for
+    tables = datagen.make_batch(5, seed=3, max_total=20_000)
+    qs = [(datagen.to_column_data(t), t.keys, t.aggs, t.predicate) for t in tables]
+    qrec, ptrs, ncols, keep, names = N._batch_args(qs, "device")
+    assert qrec.itemsize == C.sizeof(A.Query)
+    for i, (cols, keys, aggs, _pred) in enumerate(qs):
+        q = A.Query.from_address(qrec.ctypes.data + i * qrec.itemsize)
+        order = list(cols)
+        assert q.n_keys == len(keys) and [q.key_columns[k] for k in range(q.n_keys)] == [order.index(k) for k in keys]
+        assert q.n_aggs == len(aggs)
+        assert [(q.aggs[a].op, q.aggs[a].column) for a in range(q.n_aggs)] == \
+            [(A.AGG_OPS[op], -1 if op == "Len" else order.index(c)) for op, c, _ in aggs]
+        assert bool(q.predicate) and q.strategy == A.STRATEGIES["auto"] and q.output_on_device == 1
+        assert ncols[i] == len(cols)
+        col = (A.Column * len(cols)).from_address(int(ptrs[i]))
+        for j, cd in enumerate(cols.values()):
+            assert col[j].data == cd.data.data_ptr() and col[j].length == cd.length and col[j].dtype == cd.dtype
+            assert (col[j].validity or 0) == (cd.validity.data_ptr() if cd.validity is not None else 0)
+            assert col[j].on_device == 0
+        assert names[i] == list(keys) + [a[2] for a in aggs]
