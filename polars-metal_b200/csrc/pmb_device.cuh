@@ -86,6 +86,30 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // MurmurHash3 64-bit finalizer (Appleby, public domain)
+// fire-and-forget reductions on global memory (red.global: no value comes back, so nothing waits
+// for the L2 round trip)
+__device__ __forceinline__ void pmb_red_add(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+__device__ __forceinline__ void pmb_red_add(unsigned int* p, unsigned int v) {
+  asm volatile("red.relaxed.gpu.global.add.u32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v) : "memory");
+}
+__device__ __forceinline__ void pmb_red_or(unsigned int* p, unsigned int v) {
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v) : "memory");
+}
+__device__ __forceinline__ void pmb_red_min(long long* p, long long v) {
+  asm volatile("red.relaxed.gpu.global.min.s64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+__device__ __forceinline__ void pmb_red_max(long long* p, long long v) {
+  asm volatile("red.relaxed.gpu.global.max.s64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+__device__ __forceinline__ void pmb_red_min(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.min.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+__device__ __forceinline__ void pmb_red_max(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.max.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
+
 __host__ __device__ __forceinline__ uint64_t pmb_fmix64(uint64_t k) {
   k ^= k >> 33;
   k *= 0xff51afd7ed558ccdULL;

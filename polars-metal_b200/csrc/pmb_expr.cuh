@@ -323,7 +323,7 @@ __host__ __device__ inline void field_identity(int kind, uint64_t* w0, uint64_t*
 //   apply_row_shared  — the CTA-shared table (shared-memory atomics; on sm_100 only 32-bit
 //                       adds and 64-bit min/max are native there, so min/max skip when the
 //                       stored value already dominates and the rest stays low-contention);
-//   apply_row_global  — the global table (native L2 atomics, fire-and-forget where possible:
+//   apply_row_global  — the global table (L2 reductions, red.global, that return nothing:
 //                       adjacent 32-bit counters share one 64-bit add, min/max are issued only
 //                       when the row improves on a possibly stale read).
 __device__ __forceinline__ long long minmax_key(const DField& F, uint64_t b, int dt, bool is_min) {
@@ -464,7 +464,7 @@ __device__ __forceinline__ void apply_row_global(const DQuery& q, const TileCtx&
       unsigned long long inc = (F.kind == F_LEN || tc_isvalid(q, t, F.col, lr)) ? 1ULL : 0ULL;
       int w = F.off & ~7;
       if (w != pend_off) {
-        if (pend) atomicAdd((unsigned long long*)(rec + pend_off), pend);
+        if (pend) pmb_red_add((unsigned long long*)(rec + pend_off), pend);
         pend = 0;
         pend_off = w;
       }
@@ -480,46 +480,46 @@ __device__ __forceinline__ void apply_row_global(const DQuery& q, const TileCtx&
         double x = pmb_bits_to_f64(b, dt);
         unsigned fl = pmb_fx_flag(x);
         if (fl) {
-          atomicOr((unsigned int*)(p + 16), fl);
+          pmb_red_or((unsigned int*)(p + 16), fl);
         } else if (pmb_fx_in_range(x, q.fx_e[F.fx_slot])) {
           unsigned long long w0, w1;
           pmb_fx_words(x, F.fx, w0, w1);
-          if (w0) atomicAdd((unsigned long long*)p, w0);
-          if (w1) atomicAdd((unsigned long long*)p + 1, w1);
+          if (w0) pmb_red_add((unsigned long long*)p, w0);
+          if (w1) pmb_red_add((unsigned long long*)p + 1, w1);
         }
         break;
       }
-      case F_SUM_I: atomicAdd((unsigned long long*)p, (unsigned long long)pmb_bits_to_i64(b, dt)); break;
+      case F_SUM_I: pmb_red_add((unsigned long long*)p, (unsigned long long)pmb_bits_to_i64(b, dt)); break;
       // a stale read can only be weaker than the stored extreme, so skipping is safe
       case F_MIN_I: {
         long long v = (long long)pmb_bits_to_i64(b, dt);
-        if (v < *(const long long*)p) atomicMin((long long*)p, v);
+        if (v < *(const long long*)p) pmb_red_min((long long*)p, v);
         break;
       }
       case F_MAX_I: {
         long long v = (long long)pmb_bits_to_i64(b, dt);
-        if (v > *(const long long*)p) atomicMax((long long*)p, v);
+        if (v > *(const long long*)p) pmb_red_max((long long*)p, v);
         break;
       }
       case F_MIN_U:
-        if (b < *(const unsigned long long*)p) atomicMin((unsigned long long*)p, (unsigned long long)b);
+        if (b < *(const unsigned long long*)p) pmb_red_min((unsigned long long*)p, (unsigned long long)b);
         break;
       case F_MAX_U:
-        if (b > *(const unsigned long long*)p) atomicMax((unsigned long long*)p, (unsigned long long)b);
+        if (b > *(const unsigned long long*)p) pmb_red_max((unsigned long long*)p, (unsigned long long)b);
         break;
       case F_MIN_F: {
         long long k = minmax_key(F, b, dt, true);
-        if (k < *(const long long*)p) atomicMin((long long*)p, k);
+        if (k < *(const long long*)p) pmb_red_min((long long*)p, k);
         break;
       }
       default: {
         long long k = minmax_key(F, b, dt, false);
-        if (k > *(const long long*)p) atomicMax((long long*)p, k);
+        if (k > *(const long long*)p) pmb_red_max((long long*)p, k);
         break;
       }
     }
   }
-  if (pend) atomicAdd((unsigned long long*)(rec + pend_off), pend);
+  if (pend) pmb_red_add((unsigned long long*)(rec + pend_off), pend);
 }
 
 // Merges a finished record `src` into `dst` (global memory, atomics).
@@ -532,7 +532,7 @@ __device__ __forceinline__ void merge_record(const DQuery& q, uint8_t* dst, cons
       case F_LEN:
       case F_CNT: {
         unsigned int v = *(const unsigned int*)s;
-        if (v) atomicAdd((unsigned int*)d, v);
+        if (v) pmb_red_add((unsigned int*)d, v);
         break;
       }
       case F_SUM_DD: {
@@ -544,36 +544,36 @@ __device__ __forceinline__ void merge_record(const DQuery& q, uint8_t* dst, cons
       case F_SUM_FX: {
         const unsigned long long* l = (const unsigned long long*)s;
         for (int w = 0; w < 2; w++)
-          if (l[w]) atomicAdd((unsigned long long*)d + w, l[w]);
+          if (l[w]) pmb_red_add((unsigned long long*)d + w, l[w]);
         unsigned fl = *(const unsigned int*)(s + 16);
-        if (fl) atomicOr((unsigned int*)(d + 16), fl);
+        if (fl) pmb_red_or((unsigned int*)(d + 16), fl);
         break;
       }
       case F_SUM_I: {
         unsigned long long v = *(const unsigned long long*)s;
-        if (v) atomicAdd((unsigned long long*)d, v);
+        if (v) pmb_red_add((unsigned long long*)d, v);
         break;
       }
       case F_MIN_I:
       case F_MIN_F: {
         long long v = *(const long long*)s;
-        if (v != 0x7FFFFFFFFFFFFFFFLL) atomicMin((long long*)d, v);
+        if (v != 0x7FFFFFFFFFFFFFFFLL) pmb_red_min((long long*)d, v);
         break;
       }
       case F_MAX_I:
       case F_MAX_F: {
         long long v = *(const long long*)s;
-        if (v != (long long)0x8000000000000000LL) atomicMax((long long*)d, v);
+        if (v != (long long)0x8000000000000000LL) pmb_red_max((long long*)d, v);
         break;
       }
       case F_MIN_U: {
         unsigned long long v = *(const unsigned long long*)s;
-        if (v != 0xFFFFFFFFFFFFFFFFULL) atomicMin((unsigned long long*)d, v);
+        if (v != 0xFFFFFFFFFFFFFFFFULL) pmb_red_min((unsigned long long*)d, v);
         break;
       }
       default: {
         unsigned long long v = *(const unsigned long long*)s;
-        if (v) atomicMax((unsigned long long*)d, v);
+        if (v) pmb_red_max((unsigned long long*)d, v);
         break;
       }
     }

@@ -332,28 +332,28 @@ struct Gen {
         case F_SUM_FX: {
           std::string slot = std::to_string(F.fx_slot);
           b << "    double xv = (double)" << v(F.col) << ";\n    unsigned fl = pmb_fx_flag(xv);\n";
-          b << "    if (fl) atomicOr(" << at(F.off + 16, "unsigned int") << ", fl);\n";
+          b << "    if (fl) pmb_red_or(" << at(F.off + 16, "unsigned int") << ", fl);\n";
           b << "    else if (pmb_fx_in_range(xv, P.fx_e[" << slot << "])) {\n      unsigned long long w0, w1;\n";
           b << "      pmb_fx_words(xv, P.fx[" << slot << "], w0, w1);\n";
-          b << "      if (w0) atomicAdd(" << at(F.off, "unsigned long long") << ", w0);\n";
-          b << "      if (w1) atomicAdd(" << at(F.off + 8, "unsigned long long") << ", w1);\n    }\n";
+          b << "      if (w0) pmb_red_add(" << at(F.off, "unsigned long long") << ", w0);\n";
+          b << "      if (w1) pmb_red_add(" << at(F.off + 8, "unsigned long long") << ", w1);\n    }\n";
           break;
         }
         case F_SUM_DD:
           b << "    dd_atomic_add(" << at(F.off, "double") << ", " << at(F.off + 8, "double") << ", " << fval(F) << ");\n";
           break;
-        case F_SUM_I: b << "    atomicAdd(" << at(F.off, "unsigned long long") << ", " << fval(F) << ");\n"; break;
+        case F_SUM_I: b << "    pmb_red_add(" << at(F.off, "unsigned long long") << ", " << fval(F) << ");\n"; break;
         default: {
           bool mn = F.kind == F_MIN_I || F.kind == F_MIN_U || F.kind == F_MIN_F;
           const char* T = (F.kind == F_MIN_U || F.kind == F_MAX_U) ? "unsigned long long" : "long long";
-          // no read first: cold keys rarely skip an update, and a fire-and-forget atomic does not wait
-          b << "    " << (mn ? "atomicMin(" : "atomicMax(") << at(F.off, T) << ", (" << T << ")(" << fval(F) << "));\n";
+          // no read first: cold keys rarely skip an update, and a reduction (red) does not wait
+          b << "    " << (mn ? "pmb_red_min(" : "pmb_red_max(") << at(F.off, T) << ", (" << T << ")(" << fval(F) << "));\n";
         }
       }
       b << "  }\n";
     }
     for (auto& p : words)
-      b << "  atomicAdd(reinterpret_cast<unsigned long long*>(rec + " << p.first << "), " << p.second << ");\n";
+      b << "  pmb_red_add(reinterpret_cast<unsigned long long*>(rec + " << p.first << "), " << p.second << ");\n";
   }
 
   // ---- shared-memory record: native 32-bit atomics and 64-bit min/max only
@@ -440,21 +440,21 @@ struct Gen {
       switch (F.kind) {
         case F_LEN:
         case F_CNT:
-          b << "  { unsigned int x = " << CU(so) << "; if (x) atomicAdd(reinterpret_cast<unsigned int*>(d + " << gd
+          b << "  { unsigned int x = " << CU(so) << "; if (x) pmb_red_add(reinterpret_cast<unsigned int*>(d + " << gd
             << "), x); }\n";
           break;
         case F_SUM_FX:
           // the 96-bit partial P: its low 32 bits, and P >> 32 as a signed 64-bit word
-          b << "  { unsigned fl = " << CU(so + 12) << "; if (fl) atomicOr(reinterpret_cast<unsigned int*>(d + "
+          b << "  { unsigned fl = " << CU(so + 12) << "; if (fl) pmb_red_or(reinterpret_cast<unsigned int*>(d + "
             << F.off + 16 << "), fl);\n";
           b << "    unsigned w0 = " << CU(so) << ";\n    unsigned long long hi = ((unsigned long long)" << CU(so + 8)
             << " << 32) | " << CU(so + 4) << ";\n";
-          b << "    if (w0) atomicAdd(" << GU64(F.off) << ", (unsigned long long)w0);\n";
-          b << "    if (hi) atomicAdd(" << GU64(F.off + 8) << ", hi); }\n";
+          b << "    if (w0) pmb_red_add(" << GU64(F.off) << ", (unsigned long long)w0);\n";
+          b << "    if (hi) pmb_red_add(" << GU64(F.off + 8) << ", hi); }\n";
           break;
         case F_SUM_I:
           b << "  { unsigned long long x = ((unsigned long long)" << CU(so + 4) << " << 32) | " << CU(so)
-            << "; if (x) atomicAdd(" << GU64(F.off) << ", x); }\n";
+            << "; if (x) pmb_red_add(" << GU64(F.off) << ", x); }\n";
           break;
         case F_SUM_DD:
           b << "  { double hi = *reinterpret_cast<const double*>(s + " << so << "), lo = *reinterpret_cast<const double*>(s + "
@@ -470,7 +470,7 @@ struct Gen {
           std::string ident = uns ? (mn ? "0xFFFFFFFFFFFFFFFFULL" : "0ULL")
                                   : (mn ? "0x7FFFFFFFFFFFFFFFLL" : "(long long)0x8000000000000000ULL");
           b << "  { " << T << " x = *reinterpret_cast<const " << T << "*>(s + " << so << ");\n";
-          b << "    if (x != " << ident << ") " << (mn ? "atomicMin" : "atomicMax") << "(reinterpret_cast<" << T
+          b << "    if (x != " << ident << ") " << (mn ? "pmb_red_min" : "pmb_red_max") << "(reinterpret_cast<" << T
             << "*>(d + " << gd << "), x); }\n";
         }
       }
