@@ -323,7 +323,7 @@ __host__ __device__ inline void field_identity(int kind, uint64_t* w0, uint64_t*
 //   apply_row_shared  — the CTA-shared table (shared-memory atomics; on sm_100 only 32-bit
 //                       adds and 64-bit min/max are native there, so min/max skip when the
 //                       stored value already dominates and the rest stays low-contention);
-//   apply_row_global  — the global table (L2 reductions, red.global, that return nothing:
+//   apply_row_global  — the global table (fire-and-forget L2 updates, pmb_red_*:
 //                       adjacent 32-bit counters share one 64-bit add, min/max are issued only
 //                       when the row improves on a possibly stale read).
 __device__ __forceinline__ long long minmax_key(const DField& F, uint64_t b, int dt, bool is_min) {

@@ -931,7 +931,8 @@ int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, b
 }
 
 int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out) {
-  return jit_kernel(h, pmb_jit_source(cq, J) + "\n" + std::string(kBatchSkeleton), "pmb_jit_batch_agg", out);
+  return jit_kernel(h, "#define PMB_EXPLICIT_RED 1\n" + pmb_jit_source(cq, J) + "\n" + std::string(kBatchSkeleton),
+                    "pmb_jit_batch_agg", out);
 }
 
 // Internal check (not part of the C ABI in pmb.h): generates and compiles the run-time kernel of
@@ -969,7 +970,8 @@ static int debug_compile(const pmb_query* q, const pmb_column* cols, int32_t n_c
       rc = batch ? pmb_plan_jit_batch(&h, cq, 1024, 2, 232448, &J) : pmb_plan_jit(&h, cq, true, 232448, &J);
       if (rc == PMB_OK) {
         std::vector<char> cubin;
-        const std::string src = batch ? pmb_jit_source(cq, J) + "\n" + std::string(kBatchSkeleton) : pmb_jit_source(cq, J);
+        const std::string src = batch ? "#define PMB_EXPLICIT_RED 1\n" + pmb_jit_source(cq, J) + "\n" + std::string(kBatchSkeleton)
+                                      : pmb_jit_source(cq, J);
         if (const char* e = getenv("PMB_JIT_DEBUG"))
           if (e[0] == '2') fprintf(stderr, "%s\n", src.c_str());  // the generated source, for inspection
         if (!jit_compile(src, cubin, msg)) rc = PMB_E_UNSUPPORTED;
