@@ -297,10 +297,12 @@ int pmb_finish_outputs(pmb_handle* h, pmb_result* r, bool to_host) {
       free(hv);
       return pmb_fail(h, PMB_E_OOM, "host output allocation failed");
     }
-    memset(hd, 0, db ? db : 1);
-    memset(hv, 0, vb);
+    // the copies below fill every byte but the padding of the bitmaps, which is zeroed here
+    size_t copy_d = oc.dtype == PMB_BOOL ? (size_t)((n + 7) / 8) : db;
+    if (n == 0) copy_d = 0;
+    memset((uint8_t*)hd + copy_d, 0, (db ? db : 1) - copy_d);
+    memset(hv + (size_t)((n + 7) / 8), 0, vb - (size_t)((n + 7) / 8));
     if (n > 0) {
-      size_t copy_d = oc.dtype == PMB_BOOL ? (size_t)((n + 7) / 8) : db;
       PMB_CUDA(h, cudaMemcpyAsync(hd, oc.data, copy_d, cudaMemcpyDeviceToHost, h->stream));
       PMB_CUDA(h, cudaMemcpyAsync(hv, oc.validity, (size_t)((n + 7) / 8), cudaMemcpyDeviceToHost, h->stream));
       h->d2h += (int64_t)(copy_d + (size_t)((n + 7) / 8));

@@ -537,17 +537,6 @@ def _query_shape(names, keys, aggs, predicate):
     return key_arr, len(keys), agg_arr, len(aggs), expr, expr_keep
 
 
-def _query_from_shape(shape):
-    key_arr, nk, agg_arr, na, expr, expr_keep = shape
-    q = A.Query()
-    q.key_columns = key_arr
-    q.n_keys = nk
-    q.aggs = agg_arr
-    q.n_aggs = na
-    q.predicate = C.pointer(expr) if expr is not None else None
-    return q, shape
-
-
 def selector_features(columns, keys, aggs, predicate=None, handle: Handle | None = None) -> np.ndarray:
     """The learned selector's features of a query (PMB_SELECTOR_FEATURES floats), computed on the
     device from a 4096-row sample of its keys."""

@@ -125,6 +125,16 @@ def test_partitioned_partitions_and_fallbacks(hint):
     assert got.strategy == ("sort" if hint == 1 else "partitioned")
 
 
+def test_partitioned_aggregation_without_nvrtc(monkeypatch):
+    # with run-time compilation switched off the partitioned strategy aggregates with its prebuilt
+    # kernel (values gathered through a per-thread stage); results must not change
+    monkeypatch.setenv("PMB_JIT", "0")
+    t = datagen.make_sort(400_000, seed=19, pool=3_000)
+    cols = datagen.to_numpy_columns(t)
+    got = run_both(cols, t.keys, t.aggs, None, "partitioned", "partitioned, prebuilt aggregation")
+    assert got.strategy == "partitioned"
+
+
 def test_partitioned_heavy_keys_two_words_and_filter():
     rng = np.random.default_rng(37)
     n = 600_000
