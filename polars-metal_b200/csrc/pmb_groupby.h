@@ -87,8 +87,7 @@ int recompile_dd(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int3
 // keys = EMPTY, records = identity (k_table_init) on stream s
 void k_table_init_pub(unsigned long long* keys, int64_t key_words, uint64_t* recs, int64_t n_recs, int rec_words,
                       const RecInit& ri, int blocks, cudaStream_t s);
-// sort strategy (pmb_sort.cu): packed-key LSD radix sort + segmented reduce; groups come out in
-// packed-key order
+// sort strategy (pmb_sort.cu): packed-key LSD radix sort + segmented reduce
 // the sort strategy (part_groups == 0), or the partitioned strategy sized for part_groups groups
 int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r, int64_t part_groups);
 // learned selector (pmb_learned.cu): strategy and group count for AUTO; false when no selector is

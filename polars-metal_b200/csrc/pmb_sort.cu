@@ -16,12 +16,13 @@
 //                      for the tile's global offsets, the tile reordered in shared memory so that
 //                      the writes are coalesced);
 //   4. k_seg_starts  — segment starts (key differs from its predecessor) compacted in order;
-//   5. k_seg_reduce  — one thread per group folds its rows into a group record (the same record
-//                      and the same finalisation as the hash path, so both strategies give
-//                      identical results, exact float sums included) and writes the output
-//                      row; groups of more than 256 rows go to k_seg_reduce_big (one CTA per
-//                      group).
-// Output groups come out in packed-key order.
+//   5. with the run-time compiler: k_chunk_bounds cuts the sorted rows at segment starts into
+//      work items that fit a shared-memory table, and the partitioned strategy's aggregation
+//      (pmb_jit_part_agg, then k_part_finalize) reduces every item's segments there; without it,
+//      k_seg_reduce — one thread per group folds its rows into a group record and writes the
+//      output row; groups of more than 256 rows go to k_seg_reduce_big (one CTA per group).
+// Both use the hash path's records and finalisation, so every strategy gives identical results,
+// exact float sums included. The order of the output groups is not specified.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -910,6 +911,29 @@ static int pa_stage(const DQuery& q, unsigned* used, int32_t* sdoff, int32_t* sv
   return (off + 7) & ~7;
 }
 
+// run_part_agg's answer when the sort strategy should reduce its segments itself
+constexpr int kSegReduce = -77;
+
+// work-item boundaries for aggregating sorted rows in shared-memory tables: chunk c starts at the
+// first segment start at or after c * chunk (m at the end), so no group is cut
+__global__ void k_chunk_bounds(const unsigned int* __restrict__ starts, unsigned long long ng, int64_t m, int64_t chunk,
+                               int64_t n_chunks, unsigned long long* __restrict__ out) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > n_chunks) return;
+  const int64_t x = c * chunk;
+  if (c == n_chunks || x >= m) {
+    out[c] = (unsigned long long)m;
+    return;
+  }
+  unsigned long long lo = 0, hi = ng;
+  while (lo < hi) {
+    const unsigned long long mid = (lo + hi) >> 1;
+    if ((int64_t)starts[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  out[c] = lo < ng ? (unsigned long long)starts[lo] : (unsigned long long)m;
+}
+
 // float sums that left their fixed-point range: widen to the largest exponent seen (the sorted
 // order does not depend on it); true when a column must switch to double-double instead
 static bool widen_fx(CompiledQuery& cq, const unsigned int* st) {
@@ -934,7 +958,7 @@ template <int W>
 int run_part_agg(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_result* r, const unsigned long long* keys,
                  const unsigned int* idx, uint64_t cap, int64_t m, int pb, const std::vector<unsigned int>& counts,
                  int slots, int64_t groups,
-                 unsigned long long* ctr, unsigned int* status) {
+                 unsigned long long* ctr, unsigned int* status, int strategy = PMB_STRATEGY_PARTITIONED) {
   DQuery& q = cq.dq;
   const int n_out = q.n_keys + q.n_aggs;
   PartParams A;
@@ -1089,13 +1113,15 @@ int run_part_agg(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_r
         out_cap = std::max<int64_t>(m, 1);
         continue;
       }
-      // a partition had more groups than its table: the sort strategy instead
+      // a partition had more groups than its table: the sort strategy instead (the sort's own
+      // segment reduce when the caller is the sort)
+      if (strategy == PMB_STRATEGY_SORT) return kSegReduce;
       PMB_CUDA(h, cudaMemsetAsync(ctr, 0, 64, h->stream));
       return run_sort<W>(h, cq, L, r, 0);
     }
     r->n_groups = (int64_t)ng;
     r->capacity = out_cap;
-    r->strategy_used = PMB_STRATEGY_PARTITIONED;
+    r->strategy_used = strategy;
     for (int c = 0; c < n_out; c++) {
       r->columns[c].data = A.out_data[c];
       r->columns[c].validity = A.out_valid[c];
@@ -1238,6 +1264,38 @@ int run_sort(pmb_handle* h, CompiledQuery& cq, const SortKeyLayout& L, pmb_resul
     PMB_CUDA(h, cudaMemcpyAsync(&st, status, 4, cudaMemcpyDeviceToHost, h->stream));
     PMB_CUDA(h, cudaStreamSynchronize(h->stream));
     if (st & PMB_ST_TIMEOUT) return pmb_fail(h, PMB_E_TIMEOUT, "a bounded device wait timed out (sort)");
+  }
+  // with the run-time compiler, the sorted rows are cut at segment starts into work items that fit
+  // a shared-memory table, and the partitioned strategy's aggregation reduces them (values
+  // gathered once per row, records in shared memory); otherwise thread-per-segment reduces below
+  if (ng > 0 && pmb_jit_enabled(1LL << 40)) {
+    unsigned used;
+    int32_t sd[PMB_MAX_COLS], sv[PMB_MAX_COLS];
+    const int stage = pa_stage(q, &used, sd, sv);
+    int slots = 4096;
+    for (; slots >= 256; slots /= 2)
+      if (pa_layout(slots, W, q.rec_bytes, n_out, stage).bytes + 2048 <= (size_t)h->max_smem_optin) break;
+    if (slots >= 256) {
+      const int64_t chunk = (int64_t)(0.7 * slots);
+      const int64_t n_chunks = (m + chunk - 1) / chunk;
+      unsigned long long* bounds = (unsigned long long*)pmb_ws_alloc(h, (size_t)(n_chunks + 1) * 8);
+      if (!bounds) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (segment chunks)");
+      pmb_kernel_begin(h, "chunk_bounds");
+      k_chunk_bounds<<<(unsigned)((n_chunks + 1 + 255) / 256), 256, 0, h->stream>>>(starts, ng, m, chunk, n_chunks, bounds);
+      pmb_kernel_end(h);
+      PMB_CUDA(h, cudaGetLastError());
+      std::vector<unsigned long long> hb((size_t)n_chunks + 1);
+      PMB_CUDA(h, cudaMemcpyAsync(hb.data(), bounds, hb.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+      PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+      std::vector<unsigned int> counts((size_t)n_chunks);
+      for (int64_t c = 0; c < n_chunks; c++) counts[c] = (unsigned)(hb[c + 1] - hb[c]);
+      const WsMark mark = pmb_ws_mark(h);
+      const int rc = run_part_agg<W>(h, cq, L, r, k0, i0, cap, m, 0, counts, slots, (int64_t)ng, ctr, status,
+                                     PMB_STRATEGY_SORT);
+      if (rc != kSegReduce) return rc;
+      pmb_ws_release(h, mark);
+      PMB_CUDA(h, cudaMemcpyAsync(ctr + 2, &ng, 8, cudaMemcpyHostToDevice, h->stream));  // the group count again
+    }
   }
   // outputs
   ReduceParams R;

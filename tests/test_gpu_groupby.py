@@ -135,6 +135,15 @@ def test_partitioned_aggregation_without_nvrtc(monkeypatch):
     assert got.strategy == "partitioned"
 
 
+def test_sort_segment_reduce_without_nvrtc(monkeypatch):
+    # without run-time compilation the sort strategy reduces its segments thread by thread
+    monkeypatch.setenv("PMB_JIT", "0")
+    t = datagen.make_sort(400_000, seed=23, pool=3_000)
+    cols = datagen.to_numpy_columns(t)
+    got = run_both(cols, t.keys, t.aggs, None, "sort", "sort, segment reduce")
+    assert got.strategy == "sort"
+
+
 def test_partitioned_heavy_keys_two_words_and_filter():
     rng = np.random.default_rng(37)
     n = 600_000
