@@ -1,0 +1,83 @@
+"""Arrow in, Arrow out: pyarrow arrays as the group-by's input columns without copying them, and
+the result as a pyarrow table.
+
+The reference moves Arrow buffers to the GPU through its buffer crate
+(crates/polars-metal-buffer/src/bridge.rs:1-60), and its Python side copies every column into
+`bytes` first, combining chunks (python/polars_metal/_udf.py:1441-1456, 1484-1571). Here a
+single-chunk column is handed to libpmb as the Arrow buffers themselves: the value buffer from
+its start, the validity bitmap, and the array's offset, which libpmb applies to both (a bit offset
+in the bitmap included). Only a column of several chunks is combined into one (a copy).
+"""
+
+from __future__ import annotations
+
+from typing import Sequence
+
+import numpy as np
+import pyarrow as pa
+
+from . import _abi as A
+from ._native import ColumnData, GroupByResult, Handle, groupby
+
+_TO_PMB = {
+    pa.bool_(): A.BOOL,
+    pa.int8(): A.I8,
+    pa.int16(): A.I16,
+    pa.int32(): A.I32,
+    pa.int64(): A.I64,
+    pa.uint8(): A.U8,
+    pa.uint16(): A.U16,
+    pa.uint32(): A.U32,
+    pa.uint64(): A.U64,
+    pa.float32(): A.F32,
+    pa.float64(): A.F64,
+}
+_FROM_PMB = {v: k for k, v in _TO_PMB.items()}
+
+
+def column_from_arrow(arr: pa.Array | pa.ChunkedArray) -> ColumnData:
+    """A libpmb column over an Arrow array's own buffers (no copy for a single chunk)."""
+    if isinstance(arr, pa.ChunkedArray):
+        if arr.num_chunks == 1:
+            arr = arr.chunk(0)
+        elif arr.num_chunks == 0:
+            arr = pa.array([], type=arr.type)
+        else:
+            arr = arr.combine_chunks()
+    dt = _TO_PMB.get(arr.type)
+    if dt is None:
+        raise NotImplementedError(f"polars_b200: unsupported Arrow type {arr.type}")
+    n = len(arr)
+    validity_buf, data_buf = arr.buffers()[:2]
+    if data_buf is None or data_buf.size == 0:
+        data = np.zeros(max(1, (n + 7) // 8) if dt == A.BOOL else 1, np.uint8 if dt == A.BOOL else A.NUMPY_NAME[dt])
+        return ColumnData(data, None, dtype=dt, length=0, offset=0)
+    data = np.frombuffer(data_buf, dtype=np.uint8 if dt == A.BOOL else A.NUMPY_NAME[dt])
+    validity = np.frombuffer(validity_buf, dtype=np.uint8) if validity_buf is not None and arr.null_count else None
+    return ColumnData(data, validity, dtype=dt, length=n, offset=arr.offset)
+
+
+def columns_from_arrow(table: pa.Table | pa.RecordBatch, names: Sequence[str] | None = None) -> dict:
+    """{name: ColumnData} for the named columns of a table (all of them by default)."""
+    names = list(table.column_names if names is None else names)
+    return {name: column_from_arrow(table.column(name)) for name in names}
+
+
+def table_from_result(res: GroupByResult) -> pa.Table:
+    """The group-by result (host output) as a pyarrow table: keys first, then the aggregates."""
+    arrays = []
+    for data, valid, dt in zip(res.data, res.validity, res.dtypes):
+        if isinstance(data, int):
+            raise ValueError("polars_b200: the result is on the device; ask for output='host'")
+        arrays.append(pa.Array.from_buffers(_FROM_PMB[dt], res.n_groups,
+                                            [pa.py_buffer(np.ascontiguousarray(valid)),
+                                             pa.py_buffer(np.ascontiguousarray(data))]))
+    return pa.Table.from_arrays(arrays, names=list(res.names))
+
+
+def groupby_arrow(table: pa.Table | pa.RecordBatch, keys: Sequence[str], aggs: Sequence[tuple[str, str | None, str]],
+                  predicate: dict | None = None, strategy: str = "auto", handle: Handle | None = None) -> pa.Table:
+    """filter -> group_by -> aggregate of an Arrow table through libpmb; the result as an Arrow
+    table (keys, then the aggregates, in no particular group order)."""
+    res = groupby(columns_from_arrow(table), keys, aggs, predicate, strategy=strategy, output="host", handle=handle)
+    return table_from_result(res)
