@@ -782,6 +782,31 @@ def bool_or_dispatch(lhs_data: bytes, lhs_valid: bytes, rhs_data: bytes, rhs_val
     return _bool_common("pmb_bool_or", lhs_data, lhs_valid, rhs_data, rhs_valid, n_rows)
 
 
+def filter_columns(columns: dict, predicate: dict, output: str = "host", handle: Handle | None = None) -> GroupByResult:
+    """Top-level filter: the rows of `columns` whose predicate is valid and true, every column
+    compacted in one pass (pmb_filter_compact_expr; the reference's Filter node goes through
+    `_filter_via_polars`, python/polars_metal/_udf.py:550-597). The result has the input's column
+    names and dtypes; its `n_groups` is the number of rows kept."""
+    h = handle or default_handle()
+    names = list(columns)
+    cols = [c if isinstance(c, ColumnData) else ColumnData(c) for c in columns.values()]
+    abi, keep = _to_abi_columns(cols)
+    expr, ek = compile_predicate(predicate, {n: i for i, n in enumerate(names)})
+    if expr is None:
+        raise ValueError("polars_b200: filter_columns needs a predicate")
+    res_p = C.POINTER(A.Result)()
+    h.check(h._lib.pmb_filter_compact_expr(h.raw, C.byref(expr), abi, len(cols), 1 if output == "device" else 0,
+                                           C.byref(res_p)))
+    try:
+        res = res_p.contents
+        data, valid, dts = _read_result(res, names, output != "device")
+        return GroupByResult(n_groups=res.n_groups, names=names, dtypes=dts, data=data, validity=valid,
+                             strategy="filter", rehash_count=0, capacity=0)
+    finally:
+        h._lib.pmb_result_free(res_p)
+        del keep, ek
+
+
 def execute_filter_compact(pred_data: bytes, pred_valid: bytes, n_rows: int, columns: list) -> list:
     """Wire-compatible `_native.execute_filter_compact` (crates/polars-metal-core/src/udf/compact.rs:46-147):
     columns [(tag, data, valid)] -> [(data, valid, n_out)] compacted by keep = pred_data & pred_valid."""

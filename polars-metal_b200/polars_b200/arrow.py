@@ -17,7 +17,7 @@ import numpy as np
 import pyarrow as pa
 
 from . import _abi as A
-from ._native import ColumnData, GroupByResult, Handle, groupby
+from ._native import ColumnData, GroupByResult, Handle, filter_columns, groupby
 
 _TO_PMB = {
     pa.bool_(): A.BOOL,
@@ -80,4 +80,11 @@ def groupby_arrow(table: pa.Table | pa.RecordBatch, keys: Sequence[str], aggs: S
     """filter -> group_by -> aggregate of an Arrow table through libpmb; the result as an Arrow
     table (keys, then the aggregates, in no particular group order)."""
     res = groupby(columns_from_arrow(table), keys, aggs, predicate, strategy=strategy, output="host", handle=handle)
+    return table_from_result(res)
+
+
+def filter_arrow(table: pa.Table | pa.RecordBatch, predicate: dict, handle: Handle | None = None) -> pa.Table:
+    """The rows of an Arrow table whose predicate is valid and true, as an Arrow table (all its
+    columns, in row order)."""
+    res = filter_columns(columns_from_arrow(table), predicate, output="host", handle=handle)
     return table_from_result(res)

@@ -1,5 +1,6 @@
-"""GPU parity of the Arrow path (polars_b200.arrow.groupby_arrow) against the CPU oracle: sliced
-arrays (Arrow offsets, bit offsets in the validity bitmaps), nulls, a Bool key and several chunks."""
+"""GPU parity of the Arrow path (polars_b200.arrow) against the CPU oracle: groupby_arrow on sliced
+arrays (Arrow offsets, bit offsets in the validity bitmaps), nulls, a Bool key and several chunks;
+filter_arrow over every dtype."""
 
 import numpy as np
 import pyarrow as pa
@@ -8,7 +9,7 @@ import pytest
 from helpers import assert_results_match, pack
 from oracle import pyoracle
 from polars_b200 import _abi as A
-from polars_b200.arrow import column_from_arrow, groupby_arrow
+from polars_b200.arrow import column_from_arrow, filter_arrow, groupby_arrow
 
 pytestmark = pytest.mark.gpu
 
@@ -60,3 +61,28 @@ def test_arrow_chunked_input():
     got = groupby_arrow(table, ["k"], aggs)
     want = pyoracle.groupby({"k": (np.concatenate(parts), None), "v": (np.concatenate(vals), None)}, ["k"], aggs)
     assert_results_match(_arrow_as_dict(got), want, 1, aggs, "arrow chunked")
+
+
+def test_filter_arrow_every_dtype():
+    # a top-level Filter: every column of every dtype compacted in one pass, in row order
+    rng = np.random.default_rng(77)
+    n = 100_003
+    start = 5
+    dtypes = [np.int8, np.int16, np.int32, np.int64, np.uint8, np.uint16, np.uint32, np.uint64, np.float32, np.float64]
+    data = {f"c{i}": rng.integers(0, 100, n).astype(dt) for i, dt in enumerate(dtypes)}
+    nulls = {name: rng.random(n) < 0.1 for name in data}
+    data["b"] = rng.random(n) < 0.5
+    nulls["b"] = rng.random(n) < 0.05
+    table = pa.table({name: pa.array(v, mask=nulls[name]) for name, v in data.items()}).slice(start)
+    pred = {"kind": "Compare", "op": "Lt", "dtype": "I64", "lhs": {"kind": "Column", "name": "c3"},
+            "rhs": {"kind": "LiteralI64", "value": 60}}
+    got = filter_arrow(table, pred)
+    c3, c3n = data["c3"][start:], nulls["c3"][start:]
+    keep = pyoracle.filter_mask({"c3": (c3, pack(~c3n))}, pred)
+    assert got.num_rows == int(keep.sum()) and got.column_names == list(data)
+    for name, v in data.items():
+        col = got.column(name).to_numpy(zero_copy_only=False)
+        want_valid = ~nulls[name][start:][keep]
+        got_valid = ~np.asarray(got.column(name).is_null().to_numpy(zero_copy_only=False))
+        assert np.array_equal(got_valid, want_valid), name
+        assert np.array_equal(np.asarray(col)[want_valid].astype(v.dtype), v[start:][keep][want_valid]), name
