@@ -15,6 +15,7 @@ from typing import Sequence
 
 import numpy as np
 import pyarrow as pa
+import pyarrow.compute as pc
 
 from . import _abi as A
 from ._native import ColumnData, GroupByResult, Handle, filter_columns, groupby
@@ -75,12 +76,60 @@ def table_from_result(res: GroupByResult) -> pa.Table:
     return pa.Table.from_arrays(arrays, names=list(res.names))
 
 
+def _dictionary_key(col) -> tuple[pa.Array, pa.Array] | None:
+    """(int32 codes with the column's nulls, the distinct values) of a string, binary or
+    dictionary column; None for other types. Strings are encoded on the host (the reference
+    encodes them on the host too, crates/polars-metal-buffer/src/dict.rs:18-74); the group-by then
+    runs on the codes, and the output codes are decoded through the values."""
+    if isinstance(col, pa.ChunkedArray):
+        if pa.types.is_dictionary(col.type):
+            col = col.unify_dictionaries()
+        col = col.combine_chunks() if col.num_chunks else pa.array([], type=col.type)
+    t = col.type
+    if pa.types.is_dictionary(t):
+        codes, values = col.indices, col.dictionary
+    elif pa.types.is_string(t) or pa.types.is_large_string(t) or pa.types.is_binary(t) or pa.types.is_large_binary(t):
+        enc = pc.dictionary_encode(col)
+        codes, values = enc.indices, enc.dictionary
+    else:
+        return None
+    return (codes if codes.type == pa.int32() else codes.cast(pa.int32())), values
+
+
+def _predicate_columns(p, out: set) -> set:
+    if isinstance(p, dict):
+        if p.get("kind") == "Column":
+            out.add(p["name"])
+        for v in p.values():
+            _predicate_columns(v, out)
+    return out
+
+
 def groupby_arrow(table: pa.Table | pa.RecordBatch, keys: Sequence[str], aggs: Sequence[tuple[str, str | None, str]],
                   predicate: dict | None = None, strategy: str = "auto", handle: Handle | None = None) -> pa.Table:
     """filter -> group_by -> aggregate of an Arrow table through libpmb; the result as an Arrow
-    table (keys, then the aggregates, in no particular group order)."""
-    res = groupby(columns_from_arrow(table), keys, aggs, predicate, strategy=strategy, output="host", handle=handle)
-    return table_from_result(res)
+    table (keys, then the aggregates, in no particular group order). Key columns may be strings,
+    binary or dictionaries (grouped by their dictionary codes); only the columns the query reads
+    are handed to libpmb."""
+    used = set(keys) | {c for _op, c, _a in aggs if c is not None} | _predicate_columns(predicate, set())
+    names = [n for n in table.column_names if n in used]
+    missing = [n for n in used if n not in table.column_names]
+    if missing:
+        raise KeyError(f"polars_b200: column {missing[0]!r} not found in upstream columns")
+    cols, dicts = {}, {}
+    for name in names:
+        enc = _dictionary_key(table.column(name)) if name in keys else None
+        if enc is not None:
+            cols[name] = column_from_arrow(enc[0])
+            dicts[name] = enc[1]
+        else:
+            cols[name] = column_from_arrow(table.column(name))
+    res = groupby(cols, keys, aggs, predicate, strategy=strategy, output="host", handle=handle)
+    out = table_from_result(res)
+    for name, values in dicts.items():
+        i = out.column_names.index(name)
+        out = out.set_column(i, name, values.take(out.column(i)))
+    return out
 
 
 def filter_arrow(table: pa.Table | pa.RecordBatch, predicate: dict, handle: Handle | None = None) -> pa.Table:

@@ -88,3 +88,16 @@ def test_results_become_arrow_tables():
     assert t.column("k").to_pylist() == keys.tolist()
     assert t.column("s").to_pylist() == [0.5, None, 2.5, 3.5, None]
     assert t.column("n").type == pa.uint32() and t.column("n").to_pylist() == cnt.tolist()
+
+
+def test_string_and_dictionary_keys_become_codes():
+    from polars_b200.arrow import _dictionary_key
+
+    s = pa.chunked_array([pa.array(["x", None, "y"]), pa.array(["x", "zz"])])
+    codes, values = _dictionary_key(s)
+    assert codes.type == pa.int32()
+    assert values.take(codes).to_pylist() == ["x", None, "y", "x", "zz"]
+    d = pa.chunked_array([pa.array(["a", "b", "a"]).dictionary_encode(), pa.array(["c", "a"]).dictionary_encode()])
+    codes, values = _dictionary_key(d)  # chunks with different dictionaries are unified
+    assert values.take(codes).to_pylist() == ["a", "b", "a", "c", "a"]
+    assert _dictionary_key(pa.array([1, 2, 3])) is None

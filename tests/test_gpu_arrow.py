@@ -86,3 +86,29 @@ def test_filter_arrow_every_dtype():
         got_valid = ~np.asarray(got.column(name).is_null().to_numpy(zero_copy_only=False))
         assert np.array_equal(got_valid, want_valid), name
         assert np.array_equal(np.asarray(col)[want_valid].astype(v.dtype), v[start:][keep][want_valid]), name
+
+
+def test_string_keys_through_their_dictionary():
+    # a Utf8 key (with nulls) grouped by its dictionary codes; the output keys come back as strings
+    import pyarrow.compute as pc
+
+    rng = np.random.default_rng(91)
+    n = 150_000
+    words = np.array([f"w{i:05d}" for i in range(2_000)], dtype=object)
+    s = words[rng.integers(0, 2_000, n)]
+    sn = rng.random(n) < 0.03
+    g = rng.integers(0, 4, n).astype(np.int16)
+    v = rng.standard_normal(n)
+    table = pa.table({"s": pa.array(s, mask=sn, type=pa.string()), "g": pa.array(g), "v": pa.array(v),
+                      "unused": pa.array(["not read"] * n)})
+    aggs = [("Sum", "v", "sv"), ("Max", "v", "mx"), ("Len", None, "n")]
+    got = groupby_arrow(table, ["s", "g"], aggs)
+    assert got.column("s").type == pa.string()
+    enc = pc.dictionary_encode(table.column("s")).combine_chunks()
+    codes = enc.indices.to_numpy(zero_copy_only=False)
+    codes = np.where(np.isnan(codes), 0, codes).astype(np.int32) if codes.dtype.kind == "f" else codes.astype(np.int32)
+    want = pyoracle.groupby({"s": (codes, pack(~sn)), "g": (g, None), "v": (v, None)}, ["s", "g"], aggs)
+    # the product's string keys, back to the same codes
+    got_codes = pc.index_in(got.column("s"), value_set=enc.dictionary)
+    got_t = got.set_column(0, "s", got_codes.cast(pa.int32()))
+    assert_results_match(_arrow_as_dict(got_t), want, 2, aggs, "string keys")
