@@ -265,6 +265,16 @@ int pmb_bool_or(pmb_handle* h, const uint8_t* lhs_data, const uint8_t* lhs_valid
                 const uint8_t* rhs_data, const uint8_t* rhs_valid, int64_t n, uint8_t* out_data,
                 uint8_t* out_valid, int32_t on_device);
 
+/* One arithmetic expression of columns and literals (PMB_EXPR_COLUMN, _LIT_I64, _LIT_F64 and
+ * _ARITH nodes, at most 8 levels and 32 nodes) evaluated for every row into `out_data` (8 bytes a
+ * row) and `out_valid` (a bit-packed bitmap): the input column of an expression aggregate.
+ * `*out_dtype` receives PMB_F64 when a float column, a float literal or a true division takes
+ * part, else PMB_I64 (wrapping). A null operand, or an integer // or % by zero, gives null.
+ * Replaces the expression side of the reference's Expression aggregations
+ * (crates/polars-metal-core/src/udf/groupby/mod.rs:266-352, python/polars_metal/_walker.py:1205-1278). */
+int pmb_eval_expr(pmb_handle* h, const pmb_expr* expr, const pmb_column* cols, int32_t n_cols, void* out_data,
+                  uint8_t* out_valid, int32_t out_on_device, int32_t* out_dtype);
+
 /* Stream compaction of `cols` by a bit-packed predicate (keep = data & valid).
  * Replaces `_native.execute_filter_compact(pred_data, pred_valid, n_rows, columns)`
  * (crates/polars-metal-core/src/udf/compact.rs:46-147) and compute_keep_and_prefix +

@@ -66,6 +66,49 @@ __device__ __forceinline__ double pmb_py_fmod(double a, double b) {
   return r;
 }
 
+// a op b in Float64 (Polars floor division and modulo)
+__device__ __forceinline__ double pmb_arith_f64(int op, double a, double b) {
+  switch (op) {
+    case PMB_ARITH_ADD: return a + b;
+    case PMB_ARITH_SUB: return a - b;
+    case PMB_ARITH_MUL: return a * b;
+    case PMB_ARITH_TRUEDIV: return a / b;
+    case PMB_ARITH_FLOORDIV: return floor(a / b);
+    default: return pmb_py_fmod(a, b);
+  }
+}
+
+// a op b in Int64: wrapping +, -, *; floor division and modulo with the divisor's sign; `valid`
+// turns false on a division by zero
+__device__ __forceinline__ int64_t pmb_arith_i64(int op, int64_t a, int64_t b, bool& valid) {
+  const uint64_t x = (uint64_t)a, y = (uint64_t)b;
+  switch (op) {
+    case PMB_ARITH_ADD: return (int64_t)(x + y);
+    case PMB_ARITH_SUB: return (int64_t)(x - y);
+    case PMB_ARITH_MUL: return (int64_t)(x * y);
+    case PMB_ARITH_FLOORDIV: {
+      if (b == 0) {
+        valid = false;
+        return 0;
+      }
+      if (a == INT64_MIN && b == -1) return INT64_MIN;
+      int64_t qq = a / b;
+      if ((a % b != 0) && ((a < 0) != (b < 0))) qq -= 1;
+      return qq;
+    }
+    default: {
+      if (b == 0) {
+        valid = false;
+        return 0;
+      }
+      if (b == -1) return 0;
+      int64_t m = a % b;
+      if (m != 0 && ((m < 0) != (b < 0))) m += b;
+      return m;
+    }
+  }
+}
+
 __device__ __forceinline__ OpVal eval_operand(const DQuery& q, const TileCtx& t, const DOperand& o, int dt, int64_t lr) {
   OpVal a = eval_leaf(q, t, o.a, dt, lr);
   if (o.arith < 0) return a;
@@ -74,41 +117,8 @@ __device__ __forceinline__ OpVal eval_operand(const DQuery& q, const TileCtx& t,
   r.valid = a.valid && b.valid;
   r.i = 0;
   r.f = 0.0;
-  if (dt == PMB_F64) {
-    switch (o.arith) {
-      case PMB_ARITH_ADD: r.f = a.f + b.f; break;
-      case PMB_ARITH_SUB: r.f = a.f - b.f; break;
-      case PMB_ARITH_MUL: r.f = a.f * b.f; break;
-      case PMB_ARITH_TRUEDIV: r.f = a.f / b.f; break;
-      case PMB_ARITH_FLOORDIV: r.f = floor(a.f / b.f); break;
-      default: r.f = pmb_py_fmod(a.f, b.f); break;
-    }
-  } else {
-    uint64_t x = (uint64_t)a.i, y = (uint64_t)b.i;
-    switch (o.arith) {
-      case PMB_ARITH_ADD: r.i = (int64_t)(x + y); break;
-      case PMB_ARITH_SUB: r.i = (int64_t)(x - y); break;
-      case PMB_ARITH_MUL: r.i = (int64_t)(x * y); break;
-      case PMB_ARITH_FLOORDIV:
-        if (b.i == 0) r.valid = false;
-        else if (a.i == INT64_MIN && b.i == -1) r.i = INT64_MIN;
-        else {
-          int64_t qq = a.i / b.i;
-          if ((a.i % b.i != 0) && ((a.i < 0) != (b.i < 0))) qq -= 1;
-          r.i = qq;
-        }
-        break;
-      default:
-        if (b.i == 0) r.valid = false;
-        else if (b.i == -1) r.i = 0;
-        else {
-          int64_t m = a.i % b.i;
-          if (m != 0 && ((m < 0) != (b.i < 0))) m += b.i;
-          r.i = m;
-        }
-        break;
-    }
-  }
+  if (dt == PMB_F64) r.f = pmb_arith_f64(o.arith, a.f, b.f);
+  else r.i = pmb_arith_i64(o.arith, a.i, b.i, r.valid);
   return r;
 }
 

@@ -308,6 +308,58 @@ def _read_result(res: A.Result, names, to_host: bool) -> tuple[list, list, list]
     return data, valid, dts
 
 
+_AGG_BINARY_OPS = {"Add": "Add", "Sub": "Sub", "Mul": "Mul", "Div": "TrueDiv"}
+
+
+def _arith_wire(e: dict) -> dict:
+    """An aggregation expression in the reference's wire shape (Column / LiteralF64 / LiteralI64 /
+    Binary with Add, Sub, Mul, Div; crates/polars-metal-core/src/udf/groupby/mod.rs:266-352) as
+    the arithmetic nodes of the predicate wire; "Arith" nodes pass through."""
+    if not isinstance(e, dict):
+        raise ValueError("polars_b200: plan parse error: wrong type for expr")
+    kind = e.get("kind")
+    if kind in ("Column", "LiteralI64", "LiteralF64"):
+        return e
+    if kind in ("Binary", "Arith"):
+        op = _AGG_BINARY_OPS.get(e.get("op")) if kind == "Binary" else e.get("op")
+        if op is None or op not in A.ARITH_OPS:
+            raise ValueError(f"polars_b200: plan parse error: unknown op binary op {e.get('op')}")
+        return {"kind": "Arith", "op": op, "lhs": _arith_wire(e.get("lhs")), "rhs": _arith_wire(e.get("rhs"))}
+    raise ValueError(f"polars_b200: plan parse error: unknown op expr kind={kind}")
+
+
+def eval_expr(columns: dict[str, ColumnData | Any], expr: dict, handle: Handle | None = None) -> ColumnData:
+    """An arithmetic expression of the columns, evaluated on the GPU for every row (pmb_eval_expr):
+    Float64 when a float takes part or there is a true division, else Int64; null where an operand
+    is null or an integer // or % divides by zero. The new column is a CUDA tensor when an input
+    column is one, else a numpy array."""
+    h = handle or default_handle()
+    names = list(columns)
+    if not names:
+        raise ValueError("polars_b200: eval_expr needs columns")
+    cols = [c if isinstance(c, ColumnData) else ColumnData(c) for c in columns.values()]
+    abi, keep = _to_abi_columns(cols)
+    e, ek = compile_predicate(_arith_wire(expr), {nm: i for i, nm in enumerate(names)})
+    n = cols[0].length
+    dev = next((c.data.device for c in cols if _is_torch(c.data) and c.data.is_cuda), None)
+    if dev is not None:
+        import torch
+
+        data = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+        valid = torch.zeros(_bitmap_bytes(n), dtype=torch.uint8, device=dev)
+        dp, vp = data.data_ptr(), valid.data_ptr()
+    else:
+        data = np.empty(max(n, 1), np.int64)
+        valid = np.zeros(_bitmap_bytes(n), np.uint8)
+        dp, vp = data.ctypes.data, valid.ctypes.data
+    dt = C.c_int32()
+    h.check(h._lib.pmb_eval_expr(h.raw, C.byref(e), abi, len(cols), dp, vp, 1 if dev is not None else 0, C.byref(dt)))
+    del keep, ek
+    if dt.value == A.F64:
+        data = data.view(torch.float64) if dev is not None else data.view(np.float64)
+    return ColumnData(data, valid, dtype=dt.value, length=n)
+
+
 def groupby(
     columns: dict[str, ColumnData | Any],
     keys: Sequence[str],
@@ -321,8 +373,23 @@ def groupby(
     """filter -> group_by -> aggregate through libpmb.
 
     columns: name -> ColumnData (or a bare array with no nulls); aggs: (op, input column, alias)
-    with op in Sum/Mean/Count/Min/Max/Len (input None for Len); predicate: a predicate dict.
+    with op in Sum/Mean/Count/Min/Max/Len (input None for Len), the input may also be an
+    arithmetic expression dict (an expression aggregate, evaluated by eval_expr); predicate: a
+    predicate dict.
     """
+    if any(isinstance(a[1], dict) for a in aggs):
+        # expression aggregates: every expression is evaluated into a column of its own first
+        columns = dict(columns)
+        plain = []
+        for i, (op, col, alias) in enumerate(aggs):
+            if isinstance(col, dict):
+                name = f"__expr{i}"
+                while name in columns:
+                    name += "_"
+                columns[name] = eval_expr(columns, col, handle=handle)
+                col = name
+            plain.append((op, col, alias))
+        aggs = plain
     names = list(columns)
     index = {n: i for i, n in enumerate(names)}
     cols = [c if isinstance(c, ColumnData) else ColumnData(c) for c in columns.values()]
@@ -667,16 +734,22 @@ def execute_groupby(plan_dict: dict, n_rows: int, columns: list) -> list[tuple[s
                 raise ValueError(f"polars_b200: plan parse error: unknown op {a.get('op')!r}")
             aggs.append((a["op"], a.get("input_col", ""), a["output_alias"]))
         elif kind == "Expression":
-            raise NotImplementedError("polars_b200: Expression aggregations are not on this path")
+            if a.get("op") not in A.AGG_OPS or a.get("op") == "Len":
+                raise ValueError(f"polars_b200: plan parse error: unknown op {a.get('op')!r}")
+            aggs.append((a["op"], _arith_wire(a.get("expr")), a["output_alias"]))
         else:
             raise ValueError(f"polars_b200: plan parse error: unknown op kind={kind}")
     for k in keys:
         if k not in by_name:
             raise KeyError(f"polars_b200: key column {k!r} not found in upstream columns")
+    agg_cols = []
     for op, col, _ in aggs:
-        if op != "Len" and col not in by_name:
-            raise KeyError(f"polars_b200: agg input column {col!r} not found in upstream columns")
-    needed = list(dict.fromkeys(keys + [c for _, c, _ in aggs if c] + _predicate_columns(plan_dict.get("predicate"))))
+        refs = _predicate_columns(col) if isinstance(col, dict) else ([col] if op != "Len" else [])
+        for c in refs:
+            if c not in by_name:
+                raise KeyError(f"polars_b200: agg input column {c!r} not found in upstream columns")
+        agg_cols += refs
+    needed = list(dict.fromkeys(keys + agg_cols + _predicate_columns(plan_dict.get("predicate"))))
     cols = {}
     for name in needed:
         if name not in by_name:

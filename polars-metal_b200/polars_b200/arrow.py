@@ -111,7 +111,12 @@ def groupby_arrow(table: pa.Table | pa.RecordBatch, keys: Sequence[str], aggs: S
     table (keys, then the aggregates, in no particular group order). Key columns may be strings,
     binary or dictionaries (grouped by their dictionary codes); only the columns the query reads
     are handed to libpmb."""
-    used = set(keys) | {c for _op, c, _a in aggs if c is not None} | _predicate_columns(predicate, set())
+    used = set(keys) | _predicate_columns(predicate, set())
+    for _op, c, _a in aggs:
+        if isinstance(c, dict):  # an expression aggregate reads the columns of its expression
+            _predicate_columns(c, used)
+        elif c is not None:
+            used.add(c)
     names = [n for n in table.column_names if n in used]
     missing = [n for n in used if n not in table.column_names]
     if missing:

@@ -28,6 +28,7 @@ SOURCES = [
     "pmb_learned.cu",
     "pmb_jit.cu",
     "pmb_noalloc.cu",
+    "pmb_exprcol.cu",
 ]
 
 # device sources compiled at run time by NVRTC, embedded into the library as string literals

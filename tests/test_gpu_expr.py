@@ -1,0 +1,100 @@
+"""Expression aggregates (sum(a * b), max(c - 7), mean(c / a), min(c // a)) on the GPU against the
+CPU oracle run over the same expressions computed in numpy, through groupby and through the
+reference's wire (`execute_groupby` with an "Expression" aggregate)."""
+
+import numpy as np
+import pytest
+
+from helpers import as_dict, assert_results_match, pack
+from oracle import pyoracle
+from polars_b200 import _abi as A
+from polars_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+
+def col(name):
+    return {"kind": "Column", "name": name}
+
+
+def _case(n=300_000, seed=13):
+    rng = np.random.default_rng(seed)
+    k = rng.integers(0, 2_000, n).astype(np.int64)
+    a = rng.integers(-5, 6, n).astype(np.int32)
+    av = rng.random(n) > 0.05
+    b = rng.standard_normal(n)
+    bv = rng.random(n) > 0.1
+    c = rng.integers(-10**6, 10**6, n).astype(np.int64)
+    return k, a, av, b, bv, c
+
+
+def _expected_columns(k, a, av, b, bv, c):
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ab = a.astype(np.float64) * b                    # int * float -> Float64
+        cm7 = c - 7                                      # Int64
+        cda = c.astype(np.float64) / a                   # true division -> Float64 (x / 0 = +-inf or nan)
+        safe = np.where(a == 0, 1, a).astype(np.int64)
+        cfa = np.floor_divide(c, safe)                   # floor division; // 0 is null
+    return {"k": (k, None), "ab": (ab, pack(av & bv)), "cm7": (cm7, None), "cda": (cda, pack(av)),
+            "cfa": (cfa, pack(av & (a != 0)))}
+
+
+EXPRS = {
+    "ab": {"kind": "Arith", "op": "Mul", "lhs": col("a"), "rhs": col("b")},
+    "cm7": {"kind": "Arith", "op": "Sub", "lhs": col("c"), "rhs": {"kind": "LiteralI64", "value": 7}},
+    "cda": {"kind": "Arith", "op": "TrueDiv", "lhs": col("c"), "rhs": col("a")},
+    "cfa": {"kind": "Arith", "op": "FloorDiv", "lhs": col("c"), "rhs": col("a")},
+}
+OPS = [("Sum", "ab", "s_ab"), ("Max", "cm7", "mx_c"), ("Mean", "cda", "m_cda"), ("Min", "cfa", "mn_cfa"),
+       ("Len", None, "n")]
+
+
+def test_expression_aggregates_match_the_oracle():
+    k, a, av, b, bv, c = _case()
+    cols = {"k": N.ColumnData(k), "a": N.ColumnData(a, pack(av)), "b": N.ColumnData(b, pack(bv)),
+            "c": N.ColumnData(c)}
+    aggs = [(op, EXPRS[e] if e else None, alias) for op, e, alias in OPS]
+    got = N.groupby(cols, ["k"], aggs)
+    want = pyoracle.groupby(_expected_columns(k, a, av, b, bv, c), ["k"], OPS)
+    assert_results_match(as_dict(got), want, 1, OPS, "expression aggregates")
+
+
+def test_eval_expr_column_twice_in_a_row():
+    import torch
+
+    k, a, av, b, bv, c = _case(n=70_001, seed=5)
+    cols = {"a": N.ColumnData(torch.from_numpy(a).cuda(), torch.from_numpy(pack(av)).cuda()),
+            "b": N.ColumnData(torch.from_numpy(b).cuda(), torch.from_numpy(pack(bv)).cuda())}
+    want = _expected_columns(k, a, av, b, bv, c)["ab"]
+    for _ in range(2):
+        out = N.eval_expr(cols, {"kind": "Binary", "op": "Mul", "lhs": col("a"), "rhs": col("b")})
+        assert out.dtype == A.F64 and out.data.is_cuda
+        v = np.unpackbits(out.validity.cpu().numpy(), bitorder="little")[: len(a)].astype(bool)
+        assert np.array_equal(v, av & bv)
+        assert np.array_equal(out.data.cpu().numpy()[: len(a)][v], want[0][v])
+
+
+def test_expression_aggregates_on_the_reference_wire():
+    k, a, av, b, bv, c = _case(n=50_000, seed=8)
+    ones = lambda n: b"\xff" * ((n + 7) // 8)  # noqa: E731
+    columns = [("k", "I64", k.tobytes(), ones(len(k))), ("a", "I32", a.tobytes(), pack(av).tobytes()),
+               ("b", "F64", b.tobytes(), pack(bv).tobytes()), ("c", "I64", c.tobytes(), ones(len(c)))]
+    plan = {"keys": [["k", "I64"]],
+            "aggs": [{"kind": "Expression", "op": "Sum", "output_alias": "s_ab",
+                      "expr": {"kind": "Binary", "op": "Mul", "lhs": col("a"), "rhs": col("b")}},
+                     {"kind": "Expression", "op": "Max", "output_alias": "mx_c",
+                      "expr": {"kind": "Binary", "op": "Sub", "lhs": col("c"),
+                               "rhs": {"kind": "LiteralI64", "value": 7}}},
+                     {"kind": "Length", "output_alias": "n"}]}
+    out = N.execute_groupby(plan, len(k), columns)
+    assert [o[0] for o in out] == ["k", "s_ab", "mx_c", "n"]
+    ops = [("Sum", "ab", "s_ab"), ("Max", "cm7", "mx_c"), ("Len", None, "n")]
+    want = pyoracle.groupby({kk: v for kk, v in _expected_columns(k, a, av, b, bv, c).items()
+                             if kk in ("k", "ab", "cm7")}, ["k"], ops)
+    n = len(np.frombuffer(out[0][2], np.int64))
+    dts = [A.TAG_TO_DTYPE[o[1]] for o in out]
+    assert dts[:3] == [A.I64, A.F64, A.I64]
+    got = {"n_groups": n, "names": [o[0] for o in out], "dtypes": dts,
+           "data": [np.frombuffer(o[2], A.NUMPY_NAME[dt]) for o, dt in zip(out, dts)],
+           "validity": [np.frombuffer(o[3], np.uint8) for o in out]}
+    assert_results_match(got, want, 1, ops, "wire expression aggregates")
