@@ -207,6 +207,37 @@ int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32
 int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb_column* const* cols,
                         const int32_t* n_cols, int32_t n_queries, pmb_result** outs);
 
+/* Order of rows for pmb_sort_columns and pmb_groupby_sorted: `by` lists column indices, most
+ * significant first; `descending` and `nulls_last` hold one flag per `by` column (NULL = all 0:
+ * ascending, nulls first). Polars' order: NaN above every number, -0.0 equal to 0.0, nulls placed
+ * by `nulls_last` whatever the direction. Rows with equal sort keys keep their input order.
+ * `drop_nulls` = 1 leaves out the rows whose first `by` column is null (top_k / bottom_k). Then the
+ * slice of the sorted rows is kept as Polars' `slice(offset, length)` takes it: `offset` < 0
+ * counts from the end, `limit` < 0 keeps every row from `offset` on. */
+typedef struct pmb_sort_spec {
+  const int32_t* by;
+  const int32_t* descending;
+  const int32_t* nulls_last;
+  int32_t n_by;
+  int32_t drop_nulls;
+  int64_t offset;
+  int64_t limit;
+} pmb_sort_spec;
+
+/* The rows of `cols` (all of them, at most 2^32 - 1) reordered by the spec; one output column per
+ * input column. Replaces the CPU sort of the reference's Sort plans (`df.sort(by, descending,
+ * nulls_last)` then the slice, python/polars_metal/_udf.py:684-721) and its single-column F32
+ * sort routed to MLX (_build_sort_fused, python/polars_metal/_udf.py:724-790). */
+int pmb_sort_columns(pmb_handle* h, const pmb_column* cols, int32_t n_cols, const pmb_sort_spec* spec,
+                     int32_t output_on_device, pmb_result** out);
+
+/* pmb_groupby, then the sort of its result on the device in the same call (the result does not
+ * leave the device in between): `spec->by` indexes the result's columns (keys first, then the
+ * aggregations). A Sort over a GroupBy (`_build_sort` with a GroupBy input,
+ * python/polars_metal/_udf.py:684-721). */
+int pmb_groupby_sorted(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols,
+                       const pmb_sort_spec* spec, pmb_result** out);
+
 void pmb_result_free(pmb_result* r);
 
 /* ---- learned strategy selection ----

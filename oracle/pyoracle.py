@@ -200,3 +200,71 @@ def cores() -> int:
         return len(os.sched_getaffinity(0))
     except AttributeError:  # pragma: no cover
         return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------------------------ sort
+def _order_key(vals: np.ndarray, dt: int) -> np.ndarray:
+    """Polars' order of a column's values as uint64 (polars==1.40.1, the version the reference
+    pins; its Sort plans call `df.sort(by, descending, nulls_last)`, python/polars_metal/_udf.py:
+    684-721): integers by value, False before True, floats with every NaN above +inf and -0.0 equal
+    to 0.0."""
+    if dt == A.BOOL:
+        return vals.astype(np.uint64)
+    if vals.dtype.kind == "i":
+        return vals.astype(np.int64).view(np.uint64) ^ np.uint64(1 << 63)
+    if vals.dtype.kind == "u":
+        return vals.astype(np.uint64)
+    x = vals.astype(np.float64)  # exact for Float32, and the order is kept
+    x = np.where(np.isnan(x), np.float64("nan"), x)
+    x = np.where(x == 0, 0.0, x)
+    b = x.view(np.uint64)
+    neg = (b >> np.uint64(63)).astype(bool)
+    return np.where(neg, ~b, b | np.uint64(1 << 63))
+
+
+def sort_table(columns: dict, by, descending=None, nulls_last=None, drop_nulls: bool = False, offset: int = 0,
+               limit: int = -1) -> dict:
+    """Oracle sort: the rows of `columns` (name -> (data, validity | None[, dtype, length]), Bool
+    data bit-packed) ordered by the `by` columns, most significant first, stably; nulls first
+    unless nulls_last, whatever the direction; with drop_nulls the rows whose first `by` column is
+    null are left out (top_k / bottom_k); then Polars' slice(offset, limit). Returns the groupby
+    result shape, rows in order."""
+    names = list(columns)
+    cols = []
+    for name in names:
+        ent = columns[name]
+        data, valid = ent[0], ent[1]
+        dt = ent[2] if len(ent) > 2 else {v: k for k, v in A.NUMPY_NAME.items()}[np.asarray(data).dtype.name]
+        n = ent[3] if len(ent) > 3 else np.asarray(data).size
+        vals = (np.unpackbits(np.asarray(data, np.uint8), bitorder="little")[:n].astype(bool) if dt == A.BOOL
+                else np.asarray(data)[:n])
+        ok = (np.unpackbits(np.asarray(valid, np.uint8), bitorder="little")[:n].astype(bool) if valid is not None
+              else np.ones(n, bool))
+        cols.append((dt, vals, ok))
+    n = len(cols[0][1]) if cols else 0
+    desc = list(descending) if descending is not None else [False] * len(by)
+    nlast = list(nulls_last) if nulls_last is not None else [False] * len(by)
+    rows = np.arange(n)
+    if drop_nulls:
+        rows = rows[cols[names.index(by[0])][2]]
+    keys = []
+    for j in reversed(range(len(by))):  # np.lexsort: the last key is the primary one
+        dt, vals, ok = cols[names.index(by[j])]
+        o = _order_key(vals[rows], dt)
+        if desc[j]:
+            o = ~o
+        keys.append(np.where(ok[rows], o, np.uint64(0)))
+        keys.append(~ok[rows] if nlast[j] else ok[rows])
+    order = rows[np.lexsort(keys)] if len(rows) else rows
+    total = len(order)
+    start = min(offset, total) if offset >= 0 else max(0, total + offset)
+    stop = total if limit < 0 else min(total, start + limit)
+    order = order[start:stop]
+    m = len(order)
+    out_data, out_valid, dts = [], [], []
+    for dt, vals, ok in cols:
+        v = vals[order]
+        out_data.append(np.packbits(v, bitorder="little") if dt == A.BOOL else v)
+        out_valid.append(np.packbits(ok[order], bitorder="little") if m else np.zeros(1, np.uint8))
+        dts.append(dt)
+    return {"n_groups": m, "names": names, "dtypes": dts, "data": out_data, "validity": out_valid}

@@ -90,6 +90,14 @@ void k_table_init_pub(unsigned long long* keys, int64_t key_words, uint64_t* rec
 // sort strategy (pmb_sort.cu): packed-key LSD radix sort + segmented reduce
 // the sort strategy (part_groups == 0), or the partitioned strategy sized for part_groups groups
 int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r, int64_t part_groups);
+// stable LSD sort of (W-word key, u32 row index) pairs over 8-bit digits 0 .. n_passes-1, the
+// group-by sort's pass kernel (pmb_sort.cu); *k / *i end up pointing at the sorted buffers
+int pmb_sort_pairs(pmb_handle* h, int W, unsigned long long** k, unsigned long long** k_alt, unsigned int** i,
+                   unsigned int** i_alt, uint64_t cap, int64_t n, int n_passes, const unsigned int* hist_dev,
+                   const unsigned int* hist_host);
+// output sort (pmb_order.cu): the n rows of the device columns in the order of the spec, the first
+// `limit` of them, as device columns of r (r->n_groups set); the workspace is not reset
+int pmb_order_columns(pmb_handle* h, const DCol* cols, int n_cols, int64_t n, const pmb_sort_spec& s, pmb_result* r);
 // learned selector (pmb_learned.cu): strategy and group count for AUTO; false when no selector is
 // installed or its output is unusable
 bool pmb_selector_pick(pmb_handle* h, const CompiledQuery& cq, int* strategy, int64_t* groups);

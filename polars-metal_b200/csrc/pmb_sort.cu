@@ -1417,3 +1417,58 @@ int pmb_groupby_sort(pmb_handle* h, CompiledQuery& cq, pmb_result* r, int64_t pa
   if (off > 128) return pmb_fail(h, PMB_E_UNSUPPORTED, "sort strategy: packed key above 128 bits");
   return L.words == 1 ? run_sort<1>(h, cq, L, r, part_groups) : run_sort<2>(h, cq, L, r, part_groups);
 }
+
+// Stable LSD sort of (key, row index) pairs for callers outside the group-by (the output sort):
+// the same onesweep pass kernel, over the 8-bit digits 0 .. n_passes-1 of W-word keys (word-major,
+// stride cap). hist_host holds every pass's digit counts of all n keys (also at hist_dev); a digit
+// that one value fills is skipped. On return *k and *i are the sorted buffers (the inputs or the
+// alternates).
+int pmb_sort_pairs(pmb_handle* h, int W, unsigned long long** k, unsigned long long** k_alt, unsigned int** i,
+                   unsigned int** i_alt, uint64_t cap, int64_t n, int n_passes, const unsigned int* hist_dev,
+                   const unsigned int* hist_host) {
+  if (W != 1 && W != 2) return pmb_fail(h, PMB_E_INVALID, "sort: key of 1 or 2 words");
+  if (n_passes > MAX_PASSES) return pmb_fail(h, PMB_E_INVALID, "sort: more than 16 digit passes");
+  if (n <= 1 || n_passes <= 0) return PMB_OK;
+  const int64_t tiles = (n + ST_TILE - 1) / ST_TILE;
+  unsigned long long* lb = (unsigned long long*)pmb_ws_alloc(h, (size_t)tiles * RADIX * 8);
+  unsigned long long* ticket = (unsigned long long*)pmb_ws_alloc(h, 64);
+  unsigned int* status = (unsigned int*)pmb_ws_alloc(h, 64);
+  if (!lb || !ticket || !status) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sort passes)");
+  PMB_CUDA(h, cudaMemsetAsync(status, 0, 64, h->stream));
+  const size_t pass_smem = (size_t)ST_TILE * (8 * W + 4);
+  if (W == 1) PMB_CUDA(h, cudaFuncSetAttribute(k_sort_pass<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem));
+  else PMB_CUDA(h, cudaFuncSetAttribute(k_sort_pass<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem));
+  for (int p = 0; p < n_passes; p++) {
+    bool constant = false;
+    for (int d = 0; d < RADIX; d++) constant |= hist_host[(size_t)p * RADIX + d] == (unsigned)n;
+    if (constant) continue;
+    PassParams P;
+    P.kin = *k;
+    P.kout = *k_alt;
+    P.iin = *i;
+    P.iout = *i_alt;
+    P.cap = cap;
+    P.n = n;
+    P.shift = 8 * p;
+    P.hashed = 0;
+    P.hist = hist_dev + (size_t)p * RADIX;
+    P.lb = lb;
+    P.n_tiles = tiles;
+    P.ticket = ticket;
+    P.status = status;
+    PMB_CUDA(h, cudaMemsetAsync(lb, 0, (size_t)tiles * RADIX * 8, h->stream));
+    PMB_CUDA(h, cudaMemsetAsync(ticket, 0, 8, h->stream));
+    pmb_kernel_begin(h, "sort_pass");
+    if (W == 1) k_sort_pass<1><<<(unsigned)tiles, ST_NT, pass_smem, h->stream>>>(P);
+    else k_sort_pass<2><<<(unsigned)tiles, ST_NT, pass_smem, h->stream>>>(P);
+    pmb_kernel_end(h);
+    PMB_CUDA(h, cudaGetLastError());
+    std::swap(*k, *k_alt);
+    std::swap(*i, *i_alt);
+  }
+  unsigned int st = 0;
+  PMB_CUDA(h, cudaMemcpyAsync(&st, status, 4, cudaMemcpyDeviceToHost, h->stream));
+  PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (st & PMB_ST_TIMEOUT) return pmb_fail(h, PMB_E_TIMEOUT, "a bounded device wait timed out (sort)");
+  return PMB_OK;
+}

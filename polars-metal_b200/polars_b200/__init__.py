@@ -18,7 +18,9 @@ from ._native import (  # noqa: F401
     default_handle,
     execute_filter_compact,
     execute_groupby,
+    execute_sort,
     groupby,
+    sort_columns,
 )
 
 __version__ = "0.1.0"

@@ -133,6 +133,18 @@ class Result(C.Structure):
     ]
 
 
+class SortSpec(C.Structure):
+    _fields_ = [
+        ("by", C.POINTER(C.c_int32)),
+        ("descending", C.POINTER(C.c_int32)),
+        ("nulls_last", C.POINTER(C.c_int32)),
+        ("n_by", C.c_int32),
+        ("drop_nulls", C.c_int32),
+        ("offset", C.c_int64),
+        ("limit", C.c_int64),
+    ]
+
+
 MAX_STAT_KERNELS = 16
 
 
@@ -167,6 +179,10 @@ SIGNATURES = {
          C.POINTER(C.POINTER(Result))],
     ),
     "pmb_result_free": (None, [C.POINTER(Result)]),
+    "pmb_sort_columns": (C.c_int, [_H, C.POINTER(Column), C.c_int32, C.POINTER(SortSpec), C.c_int32,
+                                   C.POINTER(C.POINTER(Result))]),
+    "pmb_groupby_sorted": (C.c_int, [_H, C.POINTER(Query), C.POINTER(Column), C.c_int32, C.POINTER(SortSpec),
+                                     C.POINTER(C.POINTER(Result))]),
     "pmb_eval_expr": (C.c_int, [_H, C.POINTER(Expr), C.POINTER(Column), C.c_int32, _P, _P, C.c_int32,
                                 C.POINTER(C.c_int32)]),
     "pmb_compare": (C.c_int, [_H, C.POINTER(Column), C.POINTER(Column), C.c_int64, C.c_double, C.c_int32, _P, _P,

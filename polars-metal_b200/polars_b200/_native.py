@@ -369,13 +369,16 @@ def groupby(
     output: str = "host",
     capacity_hint: int = 0,
     handle: Handle | None = None,
+    sort: dict | None = None,
 ) -> GroupByResult:
     """filter -> group_by -> aggregate through libpmb.
 
     columns: name -> ColumnData (or a bare array with no nulls); aggs: (op, input column, alias)
     with op in Sum/Mean/Count/Min/Max/Len (input None for Len), the input may also be an
     arithmetic expression dict (an expression aggregate, evaluated by eval_expr); predicate: a
-    predicate dict.
+    predicate dict; sort: the result sorted on the device in the same call (pmb_groupby_sorted),
+    {"by": output column name(s), "descending", "nulls_last" (a flag or one per column),
+    "drop_nulls", "offset", "limit"} as sort_columns takes them.
     """
     if any(isinstance(a[1], dict) for a in aggs):
         # expression aggregates: every expression is evaluated into a column of its own first
@@ -423,10 +426,15 @@ def groupby(
     h = handle or default_handle()
     abi_cols, keep = _to_abi_columns(cols)
     res_p = C.POINTER(A.Result)()
-    h.check(h._lib.pmb_groupby(h.raw, C.byref(q), abi_cols, len(cols), C.byref(res_p)))
+    out_names = list(keys) + [a[2] for a in aggs]
+    if sort is not None:
+        spec, spec_keep = _sort_spec(out_names, **sort)
+        h.check(h._lib.pmb_groupby_sorted(h.raw, C.byref(q), abi_cols, len(cols), C.byref(spec), C.byref(res_p)))
+        del spec_keep
+    else:
+        h.check(h._lib.pmb_groupby(h.raw, C.byref(q), abi_cols, len(cols), C.byref(res_p)))
     try:
         res = res_p.contents
-        out_names = list(keys) + [a[2] for a in aggs]
         data, valid, dts = _read_result(res, out_names, output != "device")
         return GroupByResult(
             n_groups=res.n_groups,
@@ -695,7 +703,31 @@ def _wire_column(tag: str, data: bytes, valid: bytes, n_rows: int, name: str) ->
     return ColumnData(arr, v, dtype=dt, length=n_rows)
 
 
-def execute_groupby(plan_dict: dict, n_rows: int, columns: list) -> list[tuple[str, str, bytes, bytes]]:
+def execute_sort(plan: dict, n_rows: int, columns: list, slice_len: int | None = None) -> list[tuple[str, str, bytes, bytes]]:
+    """A Sort plan over a GroupBy (`_build_sort`, python/polars_metal/_udf.py:684-721), run on the
+    device in one call: the group-by of plan["input"] (execute_groupby's plan_dict), then its
+    result sorted by plan["by_columns"] with plan["descending"] / plan["nulls_last"] (one flag or
+    one per column), an optional plan["slice"] = [offset, length], then the first `slice_len` rows
+    (the UDF's n_rows). Same wire shapes as execute_groupby."""
+    if not isinstance(plan, dict) or "input" not in plan:
+        raise ValueError("polars_b200: plan parse error: missing field input")
+    by = list(plan.get("by_columns", []))
+    offset, length = 0, None
+    if plan.get("slice") is not None:
+        offset, length = int(plan["slice"][0]), plan["slice"][1]
+        length = None if length is None else int(length)
+    if slice_len is not None:
+        length = slice_len if length is None else min(length, slice_len)
+    sort = None
+    if by:
+        sort = {"by": by, "descending": plan.get("descending", False), "nulls_last": plan.get("nulls_last", False),
+                "offset": offset, "limit": length}
+    elif offset or length is not None:
+        raise ValueError("polars_b200: a slice without sort columns is not a Sort over a GroupBy")
+    return execute_groupby(plan["input"], n_rows, columns, _sort=sort)
+
+
+def execute_groupby(plan_dict: dict, n_rows: int, columns: list, _sort: dict | None = None) -> list[tuple[str, str, bytes, bytes]]:
     """Wire-compatible `_native.execute_groupby` (crates/polars-metal-core/src/udf/groupby/mod.rs:720-746).
 
     plan_dict: {"keys": [[name, tag], ...], "aggs": [{"input_col", "op", "output_alias", "kind"?}],
@@ -756,7 +788,7 @@ def execute_groupby(plan_dict: dict, n_rows: int, columns: list) -> list[tuple[s
             raise KeyError(f"polars_b200: column {name!r} not found in upstream columns")
         tag, data, valid = by_name[name]
         cols[name] = _wire_column(tag, data, valid, n_rows, name)
-    res = groupby(cols, keys, aggs, plan_dict.get("predicate"), strategy=plan_dict.get("strategy", "auto"))
+    res = groupby(cols, keys, aggs, plan_dict.get("predicate"), strategy=plan_dict.get("strategy", "auto"), sort=_sort)
     out = []
     n = res.n_groups
     for i, name in enumerate(res.names):
@@ -878,6 +910,76 @@ def filter_columns(columns: dict, predicate: dict, output: str = "host", handle:
     finally:
         h._lib.pmb_result_free(res_p)
         del keep, ek
+
+
+def _sort_spec(names: Sequence[str], by, descending=False, nulls_last=False, drop_nulls: bool = False,
+               offset: int = 0, limit: int | None = None):
+    """A pmb_sort_spec over the named columns; a single descending / nulls_last flag applies to
+    every sort column, as in Polars' `sort`."""
+    by = [by] if isinstance(by, str) else list(by)
+    if not by:
+        raise ValueError("polars_b200: sort needs at least one column")
+    index = {n: i for i, n in enumerate(names)}
+    for b in by:
+        if b not in index:
+            raise KeyError(f"polars_b200: sort column {b!r} not found")
+
+    def flags(v, what):
+        v = [bool(v)] * len(by) if isinstance(v, (bool, int, np.bool_)) else [bool(x) for x in v]
+        if len(v) != len(by):
+            raise ValueError(f"polars_b200: {what} has {len(v)} flags for {len(by)} sort columns")
+        return (C.c_int32 * len(by))(*v)
+
+    spec = A.SortSpec()
+    b = (C.c_int32 * len(by))(*[index[x] for x in by])
+    d = flags(descending, "descending")
+    nl = flags(nulls_last, "nulls_last")
+    spec.by, spec.descending, spec.nulls_last = b, d, nl
+    spec.n_by = len(by)
+    spec.drop_nulls = 1 if drop_nulls else 0
+    spec.offset = int(offset)
+    spec.limit = -1 if limit is None else int(limit)
+    if limit is not None and limit < 0:
+        raise ValueError("polars_b200: a negative slice length")
+    return spec, (b, d, nl)
+
+
+def sort_columns(columns: dict, by, descending=False, nulls_last=False, drop_nulls: bool = False, offset: int = 0,
+                 limit: int | None = None, output: str = "host", handle: Handle | None = None) -> GroupByResult:
+    """The rows of `columns` sorted by the `by` column(s) on the GPU (pmb_sort_columns), then the
+    slice(offset, limit). Polars' order: nulls first unless nulls_last, whatever the direction;
+    NaN above every number; -0.0 equal to 0.0; rows with equal keys keep their order. The reference
+    sorts with Polars on the CPU (python/polars_metal/_udf.py:684-721) and routes only one
+    null-free Float32 column to MLX (_udf.py:724-790)."""
+    h = handle or default_handle()
+    names = list(columns)
+    cols = [c if isinstance(c, ColumnData) else ColumnData(c) for c in columns.values()]
+    spec, sk = _sort_spec(names, by, descending, nulls_last, drop_nulls, offset, limit)
+    abi, keep = _to_abi_columns(cols)
+    res_p = C.POINTER(A.Result)()
+    h.check(h._lib.pmb_sort_columns(h.raw, abi, len(cols), C.byref(spec), 1 if output == "device" else 0,
+                                    C.byref(res_p)))
+    try:
+        res = res_p.contents
+        data, valid, dts = _read_result(res, names, output != "device")
+        return GroupByResult(n_groups=res.n_groups, names=names, dtypes=dts, data=data, validity=valid,
+                             strategy="sort", rehash_count=0, capacity=0)
+    finally:
+        h._lib.pmb_result_free(res_p)
+        del keep, sk
+
+
+def top_k(columns: dict, k: int, by, output: str = "host", handle: Handle | None = None) -> GroupByResult:
+    """The k rows with the largest `by` values, largest first; rows whose first `by` column is
+    null are left out (Polars lowers top_k to a sort, descending, after dropping nulls)."""
+    return sort_columns(columns, by, descending=True, nulls_last=True, drop_nulls=True, limit=k, output=output,
+                        handle=handle)
+
+
+def bottom_k(columns: dict, k: int, by, output: str = "host", handle: Handle | None = None) -> GroupByResult:
+    """The k rows with the smallest `by` values, smallest first; nulls left out as in top_k."""
+    return sort_columns(columns, by, descending=False, nulls_last=True, drop_nulls=True, limit=k, output=output,
+                        handle=handle)
 
 
 def execute_filter_compact(pred_data: bytes, pred_valid: bytes, n_rows: int, columns: list) -> list:

@@ -18,7 +18,7 @@ import pyarrow as pa
 import pyarrow.compute as pc
 
 from . import _abi as A
-from ._native import ColumnData, GroupByResult, Handle, filter_columns, groupby
+from ._native import ColumnData, GroupByResult, Handle, filter_columns, groupby, sort_columns
 
 _TO_PMB = {
     pa.bool_(): A.BOOL,
@@ -80,7 +80,8 @@ def _dictionary_key(col) -> tuple[pa.Array, pa.Array] | None:
     """(int32 codes with the column's nulls, the distinct values) of a string, binary or
     dictionary column; None for other types. Strings are encoded on the host (the reference
     encodes them on the host too, crates/polars-metal-buffer/src/dict.rs:18-74); the group-by then
-    runs on the codes, and the output codes are decoded through the values."""
+    runs on the codes, and the output codes are decoded through the values. The values are in
+    sorted (byte-wise) order, so that the codes sort as the strings do."""
     if isinstance(col, pa.ChunkedArray):
         if pa.types.is_dictionary(col.type):
             col = col.unify_dictionaries()
@@ -93,7 +94,10 @@ def _dictionary_key(col) -> tuple[pa.Array, pa.Array] | None:
         codes, values = enc.indices, enc.dictionary
     else:
         return None
-    return (codes if codes.type == pa.int32() else codes.cast(pa.int32())), values
+    order = pc.sort_indices(values)
+    rank = np.empty(len(values), np.int32)
+    rank[order.to_numpy()] = np.arange(len(values), dtype=np.int32)
+    return pc.take(pa.array(rank, pa.int32()), codes), values.take(order)
 
 
 def _predicate_columns(p, out: set) -> set:
@@ -106,11 +110,13 @@ def _predicate_columns(p, out: set) -> set:
 
 
 def groupby_arrow(table: pa.Table | pa.RecordBatch, keys: Sequence[str], aggs: Sequence[tuple[str, str | None, str]],
-                  predicate: dict | None = None, strategy: str = "auto", handle: Handle | None = None) -> pa.Table:
+                  predicate: dict | None = None, strategy: str = "auto", handle: Handle | None = None,
+                  sort: dict | None = None) -> pa.Table:
     """filter -> group_by -> aggregate of an Arrow table through libpmb; the result as an Arrow
-    table (keys, then the aggregates, in no particular group order). Key columns may be strings,
-    binary or dictionaries (grouped by their dictionary codes); only the columns the query reads
-    are handed to libpmb."""
+    table (keys, then the aggregates, in no particular group order unless `sort` orders it on the
+    device, as groupby takes it). Key columns may be strings, binary or dictionaries (grouped by
+    their dictionary codes, which sort as the strings do); only the columns the query reads are
+    handed to libpmb."""
     used = set(keys) | _predicate_columns(predicate, set())
     for _op, c, _a in aggs:
         if isinstance(c, dict):  # an expression aggregate reads the columns of its expression
@@ -129,12 +135,32 @@ def groupby_arrow(table: pa.Table | pa.RecordBatch, keys: Sequence[str], aggs: S
             dicts[name] = enc[1]
         else:
             cols[name] = column_from_arrow(table.column(name))
-    res = groupby(cols, keys, aggs, predicate, strategy=strategy, output="host", handle=handle)
-    out = table_from_result(res)
+    res = groupby(cols, keys, aggs, predicate, strategy=strategy, output="host", handle=handle, sort=sort)
+    return _decoded(table_from_result(res), dicts)
+
+
+def _decoded(out: pa.Table, dicts: dict) -> pa.Table:
     for name, values in dicts.items():
         i = out.column_names.index(name)
         out = out.set_column(i, name, values.take(out.column(i)))
     return out
+
+
+def sort_arrow(table: pa.Table | pa.RecordBatch, by, descending=False, nulls_last=False, offset: int = 0,
+               limit: int | None = None, handle: Handle | None = None) -> pa.Table:
+    """The rows of an Arrow table sorted by `by` on the GPU (sort_columns), then slice(offset,
+    limit); string, binary and dictionary columns travel as their sorted-dictionary codes."""
+    cols, dicts = {}, {}
+    for name in table.column_names:
+        enc = _dictionary_key(table.column(name))
+        if enc is not None:
+            cols[name] = column_from_arrow(enc[0])
+            dicts[name] = enc[1]
+        else:
+            cols[name] = column_from_arrow(table.column(name))
+    res = sort_columns(cols, by, descending=descending, nulls_last=nulls_last, offset=offset, limit=limit,
+                       output="host", handle=handle)
+    return _decoded(table_from_result(res), dicts)
 
 
 def filter_arrow(table: pa.Table | pa.RecordBatch, predicate: dict, handle: Handle | None = None) -> pa.Table:

@@ -29,6 +29,7 @@ SOURCES = [
     "pmb_jit.cu",
     "pmb_noalloc.cu",
     "pmb_exprcol.cu",
+    "pmb_order.cu",
 ]
 
 # device sources compiled at run time by NVRTC, embedded into the library as string literals

@@ -368,9 +368,51 @@ def kleene_cases() -> list[dict]:
              "and": exp_and, "or": exp_or}]
 
 
+def sort_cases() -> list[dict]:
+    """tests/python_integration/test_walker_sort_fused.py: Sort / top_k / bottom_k, engine vs Polars
+    CPU. `spec` is the sort (by, descending, nulls_last, drop_nulls, offset, limit as Polars lowers
+    top_k: descending + drop nulls + slice(0, k)). Closed-form inputs carry their values; the
+    seeded float inputs (`_floats(n, seed)`: standard normal, Float32) carry a `formula`, and
+    their expected values are computed from it with np.sort when the test runs."""
+    def spec(by, desc=None, nl=None, drop=False, limit=-1):
+        return {"by": by, "descending": desc or [False] * len(by), "nulls_last": nl or [False] * len(by),
+                "drop_nulls": drop, "offset": 0, "limit": limit}
+
+    x = [3.0, None, 1.0, 5.0, None, 2.0, 4.0]
+    xv = [1, 0, 1, 1, 0, 1, 1]
+    return [
+        {"name": "sort_f32_ascending", "source": "tests/python_integration/test_walker_sort_fused.py:46-50",
+         "columns": {"x": {"dtype": "F32", "values": [3.0, 1.0, 2.0, 2.0, 5.0, -1.0]}}, "spec": spec(["x"]),
+         "expected": {"x": [-1.0, 1.0, 2.0, 2.0, 3.0, 5.0]}},
+        {"name": "top_k_with_nulls", "source": "tests/python_integration/test_walker_sort_fused.py:77-83",
+         "columns": {"x": {"dtype": "F32", "values": [v if v is not None else 0.0 for v in x], "valid": xv}},
+         "spec": spec(["x"], [True], [True], drop=True, limit=3), "expected": {"x": [5.0, 4.0, 3.0]}},
+        {"name": "bottom_k_with_nulls", "source": "tests/python_integration/test_walker_sort_fused.py:86-90",
+         "columns": {"x": {"dtype": "F32", "values": [v if v is not None else 0.0 for v in x], "valid": xv}},
+         "spec": spec(["x"], [False], [True], drop=True, limit=3), "expected": {"x": [1.0, 2.0, 3.0]}},
+        {"name": "sort_nulls_first", "source": "tests/python_integration/test_walker_sort_fused.py:93-99",
+         "columns": {"x": {"dtype": "F32", "values": [3.0, 0.0, 1.0, 0.0, 2.0], "valid": [1, 0, 1, 0, 1]}},
+         "spec": spec(["x"]), "expected": {"x": [None, None, 1.0, 2.0, 3.0]}},
+        {"name": "sort_carries_other_columns", "source": "tests/python_integration/test_walker_sort_fused.py:102-113",
+         "columns": {"x": {"dtype": "F32", "values": [3.0, 1.0, 2.0]}, "y": {"dtype": "I64", "values": [10, 20, 30]}},
+         "spec": spec(["x"]), "expected": {"x": [1.0, 2.0, 3.0], "y": [20, 30, 10]}},
+        {"name": "sort_i64", "source": "tests/python_integration/test_walker_sort_fused.py:116-122",
+         "columns": {"x": {"dtype": "I64", "values": [3, 1, 2, 5, 4]}}, "spec": spec(["x"]),
+         "expected": {"x": [1, 2, 3, 4, 5]}},
+        {"name": "sort_floats_ascending", "source": "tests/python_integration/test_walker_sort_fused.py:38-43",
+         "formula": {"n": 10_000, "seed": 0x501}, "spec": spec(["x"])},
+        {"name": "sort_floats_descending", "source": "tests/python_integration/test_walker_sort_fused.py:53-57",
+         "formula": {"n": 5_000, "seed": 0x501}, "spec": spec(["x"], [True])},
+        {"name": "top_k_100", "source": "tests/python_integration/test_walker_sort_fused.py:60-67",
+         "formula": {"n": 10_000, "seed": 0x501}, "spec": spec(["x"], [True], [True], drop=True, limit=100)},
+        {"name": "bottom_k_100", "source": "tests/python_integration/test_walker_sort_fused.py:70-74",
+         "formula": {"n": 10_000, "seed": 0x501}, "spec": spec(["x"], [False], [True], drop=True, limit=100)},
+    ]
+
+
 def main():
     doc = {"groupby": groupby_cases(), "integration": integration_cases(), "compare": compare_cases(),
-           "kleene": kleene_cases()}
+           "kleene": kleene_cases(), "sort": sort_cases()}
     # the all-unique case is large; keep only its shape and check it by property
     for c in doc["integration"]:
         if c["formula"] == "all_unique":
