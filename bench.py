@@ -433,6 +433,22 @@ def main():
                                              handle=h), stream, 3, 1)
         sort_strategy = {"strategy": "sort", "ms_per_step": ms_sort, "rows_per_s": n / (ms_sort / 1e3)}
 
+    # ... and the group-by with its result sorted by the keys on the device in the same call (a Sort
+    # over a GroupBy), with the kernels of one profiled call
+    sorted_output = None
+    if args.workload == "sort":
+        def sorted_call():
+            return groupby(cols, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="device", handle=h,
+                           sort={"by": list(t.keys)})
+        ms_sorted = time_calls(sorted_call, stream, 3, 1)
+        h.set_profiling(True)
+        sorted_call()
+        st = h.last_stats()
+        h.set_profiling(False)
+        sorted_output = {"by": list(t.keys), "ms_per_step": ms_sorted, "ms_group_by_alone": ms_max,
+                         "rows_per_s": n / (ms_sorted / 1e3),
+                         "kernels_ms": {k: rec["ms"] for k, rec in st["kernels"].items()}}
+
     batched = None
     if not args.no_batched and args.workload == "hash":
         tables_b, qs_b = batch_queries(device, seed=4 + rank)
@@ -474,6 +490,7 @@ def main():
             "clocks": clocks,
             "batched": batched,
             "sort_strategy": sort_strategy,
+            "sorted_output": sorted_output,
         }
         print(json.dumps(line), flush=True)
     h.close()

@@ -15,8 +15,11 @@
 //                       the previous round's order, so the rounds compose;
 //   3. k_order_encode — keys of the rows in the current order, with the digit histograms;
 //   4. pmb_sort_pairs — the group-by sort's LSD onesweep passes over the digits that vary;
-//   5. k_order_gather — the slice of the sorted rows gathered from every column, a warp per 32
-//                       output rows so that each validity word is one ballot.
+//   5. k_order_gather — the slice of the sorted rows, a warp per 32 output rows so that each
+//                       validity word is one ballot. Integer and Bool sort columns are decoded from
+//                       the sorted keys when one round holds them all; the other columns are
+//                       gathered by row index, without reading the validity of a column that
+//                       k_null_flags found to have no nulls.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -173,41 +176,144 @@ __global__ void __launch_bounds__(OR_NT) k_order_encode(const __grid_constant__ 
   }
 }
 
+struct NullFlagCols {
+  int n;
+  const uint8_t* valid[PMB_MAX_OUT];  // null: no bitmap
+};
+
+// flags[c] = 1 when the bitmap of column c has a null among rows [0, n)
+__global__ void __launch_bounds__(OR_NT) k_null_flags(const __grid_constant__ NullFlagCols V, int64_t n,
+                                                      unsigned int* flags) {
+  const int64_t full = n >> 3;
+  const int rest = (int)(n & 7);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int c = 0; c < V.n; c++) {
+    const uint8_t* v = V.valid[c];
+    if (!v) continue;
+    bool hole = false;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= full; i += stride) {
+      if (i < full) hole |= v[i] != 0xFF;
+      else if (rest) hole |= (v[i] & ((1u << rest) - 1u)) != ((1u << rest) - 1u);
+    }
+    if (__any_sync(0xffffffffu, hole) && (threadIdx.x & 31) == 0) atomicOr(&flags[c], 1u);
+  }
+}
+
 struct GatherCols {
   int n;
   const uint8_t* data[PMB_MAX_OUT];
-  const uint8_t* valid[PMB_MAX_OUT];
+  const uint8_t* valid[PMB_MAX_OUT];  // null: every row valid
   int elem[PMB_MAX_OUT];
+  int dec[PMB_MAX_OUT];               // >= 0: decoded from the sorted keys, column dec of L
   uint8_t* out_data[PMB_MAX_OUT];
   unsigned int* out_valid[PMB_MAX_OUT];
+  const unsigned long long* keys;     // the sorted keys (word-major, stride cap), with dec >= 0
+  uint64_t cap;
+  int W;
 };
 
-// rows idx[start + p] (start + p without an order) for p < m, a warp per 32 output rows
-__global__ void __launch_bounds__(OR_NT) k_order_gather(const __grid_constant__ GatherCols G, const unsigned int* idx,
+template <int W>
+__device__ __forceinline__ unsigned long long get_bits(const unsigned long long* keys, uint64_t cap, uint64_t pos,
+                                                       int off, int bits) {
+  if (bits == 0) return 0;
+  const int wi = off >> 6, sh = off & 63;
+  unsigned long long v = keys[(uint64_t)wi * cap + pos] >> sh;
+  if (W > 1 && sh + bits > 64 && wi + 1 < W) v |= keys[(uint64_t)(wi + 1) * cap + pos] << (64 - sh);
+  return bits == 64 ? v : (v & ((1ULL << bits) - 1ULL));
+}
+
+// the raw bits of an integer or Bool value from its order key
+__device__ __forceinline__ uint64_t from_order_key(unsigned long long o, int dt) {
+  switch (dt) {
+    case PMB_I8: case PMB_I16: case PMB_I32: case PMB_I64: return o ^ 0x8000000000000000ULL;
+    default: return o;
+  }
+}
+
+constexpr int GU = 4;  // output words a warp fills per iteration: GU independent loads in flight per column
+
+// rows idx[start + p] (start + p without an order) for p < m; a warp fills GU validity words (32
+// rows each) per iteration, loading the rows of all GU words before it writes any
+template <int W>
+__global__ void __launch_bounds__(OR_NT) k_order_gather(const __grid_constant__ GatherCols G,
+                                                        const __grid_constant__ OrderLayout L, const unsigned int* idx,
                                                         int64_t start, int64_t m) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
-  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; w * 32 < m; w += warps) {
-    const int64_t p = w * 32 + lane;
-    const bool ok = p < m;
-    const int64_t r = ok ? (idx ? (int64_t)idx[start + p] : start + p) : 0;
+  for (int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32 * GU; w0 * 32 < m; w0 += warps * GU) {
+    int64_t p[GU], r[GU];
+    bool ok[GU];
+#pragma unroll
+    for (int u = 0; u < GU; u++) {
+      p[u] = (w0 + u) * 32 + lane;
+      ok[u] = p[u] < m;
+      r[u] = ok[u] ? (idx ? (int64_t)idx[start + p[u]] : start + p[u]) : 0;
+    }
     for (int c = 0; c < G.n; c++) {
       const int e = G.elem[c];
-      const uint64_t b = ok ? pmb_load_bits(G.data[c], e, r) : 0;
-      if (ok) {
-        switch (e) {
-          case 0: break;
-          case 1: G.out_data[c][p] = (uint8_t)b; break;
-          case 2: reinterpret_cast<uint16_t*>(G.out_data[c])[p] = (uint16_t)b; break;
-          case 4: reinterpret_cast<uint32_t*>(G.out_data[c])[p] = (uint32_t)b; break;
-          default: reinterpret_cast<uint64_t*>(G.out_data[c])[p] = b; break;
+      const int k = G.dec[c];
+      uint64_t b[GU];
+      bool v[GU];
+      if (k >= 0) {
+        // decoded: the null flag and the value field of the sorted key at position start + p
+#pragma unroll
+        for (int u = 0; u < GU; u++) {
+          v[u] = ok[u];
+          b[u] = 0;
+          if (!ok[u]) continue;
+          const uint64_t pos = (uint64_t)(start + p[u]);
+          if (L.null_off[k] >= 0) {
+            const bool flag = get_bits<W>(G.keys, G.cap, pos, L.null_off[k], 1) != 0;
+            v[u] = L.nulls_last[k] ? !flag : flag;
+          }
+          const unsigned long long f = get_bits<W>(G.keys, G.cap, pos, L.data_off[k], L.data_bits[k]);
+          b[u] = v[u] ? from_order_key(L.desc[k] ? L.hi[k] - f : L.lo[k] + f, L.dtype[k]) : 0;
         }
+      } else {
+        const uint8_t* d = G.data[c];
+        switch (e) {
+          case 0:
+#pragma unroll
+            for (int u = 0; u < GU; u++) b[u] = ok[u] ? (uint64_t)((d[r[u] >> 3] >> (r[u] & 7)) & 1u) : 0;
+            break;
+          case 1:
+#pragma unroll
+            for (int u = 0; u < GU; u++) b[u] = ok[u] ? (uint64_t)d[r[u]] : 0;
+            break;
+          case 2:
+#pragma unroll
+            for (int u = 0; u < GU; u++) b[u] = ok[u] ? (uint64_t)reinterpret_cast<const uint16_t*>(d)[r[u]] : 0;
+            break;
+          case 4:
+#pragma unroll
+            for (int u = 0; u < GU; u++) b[u] = ok[u] ? (uint64_t)reinterpret_cast<const uint32_t*>(d)[r[u]] : 0;
+            break;
+          default:
+#pragma unroll
+            for (int u = 0; u < GU; u++) b[u] = ok[u] ? reinterpret_cast<const uint64_t*>(d)[r[u]] : 0;
+            break;
+        }
+        const uint8_t* vb = G.valid[c];
+#pragma unroll
+        for (int u = 0; u < GU; u++) v[u] = ok[u] && (vb == nullptr || ((vb[r[u] >> 3] >> (r[u] & 7)) & 1u));
       }
-      const unsigned vb = __ballot_sync(0xffffffffu, ok && pmb_valid_bit(G.valid[c], r));
-      const unsigned db = __ballot_sync(0xffffffffu, ok && e == 0 && b);
-      if (lane == 0) {
-        G.out_valid[c][w] = vb;
-        if (e == 0) reinterpret_cast<unsigned int*>(G.out_data[c])[w] = db;
+#pragma unroll
+      for (int u = 0; u < GU; u++) {
+        if (ok[u]) {
+          switch (e) {
+            case 0: break;
+            case 1: G.out_data[c][p[u]] = (uint8_t)b[u]; break;
+            case 2: reinterpret_cast<uint16_t*>(G.out_data[c])[p[u]] = (uint16_t)b[u]; break;
+            case 4: reinterpret_cast<uint32_t*>(G.out_data[c])[p[u]] = (uint32_t)b[u]; break;
+            default: reinterpret_cast<uint64_t*>(G.out_data[c])[p[u]] = b[u]; break;
+          }
+        }
+        const unsigned vw = __ballot_sync(0xffffffffu, v[u]);
+        const unsigned dw = __ballot_sync(0xffffffffu, ok[u] && e == 0 && b[u]);
+        if (lane == 0 && (w0 + u) * 32 < m) {
+          G.out_valid[c][w0 + u] = vw;
+          if (e == 0) reinterpret_cast<unsigned int*>(G.out_data[c])[w0 + u] = dw;
+        }
       }
     }
   }
@@ -248,15 +354,29 @@ int pmb_order_columns(pmb_handle* h, const DCol* cols, int n_cols, int64_t n, co
   OrderRange got;
   memset(&got, 0, sizeof(got));
   for (int k = 0; k < PMB_MAX_KEYS; k++) got.lo[k] = ~0ULL;
+  // which columns have a null at all (a column without one is gathered without its bitmap)
+  unsigned int has_null[PMB_MAX_OUT];
+  for (int c = 0; c < n_cols; c++) has_null[c] = cols[c].valid != nullptr;
   if (n > 0) {
     OrderRange* ro = (OrderRange*)pmb_ws_alloc(h, sizeof(OrderRange));
-    if (!ro) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sort ranges)");
+    unsigned int* flags = (unsigned int*)pmb_ws_alloc(h, PMB_MAX_OUT * 4);
+    if (!ro || !flags) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sort ranges)");
     PMB_CUDA(h, cudaMemcpyAsync(ro, &got, sizeof(got), cudaMemcpyHostToDevice, h->stream));
+    PMB_CUDA(h, cudaMemsetAsync(flags, 0, PMB_MAX_OUT * 4, h->stream));
     pmb_kernel_begin(h, "order_range");
     k_order_range<<<blocks_for(h, n), OR_NT, 0, h->stream>>>(C, n, ro);
     pmb_kernel_end(h);
     PMB_CUDA(h, cudaGetLastError());
+    NullFlagCols V;
+    memset(&V, 0, sizeof(V));
+    V.n = n_cols;
+    for (int c = 0; c < n_cols; c++) V.valid[c] = cols[c].valid;
+    pmb_kernel_begin(h, "null_flags");
+    k_null_flags<<<blocks_for(h, n / 8 + 1), OR_NT, 0, h->stream>>>(V, n, flags);
+    pmb_kernel_end(h);
+    PMB_CUDA(h, cudaGetLastError());
     PMB_CUDA(h, cudaMemcpyAsync(&got, ro, sizeof(got), cudaMemcpyDeviceToHost, h->stream));
+    PMB_CUDA(h, cudaMemcpyAsync(has_null, flags, (size_t)n_cols * 4, cudaMemcpyDeviceToHost, h->stream));
     PMB_CUDA(h, cudaStreamSynchronize(h->stream));
   }
   // field widths; rounds of at most 128 bits, cut from the least significant column up
@@ -292,9 +412,11 @@ int pmb_order_columns(pmb_handle* h, const DCol* cols, int n_cols, int64_t n, co
   if (!k0 || !k1 || !i0 || !i1 || !hist) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sort keys)");
   const unsigned int* perm = nullptr;  // the order so far (none: row order)
   std::vector<unsigned int> hh((size_t)OR_PASSES * OR_RADIX);
+  OrderLayout L;  // the last round's layout
+  memset(&L, 0, sizeof(L));
+  int W = 1;
   for (const Round& rd : rounds) {
     if (rd.bits == 0 || n <= 1) continue;  // every key equal: the order stays
-    OrderLayout L;
     memset(&L, 0, sizeof(L));
     L.n = rd.last - rd.first + 1;
     int off = 0;
@@ -316,7 +438,7 @@ int pmb_order_columns(pmb_handle* h, const DCol* cols, int n_cols, int64_t n, co
       off += nbits[k];
     }
     L.bits = off;
-    const int W = off > 64 ? 2 : 1;
+    W = off > 64 ? 2 : 1;
     const int passes = (off + 7) / 8;
     PMB_CUDA(h, cudaMemsetAsync(hist, 0, (size_t)OR_PASSES * OR_RADIX * 4, h->stream));
     pmb_kernel_begin(h, "order_encode");
@@ -337,12 +459,24 @@ int pmb_order_columns(pmb_handle* h, const DCol* cols, int n_cols, int64_t n, co
   GatherCols G;
   memset(&G, 0, sizeof(G));
   G.n = n_cols;
+  G.keys = k0;
+  G.cap = cap;
+  G.W = W;
+  for (int c = 0; c < n_cols; c++) G.dec[c] = -1;
+  // one round sorted every column: integer and Bool sort columns come back out of the sorted keys
+  // (float keys are canonical in the key, -0.0 and NaN payloads, so floats are gathered)
+  if (rounds.size() == 1 && perm != nullptr) {
+    for (int k = 0; k < nb; k++) {
+      const int dt = cols[s.by[k]].dtype;
+      if (dt != PMB_F32 && dt != PMB_F64) G.dec[s.by[k]] = k - rounds[0].first;
+    }
+  }
   const int64_t words = (m + 31) / 32;
   for (int c = 0; c < n_cols; c++) {
     const int e = cols[c].elem;
     const size_t db = e ? (size_t)m * e : (size_t)words * 4;
     G.data[c] = cols[c].data;
-    G.valid[c] = cols[c].valid;
+    G.valid[c] = has_null[c] ? cols[c].valid : nullptr;
     G.elem[c] = e;
     G.out_data[c] = (uint8_t*)pmb_ws_alloc(h, db + 16);
     G.out_valid[c] = (unsigned int*)pmb_ws_alloc(h, (size_t)words * 4 + 16);
@@ -350,7 +484,9 @@ int pmb_order_columns(pmb_handle* h, const DCol* cols, int n_cols, int64_t n, co
   }
   if (m > 0) {
     pmb_kernel_begin(h, "order_gather");
-    k_order_gather<<<blocks_for(h, words * 32), OR_NT, 0, h->stream>>>(G, perm, start, m);
+    const int gb = blocks_for(h, (words + GU - 1) / GU * 32);
+    if (W == 1) k_order_gather<1><<<gb, OR_NT, 0, h->stream>>>(G, L, perm, start, m);
+    else k_order_gather<2><<<gb, OR_NT, 0, h->stream>>>(G, L, perm, start, m);
     pmb_kernel_end(h);
     PMB_CUDA(h, cudaGetLastError());
   }
