@@ -270,6 +270,9 @@ pmb_result* pmb_result_new(int32_t n_columns) {
     free(r);
     return nullptr;
   }
+  // columns hold workspace (device) pointers until pmb_finish_outputs copies them to host memory
+  // it allocates, so a result freed on an error path before that never frees a device pointer
+  for (int32_t c = 0; c < n_columns; c++) r->columns[c].on_device = 1;
   return r;
 }
 
