@@ -405,7 +405,8 @@ def main():
                 hv.copy_(c.validity)
             host[name] = ColumnData(hd, hv, dtype=c.dtype, length=c.length)
         e2e_steps = args.e2e_steps or max(3, min(args.steps, 5))
-        groupby(host, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="host", handle=h)
+        for _ in range(max(3, args.warmup)):
+            groupby(host, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="host", handle=h)
         h.set_profiling(True)
         groupby(host, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="host", handle=h)
         io = h.last_stats()

@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import ctypes as C
 import threading
+import weakref
 from dataclasses import dataclass, field
 from typing import Any, Sequence
 
@@ -286,6 +287,37 @@ def _host_copy(addr: int, nbytes: int, dtype) -> np.ndarray:
     return np.frombuffer((C.c_char * nbytes).from_address(addr), dtype=dtype).copy()
 
 
+_free = None
+_TAKE_MIN = 1 << 20  # host result buffers of at least this size are taken over instead of copied
+
+
+def _host_take(addr: int, nbytes: int, dtype) -> np.ndarray:
+    """A numpy array over host memory that libpmb malloc'd for a result, without a copy: the array
+    owns the buffer, which is freed (libc free) when the last view of it is collected."""
+    global _free
+    if _free is None:
+        libc = C.CDLL(None)
+        libc.free.argtypes = [C.c_void_p]
+        libc.free.restype = None
+        _free = libc.free
+    buf = (C.c_char * nbytes).from_address(addr)
+    weakref.finalize(buf, _free, addr)
+    return np.frombuffer(buf, dtype=dtype)
+
+
+def _host_out(oc: A.OutColumn, field: str, nbytes: int, dtype, empty: int) -> np.ndarray:
+    """One host buffer of a result column: large buffers change owner (the column's pointer is
+    cleared, so pmb_result_free leaves it), small ones are copied."""
+    addr = getattr(oc, field)
+    if not addr or nbytes == 0:
+        return np.zeros(empty, dtype)
+    if nbytes >= _TAKE_MIN:
+        arr = _host_take(addr, nbytes, dtype)
+        setattr(oc, field, None)
+        return arr
+    return _host_copy(addr, nbytes, dtype)
+
+
 def _read_result(res: A.Result, names, to_host: bool) -> tuple[list, list, list]:
     n = res.n_groups
     data, valid, dts = [], [], []
@@ -297,12 +329,11 @@ def _read_result(res: A.Result, names, to_host: bool) -> tuple[list, list, list]
             valid.append(int(oc.validity or 0))
             continue
         vb = _bitmap_bytes(n)
-        v = _host_copy(oc.validity, vb, np.uint8) if oc.validity else np.zeros(vb, np.uint8)
+        v = _host_out(oc, "validity", vb, np.uint8, vb)
         if oc.dtype == A.BOOL:
-            d = _host_copy(oc.data, vb, np.uint8) if oc.data else np.zeros(vb, np.uint8)
+            d = _host_out(oc, "data", vb, np.uint8, vb)
         else:
-            nb = n * A.DTYPE_BYTES[oc.dtype]
-            d = _host_copy(oc.data, nb, A.NUMPY_NAME[oc.dtype]) if (oc.data and nb) else np.zeros(0, A.NUMPY_NAME[oc.dtype])
+            d = _host_out(oc, "data", n * A.DTYPE_BYTES[oc.dtype], A.NUMPY_NAME[oc.dtype], 0)
         data.append(d)
         valid.append(v)
     return data, valid, dts

@@ -131,3 +131,33 @@ def test_batched_arguments_are_the_c_structs():
             assert (col[j].validity or 0) == (cd.validity.data_ptr() if cd.validity is not None else 0)
             assert col[j].on_device == 0
         assert names[i] == list(keys) + [a[2] for a in aggs]
+
+
+def test_large_host_results_change_owner_small_ones_are_copied():
+    import gc
+
+    import numpy as np
+
+    from polars_b200 import _native as N
+
+    libc = C.CDLL(None)
+    libc.malloc.restype = C.c_void_p
+    libc.malloc.argtypes = [C.c_size_t]
+    libc.free.argtypes = [C.c_void_p]
+    big, small = 1 << 21, 4096
+    oc = A.OutColumn()
+    oc.data = libc.malloc(big)
+    oc.validity = libc.malloc(small)
+    C.memset(oc.data, 7, big)
+    C.memset(oc.validity, 255, small)
+    d = N._host_out(oc, "data", big, np.uint8, 0)
+    v = N._host_out(oc, "validity", small, np.uint8, 0)
+    assert oc.data is None          # taken over: pmb_result_free would leave it
+    assert oc.validity is not None  # copied: still the result's to free
+    assert d.size == big and np.all(d == 7) and np.all(v == 255)
+    view = d[10:20]
+    del d
+    gc.collect()
+    assert np.all(view == 7)        # the buffer lives while any view of it does
+    libc.free(oc.validity)
+    assert N._host_out(A.OutColumn(), "data", 0, np.int64, 0).size == 0
