@@ -238,6 +238,10 @@ int pmb_sort_columns(pmb_handle* h, const pmb_column* cols, int32_t n_cols, cons
 int pmb_groupby_sorted(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols,
                        const pmb_sort_spec* spec, pmb_result** out);
 
+/* Frees a result. Host output buffers come from the C library's allocator (malloc, or
+ * posix_memalign for large ones) and each non-NULL one is released with free(): a caller may take
+ * a buffer over by setting its pointer in the result to NULL and calling free() on it later.
+ * Device outputs live in the handle's workspace and are not freed here. */
 void pmb_result_free(pmb_result* r);
 
 /* ---- learned strategy selection ----
