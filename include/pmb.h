@@ -66,6 +66,70 @@ typedef struct pmb_column {
   int32_t on_device;       /* 1 = device pointers, 0 = host pointers                   */
 } pmb_column;
 
+/* ---- Arrow C Data Interface and C Device Data Interface (the Apache Arrow specification's
+ *      stable ABI, declared here under its own guards as the specification asks) ---- */
+#ifndef ARROW_C_DATA_INTERFACE
+#define ARROW_C_DATA_INTERFACE
+#define ARROW_FLAG_DICTIONARY_ORDERED 1
+#define ARROW_FLAG_NULLABLE 2
+#define ARROW_FLAG_MAP_KEYS_SORTED 4
+struct ArrowSchema {
+  const char* format;
+  const char* name;
+  const char* metadata;
+  int64_t flags;
+  int64_t n_children;
+  struct ArrowSchema** children;
+  struct ArrowSchema* dictionary;
+  void (*release)(struct ArrowSchema*);
+  void* private_data;
+};
+struct ArrowArray {
+  int64_t length;
+  int64_t null_count;
+  int64_t offset;
+  int64_t n_buffers;
+  int64_t n_children;
+  const void** buffers;
+  struct ArrowArray** children;
+  struct ArrowArray* dictionary;
+  void (*release)(struct ArrowArray*);
+  void* private_data;
+};
+#endif
+#ifndef ARROW_C_DEVICE_DATA_INTERFACE
+#define ARROW_C_DEVICE_DATA_INTERFACE
+typedef int32_t ArrowDeviceType;
+#define ARROW_DEVICE_CPU 1
+#define ARROW_DEVICE_CUDA 2
+#define ARROW_DEVICE_CUDA_HOST 3
+struct ArrowDeviceArray {
+  struct ArrowArray array;
+  int64_t device_id;
+  ArrowDeviceType device_type;
+  void* sync_event;
+  int64_t reserved[3];
+};
+#endif
+
+/* A column over an exported Arrow array's own buffers, without a copy: the values buffer, the
+ * validity bitmap (NULL when the array has no nulls) and the array's offset. Primitive formats
+ * b c C s S i I l L f g (Bool, Int8..UInt64, Float32, Float64); a dictionary-encoded array gives
+ * its integer codes (group by them, then decode through the dictionary). Returns
+ * PMB_E_UNSUPPORTED for other formats and PMB_E_INVALID for a malformed or released array. The
+ * array stays owned by its producer and must outlive every call that reads the column.
+ * Replaces the reference's Arrow -> Metal buffer bridge (crates/polars-metal-buffer/src/bridge.rs:1-60)
+ * and the Python copies it is fed from (python/polars_metal/_udf.py:1441-1456). No GPU is
+ * touched; no handle is needed. */
+int pmb_column_from_arrow(const struct ArrowArray* array, const struct ArrowSchema* schema, pmb_column* out);
+
+/* The same for an array of the C Device Data Interface: ARROW_DEVICE_CUDA buffers give a device
+ * column (used in place by the kernels), ARROW_DEVICE_CPU and ARROW_DEVICE_CUDA_HOST a host one.
+ * A non-NULL `sync_event` (a cudaEvent_t* for CUDA) is left to the caller to wait on before the
+ * column is used. Other device types return PMB_E_UNSUPPORTED. */
+int pmb_column_from_arrow_device(const struct ArrowDeviceArray* array, const struct ArrowSchema* schema,
+                                 pmb_column* out);
+
 /* ---- predicate expression (PredicateAst, crates/polars-metal-core/src/plan/mod.rs:42-60,
  *      plus the Arith / Not / IsNull nodes this build adds) ---- */
 enum {

@@ -145,6 +145,53 @@ class SortSpec(C.Structure):
     ]
 
 
+class ArrowSchema(C.Structure):
+    pass
+
+
+ArrowSchema._fields_ = [
+    ("format", C.c_char_p),
+    ("name", C.c_char_p),
+    ("metadata", C.c_char_p),
+    ("flags", C.c_int64),
+    ("n_children", C.c_int64),
+    ("children", C.POINTER(C.POINTER(ArrowSchema))),
+    ("dictionary", C.POINTER(ArrowSchema)),
+    ("release", C.c_void_p),
+    ("private_data", C.c_void_p),
+]
+
+
+class ArrowArray(C.Structure):
+    pass
+
+
+ArrowArray._fields_ = [
+    ("length", C.c_int64),
+    ("null_count", C.c_int64),
+    ("offset", C.c_int64),
+    ("n_buffers", C.c_int64),
+    ("n_children", C.c_int64),
+    ("buffers", C.POINTER(C.c_void_p)),
+    ("children", C.POINTER(C.POINTER(ArrowArray))),
+    ("dictionary", C.POINTER(ArrowArray)),
+    ("release", C.c_void_p),
+    ("private_data", C.c_void_p),
+]
+
+
+class ArrowDeviceArray(C.Structure):
+    _fields_ = [
+        ("array", ArrowArray),
+        ("device_id", C.c_int64),
+        ("device_type", C.c_int32),
+        ("sync_event", C.c_void_p),
+        ("reserved", C.c_int64 * 3),
+    ]
+
+
+ARROW_DEVICE_CPU, ARROW_DEVICE_CUDA, ARROW_DEVICE_CUDA_HOST = 1, 2, 3
+
 MAX_STAT_KERNELS = 16
 
 
@@ -179,6 +226,9 @@ SIGNATURES = {
          C.POINTER(C.POINTER(Result))],
     ),
     "pmb_result_free": (None, [C.POINTER(Result)]),
+    "pmb_column_from_arrow": (C.c_int, [C.POINTER(ArrowArray), C.POINTER(ArrowSchema), C.POINTER(Column)]),
+    "pmb_column_from_arrow_device": (C.c_int, [C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema),
+                                               C.POINTER(Column)]),
     "pmb_sort_columns": (C.c_int, [_H, C.POINTER(Column), C.c_int32, C.POINTER(SortSpec), C.c_int32,
                                    C.POINTER(C.POINTER(Result))]),
     "pmb_groupby_sorted": (C.c_int, [_H, C.POINTER(Query), C.POINTER(Column), C.c_int32, C.POINTER(SortSpec),

@@ -30,6 +30,7 @@ SOURCES = [
     "pmb_noalloc.cu",
     "pmb_exprcol.cu",
     "pmb_order.cu",
+    "pmb_arrow.cu",
 ]
 
 # device sources compiled at run time by NVRTC, embedded into the library as string literals

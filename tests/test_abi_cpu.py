@@ -46,13 +46,14 @@ def test_ctypes_mirror_covers_the_header(lib_path):
 def test_struct_layouts_match_c(tmp_path):
     src = tmp_path / "sz.c"
     structs = ["pmb_column", "pmb_expr_node", "pmb_expr", "pmb_agg", "pmb_query", "pmb_out_column", "pmb_result",
-               "pmb_stats", "pmb_sort_spec"]
+               "pmb_stats", "pmb_sort_spec", "struct ArrowSchema", "struct ArrowArray", "struct ArrowDeviceArray"]
     src.write_text('#include <stdio.h>\n#include "pmb.h"\nint main(void){\n' +
                    "".join(f'printf("%zu\\n", sizeof({s}));\n' for s in structs) + "return 0;}\n")
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
-    mirror = [A.Column, A.ExprNode, A.Expr, A.Agg, A.Query, A.OutColumn, A.Result, A.Stats, A.SortSpec]
+    mirror = [A.Column, A.ExprNode, A.Expr, A.Agg, A.Query, A.OutColumn, A.Result, A.Stats, A.SortSpec,
+              A.ArrowSchema, A.ArrowArray, A.ArrowDeviceArray]
     assert sizes == [C.sizeof(m) for m in mirror]
 
 
