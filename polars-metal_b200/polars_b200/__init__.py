@@ -19,8 +19,13 @@ from ._native import (  # noqa: F401
     execute_filter_compact,
     execute_groupby,
     execute_sort,
+    bottom_k,
+    eval_expr,
+    filter_columns,
     groupby,
+    groupby_batched,
     sort_columns,
+    top_k,
 )
 
 __version__ = "0.1.0"
