@@ -130,3 +130,14 @@ def test_sort_spec_broadcasts_flags_and_checks_names():
         _sort_spec(["k"], ["z"])
     with pytest.raises(ValueError):
         _sort_spec(["k", "s"], ["k", "s"], descending=[True])
+
+
+def test_sort_plan_errors_before_any_device_work():
+    from polars_b200._native import execute_sort
+
+    with pytest.raises(ValueError, match="missing field input"):
+        execute_sort({"kind": "Sort", "by_columns": ["k"]}, 0, [])
+    with pytest.raises(ValueError, match="slice without sort columns"):
+        execute_sort({"kind": "Sort", "input": {"keys": [], "aggs": []}, "by_columns": [], "slice": [0, 5]}, 0, [])
+    with pytest.raises(ValueError, match="negative slice length"):
+        _sort_spec(["k"], "k", limit=-3)
