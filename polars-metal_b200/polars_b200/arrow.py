@@ -36,9 +36,46 @@ _TO_PMB = {
 _FROM_PMB = {v: k for k, v in _TO_PMB.items()}
 
 
-def column_from_arrow(arr: pa.Array | pa.ChunkedArray) -> ColumnData:
-    """A libpmb column over an Arrow array's own buffers (no copy for a single chunk)."""
+def _cuda() -> bool:
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except ImportError:
+        return False
+
+
+def _chunks_to_device(col: pa.ChunkedArray, dt: int) -> ColumnData:
+    """A numeric column of several chunks copied chunk by chunk into one device buffer: the values
+    are not concatenated on the host first. The validity bitmap (an eighth of a byte a row) is
+    combined on the host by pyarrow and copied after them."""
+    import torch
+
+    n = len(col)
+    elem = A.DTYPE_BYTES[dt]
+    dev = torch.empty(max(n * elem, 1), dtype=torch.uint8, device="cuda")
+    off = 0
+    for ch in col.chunks:
+        m = len(ch)
+        if m:
+            vals = np.frombuffer(ch.buffers()[1], dtype=A.NUMPY_NAME[dt])[ch.offset: ch.offset + m]
+            dev[off * elem: (off + m) * elem].copy_(torch.from_numpy(vals.view(np.uint8)))
+        off += m
+    validity = None
+    if col.null_count:
+        bits = pc.is_valid(col).combine_chunks()
+        vb = np.frombuffer(bits.buffers()[1], np.uint8)
+        validity = torch.from_numpy(np.ascontiguousarray(vb[: (n + 7) // 8])).to("cuda")
+    return ColumnData(dev, validity, dtype=dt, length=n)
+
+
+def column_from_arrow(arr: pa.Array | pa.ChunkedArray, device: bool = False) -> ColumnData:
+    """A libpmb column over an Arrow array's own buffers (no copy for a single chunk). A numeric
+    column of several chunks is combined into one host array, or with `device` copied chunk by
+    chunk into one CUDA buffer."""
     if isinstance(arr, pa.ChunkedArray):
+        if device and arr.num_chunks > 1 and _TO_PMB.get(arr.type, A.BOOL) != A.BOOL:
+            return _chunks_to_device(arr, _TO_PMB[arr.type])
         if arr.num_chunks == 1:
             arr = arr.chunk(0)
         elif arr.num_chunks == 0:
@@ -58,10 +95,11 @@ def column_from_arrow(arr: pa.Array | pa.ChunkedArray) -> ColumnData:
     return ColumnData(data, validity, dtype=dt, length=n, offset=arr.offset)
 
 
-def columns_from_arrow(table: pa.Table | pa.RecordBatch, names: Sequence[str] | None = None) -> dict:
+def columns_from_arrow(table: pa.Table | pa.RecordBatch, names: Sequence[str] | None = None,
+                       device: bool = False) -> dict:
     """{name: ColumnData} for the named columns of a table (all of them by default)."""
     names = list(table.column_names if names is None else names)
-    return {name: column_from_arrow(table.column(name)) for name in names}
+    return {name: column_from_arrow(table.column(name), device) for name in names}
 
 
 def table_from_result(res: GroupByResult) -> pa.Table:
@@ -128,13 +166,14 @@ def groupby_arrow(table: pa.Table | pa.RecordBatch, keys: Sequence[str], aggs: S
     if missing:
         raise KeyError(f"polars_b200: column {missing[0]!r} not found in upstream columns")
     cols, dicts = {}, {}
+    dev = _cuda()
     for name in names:
         enc = _dictionary_key(table.column(name)) if name in keys else None
         if enc is not None:
             cols[name] = column_from_arrow(enc[0])
             dicts[name] = enc[1]
         else:
-            cols[name] = column_from_arrow(table.column(name))
+            cols[name] = column_from_arrow(table.column(name), dev)
     res = groupby(cols, keys, aggs, predicate, strategy=strategy, output="host", handle=handle, sort=sort)
     return _decoded(table_from_result(res), dicts)
 
@@ -151,13 +190,14 @@ def sort_arrow(table: pa.Table | pa.RecordBatch, by, descending=False, nulls_las
     """The rows of an Arrow table sorted by `by` on the GPU (sort_columns), then slice(offset,
     limit); string, binary and dictionary columns travel as their sorted-dictionary codes."""
     cols, dicts = {}, {}
+    dev = _cuda()
     for name in table.column_names:
         enc = _dictionary_key(table.column(name))
         if enc is not None:
             cols[name] = column_from_arrow(enc[0])
             dicts[name] = enc[1]
         else:
-            cols[name] = column_from_arrow(table.column(name))
+            cols[name] = column_from_arrow(table.column(name), dev)
     res = sort_columns(cols, by, descending=descending, nulls_last=nulls_last, offset=offset, limit=limit,
                        output="host", handle=handle)
     return _decoded(table_from_result(res), dicts)
@@ -166,5 +206,5 @@ def sort_arrow(table: pa.Table | pa.RecordBatch, by, descending=False, nulls_las
 def filter_arrow(table: pa.Table | pa.RecordBatch, predicate: dict, handle: Handle | None = None) -> pa.Table:
     """The rows of an Arrow table whose predicate is valid and true, as an Arrow table (all its
     columns, in row order)."""
-    res = filter_columns(columns_from_arrow(table), predicate, output="host", handle=handle)
+    res = filter_columns(columns_from_arrow(table, device=_cuda()), predicate, output="host", handle=handle)
     return table_from_result(res)

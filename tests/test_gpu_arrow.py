@@ -112,3 +112,38 @@ def test_string_keys_through_their_dictionary():
     got_codes = pc.index_in(got.column("s"), value_set=enc.dictionary)
     got_t = got.set_column(0, "s", got_codes.cast(pa.int32()))
     assert_results_match(_arrow_as_dict(got_t), want, 2, aggs, "string keys")
+
+
+def test_chunked_columns_go_to_the_device_chunk_by_chunk():
+    # several chunks, sliced (chunk offsets), with nulls: values copied per chunk into one device
+    # buffer, validity combined on the host
+    from polars_b200.arrow import column_from_arrow, sort_arrow
+
+    rng = np.random.default_rng(17)
+    sizes = [40_000, 1, 0, 77_777, 12_345]
+    ks, vs, vns = [], [], []
+    kch, vch = [], []
+    for m in sizes:
+        k = rng.integers(0, 999, m + 5).astype(np.int64)
+        v = rng.standard_normal(m + 5)
+        vn = rng.random(m + 5) < 0.1
+        kch.append(pa.array(k).slice(5))
+        vch.append(pa.array(v, mask=vn).slice(5))
+        ks.append(k[5:])
+        vs.append(v[5:])
+        vns.append(vn[5:])
+    table = pa.table({"k": pa.chunked_array(kch), "v": pa.chunked_array(vch, type=pa.float64())})
+    cd = column_from_arrow(table.column("v"), device=True)
+    assert cd.data.is_cuda and cd.validity.is_cuda and cd.length == sum(sizes)
+    k, v, vn = np.concatenate(ks), np.concatenate(vs), np.concatenate(vns)
+    aggs = [("Sum", "v", "s"), ("Count", "v", "c"), ("Max", "v", "mx"), ("Len", None, "n")]
+    got = groupby_arrow(table, ["k"], aggs)
+    want = pyoracle.groupby({"k": (k, None), "v": (v, pack(~vn))}, ["k"], aggs)
+    assert_results_match(_arrow_as_dict(got), want, 1, aggs, "chunked on device")
+    pred = {"kind": "Compare", "op": "Lt", "dtype": "I64", "lhs": {"kind": "Column", "name": "k"},
+            "rhs": {"kind": "LiteralI64", "value": 100}}
+    kept = filter_arrow(table, pred)
+    assert kept.column("k").to_pylist() == k[k < 100].tolist()
+    assert kept.column("v").is_null().to_pylist() == vn[k < 100].tolist()
+    top = sort_arrow(table, ["v"], descending=True, nulls_last=True, limit=5)
+    assert top.column("v").to_pylist() == sorted(v[~vn].tolist(), reverse=True)[:5]
