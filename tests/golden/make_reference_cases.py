@@ -410,9 +410,53 @@ def sort_cases() -> list[dict]:
     ]
 
 
+def expression_cases() -> list[dict]:
+    """tests/python_integration/test_walker_expression_unfolding.py: group-by aggregates of
+    arithmetic expressions, engine vs Polars CPU. Inputs are closed forms (`formula`, built by
+    tests/helpers.py expression_columns); an expression is in the reference's aggregation wire
+    shape (Column / LiteralF64 / Binary). Expected sums: every row's product rounded to f64 as
+    Polars computes it, then summed exactly (math.fsum)."""
+    def col(c):
+        return {"kind": "Column", "name": c}
+
+    def lit(x):
+        return {"kind": "LiteralF64", "value": x}
+
+    def binop(op, a, b):
+        return {"kind": "Binary", "op": op, "lhs": a, "rhs": b}
+
+    cases = []
+    k, a, b = [0, 0, 1, 1, 2, 2], [1.0, 2.0, 3.0, 4.0, 5.0, 6.0], [0.1, 0.2, 0.3, 0.4, 0.5, 0.6]
+    rows = [(kk, aa * bb) for kk, aa, bb in zip(k, a, b)]
+    cases.append({"name": "sum_a_times_b", "source": "tests/python_integration/test_walker_expression_unfolding.py:17-35",
+                  "formula": "sum_a_times_b", "n": 6000, "keys": ["k"],
+                  "aggs": [{"kind": "Expression", "op": "Sum", "output_alias": "sum_ab",
+                            "expr": binop("Mul", col("a"), col("b"))}],
+                  "expected": {"k": [0, 1, 2], "sum_ab": [math.fsum([p for kk, p in rows if kk == g] * 1000)
+                                                          for g in (0, 1, 2)]}})
+    k, a, b = [0, 0, 1, 1], [10.0, 20.0, 30.0, 40.0], [0.05, 0.1, 0.15, 0.2]
+    rows = [(kk, aa * (1.0 - bb)) for kk, aa, bb in zip(k, a, b)]
+    cases.append({"name": "sum_a_times_one_minus_b",
+                  "source": "tests/python_integration/test_walker_expression_unfolding.py:38-56",
+                  "formula": "sum_a_times_one_minus_b", "n": 20000, "keys": ["k"],
+                  "aggs": [{"kind": "Expression", "op": "Sum", "output_alias": "disc",
+                            "expr": binop("Mul", col("a"), binop("Sub", lit(1.0), col("b")))}],
+                  "expected": {"k": [0, 1], "disc": [math.fsum([p for kk, p in rows if kk == g] * 5000)
+                                                     for g in (0, 1)]}})
+    e = col("v")
+    for _ in range(5):
+        e = binop("Add", e, lit(1.0))
+    cases.append({"name": "depth_5_chain", "source": "tests/python_integration/test_walker_expression_unfolding.py:68-78",
+                  "formula": "depth_5_chain", "n": 100, "keys": ["k"],
+                  "aggs": [{"kind": "Expression", "op": "Sum", "output_alias": "s", "expr": e}],
+                  "expected": {"k": [0], "s": [600.0]}})
+    return cases
+
+
 def main():
     doc = {"groupby": groupby_cases(), "integration": integration_cases(), "compare": compare_cases(),
-           "kleene": kleene_cases(), "sort": sort_cases()}
+           "kleene": kleene_cases(), "sort": sort_cases(),
+           "expression": expression_cases()}
     # the all-unique case is large; keep only its shape and check it by property
     for c in doc["integration"]:
         if c["formula"] == "all_unique":

@@ -88,6 +88,34 @@ def formula_columns(formula: str, n: int) -> dict:
     raise KeyError(formula)
 
 
+def expression_columns(formula: str, n: int) -> dict:
+    """Closed-form inputs of tests/python_integration/test_walker_expression_unfolding.py (see
+    make_reference_cases.py): the test's short lists repeated to n rows."""
+    def rep(vals, dtype):
+        v = np.array(vals, dtype=dtype)
+        return np.tile(v, n // len(v))
+    if formula == "sum_a_times_b":
+        return {"k": (rep([0, 0, 1, 1, 2, 2], np.int64), None), "a": (rep([1.0, 2.0, 3.0, 4.0, 5.0, 6.0], np.float64), None),
+                "b": (rep([0.1, 0.2, 0.3, 0.4, 0.5, 0.6], np.float64), None)}
+    if formula == "sum_a_times_one_minus_b":
+        return {"k": (rep([0, 0, 1, 1], np.int64), None), "a": (rep([10.0, 20.0, 30.0, 40.0], np.float64), None),
+                "b": (rep([0.05, 0.1, 0.15, 0.2], np.float64), None)}
+    if formula == "depth_5_chain":
+        return {"k": (np.zeros(n, np.int64), None), "v": (np.ones(n, np.float64), None)}
+    raise KeyError(formula)
+
+
+def numpy_expr(e: dict, cols: dict) -> np.ndarray:
+    """An aggregation expression (reference wire shape) evaluated row by row in numpy, f64."""
+    kind = e["kind"]
+    if kind == "Column":
+        return cols[e["name"]][0].astype(np.float64)
+    if kind in ("LiteralF64", "LiteralI64"):
+        return np.float64(e["value"])
+    lhs, rhs = numpy_expr(e["lhs"], cols), numpy_expr(e["rhs"], cols)
+    return {"Add": np.add, "Sub": np.subtract, "Mul": np.multiply, "Div": np.divide}[e["op"]](lhs, rhs)
+
+
 def _values(dt: int, data: np.ndarray, n: int) -> np.ndarray:
     if dt == A.BOOL:
         return unpack(data, n)

@@ -48,3 +48,22 @@ def test_arrow_path_hands_over_expression_columns(monkeypatch):
     with pytest.raises(RuntimeError, match="stop"):
         arrow.groupby_arrow(t, ["k"], [("Sum", {"kind": "Arith", "op": "Mul", "lhs": col("a"), "rhs": col("b")}, "s")])
     assert seen["cols"] == ["a", "b", "k"]
+
+
+@pytest.mark.parametrize("case", __import__("helpers").load_golden()["expression"], ids=lambda c: c["name"])
+def test_oracle_pinned_to_the_reference_expression_cases(case):
+    # the expression evaluated row by row in numpy, then the oracle's group-by sum of it
+    import math
+
+    from helpers import expression_columns, numpy_expr
+    from oracle import pyoracle
+
+    cols = expression_columns(case["formula"], case["n"])
+    agg = case["aggs"][0]
+    x = numpy_expr(agg["expr"], cols)
+    res = pyoracle.groupby({"k": cols["k"], "x": (x, None)}, ["k"], [("Sum", "x", agg["output_alias"])])
+    order = sorted(range(res["n_groups"]), key=lambda i: res["data"][0][i])
+    assert [int(res["data"][0][i]) for i in order] == case["expected"]["k"]
+    got = [float(res["data"][1][i]) for i in order]
+    want = case["expected"][agg["output_alias"]]
+    assert all(math.isclose(g, w, rel_tol=1e-12) for g, w in zip(got, want)), (got, want)

@@ -98,3 +98,24 @@ def test_expression_aggregates_on_the_reference_wire():
            "data": [np.frombuffer(o[2], A.NUMPY_NAME[dt]) for o, dt in zip(out, dts)],
            "validity": [np.frombuffer(o[3], np.uint8) for o in out]}
     assert_results_match(got, want, 1, ops, "wire expression aggregates")
+
+
+@pytest.mark.parametrize("case", __import__("helpers").load_golden()["expression"], ids=lambda c: c["name"])
+def test_reference_expression_cases_through_the_wire(case):
+    import math
+
+    from helpers import expression_columns
+
+    cols = expression_columns(case["formula"], case["n"])
+    n = case["n"]
+    ones = b"\xff" * ((n + 7) // 8)
+    tags = {np.dtype(np.int64): "I64", np.dtype(np.float64): "F64"}
+    columns = [(name, tags[d.dtype], d.tobytes(), ones) for name, (d, _v) in cols.items()]
+    plan = {"keys": [["k", "I64"]], "aggs": case["aggs"]}
+    out = N.execute_groupby(plan, n, columns)
+    k = np.frombuffer(out[0][2], np.int64)
+    s = np.frombuffer(out[1][2], np.float64)
+    order = np.argsort(k)
+    assert k[order].tolist() == case["expected"]["k"]
+    want = case["expected"][case["aggs"][0]["output_alias"]]
+    assert all(math.isclose(g, w, rel_tol=1e-12) for g, w in zip(s[order].tolist(), want)), (s[order], want)
