@@ -9,8 +9,15 @@ Reference functions mirrored (same names, argument meaning and error classes):
 Errors: ValueError (parse / length), KeyError (missing column), NotImplementedError (outside
 this build), MemoryError, RuntimeError (device failures; the reference's ComputeError).
 
+Also on the reference's wire: execute_sort(plan, n_rows, columns) for a Sort plan over a
+GroupBy (python/polars_metal/_udf.py:684-721), and Expression aggregates inside execute_groupby
+(crates/polars-metal-core/src/udf/groupby/mod.rs:266-352).
+
 Beyond the wire-format functions, `groupby()` takes numpy arrays or CUDA tensors directly
-(zero-copy for device-resident columns) and `Handle` exposes streams and per-kernel timings.
+(zero-copy for device-resident columns; `sort=` orders the result on the device), and so do
+`sort_columns` / `top_k` / `bottom_k`, `filter_columns`, `eval_expr` and `groupby_batched`.
+Host results of 1 MB or more are numpy arrays over the library's own buffers (no copy). `Handle`
+exposes streams and per-kernel timings.
 """
 
 from __future__ import annotations
