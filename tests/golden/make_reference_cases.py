@@ -453,10 +453,94 @@ def expression_cases() -> list[dict]:
     return cases
 
 
+def compare_i64_cases() -> list[dict]:
+    """crates/polars-metal-kernels/tests/test_cmp_i64.rs known answers: column-column and
+    column-scalar compares with nulls, an unaligned row count, extreme values. `scalar` marks a
+    column-scalar case; expected bits written out from each test's assertions."""
+    src = "crates/polars-metal-kernels/tests/test_cmp_i64.rs"
+    lo, hi = -(1 << 63), (1 << 63) - 1
+    cases = [
+        {"name": "lt_basic", "source": f"{src}:127-153", "op": "Lt", "lhs": [1, 2, 3, 4, 5, 6, 7, 8], "rhs": [5] * 8,
+         "lhs_valid": [1] * 8, "rhs_valid": [1] * 8, "expected_data": [1, 1, 1, 1, 0, 0, 0, 0],
+         "expected_valid": [1] * 8},
+        {"name": "eq_with_nulls", "source": f"{src}:156-183", "op": "Eq", "lhs": [10] * 4, "rhs": [10] * 4,
+         "lhs_valid": [0, 0, 1, 1], "rhs_valid": [1] * 4, "expected_data": [0, 0, 1, 1], "expected_valid": [0, 0, 1, 1]},
+        {"name": "lt_scalar_basic", "source": f"{src}:186-208", "op": "Lt", "lhs": list(range(8)), "scalar": 4,
+         "lhs_valid": [1] * 8, "expected_data": [1, 1, 1, 1, 0, 0, 0, 0], "expected_valid": [1] * 8},
+        {"name": "scalar_with_nulls", "source": f"{src}:211-237", "op": "Lt", "lhs": list(range(8)), "scalar": 5,
+         "lhs_valid": [1, 0, 1, 0, 1, 0, 1, 0], "expected_data": [1, 0, 1, 0, 1, 0, 0, 0],
+         "expected_valid": [1, 0, 1, 0, 1, 0, 1, 0]},
+        {"name": "unaligned_row_count", "source": f"{src}:344-387", "op": "Lt", "lhs": list(range(13)), "rhs": [6] * 13,
+         "lhs_valid": [1] * 13, "rhs_valid": [1] * 13, "expected_data": [1] * 6 + [0] * 7, "expected_valid": [1] * 13},
+        {"name": "extreme_values", "source": f"{src}:501-528", "op": "Lt", "lhs": [lo, -1, 0, 1, hi], "rhs": [0] * 5,
+         "lhs_valid": [1] * 5, "rhs_valid": [1] * 5, "expected_data": [1, 1, 0, 0, 0], "expected_valid": [1] * 5},
+    ]
+    return cases
+
+
+def pipeline_cases() -> list[dict]:
+    """crates/polars-metal-kernels/tests/test_groupby_pipeline.rs known answers (sum and len of an
+    i64 column per i64 key; the empty input; a single row). Expected rows in key order."""
+    src = "crates/polars-metal-kernels/tests/test_groupby_pipeline.rs"
+    n = 1024
+    return [
+        {"name": "four_groups_single_i64_key", "source": f"{src}:244-316",
+         "columns": {"a": {"dtype": "I64", "values": [i % 4 for i in range(n)]},
+                     "v": {"dtype": "I64", "values": list(range(n))}},
+         "keys": ["a"], "aggs": [["Sum", "v", "s"], ["Len", None, "n"]],
+         "expected": {"a": [0, 1, 2, 3], "s": [sum(i for i in range(n) if i % 4 == k) for k in range(4)],
+                      "n": [256] * 4},
+         "dtypes": {"a": "I64", "s": "I64", "n": "U32"}},
+        {"name": "empty_input", "source": f"{src}:319-359",
+         "columns": {"k": {"dtype": "I64", "values": []}, "v": {"dtype": "I64", "values": []}},
+         "keys": ["k"], "aggs": [["Sum", "v", "s"]], "expected": {"k": [], "s": []},
+         "dtypes": {"k": "I64", "s": "I64"}},
+        {"name": "single_row", "source": f"{src}:362-407",
+         "columns": {"k": {"dtype": "I64", "values": [42]}, "v": {"dtype": "I64", "values": [100]}},
+         "keys": ["k"], "aggs": [["Sum", "v", "s"]], "expected": {"k": [42], "s": [100]},
+         "dtypes": {"k": "I64", "s": "I64"}},
+    ]
+
+
+def compact_cases() -> list[dict]:
+    """crates/polars-metal-kernels/tests/test_compaction_pipeline.rs known answers: columns
+    compacted by a predicate bitmap (keep = data & valid). `columns` holds the inputs; the expected
+    kept values follow each test's assertions (a `formula` stands for a long closed form)."""
+    src = "crates/polars-metal-kernels/tests/test_compaction_pipeline.rs"
+    even = [1, 0] * 8
+    nan_ = nan()
+    return [
+        {"name": "i64_basic", "source": f"{src}:139-161", "columns": {"a": {"dtype": "I64", "values": list(range(16))}},
+         "pred_data": even, "pred_valid": [1] * 16, "expected": {"a": list(range(0, 16, 2))}},
+        {"name": "i64_empty_result", "source": f"{src}:164-183", "columns": {"a": {"dtype": "I64", "values": list(range(8))}},
+         "pred_data": [0] * 8, "pred_valid": [1] * 8, "expected": {"a": []}},
+        {"name": "i64_all_kept", "source": f"{src}:208-227", "columns": {"a": {"dtype": "I64", "values": list(range(16))}},
+         "pred_data": [1] * 16, "pred_valid": [1] * 16, "expected": {"a": list(range(16))}},
+        {"name": "i64_threadgroup_boundary_10k", "source": f"{src}:230-259", "formula": "keep_mod3", "n": 10_000},
+        {"name": "reusable_across_columns", "source": f"{src}:262-295",
+         "columns": {"a": {"dtype": "I64", "values": list(range(16))},
+                     "b": {"dtype": "I64", "values": list(range(100, 116))}},
+         "pred_data": even, "pred_valid": [1] * 16,
+         "expected": {"a": list(range(0, 16, 2)), "b": list(range(100, 116, 2))}},
+        {"name": "f64_preserves_nan", "source": f"{src}:298-326",
+         "columns": {"a": {"dtype": "F64", "values": [1.0, nan_, 3.0, nan_]}},
+         "pred_data": [1] * 4, "pred_valid": [1] * 4, "expected": {"a": [1.0, nan_, 3.0, nan_]}},
+        {"name": "bool_round_trips", "source": f"{src}:329-349",
+         "columns": {"a": {"dtype": "Bool", "values": [0, 0, 1, 0, 1, 1, 0, 1]}},
+         "pred_data": [1] * 8, "pred_valid": [1] * 8, "expected": {"a": [False, False, True, False, True, True, False, True]}},
+        {"name": "i64_single_row", "source": f"{src}:352-374", "columns": {"a": {"dtype": "I64", "values": [42]}},
+         "pred_data": [1], "pred_valid": [1], "expected": {"a": [42]}},
+        {"name": "null_predicate_drops_row", "source": f"{src}:377-401",
+         "columns": {"a": {"dtype": "I64", "values": [10, 20, 30, 40]}},
+         "pred_data": [1, 1, 1, 1], "pred_valid": [0, 1, 0, 1], "expected": {"a": [20, 40]}},
+    ]
+
+
 def main():
     doc = {"groupby": groupby_cases(), "integration": integration_cases(), "compare": compare_cases(),
            "kleene": kleene_cases(), "sort": sort_cases(),
-           "expression": expression_cases()}
+           "expression": expression_cases(), "compare_i64": compare_i64_cases(), "pipeline": pipeline_cases(),
+           "compact": compact_cases()}
     # the all-unique case is large; keep only its shape and check it by property
     for c in doc["integration"]:
         if c["formula"] == "all_unique":

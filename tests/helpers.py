@@ -11,6 +11,7 @@ Rows are sorted by the key columns (nulls first) before comparison.
 from __future__ import annotations
 
 import json
+import math
 import sys
 from pathlib import Path
 
@@ -206,3 +207,34 @@ def expected_to_result(case: dict) -> dict:
         valid.append(pack(mask))
         dtypes.append(dt)
     return {"n_groups": n, "names": names, "dtypes": dtypes, "data": data, "validity": valid}
+
+
+def compact_case_inputs(case: dict):
+    """A compaction golden case -> (columns {name: (data, validity | None, dtype, n)}, keep data
+    bits, keep validity bits, n); `keep_mod3` is the closed form of the 10k-row case."""
+    if case.get("formula") == "keep_mod3":
+        n = case["n"]
+        r = np.arange(n)
+        return {"a": (r.astype(np.int64), None, A.I64, n)}, list((r % 3 == 0).astype(int)), [1] * n, n
+    cols = case_columns(case)
+    n = len(case["pred_data"])
+    return cols, case["pred_data"], case["pred_valid"], n
+
+
+def compact_case_expected(case: dict) -> dict:
+    if case.get("formula") == "keep_mod3":
+        return {"a": list(range(0, case["n"], 3))}
+    return case["expected"]
+
+
+def same_values(got: list, want: list) -> bool:
+    """Element-wise equality with NaN equal to NaN."""
+    if len(got) != len(want):
+        return False
+    for g, w in zip(got, want):
+        if isinstance(w, float) and math.isnan(w):
+            if not (isinstance(g, float) and math.isnan(g)):
+                return False
+        elif g != w:
+            return False
+    return True

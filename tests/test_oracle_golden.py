@@ -8,6 +8,7 @@ import pytest
 from helpers import (assert_results_match, case_columns, expected_to_result, formula_columns, load_golden, pack,
                      unpack)
 from oracle import pyoracle
+from polars_b200 import _abi as A
 
 GOLD = load_golden()
 
@@ -104,3 +105,39 @@ def test_oracle_exact_sum_beats_naive_on_cancellation():
     got = pyoracle.groupby({"k": (np.zeros(v.size, np.int32), None), "v": (v, None)}, ["k"], [("Sum", "v", "s")])
     assert got["data"][1][0] == 2000.0
     assert math.fsum(v) == 2000.0
+
+
+@pytest.mark.parametrize("case", GOLD["compare_i64"], ids=lambda c: c["name"])
+def test_oracle_compare_i64_known_answers(case):
+    n = len(case["lhs"])
+    cols = {"l": (np.array(case["lhs"], np.int64), pack(case["lhs_valid"]))}
+    rhs = {"kind": "LiteralI64", "value": case["scalar"]} if "scalar" in case else {"kind": "Column", "name": "r"}
+    if "rhs" in case:
+        cols["r"] = (np.array(case["rhs"], np.int64), pack(case["rhs_valid"]))
+    pred = {"kind": "Compare", "op": case["op"], "dtype": "I64", "lhs": {"kind": "Column", "name": "l"}, "rhs": rhs}
+    d, v = pyoracle.predicate_bits(cols, pred)
+    valid = list(unpack(v, n).astype(int))
+    assert valid == case["expected_valid"]
+    assert [b for b, ok in zip(unpack(d, n).astype(int), valid) if ok] == \
+        [b for b, ok in zip(case["expected_data"], valid) if ok]
+
+
+@pytest.mark.parametrize("case", GOLD["pipeline"], ids=lambda c: c["name"])
+def test_oracle_pipeline_known_answers(case):
+    got = pyoracle.groupby(case_columns(case), case["keys"], [tuple(a) for a in case["aggs"]])
+    assert_results_match(got, expected_to_result(case), len(case["keys"]), case["aggs"], case["name"])
+
+
+@pytest.mark.parametrize("case", GOLD["compact"], ids=lambda c: c["name"])
+def test_oracle_compaction_known_answers(case):
+    from helpers import compact_case_expected, compact_case_inputs, same_values
+
+    cols, pd, pv, n = compact_case_inputs(case)
+    keep = np.array(pd, bool) & np.array(pv, bool)
+    n_out, out = pyoracle.filter_compact(keep, cols)
+    want = compact_case_expected(case)
+    assert n_out == len(next(iter(want.values())))
+    for (name, vals), (dt, data, valid) in zip(want.items(), out):
+        got = list(unpack(data, n_out)) if dt == A.BOOL else list(np.asarray(data)[:n_out])
+        assert same_values([x.item() if hasattr(x, "item") else x for x in got], vals), name
+        assert unpack(valid, n_out).all()
