@@ -536,11 +536,33 @@ def compact_cases() -> list[dict]:
     ]
 
 
+def sort_build_cases() -> list[dict]:
+    """The sort build's known answers (crates/polars-metal-kernels/tests/test_groupby_segment.rs,
+    test_groupby_build_sort_reference.rs): group counts of key lanes, here as an Int64 key column
+    with the rows per group (Len), expected in key order."""
+    seg = "crates/polars-metal-kernels/tests/test_groupby_segment.rs"
+    ref = "crates/polars-metal-kernels/tests/test_groupby_build_sort_reference.rs"
+
+    def case(name, source, keys):
+        ks = sorted(set(keys))
+        return {"name": name, "source": source, "columns": {"k": {"dtype": "I64", "values": keys}},
+                "keys": ["k"], "aggs": [["Len", None, "n"]],
+                "expected": {"k": ks, "n": [keys.count(k) for k in ks]}, "dtypes": {"k": "I64", "n": "U32"}}
+
+    return [
+        case("empty_input", f"{seg}:9-14", []),
+        case("all_same_100", f"{seg}:17-23", [42] * 100),
+        case("all_distinct_200", f"{seg}:26-31", list(range(200))),
+        case("all_unique_1000", f"{ref}:10-14", list(range(1000))),
+        case("duplicates_collapsed", f"{ref}:25-33", [10, 20, 10, 30, 20, 10]),
+    ]
+
+
 def main():
     doc = {"groupby": groupby_cases(), "integration": integration_cases(), "compare": compare_cases(),
            "kleene": kleene_cases(), "sort": sort_cases(),
            "expression": expression_cases(), "compare_i64": compare_i64_cases(), "pipeline": pipeline_cases(),
-           "compact": compact_cases()}
+           "compact": compact_cases(), "sort_build": sort_build_cases()}
     # the all-unique case is large; keep only its shape and check it by property
     for c in doc["integration"]:
         if c["formula"] == "all_unique":

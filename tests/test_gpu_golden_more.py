@@ -57,3 +57,11 @@ def test_compaction_known_answers(case):
         assert same_values(got, vals), name
         if n_out:
             assert unpack(np.frombuffer(vbytes, np.uint8), n_out).all()
+
+
+@pytest.mark.parametrize("strategy", ["sort", "partitioned", "global_hash", "smem_hash"])
+@pytest.mark.parametrize("case", GOLD["sort_build"], ids=lambda c: c["name"])
+def test_sort_build_known_answers(case, strategy):
+    cols = {k: N.ColumnData(v[0], v[1], dtype=v[2], length=v[3]) for k, v in case_columns(case).items()}
+    got = N.groupby(cols, case["keys"], [tuple(a) for a in case["aggs"]], strategy=strategy)
+    assert_results_match(as_dict(got), expected_to_result(case), 1, case["aggs"], f"{case['name']} {strategy}")

@@ -141,3 +141,9 @@ def test_oracle_compaction_known_answers(case):
         got = list(unpack(data, n_out)) if dt == A.BOOL else list(np.asarray(data)[:n_out])
         assert same_values([x.item() if hasattr(x, "item") else x for x in got], vals), name
         assert unpack(valid, n_out).all()
+
+
+@pytest.mark.parametrize("case", GOLD["sort_build"], ids=lambda c: c["name"])
+def test_oracle_sort_build_known_answers(case):
+    got = pyoracle.groupby(case_columns(case), case["keys"], [tuple(a) for a in case["aggs"]])
+    assert_results_match(got, expected_to_result(case), 1, case["aggs"], case["name"])
