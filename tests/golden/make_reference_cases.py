@@ -533,6 +533,19 @@ def compact_cases() -> list[dict]:
         {"name": "null_predicate_drops_row", "source": f"{src}:377-401",
          "columns": {"a": {"dtype": "I64", "values": [10, 20, 30, 40]}},
          "pred_data": [1, 1, 1, 1], "pred_valid": [0, 1, 0, 1], "expected": {"a": [20, 40]}},
+        # test_filter_scatter_f64.rs / test_filter_scatter_bool.rs: source nulls keep their place
+        {"name": "f64_null_inputs_stay_null", "source": "crates/polars-metal-kernels/tests/test_filter_scatter_f64.rs:220-245",
+         "columns": {"a": {"dtype": "F64", "values": [i * 1.5 for i in range(8)], "valid": [1, 1, 0, 1, 1, 0, 1, 1]}},
+         "pred_data": [1] * 8, "pred_valid": [1] * 8,
+         "expected": {"a": [0.0, 1.5, None, 4.5, 6.0, None, 9.0, 10.5]}},
+        {"name": "bool_null_propagates", "source": "crates/polars-metal-kernels/tests/test_filter_scatter_bool.rs:151-189",
+         "columns": {"a": {"dtype": "Bool", "values": [1] * 8, "valid": [1, 1, 0, 1, 1, 0, 1, 1]}},
+         "pred_data": [1] * 8, "pred_valid": [1] * 8,
+         "expected": {"a": [True, True, None, True, True, None, True, True]}},
+        {"name": "bool_unaligned_row_count", "source": "crates/polars-metal-kernels/tests/test_filter_scatter_bool.rs:404-440",
+         "columns": {"a": {"dtype": "Bool", "values": [0, 1, 0, 1, 0, 1, 0, 1, 1, 1, 1, 0, 0]}},
+         "pred_data": [1] * 13, "pred_valid": [1] * 13,
+         "expected": {"a": [False, True, False, True, False, True, False, True, True, True, True, False, False]}},
     ]
 
 
