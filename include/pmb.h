@@ -365,14 +365,20 @@ int pmb_bool_or(pmb_handle* h, const uint8_t* lhs_data, const uint8_t* lhs_valid
                 uint8_t* out_valid, int32_t on_device);
 
 /* One arithmetic expression of columns and literals (PMB_EXPR_COLUMN, _LIT_I64, _LIT_F64 and
- * _ARITH nodes, at most 8 levels and 32 nodes) evaluated for every row into `out_data` (8 bytes a
- * row) and `out_valid` (a bit-packed bitmap): the input column of an expression aggregate.
- * `*out_dtype` receives PMB_F64 when a float column, a float literal or a true division takes
- * part, else PMB_I64 (wrapping). A null operand, or an integer // or % by zero, gives null.
+ * _ARITH nodes, at most 8 levels and 32 nodes) evaluated for every row into `out_data` and
+ * `out_valid` (a bit-packed bitmap): the input column of an expression aggregate. Types follow
+ * Polars: each node computes in the supertype of its operands (literals take the other operand's
+ * type; an integer true division is Float64), wrapping or rounding to it, and `*out_dtype`
+ * receives the root's type; `out_data` holds one value of that type a row (allocate 8 bytes a row
+ * to take any). A null operand, or an integer // or % by zero, gives null.
  * Replaces the expression side of the reference's Expression aggregations
  * (crates/polars-metal-core/src/udf/groupby/mod.rs:266-352, python/polars_metal/_walker.py:1205-1278). */
 int pmb_eval_expr(pmb_handle* h, const pmb_expr* expr, const pmb_column* cols, int32_t n_cols, void* out_data,
                   uint8_t* out_valid, int32_t out_on_device, int32_t* out_dtype);
+
+/* The type pmb_eval_expr gives an expression over these columns (only their dtypes are read); no
+ * GPU is touched and no handle is needed. PMB_E_INVALID for an expression pmb_eval_expr refuses. */
+int pmb_expr_dtype(const pmb_expr* expr, const pmb_column* cols, int32_t n_cols, int32_t* out_dtype);
 
 /* Stream compaction of `cols` by a bit-packed predicate (keep = data & valid).
  * Replaces `_native.execute_filter_compact(pred_data, pred_valid, n_rows, columns)`

@@ -235,6 +235,7 @@ SIGNATURES = {
                                      C.POINTER(C.POINTER(Result))]),
     "pmb_eval_expr": (C.c_int, [_H, C.POINTER(Expr), C.POINTER(Column), C.c_int32, _P, _P, C.c_int32,
                                 C.POINTER(C.c_int32)]),
+    "pmb_expr_dtype": (C.c_int, [C.POINTER(Expr), C.POINTER(Column), C.c_int32, C.POINTER(C.c_int32)]),
     "pmb_compare": (C.c_int, [_H, C.POINTER(Column), C.POINTER(Column), C.c_int64, C.c_double, C.c_int32, _P, _P,
                               C.c_int32]),
     "pmb_bool_and": (C.c_int, [_H, _P, _P, _P, _P, C.c_int64, _P, _P, C.c_int32]),

@@ -366,11 +366,25 @@ def _arith_wire(e: dict) -> dict:
     raise ValueError(f"polars_b200: plan parse error: unknown op expr kind={kind}")
 
 
+def expr_dtype(columns: dict[str, ColumnData | Any], expr: dict) -> int:
+    """The dtype eval_expr gives `expr` over these columns (pmb_expr_dtype; no GPU work)."""
+    names = list(columns)
+    cols = [c if isinstance(c, ColumnData) else ColumnData(c) for c in columns.values()]
+    abi, keep = _to_abi_columns(cols)
+    e, ek = compile_predicate(_arith_wire(expr), {nm: i for i, nm in enumerate(names)})
+    dt = C.c_int32()
+    if A.lib().pmb_expr_dtype(C.byref(e), abi, len(cols), C.byref(dt)) != A.PMB_OK:
+        raise ValueError("polars_b200: not an arithmetic expression of these columns")
+    del keep, ek
+    return dt.value
+
+
 def eval_expr(columns: dict[str, ColumnData | Any], expr: dict, handle: Handle | None = None) -> ColumnData:
-    """An arithmetic expression of the columns, evaluated on the GPU for every row (pmb_eval_expr):
-    Float64 when a float takes part or there is a true division, else Int64; null where an operand
-    is null or an integer // or % divides by zero. The new column is a CUDA tensor when an input
-    column is one, else a numpy array."""
+    """An arithmetic expression of the columns, evaluated on the GPU for every row (pmb_eval_expr),
+    typed as Polars types it (operands cast to their supertype, literals take the other side's
+    type, integer true division gives Float64; 32-bit results wrap or round as Polars' do); null
+    where an operand is null or an integer // or % divides by zero. The new column is a CUDA tensor
+    when an input column is one, else a numpy array."""
     h = handle or default_handle()
     names = list(columns)
     if not names:
@@ -393,8 +407,10 @@ def eval_expr(columns: dict[str, ColumnData | Any], expr: dict, handle: Handle |
     dt = C.c_int32()
     h.check(h._lib.pmb_eval_expr(h.raw, C.byref(e), abi, len(cols), dp, vp, 1 if dev is not None else 0, C.byref(dt)))
     del keep, ek
-    if dt.value == A.F64:
-        data = data.view(torch.float64) if dev is not None else data.view(np.float64)
+    if dev is not None:
+        data = data.view(getattr(torch, A.NUMPY_NAME[dt.value]))
+    else:
+        data = data.view(A.NUMPY_NAME[dt.value])
     return ColumnData(data, valid, dtype=dt.value, length=n)
 
 

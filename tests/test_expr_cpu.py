@@ -67,3 +67,61 @@ def test_oracle_pinned_to_the_reference_expression_cases(case):
     got = [float(res["data"][1][i]) for i in order]
     want = case["expected"][agg["output_alias"]]
     assert all(math.isclose(g, w, rel_tol=1e-12) for g, w in zip(got, want)), (got, want)
+
+
+def _c(dtype, n=4):
+    import numpy as np
+
+    return np.zeros(n, dtype)
+
+
+def _bin(op, lhs, rhs):
+    return {"kind": "Arith", "op": op, "lhs": lhs, "rhs": rhs}
+
+
+@pytest.mark.parametrize("a,b,op,want", [
+    ("int32", "int32", "Mul", "I32"), ("int32", "float64", "Mul", "F64"), ("float32", "float32", "Mul", "F32"),
+    ("float32", "int16", "Add", "F32"), ("float32", "int32", "Add", "F64"), ("int8", "uint8", "Add", "I16"),
+    ("int32", "uint32", "Sub", "I64"), ("int64", "uint64", "Add", "F64"), ("uint16", "uint8", "Add", "U16"),
+    ("int64", "int32", "TrueDiv", "F64"), ("float32", "float32", "TrueDiv", "F32"), ("int32", "int32", "FloorDiv", "I32"),
+    ("uint64", "uint32", "Mod", "U64"),
+])
+def test_expression_types_follow_polars(a, b, op, want):
+    from polars_b200 import _abi as A
+    from polars_b200._native import expr_dtype
+
+    got = expr_dtype({"a": _c(a), "b": _c(b)}, _bin(op, col("a"), col("b")))
+    assert got == A.TAG_TO_DTYPE[want]
+
+
+def test_literals_take_the_other_operands_type():
+    from polars_b200 import _abi as A
+    from polars_b200._native import expr_dtype
+
+    cols = {"u": _c("uint16"), "f": _c("float32"), "i": _c("int32")}
+    lit_i = {"kind": "LiteralI64", "value": 7}
+    lit_f = {"kind": "LiteralF64", "value": 1.5}
+    assert expr_dtype(cols, _bin("Sub", col("u"), lit_i)) == A.U16
+    assert expr_dtype(cols, _bin("Mul", col("f"), lit_f)) == A.F32
+    assert expr_dtype(cols, _bin("Mul", col("i"), lit_f)) == A.F64
+    assert expr_dtype(cols, _bin("Mul", _bin("Add", lit_i, lit_i), col("i"))) == A.I32
+    assert expr_dtype(cols, _bin("TrueDiv", col("i"), lit_i)) == A.F64
+    assert expr_dtype(cols, _bin("Add", lit_i, lit_i)) == A.I32
+    # the reference's Q1 shape over Float32 columns stays Float32
+    assert expr_dtype(cols, _bin("Mul", col("f"), _bin("Sub", lit_f, col("f")))) == A.F32
+
+
+def test_bool_columns_and_deep_trees_are_refused():
+    import numpy as np
+
+    from polars_b200 import _abi as A
+    from polars_b200._native import ColumnData, expr_dtype
+
+    b = ColumnData(np.zeros(1, np.uint8), None, dtype=A.BOOL, length=4)
+    with pytest.raises(ValueError):
+        expr_dtype({"b": b, "i": _c("int32")}, _bin("Add", col("b"), col("i")))
+    e = col("i")
+    for _ in range(9):
+        e = _bin("Add", e, {"kind": "LiteralI64", "value": 1})
+    with pytest.raises(ValueError):
+        expr_dtype({"i": _c("int32")}, e)

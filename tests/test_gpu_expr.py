@@ -119,3 +119,50 @@ def test_reference_expression_cases_through_the_wire(case):
     assert k[order].tolist() == case["expected"]["k"]
     want = case["expected"][case["aggs"][0]["output_alias"]]
     assert all(math.isclose(g, w, rel_tol=1e-12) for g, w in zip(s[order].tolist(), want)), (s[order], want)
+
+
+def _bin(op, lhs, rhs):
+    return {"kind": "Arith", "op": op, "lhs": lhs, "rhs": rhs}
+
+
+def test_polars_types_wrap_and_round_on_the_gpu():
+    # 32-bit integer products wrap, Float32 arithmetic rounds at every node, a UInt16 minus a
+    # literal wraps: as numpy (and Polars) compute them in those types
+    rng = np.random.default_rng(31)
+    n = 100_003
+    a = rng.integers(-2**31, 2**31, n).astype(np.int32)
+    b = rng.integers(-2**31, 2**31, n).astype(np.int32)
+    fa = rng.standard_normal(n).astype(np.float32)
+    fb = rng.standard_normal(n).astype(np.float32)
+    u = rng.integers(0, 20, n).astype(np.uint16)
+    s = rng.integers(-300, 300, n).astype(np.int16)
+    cols = {"a": a, "b": b, "fa": fa, "fb": fb, "u": u, "s": s}
+    lit = {"kind": "LiteralF64", "value": 1.5}
+    seven = {"kind": "LiteralI64", "value": 7}
+    cases = [
+        (_bin("Mul", col("a"), col("b")), A.I32, a * b),
+        (_bin("Mul", col("fa"), col("fb")), A.F32, fa * fb),
+        (_bin("Mul", col("fa"), _bin("Sub", lit, col("fb"))), A.F32, fa * (np.float32(1.5) - fb)),
+        (_bin("Sub", col("u"), seven), A.U16, u - np.uint16(7)),
+        (_bin("Mul", col("s"), col("fa")), A.F32, s.astype(np.float32) * fa),
+    ]
+    for e, dt, want in cases:
+        out = N.eval_expr(cols, e)
+        assert out.dtype == dt
+        got = np.asarray(out.data)[:n]
+        assert got.dtype == want.dtype and np.array_equal(got, want), e
+        assert np.unpackbits(np.asarray(out.validity), bitorder="little")[:n].all()
+
+
+def test_reference_fused_float32_sum_of_products():
+    # crates/polars-metal-kernels/tests/test_dispatch_groupby_fused.rs:185-260: sum(a * b) per
+    # i % 4 over Float32 columns a = i * 0.1, b = i * 0.05 + 1, 6000 rows
+    n = 6000
+    i = np.arange(n)
+    k = (i % 4).astype(np.int32)
+    fa = (i.astype(np.float32) * np.float32(0.1)).astype(np.float32)
+    fb = (i.astype(np.float32) * np.float32(0.05) + np.float32(1.0)).astype(np.float32)
+    got = N.groupby({"k": k, "a": fa, "b": fb}, ["k"], [("Sum", _bin("Mul", col("a"), col("b")), "sum_ab")])
+    want = pyoracle.groupby({"k": (k, None), "ab": (fa * fb, None)}, ["k"], [("Sum", "ab", "sum_ab")])
+    assert got.dtypes[1] == A.F32
+    assert_results_match(as_dict(got), want, 1, [("Sum", "ab", "sum_ab")], "f32 sum of products")
