@@ -571,11 +571,29 @@ def sort_build_cases() -> list[dict]:
     ]
 
 
+def predicate_mask_cases() -> list[dict]:
+    """crates/polars-metal-kernels/tests/test_filter_predicate.rs: a predicate's (data, valid) bits
+    to the keep mask, keep = data & valid, bits past the last row ignored."""
+    src = "crates/polars-metal-kernels/tests/test_filter_predicate.rs"
+    return [
+        {"name": "all_true_no_nulls", "source": f"{src}:31-43", "data": [1] * 16, "valid": [1] * 16,
+         "n": 16, "expected": [1] * 16},
+        {"name": "null_rows_mask_to_zero", "source": f"{src}:46-54", "data": [1] * 8, "valid": [1, 1, 1, 1, 0, 0, 0, 0],
+         "n": 8, "expected": [1, 1, 1, 1, 0, 0, 0, 0]},
+        {"name": "false_rows_mask_to_zero", "source": f"{src}:57-65", "data": [1, 1, 1, 1, 0, 0, 0, 0], "valid": [1] * 8,
+         "n": 8, "expected": [1, 1, 1, 1, 0, 0, 0, 0]},
+        {"name": "empty_input", "source": f"{src}:68-78", "data": [], "valid": [], "n": 0, "expected": []},
+        {"name": "padding_bits_ignored", "source": f"{src}:81-96", "data": [1, 0, 1, 1, 1, 1, 0, 1], "valid": [1] * 8,
+         "n": 7, "expected": [1, 0, 1, 1, 1, 1, 0]},
+    ]
+
+
 def main():
     doc = {"groupby": groupby_cases(), "integration": integration_cases(), "compare": compare_cases(),
            "kleene": kleene_cases(), "sort": sort_cases(),
            "expression": expression_cases(), "compare_i64": compare_i64_cases(), "pipeline": pipeline_cases(),
-           "compact": compact_cases(), "sort_build": sort_build_cases()}
+           "compact": compact_cases(), "sort_build": sort_build_cases(),
+           "predicate_mask": predicate_mask_cases()}
     # the all-unique case is large; keep only its shape and check it by property
     for c in doc["integration"]:
         if c["formula"] == "all_unique":

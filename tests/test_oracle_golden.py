@@ -149,3 +149,13 @@ def test_oracle_compaction_known_answers(case):
 def test_oracle_sort_build_known_answers(case):
     got = pyoracle.groupby(case_columns(case), case["keys"], [tuple(a) for a in case["aggs"]])
     assert_results_match(got, expected_to_result(case), 1, case["aggs"], case["name"])
+
+
+@pytest.mark.parametrize("case", GOLD["predicate_mask"], ids=lambda c: c["name"])
+def test_oracle_predicate_mask_known_answers(case):
+    # the oracle's compaction keeps exactly the rows of keep = data & valid (row ids carried along)
+    n = case["n"]
+    keep = np.array(case["data"][:n], bool) & np.array(case["valid"][:n], bool)
+    n_out, out = pyoracle.filter_compact(keep, {"rid": (np.arange(n, dtype=np.int64), None)})
+    assert n_out == sum(case["expected"])
+    assert list(np.asarray(out[0][1])[:n_out]) == [i for i, k in enumerate(case["expected"]) if k]
