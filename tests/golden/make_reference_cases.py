@@ -588,12 +588,134 @@ def predicate_mask_cases() -> list[dict]:
     ]
 
 
+def polars_shape_cases() -> list[dict]:
+    """Engine-vs-Polars cases of the reference's Python integration tests with closed-form inputs
+    (small integer keys, string keys, several chunks, filter edges). A case gives its table as
+    `chunks` (a list of column dicts, each list one chunk; None is a null), the query (`keys`,
+    `aggs`, optional `predicate` in the wire shape, or `filter` alone), and the expected rows in the
+    order the test sorts them (`expected`, by column). Float sums are exact sums (math.fsum). A long
+    column is a generator: {"gen": "mod", "m", "n"} is i % m, {"gen": "scale", "c", "n"} is i * c,
+    {"gen": "tile", "values", "times"} repeats the values, and `chunk_rows` cuts a generated table
+    into chunks of that many rows (tests/helpers.py shape_table builds them)."""
+    it = "tests/python_integration"
+    cases = []
+
+    def grouped(rows, keyf, vals, n_keys=1):
+        out = {}
+        for r in rows:
+            out.setdefault(keyf(r), []).append(vals(r))
+        return out
+
+    def sort_key(k):
+        return tuple((0, "") if x is None else (1, x) for x in (k if isinstance(k, tuple) else (k,)))
+
+    n = 10_000
+    for tag, src in (("Int8", "22-23"), ("Int16", "26-27"), ("Int32", "30-32"), ("UInt8", "35-36")):
+        g = grouped(range(n), lambda i: i % 4, lambda i: i * 1.5)
+        ks = sorted(g)
+        cases.append({"name": f"small_int_key_{tag}", "source": f"{it}/test_groupby_small_int_keys.py:{src}",
+                      "chunks": [{"k": {"gen": "mod", "m": 4, "n": n}, "v": {"gen": "scale", "c": 1.5, "n": n}}],
+                      "dtypes": {"k": tag, "v": "Float64"}, "keys": ["k"], "aggs": [["Sum", "v", "v"], ["Len", None, "len"]],
+                      "expected": {"k": ks, "v": [math.fsum(g[k]) for k in ks], "len": [len(g[k]) for k in ks]}})
+    g = grouped(range(n), lambda i: (i % 4, i % 8), lambda i: i * 1.5)
+    ks = sorted(g)
+    cases.append({"name": "u16_u32_mixed_keys", "source": f"{it}/test_groupby_small_int_keys.py:39-49",
+                  "chunks": [{"k1": {"gen": "mod", "m": 4, "n": n}, "k2": {"gen": "mod", "m": 8, "n": n},
+                              "v": {"gen": "scale", "c": 1.5, "n": n}}],
+                  "dtypes": {"k1": "UInt16", "k2": "UInt32", "v": "Float64"}, "keys": ["k1", "k2"], "aggs": [["Sum", "v", "v"]],
+                  "expected": {"k1": [a for a, _ in ks], "k2": [b for _, b in ks], "v": [math.fsum(g[k]) for k in ks]}})
+
+    def string_case(name, src, pattern, times, keys, dtypes):
+        cols = {c: vals * times for c, vals in pattern.items()}
+        m = len(cols["v"])
+        g = grouped(range(m), lambda i: tuple(cols[k][i] for k in keys), lambda i: cols["v"][i])
+        ks = sorted(g, key=sort_key)
+        exp = {k: [key[j] for key in ks] for j, k in enumerate(keys)}
+        exp["s"] = [math.fsum(g[key]) for key in ks]
+        chunk = {c: {"gen": "tile", "values": vals, "times": times} for c, vals in pattern.items()}
+        return {"name": name, "source": src, "chunks": [chunk], "dtypes": dtypes, "keys": keys,
+                "aggs": [["Sum", "v", "s"]], "expected": exp}
+
+    cases.append(string_case("string_low_cardinality", f"{it}/test_string_groupby.py:17-27",
+                             {"k": ["A", "B", "A", "C", "B", "A"], "v": [1.0, 2.0, 3.0, 4.0, 5.0, 6.0]}, 1000,
+                             ["k"], {"k": "Utf8", "v": "Float64"}))
+    cases.append(string_case("string_null_keys", f"{it}/test_string_groupby.py:30-40",
+                             {"k": ["A", None, "A", "B", None, "B"], "v": [1.0, 2.0, 3.0, 4.0, 5.0, 6.0]}, 100,
+                             ["k"], {"k": "Utf8", "v": "Float64"}))
+    cases.append(string_case("string_and_int_keys", f"{it}/test_string_groupby.py:43-54",
+                             {"k_s": ["X", "Y", "X", "Z"], "k_i": [1, 2, 1, 3], "v": [1.0, 2.0, 3.0, 4.0]}, 1000,
+                             ["k_s", "k_i"], {"k_s": "Utf8", "k_i": "Int64", "v": "Float64"}))
+
+    def chunked_case(name, src, chunks, dtypes, predicate=None, keep=lambda v: True):
+        ks_all = [k for c in chunks for k in c["k"]]
+        vs_all = [v for c in chunks for v in c["v"]]
+        g = grouped([i for i in range(len(vs_all)) if keep(vs_all[i])], lambda i: ks_all[i], lambda i: vs_all[i])
+        ks = sorted(g, key=sort_key)
+        case = {"name": name, "source": src, "chunks": chunks, "dtypes": dtypes, "keys": ["k"],
+                "aggs": [["Sum", "v", "s"]], "expected": {"k": ks, "s": [math.fsum(g[k]) for k in ks]}}
+        if predicate:
+            case["predicate"] = predicate
+        return case
+
+    cases.append(chunked_case("two_chunks", f"{it}/test_multichunk.py:19-29",
+                              [{"k": [0, 0, 1, 1], "v": [1.0, 2.0, 3.0, 4.0]}, {"k": [0, 1, 0, 1], "v": [5.0, 6.0, 7.0, 8.0]}],
+                              {"k": "Int64", "v": "Float64"}))
+    c = chunked_case("thousand_chunks", f"{it}/test_multichunk.py:32-41",
+                     [{"k": [i % 4], "v": [float(i)]} for i in range(1000)], {"k": "Int64", "v": "Float64"})
+    # stored as one generated table cut into 1000 one-row chunks
+    c["chunks"] = [{"k": {"gen": "mod", "m": 4, "n": 1000}, "v": {"gen": "scale", "c": 1.0, "n": 1000}}]
+    c["chunk_rows"] = 1
+    cases.append(c)
+    cases.append(chunked_case("string_keys_two_chunks", f"{it}/test_multichunk.py:44-54",
+                              [{"k": ["A", "A", "B"], "v": [1.0, 2.0, 3.0]}, {"k": ["B", "C", "A"], "v": [4.0, 5.0, 6.0]}],
+                              {"k": "Utf8", "v": "Float64"}))
+    cases.append(chunked_case("filter_two_chunks", f"{it}/test_multichunk.py:57-67",
+                              [{"k": [0, 1, 2, 0], "v": [10.0, 20.0, 30.0, 40.0]}, {"k": [1, 2, 0, 1], "v": [50.0, 60.0, 70.0, 80.0]}],
+                              {"k": "Int64", "v": "Float64"},
+                              predicate={"kind": "Compare", "op": "Gt", "dtype": "F64", "lhs": {"kind": "Column", "name": "v"},
+                                         "rhs": {"kind": "LiteralF64", "value": 25.0}},
+                              keep=lambda v: v > 25.0))
+
+    # test_filter_edges.py: top-level filters; `expected` = the kept rows of every column
+    fe = f"{it}/test_filter_edges.py"
+
+    def col_(c):
+        return {"kind": "Column", "name": c}
+
+    def cmp_(op, l, r, dt):
+        return {"kind": "Compare", "op": op, "dtype": dt, "lhs": l, "rhs": r}
+
+    def filt(name, src, cols, dtypes, pred, kept_rows):
+        return {"name": name, "source": f"{fe}:{src}", "chunks": [cols], "dtypes": dtypes, "filter": pred,
+                "expected": {c: [cols[c][i] for i in kept_rows] for c in cols}}
+
+    lit0 = {"kind": "LiteralI64", "value": 0}
+    cases += [
+        filt("empty_frame", "23-29", {"a": []}, {"a": "Int64"}, cmp_("Gt", col_("a"), lit0, "I64"), []),
+        filt("single_row_true", "32-36", {"a": [5], "mask": [True]}, {"a": "Int64", "mask": "Bool"}, col_("mask"), [0]),
+        filt("single_row_false", "39-43", {"a": [5], "mask": [False]}, {"a": "Int64", "mask": "Bool"}, col_("mask"), []),
+        filt("single_row_null", "46-51", {"a": [5], "mask": [None]}, {"a": "Int64", "mask": "Bool"}, col_("mask"), []),
+        filt("all_null_column", "54-60", {"a": [None] * 4}, {"a": "Int64"}, cmp_("Gt", col_("a"), lit0, "I64"), []),
+        filt("predicate_all_true", "63-70", {"a": [1, 2, 3, 4], "b": [10, 20, 30, 40]}, {"a": "Int64", "b": "Int64"},
+             cmp_("Eq", col_("a"), col_("a"), "I64"), [0, 1, 2, 3]),
+        filt("predicate_all_false", "73-79", {"a": [1, 2, 3, 4], "b": [10, 20, 30, 40]}, {"a": "Int64", "b": "Int64"},
+             cmp_("Ne", col_("a"), col_("a"), "I64"), []),
+        filt("predicate_all_null", "82-93", {"a": [1, 2, 3, 4], "mask": [None] * 4}, {"a": "Int64", "mask": "Bool"},
+             col_("mask"), []),
+        filt("predicate_empty_subset", "95-101", {"a": [1, 2, 3, 4], "b": [10, 20, 30, 40]}, {"a": "Int64", "b": "Int64"},
+             cmp_("Gt", col_("a"), {"kind": "LiteralI64", "value": 1000}, "I64"), []),
+        filt("finite_f64_predicate", "104-110", {"x": [-1.5, 0.0, 1.5, 2.5]}, {"x": "Float64"},
+             cmp_("Gt", col_("x"), {"kind": "LiteralF64", "value": 0.0}, "F64"), [2, 3]),
+    ]
+    return cases
+
+
 def main():
     doc = {"groupby": groupby_cases(), "integration": integration_cases(), "compare": compare_cases(),
            "kleene": kleene_cases(), "sort": sort_cases(),
            "expression": expression_cases(), "compare_i64": compare_i64_cases(), "pipeline": pipeline_cases(),
            "compact": compact_cases(), "sort_build": sort_build_cases(),
-           "predicate_mask": predicate_mask_cases()}
+           "predicate_mask": predicate_mask_cases(), "polars_shapes": polars_shape_cases()}
     # the all-unique case is large; keep only its shape and check it by property
     for c in doc["integration"]:
         if c["formula"] == "all_unique":

@@ -238,3 +238,79 @@ def same_values(got: list, want: list) -> bool:
         elif g != w:
             return False
     return True
+
+
+_PA_TYPES = {"Int8": "int8", "Int16": "int16", "Int32": "int32", "Int64": "int64", "UInt8": "uint8", "UInt16": "uint16",
+             "UInt32": "uint32", "UInt64": "uint64", "Float32": "float32", "Float64": "float64", "Bool": "bool_",
+             "Utf8": "string"}
+
+
+def _gen_column(spec):
+    if isinstance(spec, list):
+        return spec
+    g = spec["gen"]
+    if g == "mod":
+        return [i % spec["m"] for i in range(spec["n"])]
+    if g == "scale":
+        return [i * spec["c"] for i in range(spec["n"])]
+    if g == "tile":
+        return spec["values"] * spec["times"]
+    raise KeyError(g)
+
+
+def shape_table(case: dict):
+    """The pyarrow table of a polars_shapes golden case, with its chunks."""
+    import pyarrow as pa
+
+    names = list(case["dtypes"])
+    types = {n: getattr(pa, _PA_TYPES[case["dtypes"][n]])() for n in names}
+    chunks = {n: [] for n in names}
+    for ch in case["chunks"]:
+        cols = {n: _gen_column(ch[n]) for n in names}
+        rows = case.get("chunk_rows") or max(1, len(cols[names[0]]))
+        total = len(cols[names[0]])
+        for start in range(0, max(total, 1), rows):
+            for n in names:
+                chunks[n].append(pa.array(cols[n][start:start + rows], type=types[n]))
+    return pa.table({n: pa.chunked_array(chunks[n], type=types[n]) for n in names})
+
+
+def arrow_to_oracle_columns(table, dict_columns=()):
+    """Oracle inputs of an Arrow table: numeric columns as (values, validity bitmap | None), Bool
+    columns bit-packed, and the named string columns as their sorted-dictionary codes through the
+    product's host encoder (polars_b200.arrow._dictionary_key). Returns (columns, dictionaries)."""
+    import pyarrow as pa
+
+    from polars_b200.arrow import _dictionary_key
+
+    cols, dicts = {}, {}
+    for name in table.column_names:
+        col = table.column(name)
+        if name in dict_columns:
+            codes, values = _dictionary_key(col)
+            dicts[name] = values
+            arr = codes
+        else:
+            arr = col.combine_chunks() if col.num_chunks else pa.array([], type=col.type)
+        n = len(arr)
+        ok = ~np.asarray(arr.is_null().to_numpy(zero_copy_only=False), bool) if n else np.zeros(0, bool)
+        valid = pack(ok) if arr.null_count else None
+        if pa.types.is_boolean(arr.type):
+            vals = np.asarray(arr.fill_null(False).to_numpy(zero_copy_only=False), bool)
+            cols[name] = (pack(vals), valid, A.BOOL, n)
+        else:
+            np_type = np.dtype(arr.type.to_pandas_dtype())
+            vals = np.asarray(arr.fill_null(0).to_numpy(zero_copy_only=False)).astype(np_type) if n else np.zeros(0, np_type)
+            cols[name] = (vals, valid, {v: k for k, v in A.NUMPY_NAME.items()}[np_type.name], n)
+    return cols, dicts
+
+
+def result_columns(res: dict) -> dict:
+    """Result dict -> {name: list of Python values, None for null}."""
+    n = int(res["n_groups"])
+    out = {}
+    for name, dt, d, v in zip(res["names"], res["dtypes"], res["data"], res["validity"]):
+        vals = unpack(d, n) if dt == A.BOOL else np.asarray(d)[:n]
+        ok = unpack(v, n)
+        out[name] = [vals[i].item() if ok[i] else None for i in range(n)]
+    return out

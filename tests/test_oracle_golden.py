@@ -159,3 +159,40 @@ def test_oracle_predicate_mask_known_answers(case):
     n_out, out = pyoracle.filter_compact(keep, {"rid": (np.arange(n, dtype=np.int64), None)})
     assert n_out == sum(case["expected"])
     assert list(np.asarray(out[0][1])[:n_out]) == [i for i, k in enumerate(case["expected"]) if k]
+
+
+def _rows_sorted(rows):
+    return sorted(rows, key=lambda r: tuple((0, "") if x is None else (1, x) for x in r[:1]) +
+                  tuple((0, "") if x is None else (1, x) for x in r[1:]))
+
+
+@pytest.mark.parametrize("case", GOLD["polars_shapes"], ids=lambda c: c["name"])
+def test_oracle_polars_shapes_through_the_arrow_layer(case):
+    from helpers import arrow_to_oracle_columns, result_columns, shape_table
+
+    table = shape_table(case)
+    strings = [n for n, t in case["dtypes"].items() if t == "Utf8"]
+    cols, dicts = arrow_to_oracle_columns(table, strings)
+    want = case["expected"]
+    if "filter" in case:
+        keep = pyoracle.filter_mask(cols, case["filter"]) if len(table) else np.zeros(0, bool)
+        for name, vals in want.items():
+            got = [v for v, k in zip(table.column(name).to_pylist(), keep) if k]
+            assert got == vals, name
+        return
+    keys = case["keys"]
+    aggs = [tuple(a) for a in case["aggs"]]
+    res = pyoracle.groupby(cols, keys, aggs, case.get("predicate"))
+    got = result_columns(res)
+    for name, values in dicts.items():
+        got[name] = [None if c is None else values[c].as_py() for c in got[name]]
+    names = keys + [a[2] for a in aggs]
+    got_rows = _rows_sorted(list(zip(*[got[n] for n in names])))
+    want_rows = list(zip(*[want[n] for n in names]))
+    assert len(got_rows) == len(want_rows)
+    for g, w in zip(got_rows, want_rows):
+        for x, y in zip(g, w):
+            if isinstance(y, float):
+                assert math.isclose(x, y, rel_tol=1e-12), (g, w)
+            else:
+                assert x == y, (g, w)
