@@ -189,6 +189,160 @@ def cpu_baseline(workload: str, threads: int, sample_rows: int, reps: int = 3) -
             "sample": f"first {sample_rows:,} rows of the same generator (seed 99), median of {reps} after 1 warm-up"}
 
 
+F64_RTOL, F64_ATOL = 1e-12, 1e-15  # float sums and means against the oracle's compensated sums
+
+
+def _sorted_by_keys(res: dict, n_keys: int) -> list:
+    """[(values, valid)] per column of a result dict, rows ordered by the keys (nulls first)."""
+    import numpy as np
+
+    from polars_b200 import _abi as A
+
+    n = int(res["n_groups"])
+    cols = []
+    for dt, d, v in zip(res["dtypes"], res["data"], res["validity"]):
+        vals = np.asarray(d)
+        vals = np.unpackbits(vals.view(np.uint8), bitorder="little")[:n].astype(bool) if dt == A.BOOL else vals[:n]
+        valid = np.unpackbits(np.asarray(v, dtype=np.uint8), bitorder="little")[:n].astype(bool)
+        cols.append((vals, valid))
+    sort_keys = []
+    for j in reversed(range(n_keys)):
+        vals, valid = cols[j]
+        vv = np.where(valid, vals, np.zeros_like(vals))
+        if vv.dtype.kind == "f":
+            vv = vv.view(np.int32 if vv.dtype == np.float32 else np.int64)
+        sort_keys += [vv, valid]
+    order = np.lexsort(sort_keys) if n_keys and n else np.arange(n)
+    return [(vals[order], valid[order]) for vals, valid in cols]
+
+
+def compare_results(got: dict, want: dict, n_keys: int, aggs: list) -> dict:
+    """The parity rules of the test suite, as figures: keys, counts, integer aggregates and min/max
+    bit-exact; float64 sums and means within 1e-12 relative (+1e-15 absolute); float32 sums and
+    means within 1 ulp of the oracle's float64 result rounded to float32."""
+    import numpy as np
+
+    out = {"checked": True, "groups": int(want["n_groups"]), "n_groups_equal": int(got["n_groups"]) == int(want["n_groups"]),
+           "dtypes_equal": list(got["dtypes"]) == list(want["dtypes"]), "exact_int": True, "validity_equal": True,
+           "max_rel_err_f64": 0.0, "max_ulps_f32": 0, "bad_values": 0}
+    if not (out["n_groups_equal"] and out["dtypes_equal"]):
+        out["ok"] = False
+        return out
+    g, w = _sorted_by_keys(got, n_keys), _sorted_by_keys(want, n_keys)
+    ops = [None] * n_keys + [a[0] for a in aggs]
+    for (gv, gval), (wv, wval), op in zip(g, w, ops):
+        if not np.array_equal(gval, wval):
+            out["validity_equal"] = False
+            continue
+        gv, wv = gv[wval], wv[wval]
+        if gv.dtype.kind == "f" and op in ("Sum", "Mean"):
+            nan = np.isnan(gv) & np.isnan(wv)
+            if gv.dtype == np.float32:
+                ia = gv.view(np.int32).astype(np.int64)
+                ib = wv.astype(np.float32).view(np.int32).astype(np.int64)
+                ia = np.where(ia < 0, -(ia & 0x7FFFFFFF), ia)
+                ib = np.where(ib < 0, -(ib & 0x7FFFFFFF), ib)
+                u = np.where(nan, 0, np.abs(ia - ib))
+                out["max_ulps_f32"] = max(out["max_ulps_f32"], int(u.max()) if u.size else 0)
+                out["bad_values"] += int((u > 1).sum())
+            else:
+                with np.errstate(invalid="ignore", divide="ignore"):
+                    diff = np.where(nan | (gv == wv), 0.0, np.abs(gv - wv))
+                    rel = np.where(diff == 0, 0.0, diff / np.maximum(np.abs(wv), F64_ATOL))
+                out["max_rel_err_f64"] = max(out["max_rel_err_f64"], float(rel.max()) if rel.size else 0.0)
+                out["bad_values"] += int((diff > F64_RTOL * np.abs(wv) + F64_ATOL).sum())
+        else:
+            same = (gv == wv) | (np.isnan(gv) & np.isnan(wv)) if gv.dtype.kind == "f" else (gv == wv)
+            if not same.all():
+                out["exact_int"] = False
+                out["bad_values"] += int((~same).sum())
+    out["ok"] = out["validity_equal"] and out["exact_int"] and out["bad_values"] == 0
+    return out
+
+
+def parity_against_oracle(got, table, threads: int) -> dict:
+    """The CPU checker after the timed region: the oracle's group-by of the same table (copied to
+    host memory) against the device result `got` (a host-output GroupByResult)."""
+    from oracle import pyoracle
+    from polars_b200 import datagen
+
+    t0 = time.perf_counter()
+    want = pyoracle.groupby(datagen.to_numpy_columns(table), table.keys, table.aggs, table.predicate,
+                            n_threads=threads)
+    g = {"n_groups": got.n_groups, "names": got.names, "dtypes": got.dtypes, "data": got.data,
+         "validity": got.validity}
+    rep = compare_results(g, want, len(table.keys), table.aggs)
+    rep["rows"] = table.n_rows
+    rep["oracle_s"] = time.perf_counter() - t0
+    return rep
+
+
+def sort_extras(t, cols, h, stream, strategy: str, used: str, ms_group_by: float):
+    """The sort workload's LSD radix sort + segmented reduce strategy (when AUTO picked another)
+    and the group-by with its result sorted by the keys on the device in the same call (a Sort
+    over a GroupBy), with the kernels of one profiled call."""
+    from polars_b200._native import groupby
+
+    n = t.n_rows
+    sort_strategy = None
+    if used != "sort":
+        ms_sort = time_calls(lambda: groupby(cols, t.keys, t.aggs, t.predicate, strategy="sort", output="device",
+                                             handle=h), stream, 3, 1)
+        sort_strategy = {"strategy": "sort", "ms_per_step": ms_sort, "rows_per_s": n / (ms_sort / 1e3)}
+
+    def sorted_call():
+        return groupby(cols, t.keys, t.aggs, t.predicate, strategy=strategy, output="device", handle=h,
+                       sort={"by": list(t.keys)})
+    ms_sorted = time_calls(sorted_call, stream, 3, 1)
+    h.set_profiling(True)
+    sorted_call()
+    st = h.last_stats()
+    h.set_profiling(False)
+    sorted_output = {"by": list(t.keys), "ms_per_step": ms_sorted, "ms_group_by_alone": ms_group_by,
+                     "rows_per_s": n / (ms_sorted / 1e3), "kernels_ms": {k: rec["ms"] for k, rec in st["kernels"].items()}}
+    return sort_strategy, sorted_output
+
+
+def sort_subrecord(device, h, stream, threads: int | None) -> dict:
+    """The sort workload (200M rows, two-column key, ~49M groups) on device-resident inputs: AUTO
+    (the partitioned strategy), the sort strategy, the sorted group-by, its dominant kernel against
+    the HBM roofline, and (with `threads`) parity of the AUTO result against the oracle."""
+    import torch
+
+    from polars_b200 import datagen
+    from polars_b200._native import groupby
+
+    n = WORKLOADS["sort"][1]
+    t = datagen.make_sort(n, seed=1234, device=device)
+    torch.cuda.synchronize()
+    cols = datagen.to_column_data(t)
+
+    def call():
+        return groupby(cols, t.keys, t.aggs, None, output="device", handle=h)
+    r = call()
+    ms = time_calls(call, stream, 5, 2)
+    h.set_profiling(True)
+    call()
+    st = h.last_stats()
+    h.set_profiling(False)
+    kern = {k: rec["ms"] for k, rec in st["kernels"].items()}
+    peak, peak_kind = load_peaks()
+    bpr = t.bytes_per_row()
+    sort_strategy, sorted_output = sort_extras(t, cols, h, stream, "auto", r.strategy, ms)
+    rec = {"workload": WORKLOADS["sort"][2], "rows": n, "groups": r.n_groups, "strategy": r.strategy,
+           "ms_per_step": ms, "rows_per_s": n / (ms / 1e3), "bytes_per_row": bpr,
+           "pipeline_frac": (bpr * n / (ms / 1e3) / 1e9) / peak, "peak_kind": peak_kind, "kernels_ms": kern,
+           "sort_strategy": sort_strategy, "sorted_output": sorted_output, "parity": None}
+    if threads:
+        got = groupby(cols, t.keys, t.aggs, None, output="host", handle=h)
+        rec["parity"] = parity_against_oracle(got, t, threads)
+        del got
+    del cols, t
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return rec
+
+
 def batch_queries(device, seed: int, stop_rows: int | None = None, max_total: int = BATCH_ROWS):
     """The batched workload's tables and their (columns, keys, aggs, predicate) tuples."""
     from polars_b200 import datagen
@@ -228,6 +382,33 @@ def batch_vs_plain(qs, rows: int, stream, h_learned, h_plain, steps: int = 3, pl
             "batched_learned": {"rows_per_s": rows / (ms_b / 1e3), "ms_per_step": ms_b, "steps": steps},
             "plain_heuristic": {"rows_per_s": rows / (ms_p / 1e3), "ms_per_step": ms_p, "steps": plain_steps},
             "speedup": ms_p / ms_b}
+
+
+def batch_parity(tables, qs, h, threads: int) -> dict:
+    """The checker after the timed region: every query of the batch through pmb_groupby_batched
+    (host outputs) against the oracle's group-by of the same query."""
+    from oracle import pyoracle
+    from polars_b200 import datagen
+    from polars_b200._native import groupby_batched
+
+    t0 = time.perf_counter()
+    res = groupby_batched(qs, output="host", handle=h)
+    agg = {"checked": True, "queries": len(tables), "rows": sum(t.n_rows for t in tables), "ok": True,
+           "exact_int": True, "validity_equal": True, "max_rel_err_f64": 0.0, "bad_values": 0, "failed_queries": 0}
+    for t, got in zip(tables, res):
+        want = pyoracle.groupby(datagen.to_numpy_columns(t), t.keys, t.aggs, t.predicate, n_threads=threads)
+        g = {"n_groups": got.n_groups, "names": got.names, "dtypes": got.dtypes, "data": got.data,
+             "validity": got.validity}
+        rep = compare_results(g, want, len(t.keys), t.aggs)
+        if not rep["ok"]:
+            agg["failed_queries"] += 1
+            agg["ok"] = False
+        for k in ("exact_int", "validity_equal"):
+            agg[k] = agg[k] and rep.get(k, False)
+        agg["max_rel_err_f64"] = max(agg["max_rel_err_f64"], rep.get("max_rel_err_f64", 0.0))
+        agg["bad_values"] += rep.get("bad_values", 0)
+    agg["oracle_s"] = time.perf_counter() - t0
+    return agg
 
 
 def batch_cpu_sample(threads: int, stop_rows: int, reps: int = 3) -> tuple[float, int, int]:
@@ -315,7 +496,8 @@ def main():
     ap.add_argument("--rows", type=int, default=0,
                     help="override the workload's row count (batch: the total over its 4096 queries)")
     ap.add_argument("--e2e-steps", type=int, default=0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="leave out the CPU legs: baseline and parity check")
+    ap.add_argument("--no-sort", action="store_true", help="leave the sort workload out of the default line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -422,33 +604,27 @@ def main():
                "d2h_bytes_per_step": int(io["d2h_bytes"]), "ms_per_step": e2e_ms_max, "steps": e2e_steps}
 
     cpu = None
+    parity = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = len(os.sched_getaffinity(0))
         sample = {"hash": 10_000_000, "small": 1_000_000, "sort": 10_000_000}[args.workload]
         cpu = cpu_baseline(args.workload, threads, sample)
+        # the checker, after the timed region: the same call's result against the oracle over all rows
+        got = groupby(cols, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="host", handle=h)
+        parity = parity_against_oracle(got, t, threads)
+        del got
 
-    # the sort workload also reports the LSD radix sort + segmented reduce strategy itself
-    sort_strategy = None
-    if args.workload == "sort" and r.strategy != "sort":
-        ms_sort = time_calls(lambda: groupby(cols, t.keys, t.aggs, t.predicate, strategy="sort", output="device",
-                                             handle=h), stream, 3, 1)
-        sort_strategy = {"strategy": "sort", "ms_per_step": ms_sort, "rows_per_s": n / (ms_sort / 1e3)}
-
-    # ... and the group-by with its result sorted by the keys on the device in the same call (a Sort
-    # over a GroupBy), with the kernels of one profiled call
-    sorted_output = None
+    sort_strategy = sorted_output = None
     if args.workload == "sort":
-        def sorted_call():
-            return groupby(cols, t.keys, t.aggs, t.predicate, strategy=args.strategy, output="device", handle=h,
-                           sort={"by": list(t.keys)})
-        ms_sorted = time_calls(sorted_call, stream, 3, 1)
-        h.set_profiling(True)
-        sorted_call()
-        st = h.last_stats()
-        h.set_profiling(False)
-        sorted_output = {"by": list(t.keys), "ms_per_step": ms_sorted, "ms_group_by_alone": ms_max,
-                         "rows_per_s": n / (ms_sorted / 1e3),
-                         "kernels_ms": {k: rec["ms"] for k, rec in st["kernels"].items()}}
+        sort_strategy, sorted_output = sort_extras(t, cols, h, stream, args.strategy, r.strategy, ms_max)
+
+    # the default line also carries the sort workload (200M rows, ~49M groups) as a sub-record
+    sort_rec = None
+    if args.workload == "hash" and not args.no_sort and world == 1:
+        del cols, t
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        sort_rec = sort_subrecord(device, h, stream, None if args.no_cpu_baseline else len(os.sched_getaffinity(0)))
 
     batched = None
     if not args.no_batched and args.workload == "hash":
@@ -458,6 +634,8 @@ def main():
         h_plain.set_stream(stream.cuda_stream)
         batched = batch_vs_plain(qs_b, sum(tb.n_rows for tb in tables_b), stream, h, h_plain)
         h_plain.close()
+        if not args.no_cpu_baseline:
+            batched["parity"] = batch_parity(tables_b, qs_b, h, len(os.sched_getaffinity(0)))
         del tables_b, qs_b
 
     if rank == 0:
@@ -489,9 +667,11 @@ def main():
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clocks,
+            "parity": parity,
             "batched": batched,
             "sort_strategy": sort_strategy,
             "sorted_output": sorted_output,
+            "sort": sort_rec,
         }
         print(json.dumps(line), flush=True)
     h.close()
@@ -536,7 +716,10 @@ def run_batch(args, device, rank: int, local_rank: int, world: int) -> None:
     st = h.last_stats()
     h.set_profiling(False)
     kern = {k: v["ms"] for k, v in st["kernels"].items()}
-    agg_ms = st["kernels"]["batch_agg"]["ms"] / max(1, st["kernels"]["batch_agg"]["launches"])
+    # every launch of the batched kernel in one call (a first round, and a second one for the queries
+    # whose tables overflowed) together reads the batch's bytes once: divide by their summed time
+    agg_ms = st["kernels"]["batch_agg"]["ms"]
+    agg_launches = st["kernels"]["batch_agg"]["launches"]
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (agg_ms / 1e3) / 1e9
     groups = sum(r.n_groups for r in res)
@@ -587,7 +770,8 @@ def run_batch(args, device, rank: int, local_rank: int, world: int) -> None:
                        "bytes_per_row": bytes_per_row, "selector": "learned (shipped parameters)"},
             "roofline": {"bound": "hbm", "kernel": "batch_agg", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": ncu_traffic("batch_agg"),
-                         "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": agg_ms,
+                         "algorithmic_bytes_per_call": alg_bytes, "launches_per_call": agg_launches,
+                         "summed_launch_ms": agg_ms,
                          "pipeline_frac": (alg_bytes / (ms / 1e3) / 1e9) / peak},
             "kernels_ms_per_step": kern,
             "cpu_baseline": cpu,

@@ -115,7 +115,9 @@ struct ArrowDeviceArray {
 /* A column over an exported Arrow array's own buffers, without a copy: the values buffer, the
  * validity bitmap (NULL when the array has no nulls) and the array's offset. Primitive formats
  * b c C s S i I l L f g (Bool, Int8..UInt64, Float32, Float64); a dictionary-encoded array gives
- * its integer codes (group by them, then decode through the dictionary). Returns
+ * its integer codes: such a column is only meaningful as a group key (group by the codes, then
+ * decode through the dictionary); summing, comparing or filtering it works on the codes, not on
+ * the dictionary's values. `pmb_column_is_dictionary` tells such arrays apart. Returns
  * PMB_E_UNSUPPORTED for other formats and PMB_E_INVALID for a malformed or released array. The
  * array stays owned by its producer and must outlive every call that reads the column.
  * Replaces the reference's Arrow -> Metal buffer bridge (crates/polars-metal-buffer/src/bridge.rs:1-60)
@@ -125,10 +127,19 @@ int pmb_column_from_arrow(const struct ArrowArray* array, const struct ArrowSche
 
 /* The same for an array of the C Device Data Interface: ARROW_DEVICE_CUDA buffers give a device
  * column (used in place by the kernels), ARROW_DEVICE_CPU and ARROW_DEVICE_CUDA_HOST a host one.
+ * A CUDA array must live on the calling thread's current CUDA device (`device_id` equal to it, and
+ * the handle that reads the column opened on that device): another device's array returns
+ * PMB_E_INVALID, and a process without a usable CUDA device PMB_E_UNSUPPORTED. The handle checks
+ * the pointers of every device column again when a call stages them.
  * A non-NULL `sync_event` (a cudaEvent_t* for CUDA) is left to the caller to wait on before the
  * column is used. Other device types return PMB_E_UNSUPPORTED. */
 int pmb_column_from_arrow_device(const struct ArrowDeviceArray* array, const struct ArrowSchema* schema,
                                  pmb_column* out);
+
+/* 1 when `schema` describes a dictionary-encoded array (its column holds codes: use it only as a
+ * group key), 0 when it does not, PMB_E_INVALID for a NULL or released schema. The reference keeps
+ * the dictionary beside the codes in its Utf8 key path (crates/polars-metal-buffer/src/dict.rs:18-74). */
+int pmb_column_is_dictionary(const struct ArrowSchema* schema);
 
 /* ---- predicate expression (PredicateAst, crates/polars-metal-core/src/plan/mod.rs:42-60,
  *      plus the Arith / Not / IsNull nodes this build adds) ---- */

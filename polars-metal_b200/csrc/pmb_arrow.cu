@@ -5,6 +5,8 @@
 // plus `struct ArrowSchema`; the column here points at the array's own buffers. The reference
 // bridges Arrow buffers to Metal in crates/polars-metal-buffer/src/bridge.rs:1-60, and its Python
 // side first copies every column into `bytes` (python/polars_metal/_udf.py:1441-1456).
+#include <cuda_runtime.h>
+
 #include <cstring>
 
 #include "pmb.h"
@@ -59,9 +61,24 @@ extern "C" int pmb_column_from_arrow_device(const struct ArrowDeviceArray* array
                                             pmb_column* out) {
   if (!array) return PMB_E_INVALID;
   switch (array->device_type) {
-    case ARROW_DEVICE_CUDA: return fill(&array->array, schema, 1, out);
+    case ARROW_DEVICE_CUDA: {
+      // the kernels dereference the buffers on the current device: an array of another GPU
+      // would be read through a peer mapping or fault, so it is refused here
+      int cur = -1;
+      if (cudaGetDevice(&cur) != cudaSuccess) {
+        cudaGetLastError();
+        return PMB_E_UNSUPPORTED;  // no usable CUDA device in this process
+      }
+      if (array->device_id != (int64_t)cur) return PMB_E_INVALID;
+      return fill(&array->array, schema, 1, out);
+    }
     case ARROW_DEVICE_CPU:
     case ARROW_DEVICE_CUDA_HOST: return fill(&array->array, schema, 0, out);
     default: return PMB_E_UNSUPPORTED;
   }
+}
+
+extern "C" int pmb_column_is_dictionary(const struct ArrowSchema* schema) {
+  if (!schema || !schema->release) return PMB_E_INVALID;
+  return schema->dictionary ? 1 : 0;
 }

@@ -9,8 +9,11 @@
 // writes then goes into pmb_groupby like any other. Types follow Polars: both operands of a node
 // are cast to their supertype (the wider integer; a signed and an unsigned integer to the signed
 // type that holds both, Float64 past 64 bits; Float32 with an 8- or 16-bit integer, Float64 with a
-// wider one), literals take the type of the other operand, and a true division of integers is
-// Float64. Every node's value is wrapped (integers) or rounded (Float32) to its type, so 32-bit
+// wider one), a float literal takes the other operand's float type (Float64 beside an integer), an
+// integer literal takes the supertype of the other operand and the smallest integer type that holds
+// its value (UInt8 - 1 is Int16, Int8 + 1000 is Int16, UInt64 with a negative literal is Int64), a
+// subtree of literals alone is folded to its value first (Int32 when that fits, else Int64), and a
+// true division of integers is Float64. Every node's value is wrapped (integers) or rounded (Float32) to its type, so 32-bit
 // arithmetic wraps and rounds as Polars' does; the column has the root's type. Floor division and
 // modulo follow Polars (floor, the sign of the divisor); a null operand, or an integer // or % by
 // zero, makes the row null.
@@ -162,11 +165,66 @@ int ec_supertype(int a, int b) {
   return 2 * ec_bits(un) <= 64 ? ec_signed_of_bits(2 * ec_bits(un)) : PMB_F64;
 }
 
-int ec_adopt(int dyn, int t) { return dyn == DYN_INT ? t : (ec_float(t) ? t : PMB_F64); }
+bool ec_unsigned(int dt) { return dt == PMB_U8 || dt == PMB_U16 || dt == PMB_U32 || dt == PMB_U64; }
 
-int ec_concrete(int t, int ctx) {
+// the smallest integer type that holds v: unsigned when `want_unsigned` and v >= 0, else signed
+int ec_fit(long long v, bool want_unsigned) {
+  if (want_unsigned && v >= 0) {
+    const unsigned long long u = (unsigned long long)v;
+    return u <= 0xFFull ? PMB_U8 : u <= 0xFFFFull ? PMB_U16 : u <= 0xFFFFFFFFull ? PMB_U32 : PMB_U64;
+  }
+  if (v >= -128 && v <= 127) return PMB_I8;
+  if (v >= -32768 && v <= 32767) return PMB_I16;
+  if (v >= -2147483648LL && v <= 2147483647LL) return PMB_I32;
+  return PMB_I64;
+}
+
+// the type of an integer literal of value v (when `known`) beside an operand of type t: Polars'
+// supertype of t and the smallest type holding v (its rule for a dynamic integer literal); a
+// literal beside a float operand takes the float type
+int ec_adopt_int(long long v, bool known, int t) {
+  if (ec_float(t)) return t;
+  if (!known) return t;
+  const int fit = ec_fit(v, ec_unsigned(t));
+  if (t == PMB_U64 && ec_signed(fit)) return PMB_I64;  // not Float64: a literal never forces floats
+  return ec_supertype(t, fit);
+}
+
+int ec_adopt_float(int t) { return ec_float(t) ? t : PMB_F64; }
+
+// a subtree of integer literals alone, folded to one value (Polars folds literal arithmetic before
+// typing); false when the fold divides by zero
+bool ec_fold(int op, long long a, long long b, long long* out) {
+  const unsigned long long ua = (unsigned long long)a, ub = (unsigned long long)b;
+  switch (op) {
+    case PMB_ARITH_ADD: *out = (long long)(ua + ub); return true;
+    case PMB_ARITH_SUB: *out = (long long)(ua - ub); return true;
+    case PMB_ARITH_MUL: *out = (long long)(ua * ub); return true;
+    case PMB_ARITH_FLOORDIV:
+    case PMB_ARITH_MOD: {
+      if (b == 0) return false;
+      if (b == -1) {
+        *out = op == PMB_ARITH_MOD ? 0 : (long long)(0ull - ua);
+        return true;
+      }
+      long long q = a / b, m = a % b;
+      if (m != 0 && ((m < 0) != (b < 0))) {
+        q -= 1;
+        m += b;
+      }
+      *out = op == PMB_ARITH_MOD ? m : q;
+      return true;
+    }
+    default: return false;
+  }
+}
+
+int ec_concrete(int t, int ctx, long long v, bool known) {
   if (t >= 0) return t;
-  if (t == DYN_INT) return ctx >= 0 ? ctx : PMB_I32;
+  if (t == DYN_INT) {
+    if (ctx >= 0) return ctx;
+    return (known && ec_fit(v, false) == PMB_I64) ? PMB_I64 : PMB_I32;  // Int32 unless the value needs 64 bits
+  }
   return (ctx >= 0 && ec_float(ctx)) ? ctx : PMB_F64;
 }
 
@@ -178,6 +236,8 @@ struct Flatten {
   std::vector<int> slot_of;  // user column -> slot
   std::vector<int> user_of;  // slot -> user column
   std::vector<int> node_t;   // per node: its type, or DYN_INT / DYN_FLOAT
+  std::vector<long long> node_v;  // per DYN_INT node: its folded value
+  std::vector<char> node_known;   // ... when the fold succeeded
   std::string err;
   int count = 0;
 
@@ -196,17 +256,33 @@ struct Flatten {
         *t = dt;
         break;
       }
-      case PMB_EXPR_LIT_I64: *t = DYN_INT; break;
+      case PMB_EXPR_LIT_I64:
+        *t = DYN_INT;
+        node_v[i] = nd.lit_i64;
+        node_known[i] = 1;
+        break;
       case PMB_EXPR_LIT_F64: *t = DYN_FLOAT; break;
       case PMB_EXPR_ARITH: {
         if (nd.op < PMB_ARITH_ADD || nd.op > PMB_ARITH_MOD) return fail("unknown arithmetic op");
         int a, b;
         if (!type(nd.lhs, depth + 1, &a) || !type(nd.rhs, depth + 1, &b)) return false;
         int r;
-        if (a < 0 && b < 0) r = (a == DYN_FLOAT || b == DYN_FLOAT || nd.op == PMB_ARITH_TRUEDIV) ? DYN_FLOAT : DYN_INT;
-        else if (a < 0) r = ec_adopt(a, b);
-        else if (b < 0) r = ec_adopt(b, a);
-        else r = ec_supertype(a, b);
+        if (a < 0 && b < 0) {
+          r = (a == DYN_FLOAT || b == DYN_FLOAT || nd.op == PMB_ARITH_TRUEDIV) ? DYN_FLOAT : DYN_INT;
+          if (r == DYN_INT && node_known[nd.lhs] && node_known[nd.rhs]) {
+            long long v;
+            if (ec_fold(nd.op, node_v[nd.lhs], node_v[nd.rhs], &v)) {
+              node_v[i] = v;
+              node_known[i] = 1;
+            }
+          }
+        } else if (a < 0) {
+          r = a == DYN_INT ? ec_adopt_int(node_v[nd.lhs], node_known[nd.lhs], b) : ec_adopt_float(b);
+        } else if (b < 0) {
+          r = b == DYN_INT ? ec_adopt_int(node_v[nd.rhs], node_known[nd.rhs], a) : ec_adopt_float(a);
+        } else {
+          r = ec_supertype(a, b);
+        }
         if (r >= 0 && nd.op == PMB_ARITH_TRUEDIV && !ec_float(r)) r = PMB_F64;
         *t = r;
         break;
@@ -221,7 +297,7 @@ struct Flatten {
   // pass 2: literals and literal-only nodes take their context's type; postfix program
   bool emit(int i, int ctx, int* out_t) {
     const pmb_expr_node& nd = e->nodes[i];
-    const int t = ec_concrete(node_t[i], ctx);
+    const int t = ec_concrete(node_t[i], ctx, node_v[i], node_known[i] != 0);
     if (P->n >= EC_MAX) return fail("expression has more than 32 nodes");
     switch (nd.kind) {
       case PMB_EXPR_COLUMN:
@@ -259,6 +335,8 @@ struct Flatten {
 
   bool run(int root) {
     node_t.assign(e->n_nodes, 0);
+    node_v.assign(e->n_nodes, 0);
+    node_known.assign(e->n_nodes, 0);
     int t;
     if (!type(root, 0, &t)) return false;
     int out;
@@ -285,7 +363,7 @@ extern "C" int pmb_eval_expr(pmb_handle* h, const pmb_expr* expr, const pmb_colu
     if (cols[c].length != n) return pmb_fail(h, PMB_E_INVALID, "expression columns differ in length");
   ECProg P;
   memset(&P, 0, sizeof(P));
-  Flatten F{expr, n_cols, cols, &P, std::vector<int>(n_cols, -1), {}, {}, {}};
+  Flatten F{expr, n_cols, cols, &P, std::vector<int>(n_cols, -1), {}, {}, {}, {}, {}};
   if (!F.run(expr->root)) return pmb_fail(h, PMB_E_INVALID, "expression: " + F.err);
   *out_dtype = P.out_dtype;
   PMB_CUDA(h, cudaSetDevice(h->device));
@@ -329,7 +407,7 @@ extern "C" int pmb_expr_dtype(const pmb_expr* expr, const pmb_column* cols, int3
   if (!expr || !expr->nodes || !cols || n_cols <= 0 || !out_dtype) return PMB_E_INVALID;
   ECProg P;
   memset(&P, 0, sizeof(P));
-  Flatten F{expr, n_cols, cols, &P, std::vector<int>(n_cols, -1), {}, {}, {}};
+  Flatten F{expr, n_cols, cols, &P, std::vector<int>(n_cols, -1), {}, {}, {}, {}, {}};
   if (!F.run(expr->root)) return PMB_E_INVALID;
   *out_dtype = P.out_dtype;
   return PMB_OK;

@@ -146,6 +146,8 @@ struct DQuery {
   int32_t rec_bytes; // bytes per group record
   int64_t n_rows;
   int16_t fx_e[8];   // exact float sums: every value of slot i satisfies |x| < 2^fx_e[i]
+  uint32_t valid_if_kept;  // bit c: column c is non-null in every row the filter keeps
+  uint32_t pad_vk;
   DCol col[PMB_MAX_COLS];
   DKey key[PMB_MAX_KEYS];
   DField field[PMB_MAX_FIELDS];

@@ -115,6 +115,8 @@ struct Gen {
 
   std::string v(int c) { return "r.v" + std::to_string(c); }
   std::string ok(int c) { return q.col[c].valid ? "r.ok" + std::to_string(c) : std::string("true"); }
+  // validity of column c in a row the filter kept: the filter may already imply it
+  std::string okk(int c) { return ((q.valid_if_kept >> c) & 1u) ? std::string("true") : ok(c); }
 
   void mark_leaf(const DLeaf& L) {
     if (L.col >= 0) need_val[L.col] = need_valid[L.col] = pred_col[L.col] = true;
@@ -313,7 +315,7 @@ struct Gen {
     std::vector<std::pair<int, std::string>> words;  // (word offset, increment expression)
     for (int i = 0; i < q.n_fields; i++) {
       const DField& F = q.field[i];
-      std::string okc = F.kind == F_LEN ? std::string("true") : ok(F.col);
+      std::string okc = F.kind == F_LEN ? std::string("true") : okk(F.col);
       if (F.kind == F_LEN || F.kind == F_CNT) {
         std::string inc = F.kind == F_LEN ? "1ULL" : "(" + okc + " ? 1ULL : 0ULL)";
         int w = F.off & ~7;
@@ -365,7 +367,7 @@ struct Gen {
         b << "  atomicAdd(" << at(so, "unsigned int") << ", 1u);\n";
         continue;
       }
-      b << "  if (" << ok(F.col) << ") {\n";
+      b << "  if (" << okk(F.col) << ") {\n";
       switch (F.kind) {
         case F_CNT: b << "    atomicAdd(" << at(so, "unsigned int") << ", 1u);\n"; break;
         case F_SUM_FX: {
@@ -530,7 +532,7 @@ struct Gen {
       const DField& F = q.field[i];
       if (F.kind != F_SUM_FX) continue;
       std::string slot = std::to_string(F.fx_slot);
-      b << "  if (" << ok(F.col) << ") {\n    double xv = (double)" << v(F.col) << ";\n";
+      b << "  if (" << okk(F.col) << ") {\n    double xv = (double)" << v(F.col) << ";\n";
       b << "    if (!pmb_fx_flag(xv) && !pmb_fx_in_range(xv, P.fx_e[" << slot << "])) {\n";
       b << "      unsigned ex = (unsigned)pmb_fx_expo(xv);\n";
       b << "      if (ex > *(volatile unsigned int*)&P.status[4 + " << slot << "]) atomicMax(&P.status[4 + " << slot

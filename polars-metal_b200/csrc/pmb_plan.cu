@@ -211,6 +211,50 @@ int pmb_compile_predicate(pmb_handle* h, const pmb_expr* e, ColMap* map, const p
   return pc.boolean(e->root, 0);
 }
 
+// User columns that are non-null in every row where node `i` of the predicate is `pol` (true or
+// false; a null verdict is neither) under Kleene logic: a compare or a Bool column is true or false
+// only where its columns are valid, is_null is false and is_not_null true only on valid rows, AND
+// is true where both sides are (false where either is), OR the other way round, NOT flips.
+static void implied_valid(const pmb_expr* e, int i, bool pol, int n_user, std::vector<char>& out, int depth = 0) {
+  out.assign(n_user, 0);
+  if (!e || i < 0 || i >= e->n_nodes || depth > 64) return;
+  const pmb_expr_node& n = e->nodes[i];
+  auto columns_under = [&](auto&& self, int j, int d) -> void {
+    if (j < 0 || j >= e->n_nodes || d > 64) return;
+    const pmb_expr_node& m = e->nodes[j];
+    if (m.kind == PMB_EXPR_COLUMN) {
+      if (m.column >= 0 && m.column < n_user) out[m.column] = 1;
+    } else if (m.kind == PMB_EXPR_ARITH) {
+      self(self, m.lhs, d + 1);
+      self(self, m.rhs, d + 1);
+    }
+  };
+  switch (n.kind) {
+    case PMB_EXPR_COMPARE:
+      columns_under(columns_under, n.lhs, depth + 1);
+      columns_under(columns_under, n.rhs, depth + 1);
+      break;
+    case PMB_EXPR_COLUMN: columns_under(columns_under, i, depth); break;
+    case PMB_EXPR_IS_NULL:
+      if (!pol) columns_under(columns_under, n.lhs, depth + 1);
+      break;
+    case PMB_EXPR_IS_NOT_NULL:
+      if (pol) columns_under(columns_under, n.lhs, depth + 1);
+      break;
+    case PMB_EXPR_NOT: implied_valid(e, n.lhs, !pol, n_user, out, depth + 1); break;
+    case PMB_EXPR_AND:
+    case PMB_EXPR_OR: {
+      std::vector<char> a, b;
+      implied_valid(e, n.lhs, pol, n_user, a, depth + 1);
+      implied_valid(e, n.rhs, pol, n_user, b, depth + 1);
+      const bool uni = (n.kind == PMB_EXPR_AND) == pol;  // both sides hold: union; either: intersection
+      for (int c = 0; c < n_user; c++) out[c] = uni ? (a[c] | b[c]) : (a[c] & b[c]);
+      break;
+    }
+    default: break;
+  }
+}
+
 int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols, CompiledQuery* cq) {
   memset(&cq->dq, 0, sizeof(DQuery));
   cq->map.user.clear();
@@ -243,6 +287,13 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
     return pmb_fail(h, PMB_E_UNSUPPORTED, "composite key width " + std::to_string(off) + " bits exceeds 128-bit budget");
   d.n_keys = q->n_keys;
   d.key_bits = off;
+
+  // columns the filter only keeps where they are valid: their non-null count is the row count
+  std::vector<char> kept_valid;
+  if (q->predicate && q->predicate->nodes && q->predicate->n_nodes > 0)
+    implied_valid(q->predicate, q->predicate->root, true, n_cols, kept_valid);
+  else
+    kept_valid.assign(n_cols, 0);
 
   // fields (deduplicated by kind + column)
   std::vector<DField> fields;
@@ -278,7 +329,7 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
     o.out_dtype = (int8_t)pmb_agg_out_dtype(A.op, dt);
     // the column's non-null count, created only for the aggregates that read it (count, mean, and
     // integer min/max, whose identity value is also a valid value); sums and float min/max need none
-    auto cnt = [&]() { return (int16_t)(nullable ? field(F_CNT, c) : field(F_LEN, 0)); };
+    auto cnt = [&]() { return (int16_t)(nullable && !kept_valid[A.column] ? field(F_CNT, c) : field(F_LEN, 0)); };
     const int fsum = std::find(cq->dd_user_cols.begin(), cq->dd_user_cols.end(), A.column) != cq->dd_user_cols.end()
                          ? F_SUM_DD
                          : F_SUM_FX;
@@ -346,9 +397,11 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
 
   // columns and row count (pointers are filled in when the columns are staged)
   d.n_cols = (int)cq->map.user.size();
+  d.valid_if_kept = 0;
   for (int c = 0; c < d.n_cols; c++) {
     d.col[c].dtype = cols[cq->map.user[c]].dtype;
     d.col[c].elem = pmb_dtype_bytes(d.col[c].dtype);
+    if (kept_valid[cq->map.user[c]]) d.valid_if_kept |= 1u << c;
   }
   int64_t n = cols[cq->map.user[0]].length;
   for (int u : cq->map.user) {

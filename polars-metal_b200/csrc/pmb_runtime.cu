@@ -233,12 +233,35 @@ static int stage_bits(pmb_handle* h, const uint8_t* base, int64_t offset, int64_
   return PMB_OK;
 }
 
+static int check_device_pointer(pmb_handle* h, const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return pmb_fail(h, PMB_E_INVALID, "device column pointer is not CUDA memory");
+  }
+  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) {
+    if (a.device != h->device)
+      return pmb_fail(h, PMB_E_INVALID, "device column lives on GPU " + std::to_string(a.device) +
+                                            ", the handle on GPU " + std::to_string(h->device));
+    return PMB_OK;
+  }
+  if (a.type == cudaMemoryTypeHost) return PMB_OK;  // pinned host memory, mapped for the device
+  return pmb_fail(h, PMB_E_INVALID, "device column pointer is not CUDA memory (pageable host memory?)");
+}
+
 int pmb_stage_column(pmb_handle* h, const pmb_column& c, int64_t n, DCol* out) {
   out->dtype = c.dtype;
   out->elem = pmb_dtype_bytes(c.dtype);
   if (c.offset < 0) return pmb_fail(h, PMB_E_INVALID, "negative column offset");
   if (n > 0 && c.data == nullptr) return pmb_fail(h, PMB_E_INVALID, "column data pointer is NULL");
   bool dev = c.on_device != 0;
+  if (dev && n > 0) {
+    // a device column must be memory of this handle's GPU: another GPU's buffer would be read
+    // through a peer mapping or fault in the kernels, and pageable host memory would fault
+    int rc = check_device_pointer(h, c.data);
+    if (!rc && c.validity) rc = check_device_pointer(h, c.validity);
+    if (rc) return rc;
+  }
   if (c.dtype == PMB_BOOL) {
     int rc = stage_bits(h, (const uint8_t*)c.data, c.offset, n, dev, &out->data);
     if (rc) return rc;

@@ -229,6 +229,7 @@ SIGNATURES = {
     "pmb_column_from_arrow": (C.c_int, [C.POINTER(ArrowArray), C.POINTER(ArrowSchema), C.POINTER(Column)]),
     "pmb_column_from_arrow_device": (C.c_int, [C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema),
                                                C.POINTER(Column)]),
+    "pmb_column_is_dictionary": (C.c_int, [C.POINTER(ArrowSchema)]),
     "pmb_sort_columns": (C.c_int, [_H, C.POINTER(Column), C.c_int32, C.POINTER(SortSpec), C.c_int32,
                                    C.POINTER(C.POINTER(Result))]),
     "pmb_groupby_sorted": (C.c_int, [_H, C.POINTER(Query), C.POINTER(Column), C.c_int32, C.POINTER(SortSpec),

@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG_DIR = Path(__file__).resolve().parent
@@ -91,14 +92,16 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     ]
     if extra:
         common += extra
-    objs = []
-    for s in srcs:
-        o = obj_dir / (s.stem + ".o")
-        cmd = [nvcc, *common, "-c", str(s), "-o", str(o)]
-        if verbose:
+    objs = [obj_dir / (s.stem + ".o") for s in srcs]
+    cmds = [[nvcc, *common, "-c", str(s), "-o", str(o)] for s, o in zip(srcs, objs)]
+    if verbose:
+        for cmd in cmds:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
-        objs.append(o)
+    # one nvcc per source, in parallel (each is single-threaded)
+    workers = max(1, min(len(cmds), len(os.sched_getaffinity(0))))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     tmp = LIB_PATH.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart", "-ldl"]
     if verbose:

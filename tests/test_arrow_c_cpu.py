@@ -51,16 +51,13 @@ def test_arrays_become_columns_over_their_buffers(typ, dt, device):
     _release(schema)
 
 
-def test_no_nulls_means_no_bitmap_and_cuda_arrays_are_device_columns():
+def test_no_nulls_means_no_bitmap_and_other_device_types_are_refused():
     lib = A.lib()
     arr = pa.array(np.arange(10, dtype=np.int64))
     out, schema = _export(arr, device=True)
     col = A.Column()
     assert lib.pmb_column_from_arrow_device(C.byref(out), C.byref(schema), C.byref(col)) == 0
     assert col.validity is None and col.on_device == 0
-    out.device_type = A.ARROW_DEVICE_CUDA  # as a CUDA producer would export it
-    assert lib.pmb_column_from_arrow_device(C.byref(out), C.byref(schema), C.byref(col)) == 0
-    assert col.on_device == 1
     out.device_type = 7  # another device type
     assert lib.pmb_column_from_arrow_device(C.byref(out), C.byref(schema), C.byref(col)) == 5  # PMB_E_UNSUPPORTED
     out.device_type = A.ARROW_DEVICE_CPU
@@ -84,3 +81,40 @@ def test_dictionary_arrays_give_their_codes_and_other_types_are_refused():
     _release(schema)
     released = A.ArrowArray()
     assert lib.pmb_column_from_arrow(C.byref(released), C.byref(schema), C.byref(col)) == 1  # PMB_E_INVALID
+
+
+def test_cuda_arrays_of_another_device_or_without_a_device_are_refused():
+    # a CUDA array must live on the current device; in a process without a CUDA device (this
+    # test's CPU run) every CUDA array is refused, whatever its device_id
+    import torch
+
+    lib = A.lib()
+    arr = pa.array(np.arange(10, dtype=np.int64))
+    out, schema = _export(arr, device=True)
+    col = A.Column()
+    out.device_type = A.ARROW_DEVICE_CUDA
+    cur = torch.cuda.current_device() if torch.cuda.is_available() else None
+    out.device_id = 5 if cur is None else cur + 1
+    rc = lib.pmb_column_from_arrow_device(C.byref(out), C.byref(schema), C.byref(col))
+    assert rc == (5 if cur is None else 1)  # PMB_E_UNSUPPORTED without a device, else PMB_E_INVALID
+    if cur is not None:
+        out.device_id = cur
+        assert lib.pmb_column_from_arrow_device(C.byref(out), C.byref(schema), C.byref(col)) == 0
+        assert col.on_device == 1
+    out.device_type = A.ARROW_DEVICE_CPU
+    _release(out.array)
+    _release(schema)
+
+
+def test_dictionary_schemas_are_told_apart():
+    lib = A.lib()
+    d = pa.array(["b", "a", None, "b"]).dictionary_encode()
+    out, schema = _export(d)
+    assert lib.pmb_column_is_dictionary(C.byref(schema)) == 1
+    _release(out)
+    _release(schema)
+    out, schema = _export(pa.array([1, 2, 3]))
+    assert lib.pmb_column_is_dictionary(C.byref(schema)) == 0
+    _release(out)
+    _release(schema)
+    assert lib.pmb_column_is_dictionary(None) == 1  # PMB_E_INVALID

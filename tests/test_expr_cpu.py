@@ -125,3 +125,35 @@ def test_bool_columns_and_deep_trees_are_refused():
         e = _bin("Add", e, {"kind": "LiteralI64", "value": 1})
     with pytest.raises(ValueError):
         expr_dtype({"i": _c("int32")}, e)
+
+
+@pytest.mark.parametrize("dtype,value,want", [
+    # an integer literal widens its operand's type to hold its value (Polars' dynamic integers)
+    ("uint8", -1, "I16"), ("uint8", 255, "U8"), ("uint8", 256, "U16"), ("int8", 1000, "I16"), ("int8", 127, "I8"),
+    ("int8", -129, "I16"), ("uint16", -1, "I32"), ("int16", 40_000, "I32"), ("uint32", -1, "I64"),
+    ("int32", 2**31, "I64"), ("uint32", 2**32, "U64"), ("uint64", -1, "I64"), ("int64", -(2**40), "I64"),
+    ("float32", 10**9, "F32"), ("int32", 7, "I32"),
+])
+def test_integer_literals_widen_to_hold_their_value(dtype, value, want):
+    from polars_b200 import _abi as A
+    from polars_b200._native import expr_dtype
+
+    lit = {"kind": "LiteralI64", "value": value}
+    got = expr_dtype({"c": _c(dtype)}, _bin("Mul", col("c"), lit))
+    assert got == A.TAG_TO_DTYPE[want], (dtype, value)
+    assert expr_dtype({"c": _c(dtype)}, _bin("Add", lit, col("c"))) == A.TAG_TO_DTYPE[want]
+
+
+def test_literal_only_subtrees_fold_before_typing():
+    from polars_b200 import _abi as A
+    from polars_b200._native import expr_dtype
+
+    big = {"kind": "LiteralI64", "value": 3_000_000_000}
+    one = {"kind": "LiteralI64", "value": 1}
+    cols = {"u": _c("uint8"), "i": _c("int32")}
+    assert expr_dtype(cols, _bin("Add", big, one)) == A.I64  # beyond Int32: Int64, not a wrapped Int32
+    assert expr_dtype(cols, _bin("Add", one, one)) == A.I32
+    # (300 - 1) beside a UInt8 column needs UInt16
+    assert expr_dtype(cols, _bin("Mul", col("u"), _bin("Sub", {"kind": "LiteralI64", "value": 300}, one))) == A.U16
+    # (0 - 1) beside a UInt8 column is negative: Int16
+    assert expr_dtype(cols, _bin("Mul", col("u"), _bin("Sub", {"kind": "LiteralI64", "value": 0}, one))) == A.I16

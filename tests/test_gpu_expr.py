@@ -154,6 +154,30 @@ def test_polars_types_wrap_and_round_on_the_gpu():
         assert np.unpackbits(np.asarray(out.validity), bitorder="little")[:n].all()
 
 
+def test_integer_literals_beyond_the_column_type_widen_on_the_gpu():
+    # UInt8 * -1 is Int16 (not a wrapped UInt8), Int8 + 1000 is Int16, UInt32 - 5_000_000_000 is
+    # Int64, a literal-only 3e9 + 1 is Int64: Polars' dynamic-integer rule
+    rng = np.random.default_rng(37)
+    n = 50_001
+    u8 = rng.integers(0, 256, n).astype(np.uint8)
+    i8 = rng.integers(-128, 128, n).astype(np.int8)
+    u32 = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    cols = {"u8": u8, "i8": i8, "u32": u32}
+    lit = lambda v: {"kind": "LiteralI64", "value": v}  # noqa: E731
+    cases = [
+        (_bin("Mul", col("u8"), lit(-1)), A.I16, u8.astype(np.int16) * np.int16(-1)),
+        (_bin("Add", col("i8"), lit(1000)), A.I16, i8.astype(np.int16) + np.int16(1000)),
+        (_bin("Sub", col("u32"), lit(5_000_000_000)), A.I64, u32.astype(np.int64) - np.int64(5_000_000_000)),
+        (_bin("Mul", col("u8"), _bin("Add", lit(3_000_000_000), lit(1))), A.I64,
+         u8.astype(np.int64) * np.int64(3_000_000_001)),
+    ]
+    for e, dt, want in cases:
+        out = N.eval_expr(cols, e)
+        assert out.dtype == dt, e
+        got = np.asarray(out.data)[:n]
+        assert got.dtype == want.dtype and np.array_equal(got, want), e
+
+
 def test_reference_fused_float32_sum_of_products():
     # crates/polars-metal-kernels/tests/test_dispatch_groupby_fused.rs:185-260: sum(a * b) per
     # i % 4 over Float32 columns a = i * 0.1, b = i * 0.05 + 1, 6000 rows
