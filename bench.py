@@ -277,6 +277,81 @@ def parity_against_oracle(got, table, threads: int) -> dict:
     return rep
 
 
+def filter_subrecord(t, cols, h, stream, threads: int | None) -> dict:
+    """The top-level filter of the hash workload (every column compacted by the predicate, one
+    pass) and the u8 -> u32 inclusive scan over 100M keep bytes, on device-resident inputs: device
+    time, the dominant kernel's HBM roofline, and (with `threads`) parity against the oracle."""
+    import numpy as np
+    import torch
+
+    from polars_b200._native import filter_columns
+
+    n = t.n_rows
+
+    def call():
+        return filter_columns(cols, t.predicate, output="device", handle=h)
+    res = call()
+    ms = time_calls(call, stream, 5, 2)
+    h.set_profiling(True)
+    call()
+    st = h.last_stats()
+    h.set_profiling(False)
+    kern = {k: rec["ms"] for k, rec in st["kernels"].items()}
+    kept = int(res.n_groups)
+    in_bytes = t.bytes_per_row() * n
+    out_bytes = kept * sum(d.element_size() + (1.0 / 8.0 if v is not None else 0.0) for d, v in t.columns.values())
+    peak, peak_kind = load_peaks()
+    dom = max(kern, key=kern.get)
+    rec = {"workload": "top-level filter (v1>-0.5)&(v3%7!=0) of the hash workload's 100M rows, 4 columns compacted",
+           "rows": n, "kept": kept, "ms_per_step": ms, "rows_per_s": n / (ms / 1e3), "kernels_ms": kern,
+           "roofline": {"kernel": dom, "algorithmic_bytes": in_bytes + out_bytes,
+                        "achieved": (in_bytes + out_bytes) / (kern[dom] / 1e3) / 1e9, "peak": peak,
+                        "frac": (in_bytes + out_bytes) / (kern[dom] / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
+           "parity": None}
+    # the u8 -> u32 inclusive scan (the reference's MLX cumsum), 100M device bytes in, 400 MB out
+    g = torch.Generator(device=t.columns["k"][0].device)
+    g.manual_seed(5)
+    u8 = torch.randint(0, 256, (n,), dtype=torch.uint8, device=t.columns["k"][0].device, generator=g)
+    o32 = torch.empty(n, dtype=torch.int32, device=u8.device)
+
+    def scan():
+        h.check(h._lib.pmb_cumsum_u8_to_u32(h.raw, u8.data_ptr(), o32.data_ptr(), n, 1))
+    ms_scan = time_calls(scan, stream, 5, 2)
+    h.set_profiling(True)
+    scan()
+    kscan = {k: r["ms"] for k, r in h.last_stats()["kernels"].items()}
+    h.set_profiling(False)
+    sdom = max(kscan, key=kscan.get)
+    rec["scan"] = {"rows": n, "ms_per_step": ms_scan, "kernels_ms": kscan,
+                   "roofline": {"kernel": sdom, "algorithmic_bytes": 5 * n,
+                                "achieved": 5 * n / (kscan[sdom] / 1e3) / 1e9, "peak": peak,
+                                "frac": 5 * n / (kscan[sdom] / 1e3) / 1e9 / peak}}
+    if threads:
+        from oracle import pyoracle
+        from polars_b200 import datagen
+
+        t0 = time.perf_counter()
+        host_cols = datagen.to_numpy_columns(t)
+        keep = pyoracle.filter_mask(host_cols, t.predicate, n_threads=threads)
+        got = filter_columns(cols, t.predicate, output="host", handle=h)
+        ok = int(got.n_groups) == int(keep.sum())
+        bad_cols = []
+        for j, name in enumerate(got.names):
+            d, v = host_cols[name]
+            want = d[keep]
+            gd = np.asarray(got.data[j])[: got.n_groups]
+            gv = np.unpackbits(np.asarray(got.validity[j], dtype=np.uint8), bitorder="little")[: got.n_groups].astype(bool)
+            wv = np.ones(want.size, bool) if v is None else np.unpackbits(v, bitorder="little")[:n].astype(bool)[keep]
+            if not (np.array_equal(gv, wv) and np.array_equal(gd[wv].view(np.uint8), want[wv].view(np.uint8))):
+                bad_cols.append(name)
+        scan_ok = bool(np.array_equal(o32.cpu().numpy().view(np.uint32), pyoracle.cumsum_u8_to_u32(u8.cpu().numpy())))
+        rec["parity"] = {"checked": True, "rows": n, "kept_equal": ok, "bit_exact_columns": not bad_cols,
+                         "bad_columns": bad_cols, "scan_bit_exact": scan_ok, "ok": ok and not bad_cols and scan_ok,
+                         "oracle_s": time.perf_counter() - t0}
+    del u8, o32
+    return rec
+
+
 def sort_extras(t, cols, h, stream, strategy: str, used: str, ms_group_by: float):
     """The sort workload's LSD radix sort + segmented reduce strategy (when AUTO picked another)
     and the group-by with its result sorted by the keys on the device in the same call (a Sort
@@ -369,19 +444,32 @@ def time_calls(fn, stream, steps: int, warmup: int) -> float:
 
 
 def batch_vs_plain(qs, rows: int, stream, h_learned, h_plain, steps: int = 3, plain_steps: int = 2) -> dict:
-    """Batched + learned selector against the plain loop (one pmb_groupby per query, heuristic)."""
+    """Batched + learned selector against three other forms of the same queries: batched with the
+    plain cardinality heuristic (the selector's share), the plain loop in C (one pmb_groupby per
+    query inside the library, host outputs: the batching's share) and the plain loop in Python
+    (one ctypes groupby call per query, device outputs: adds the binding's per-call cost)."""
     from polars_b200._native import groupby, groupby_batched
 
     def plain():
         for c, k, a, p in qs:
             groupby(c, k, a, p, output="device", handle=h_plain)
 
+    def c_loop():
+        h_plain.set_batching(False)
+        try:
+            groupby_batched(qs, output="host", handle=h_plain)
+        finally:
+            h_plain.set_batching(True)
+
     ms_b = time_calls(lambda: groupby_batched(qs, output="device", handle=h_learned), stream, steps, 3)
+    ms_bh = time_calls(lambda: groupby_batched(qs, output="device", handle=h_plain), stream, steps, 3)
+    ms_c = time_calls(c_loop, stream, plain_steps, 1)
     ms_p = time_calls(plain, stream, plain_steps, 1)
+    arm = lambda ms, st: {"rows_per_s": rows / (ms / 1e3), "ms_per_step": ms, "steps": st}  # noqa: E731
     return {"workload": BATCH_DESC, "queries": len(qs), "rows": rows,
-            "batched_learned": {"rows_per_s": rows / (ms_b / 1e3), "ms_per_step": ms_b, "steps": steps},
-            "plain_heuristic": {"rows_per_s": rows / (ms_p / 1e3), "ms_per_step": ms_p, "steps": plain_steps},
-            "speedup": ms_p / ms_b}
+            "batched_learned": arm(ms_b, steps), "batched_heuristic": arm(ms_bh, steps),
+            "plain_loop_c": arm(ms_c, plain_steps), "plain_heuristic": arm(ms_p, plain_steps),
+            "speedup": ms_p / ms_b, "speedup_vs_c_loop": ms_c / ms_b, "selector_gain": ms_bh / ms_b}
 
 
 def batch_parity(tables, qs, h, threads: int) -> dict:
@@ -498,6 +586,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true", help="leave out the CPU legs: baseline and parity check")
     ap.add_argument("--no-sort", action="store_true", help="leave the sort workload out of the default line")
+    ap.add_argument("--no-filter", action="store_true", help="leave the top-level filter out of the default line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -614,6 +703,10 @@ def main():
         parity = parity_against_oracle(got, t, threads)
         del got
 
+    filt = None
+    if args.workload == "hash" and not args.no_filter:
+        filt = filter_subrecord(t, cols, h, stream, None if args.no_cpu_baseline else len(os.sched_getaffinity(0)))
+
     sort_strategy = sorted_output = None
     if args.workload == "sort":
         sort_strategy, sorted_output = sort_extras(t, cols, h, stream, args.strategy, r.strategy, ms_max)
@@ -668,6 +761,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks,
             "parity": parity,
+            "filter": filt,
             "batched": batched,
             "sort_strategy": sort_strategy,
             "sorted_output": sorted_output,

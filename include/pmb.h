@@ -282,6 +282,12 @@ int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32
 int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb_column* const* cols,
                         const int32_t* n_cols, int32_t n_queries, pmb_result** outs);
 
+/* 0 = pmb_groupby_batched runs every query alone through pmb_groupby, in a loop inside the
+ * library (host outputs only): the plain single-query form of a batch, without the batching; 1 =
+ * batch where it can (the default). No reference counterpart (the reference runs one query per
+ * call). */
+int pmb_set_batching(pmb_handle* h, int32_t enabled);
+
 /* Order of rows for pmb_sort_columns and pmb_groupby_sorted: `by` lists column indices, most
  * significant first; `descending` and `nulls_last` hold one flag per `by` column (NULL = all 0:
  * ascending, nulls first). Polars' order: NaN above every number, -0.0 equal to 0.0, nulls placed

@@ -634,7 +634,7 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
     (ok ? batch : single).push_back(i);
   }
   int rc = PMB_OK;
-  if (batch.size() < 2 || batch.size() != (size_t)n_queries) {
+  if (!h->batching || batch.size() < 2 || batch.size() != (size_t)n_queries) {
     // one by one: every call resets the handle's workspace, so only host outputs survive
     for (int i = 0; i < n_queries; i++)
       if (qs[i].output_on_device)

@@ -133,7 +133,7 @@ __host__ __device__ __forceinline__ uint64_t pmb_fmix64(uint64_t k) {
 }
 
 // a second 32-bit mixer, independent of the key hash (C. Wellons' "lowbias32", public domain):
-// the alternative bucket of a cuckoo table
+// the alternative bucket of a two-choice bucketed table
 __host__ __device__ __forceinline__ uint32_t pmb_mix32b(uint32_t a) {
   a ^= a >> 16;
   a *= 0x7feb352dU;

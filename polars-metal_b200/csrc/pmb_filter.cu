@@ -195,10 +195,22 @@ __global__ void __launch_bounds__(SC_NT) k_cumsum_u8(const uint8_t* __restrict__
   const int64_t r0 = tile * SC_TILE + (int64_t)tid * SC_PER;  // thread-contiguous rows
   uint32_t v[SC_PER];
   uint32_t sum = 0;
-  for (int j = 0; j < SC_PER; j++) {
-    int64_t r = r0 + j;
-    v[j] = r < n ? in[r] : 0u;
-    sum += v[j];
+  // a whole run of 16 rows at a 16-byte aligned address: one 128-bit load (streaming: read once)
+  const bool full = r0 + SC_PER <= n;
+  if (full && ((reinterpret_cast<uintptr_t>(in) & 15u) == 0u)) {
+    const uint4 w = __ldcs(reinterpret_cast<const uint4*>(in + r0));
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int j = 0; j < SC_PER; j++) {
+      v[j] = (ws[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+      sum += v[j];
+    }
+  } else {
+    for (int j = 0; j < SC_PER; j++) {
+      int64_t r = r0 + j;
+      v[j] = r < n ? in[r] : 0u;
+      sum += v[j];
+    }
   }
   // warp inclusive scan of per-thread sums
   uint32_t x = sum;
@@ -219,10 +231,21 @@ __global__ void __launch_bounds__(SC_NT) k_cumsum_u8(const uint8_t* __restrict__
   }
   __syncthreads();
   uint32_t run = (uint32_t)s_base + s_warp[warp] + (x - sum);
+#pragma unroll
   for (int j = 0; j < SC_PER; j++) {
     run += v[j];
-    int64_t r = r0 + j;
-    if (r < n) out[r] = run;
+    v[j] = run;
+  }
+  if (full && ((reinterpret_cast<uintptr_t>(out) & 15u) == 0u)) {
+    // four 128-bit streaming stores (the output is not read again by this kernel)
+    uint4* o = reinterpret_cast<uint4*>(out + r0);
+#pragma unroll
+    for (int j = 0; j < SC_PER / 4; j++) __stcs(o + j, make_uint4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]));
+  } else {
+    for (int j = 0; j < SC_PER; j++) {
+      int64_t r = r0 + j;
+      if (r < n) out[r] = v[j];
+    }
   }
 }
 

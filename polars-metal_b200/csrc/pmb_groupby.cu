@@ -126,6 +126,66 @@ __global__ void k_sketch_select(const unsigned long long* __restrict__ set_keys,
   }
 }
 
+// The run-time kernel's table of sampled keys, built on the device from the hot and warm lists so
+// the host never reads them back: `tnb` buckets of 4 slots, keys (4-byte keys when `narrow`, else
+// 8-byte) then 16-bit values (J_HOTBIT-style 0x8000 | hot index, or the warm index). A key goes to
+// the emptier of its two candidate buckets (the kernel's j_hash and the same two bucket choices),
+// hot keys first; a key that finds both buckets full is left out and its rows take the global
+// table, which gives the same results. Empty slots hold the value 0xFFFF, which the lookup reads as
+// a miss whatever their key word. One CTA.
+__device__ __forceinline__ void sample_table_insert(unsigned long long k, unsigned short v, unsigned tnb, bool narrow,
+                                                    unsigned char* tab, unsigned int* fill) {
+  if (k == PMB_EMPTY64 || (narrow && k > 0xFFFFFFFFull)) return;  // never looked up in the table
+  unsigned long long hk;
+  if (narrow) {
+    const uint32_t x = pmb_fmix32((uint32_t)k);
+    hk = ((unsigned long long)x << 32) | x;
+  } else {
+    hk = pmb_fmix64(k);
+  }
+  const unsigned a = (unsigned)(hk >> 32), b = pmb_mix32b(a);
+  unsigned b1 = __umulhi(a, tnb), b2 = __umulhi(b, tnb);
+  if (*(volatile unsigned int*)&fill[b2] < *(volatile unsigned int*)&fill[b1]) {
+    const unsigned t = b1;
+    b1 = b2;
+    b2 = t;
+  }
+  unsigned bk = b1, sl = atomicAdd(&fill[b1], 1u);
+  if (sl >= 4u) {
+    bk = b2;
+    sl = atomicAdd(&fill[b2], 1u);
+    if (sl >= 4u) return;
+  }
+  const unsigned at = 4u * bk + sl;
+  if (narrow) reinterpret_cast<unsigned int*>(tab)[at] = (unsigned int)k;
+  else reinterpret_cast<unsigned long long*>(tab)[at] = k;
+  reinterpret_cast<unsigned short*>(tab + (size_t)tnb * 4u * (narrow ? 4u : 8u))[at] = v;
+}
+
+__global__ void __launch_bounds__(1024) k_sample_table(const unsigned long long* __restrict__ hot,
+                                                       const unsigned int* __restrict__ hot_n, unsigned hot_cap,
+                                                       const unsigned long long* __restrict__ warm,
+                                                       const unsigned int* __restrict__ warm_n, unsigned warm_cap,
+                                                       unsigned tnb, int narrow, unsigned char* __restrict__ tab,
+                                                       unsigned int* __restrict__ fill) {
+  const unsigned slots = 4u * tnb;
+  const unsigned kb = slots * (narrow ? 4u : 8u);
+  for (unsigned i = threadIdx.x; i < slots; i += blockDim.x) {
+    if (narrow) reinterpret_cast<unsigned int*>(tab)[i] = 0xFFFFFFFFu;
+    else reinterpret_cast<unsigned long long*>(tab)[i] = PMB_EMPTY64;
+    reinterpret_cast<unsigned short*>(tab + kb)[i] = 0xFFFFu;
+  }
+  for (unsigned i = threadIdx.x; i < tnb; i += blockDim.x) fill[i] = 0u;
+  __syncthreads();
+  const unsigned nh = hot ? min(*hot_n, hot_cap) : 0u;
+  for (unsigned i = threadIdx.x; i < nh; i += blockDim.x)
+    sample_table_insert(hot[i], (unsigned short)(0x8000u | i), tnb, narrow != 0, tab, fill);
+  __syncthreads();
+  const unsigned nw = warm ? min(*warm_n, warm_cap) : 0u;
+  for (unsigned i = threadIdx.x; i < nw; i += blockDim.x)
+    sample_table_insert(warm[i], (unsigned short)i, tnb, narrow != 0, tab, fill);
+}
+
 // ============================================================================ table init
 __global__ void k_table_init(unsigned long long* __restrict__ keys, int64_t key_words, uint64_t* __restrict__ recs,
                              int64_t n_recs, int rec_words, const __grid_constant__ RecInit ri) {
@@ -812,6 +872,7 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     if (pmb_jit_hash_kernel(h, cq, J, &jk) != PMB_OK) jk = nullptr;  // prebuilt generic kernel: same results
     h->err = keep_err;
   }
+  pmb_phase(h, "jit");
   const int hot_cap = jk ? J.hot_cap : P.hot_cap;
   const int S = jk ? 2 * J.warm_cap : P.smem_slots;
   const int rec = q.rec_bytes;
@@ -857,27 +918,24 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     P.hot_cap = 0;
     P.hot_lut_slots = 0;
   }
-  // run-time kernel: its sampled-key table is built here from the selected key lists
-  std::vector<uint8_t> ttab_host;
+  // run-time kernel: its sampled-key table is built on the device from the selected key lists,
+  // so the launches of this call follow each other without a host round trip
   uint8_t* ttab = nullptr;
   int tnb = 0;
-  if (jk && P.hot_n && (P.hot_keys || P.warm_keys)) {
-    unsigned int cnt[2] = {0, 0};
-    PMB_CUDA(h, cudaMemcpyAsync(cnt, P.hot_n, 8, cudaMemcpyDeviceToHost, h->stream));
-    PMB_CUDA(h, cudaStreamSynchronize(h->stream));
-    const int nh = P.hot_keys ? (int)std::min<unsigned>(cnt[0], (unsigned)hot_cap) : 0;
-    const int nw = P.warm_keys ? (int)std::min<unsigned>(cnt[1], (unsigned)(S / 2)) : 0;
-    std::vector<unsigned long long> hk(nh), wk(nw);
-    if (nh) PMB_CUDA(h, cudaMemcpy(hk.data(), P.hot_keys, 8 * (size_t)nh, cudaMemcpyDeviceToHost));
-    if (nw) PMB_CUDA(h, cudaMemcpy(wk.data(), P.warm_keys, 8 * (size_t)nw, cudaMemcpyDeviceToHost));
-    tnb = pmb_jit_sampled_table(cq, J, hk.data(), nh, wk.data(), nw, &ttab_host);
-    if (tnb > 0) {
-      ttab = (uint8_t*)pmb_ws_alloc(h, ttab_host.size());
-      if (!ttab) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sampled-key table)");
-      PMB_CUDA(h, cudaMemcpyAsync(ttab, ttab_host.data(), ttab_host.size(), cudaMemcpyHostToDevice, h->stream));
-    }
+  if (jk && P.hot_n && (P.hot_keys || P.warm_keys) && J.tnb > 0) {
+    tnb = J.tnb;
+    const size_t tbytes = (size_t)tnb * 4 * (J.tkey + 2);
+    ttab = (uint8_t*)pmb_ws_alloc(h, tbytes + 16);
+    unsigned int* fill = (unsigned int*)pmb_ws_alloc(h, 4 * (size_t)tnb + 16);
+    if (!ttab || !fill) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (sampled-key table)");
+    pmb_kernel_begin(h, "sample_table");
+    k_sample_table<<<1, 1024, 0, h->stream>>>(P.hot_keys, P.hot_n, (unsigned)hot_cap, P.warm_keys, P.warm_n,
+                                              (unsigned)(S / 2), (unsigned)tnb, J.tkey == 4 ? 1 : 0, ttab, fill);
+    pmb_kernel_end(h);
+    PMB_CUDA(h, cudaGetLastError());
   }
   const int64_t n = q.n_rows;
+  pmb_phase(h, "keys");
 
   // Capacity: 4 slots per estimated group (any size: slots come from a multiply-shift, not a
   // mask; sample estimates of skewed keys run low), 2 per group of a caller's hint. A table that
@@ -981,9 +1039,11 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     F.n_groups = lb + fin_tiles + 1;
     rc = K128 ? launch_finalize<true>(h, F, nslots) : launch_finalize<false>(h, F, nslots);
     if (rc) return rc;
+    pmb_phase(h, "launch");
     PMB_CUDA(h, cudaMemcpyAsync(h->pinned, status, 8, cudaMemcpyDeviceToHost, h->stream));
     PMB_CUDA(h, cudaMemcpyAsync(h->pinned + 8, F.n_groups, 8, cudaMemcpyDeviceToHost, h->stream));
     PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+    pmb_phase(h, "device");
     unsigned int st = *(unsigned int*)h->pinned;
     if (st & PMB_ST_TIMEOUT) return pmb_fail(h, PMB_E_TIMEOUT, "a bounded device wait timed out");
     if (st & PMB_ST_FXRANGE) {
@@ -1051,6 +1111,7 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
   rc = pmb_ws_begin(h);
   if (rc) return rc;
   pmb_call_begin(h);
+  pmb_phase(h, "compile");
   pmb_result* r = pmb_result_new(cq.dq.n_keys + cq.dq.n_aggs);
   if (!r) return pmb_fail(h, PMB_E_OOM, "host allocation failed");
   build_output_columns(cq, r, cols);
@@ -1063,6 +1124,7 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     rc = pmb_stage_column(h, cols[cq.map.user[c]], cq.dq.n_rows, &cq.dq.col[c]);
     if (rc) return bail(rc);
   }
+  pmb_phase(h, "stage");
   if (cq.dq.n_rows == 0) {
     r->n_groups = 0;
     r->strategy_used = q->strategy ? q->strategy : PMB_STRATEGY_GLOBAL_HASH;
@@ -1075,8 +1137,11 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     int64_t est = q->capacity_hint;
     static thread_local SketchOut sk;  // large (histogram); one per host thread
     bool have_sk = true;
+    // the selector's kernels go in before the sketch's readback, whose synchronisation serves both
+    const bool sel = strategy == PMB_STRATEGY_AUTO && pmb_selector_launch(h, cq);
     rc = pmb_groupby_sketch(h, cq, &sk);
     if (rc) return bail(rc);
+    pmb_phase(h, "sketch");
     // fixed-point range of the float sums: sample maximum with 8x headroom; partial sums of a
     // CTA (at most n / SMs values, with margin) must fit as well
     int pbits = 2, tbits = 2;
@@ -1096,7 +1161,7 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
       // one only its initialisation
       int s = 0;
       int64_t g = 0;
-      if (pmb_selector_pick(h, cq, &s, &g)) {
+      if (sel && pmb_selector_read(h, cq, &s, &g)) {
         strategy = s;
         if (est <= 0) est = std::max<int64_t>(e, std::min<int64_t>(g, cq.dq.n_rows));
       } else {
@@ -1106,6 +1171,7 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     }
     if (est <= 0) est = e;
     if (q->strategy == PMB_STRATEGY_AUTO && pmb_prefer_partitioned(cq, sk, strategy, est)) strategy = PMB_STRATEGY_PARTITIONED;
+    pmb_phase(h, "choose");
     if (strategy == PMB_STRATEGY_SORT) rc = pmb_groupby_sort(h, cq, r, 0);
     else if (strategy == PMB_STRATEGY_PARTITIONED) rc = pmb_groupby_sort(h, cq, r, std::max<int64_t>(est, 1));
     else rc = pmb_groupby_hash(h, cq, q, strategy, est, have_sk ? &sk : nullptr, r);
@@ -1118,9 +1184,11 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
     if (rc) return bail(rc == PMB_RETRY_DD ? pmb_fail(h, PMB_E_CUDA, "float-sum range did not converge") : rc);
     break;
   }
+  pmb_phase(h, "strategy");
   rc = pmb_finish_outputs(h, r, q->output_on_device == 0);
   if (rc) return bail(rc);
   PMB_CUDA(h, cudaStreamSynchronize(h->stream));
+  pmb_phase(h, "outputs");
   pmb_call_end(h);
   *out = r;
   return PMB_OK;

@@ -101,6 +101,12 @@ int pmb_order_columns(pmb_handle* h, const DCol* cols, int n_cols, int64_t n, co
 // learned selector (pmb_learned.cu): strategy and group count for AUTO; false when no selector is
 // installed or its output is unusable
 bool pmb_selector_pick(pmb_handle* h, const CompiledQuery& cq, int* strategy, int64_t* groups);
+// the same in two halves: the launch queues the selector's kernels and the copy of its outputs into
+// the pinned staging at PMB_SEL_PINNED_OFF (false: no selector); the read decodes them after the
+// caller's next stream synchronisation
+#define PMB_SEL_PINNED_OFF 61440
+bool pmb_selector_launch(pmb_handle* h, const CompiledQuery& cq);
+bool pmb_selector_read(pmb_handle* h, const CompiledQuery& cq, int* strategy, int64_t* groups);
 // group counts the selector predicts for a batch of queries (device DQuery array); false without
 // an installed selector
 bool pmb_selector_predict_batch(pmb_handle* h, const DQuery* d_qs, int nq, int64_t* out_groups, const int64_t* n_rows);

@@ -183,6 +183,11 @@ struct pmb_handle {
   size_t hstage_cap = 0, hstage_used = 0, hstage_want = 0;
   // profiling
   bool profiling = false;
+  bool batching = true;  // pmb_groupby_batched may batch (else: one pmb_groupby per query)
+  // host phases of a call (PMB_CALL_TIMING=1 prints them to stderr at the end of the call)
+  bool phase_timing = false;
+  std::vector<std::pair<const char*, double>> phases;
+  double phase_t0 = 0.0;
   std::vector<KernelTiming> timings;
   std::vector<cudaEvent_t> event_pool;
   size_t event_next = 0;
@@ -225,6 +230,7 @@ inline size_t pmb_align(size_t x, size_t a) { return (x + a - 1) / a * a; }
 // profiling around launches (pmb_runtime.cu)
 void pmb_call_begin(pmb_handle* h);
 void pmb_call_end(pmb_handle* h);  // after the final stream synchronisation
+void pmb_phase(pmb_handle* h, const char* name);  // host time since the previous phase mark
 void pmb_kernel_begin(pmb_handle* h, const char* name);
 void pmb_kernel_end(pmb_handle* h);
 

@@ -210,6 +210,29 @@ struct Gen {
     return {xv, ov};
   }
 
+  // "x is a multiple of d" for a signed 64-bit x and a literal d != 0 without a division: with
+  // |d| = 2^k * o (o odd), the low k bits of x are zero and, for o > 1, x * o^-1 + c <= 2c modulo
+  // 2^64 where c = floor((2^63 - 1) / o) (the multiplicative-inverse divisibility test of Granlund
+  // and Montgomery, 1994, in its signed form; Lemire, Kaser and Kurz, 2019)
+  static std::string divisible(const std::string& x, long long d) {
+    unsigned long long a = d < 0 ? 0ULL - (unsigned long long)d : (unsigned long long)d;
+    int k = 0;
+    while (((a >> k) & 1ULL) == 0ULL) k++;
+    const unsigned long long o = a >> k;
+    std::string e = "(";
+    if (k > 0) e += "((unsigned long long)(" + x + ") & " + std::to_string((1ULL << k) - 1ULL) + "ULL) == 0ULL";
+    if (o > 1) {
+      unsigned long long inv = o;  // Newton iteration for the inverse modulo 2^64 (5 steps from 3 bits)
+      for (int i = 0; i < 5; i++) inv *= 2ULL - o * inv;
+      const unsigned long long c = 0x7FFFFFFFFFFFFFFFULL / o;
+      if (k > 0) e += " && ";
+      e += "((unsigned long long)(" + x + ") * " + std::to_string(inv) + "ULL + " + std::to_string(c) + "ULL) <= " +
+           std::to_string(2 * c) + "ULL";
+    }
+    if (k == 0 && o == 1) e += "true";
+    return e + ")";
+  }
+
   std::string predicate(std::ostringstream& b) {
     const DProgram& PR = q.prog;
     if (PR.n_ops == 0) return "true";
@@ -230,8 +253,7 @@ struct Gen {
                 T.rhs.a.i == 0) {
               auto x = leaf(T.lhs.a, T.dtype);
               b << "    bool " << t << "v = " << x.second << ";\n";
-              b << "    bool " << t << "c = (" << x.first << " % " << lit_i64(T.lhs.b.i) << ") "
-                << (T.op == PMB_CMP_EQ ? "==" : "!=") << " 0LL;\n";
+              b << "    bool " << t << "c = " << (T.op == PMB_CMP_EQ ? "" : "!") << divisible(x.first, T.lhs.b.i) << ";\n";
               b << "    bool " << t << " = " << t << "v && " << t << "c, " << f << " = " << t << "v && !" << t << "c;\n";
               break;
             }
@@ -1006,90 +1028,6 @@ extern "C" int pmb_debug_jit_compile_batch(const pmb_query* q, const pmb_column*
 extern "C" int pmb_debug_jit_compile_part(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,
                                           int64_t log_cap) {
   return debug_compile(q, cols, n_cols, log, log_cap, 2);
-}
-
-int pmb_jit_sampled_table(const CompiledQuery& cq, const JitPlan& J, const unsigned long long* hot, int n_hot,
-                          const unsigned long long* warm, int n_warm, std::vector<uint8_t>* out) {
-  out->clear();
-  const int n = n_hot + n_warm;
-  if (n == 0 || J.tnb == 0) return 0;
-  const bool narrow = J.tkey == 4;
-  // the kernel's key hash (j_hash) and the two candidate buckets
-  auto hash = [&](unsigned long long k) -> unsigned long long {
-    if (narrow) {
-      uint32_t x = pmb_fmix32((uint32_t)k);
-      return ((unsigned long long)x << 32) | x;
-    }
-    return pmb_fmix64(k);
-  };
-  std::vector<unsigned long long> keys;
-  std::vector<uint16_t> vals;
-  keys.reserve(n);
-  for (int i = 0; i < n_hot; i++) {
-    keys.push_back(hot[i]);
-    vals.push_back((uint16_t)(0x8000u | (unsigned)i));
-  }
-  for (int i = 0; i < n_warm; i++) {
-    keys.push_back(warm[i]);
-    vals.push_back((uint16_t)i);
-  }
-  // a marker key outside the sampled set for empty slots (its rows miss, as they should)
-  unsigned long long mark = narrow ? 0xFFFFFFFFull : PMB_EMPTY64;
-  {
-    std::vector<unsigned long long> sorted(keys);
-    std::sort(sorted.begin(), sorted.end());
-    while (std::binary_search(sorted.begin(), sorted.end(), mark)) mark--;
-  }
-  int nb = std::min(J.tnb, std::max(2, (((n * 5) / 16 + 2) + 1) & ~1));
-  std::vector<unsigned long long> tk;
-  std::vector<uint16_t> tv;
-  uint32_t rng = 0x9E3779B9u;
-  for (;;) {
-    tk.assign((size_t)nb * 4, mark);
-    tv.assign((size_t)nb * 4, 0xFFFFu);
-    int dropped = 0;
-    for (size_t i = 0; i < keys.size(); i++) {
-      unsigned long long k = keys[i];
-      uint16_t v = vals[i];
-      if (k == PMB_EMPTY64 || (narrow && k > 0xFFFFFFFFull)) continue;  // never looked up in the table
-      bool placed = false;
-      for (int step = 0; step < 512 && !placed; step++) {
-        const unsigned long long hk = hash(k);
-        const uint32_t a = (uint32_t)(hk >> 32), b = pmb_mix32b(a);
-        const uint32_t bk[2] = {(uint32_t)(((uint64_t)a * (uint32_t)nb) >> 32),
-                                (uint32_t)(((uint64_t)b * (uint32_t)nb) >> 32)};
-        for (int c = 0; c < 2 && !placed; c++)
-          for (int sl = 0; sl < 4; sl++)
-            if (tk[(size_t)bk[c] * 4 + sl] == mark) {
-              tk[(size_t)bk[c] * 4 + sl] = k;
-              tv[(size_t)bk[c] * 4 + sl] = v;
-              placed = true;
-              break;
-            }
-        if (placed) break;
-        // both buckets full: displace a random resident and re-insert it
-        rng = rng * 1664525u + 1013904223u;
-        const size_t at = (size_t)bk[(rng >> 16) & 1] * 4 + ((rng >> 20) & 3);
-        std::swap(k, tk[at]);
-        std::swap(v, tv[at]);
-      }
-      if (!placed) dropped++;  // the key left over is served by the global table
-    }
-    if (dropped == 0 || nb >= J.tnb) break;
-    nb = std::min(J.tnb, ((nb + nb / 8 + 2) + 1) & ~1);
-  }
-  const size_t kb = (size_t)nb * 4 * J.tkey, vb = (size_t)nb * 8;
-  out->assign(kb + vb, 0);
-  for (size_t i = 0; i < (size_t)nb * 4; i++) {
-    if (narrow) {
-      uint32_t k32 = (uint32_t)tk[i];
-      memcpy(out->data() + 4 * i, &k32, 4);
-    } else {
-      memcpy(out->data() + 8 * i, &tk[i], 8);
-    }
-  }
-  memcpy(out->data() + kb, tv.data(), vb);
-  return nb;
 }
 
 int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const JitPlan& J, const HashParams& P,

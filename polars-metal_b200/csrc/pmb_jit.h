@@ -54,14 +54,6 @@ void pmb_jit_slayout(const DQuery& q, JitSLayout* S);
 
 int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int max_smem_optin, JitPlan* J);
 
-// Builds the sampled-key table of the run-time kernel on the host: a bucketed cuckoo table (two
-// candidate buckets of 4 slots per key) holding the hot keys (value 0x8000 | index) and the warm
-// keys (value index), laid out as keys of all buckets then 16-bit values. Keys that do not fit
-// are left out (their rows take the global table: slower, same results). Returns the bucket
-// count (even, at most J.tnb) and the bytes in `out`.
-int pmb_jit_sampled_table(const CompiledQuery& cq, const JitPlan& J, const unsigned long long* hot, int n_hot,
-                          const unsigned long long* warm, int n_warm, std::vector<uint8_t>* out);
-
 // JIT policy: PMB_JIT=0 never, PMB_JIT=1 always, otherwise inputs of at least 2M rows
 bool pmb_jit_enabled(int64_t n_rows);
 // compiled kernel for this signature and layout (cached); PMB_E_UNSUPPORTED when unavailable

@@ -45,7 +45,7 @@ struct JParams {
   const unsigned long long* warm_keys;
   const unsigned int* warm_n;
   unsigned long long* kstats;
-  const unsigned char* ttab;  // sampled-key table built by the host: keys of all buckets, then values
+  const unsigned char* ttab;  // sampled-key table (k_sample_table): keys of all buckets, then values
   int tnb;                    // its buckets (4 slots each), at most J_TNB
   int flags;                  // batched kernel: bit 0 = fill the CTA's warm table
   int fx[8];    // fraction bits F of each exact float-sum slot (sums hold x * 2^F)
@@ -96,9 +96,9 @@ __device__ __forceinline__ long long j_gfind(const JParams& P, unsigned long lon
   return j_gresolve(P, key, h, claimed);
 }
 
-// The CTA's table of sampled keys (hot and warm), built by the host as a bucketed cuckoo table:
-// every key sits in one of its two 4-slot buckets, so a lookup is two bucket loads and no loop.
-// Empty slots hold a key outside the sampled set and the value 0xFFFF. Returns the key's value
+// The CTA's table of sampled keys (hot and warm), built on the device by k_sample_table: every
+// placed key sits in one of its two 4-slot buckets, so a lookup is two bucket loads and no loop.
+// Empty slots hold the value 0xFFFF (a miss whatever their key word). Returns the key's value
 // (J_HOTBIT | hot index, or warm index) or J_MISS.
 __device__ __forceinline__ unsigned j_tvalue(unsigned short v) {
   return v == 0xFFFFu ? J_MISS : ((v & 0x8000u) ? (J_HOTBIT | (v & 0x7FFFu)) : (unsigned)v);

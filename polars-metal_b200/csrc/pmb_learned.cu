@@ -308,6 +308,43 @@ bool pmb_selector_predict_batch(pmb_handle* h, const DQuery* d_qs, int nq, int64
 
 // AUTO strategy with the installed selector: false when none is installed or its output is not
 // usable (the caller then takes the cardinality heuristic)
+// The selector's scores and group count from its outputs (false when unusable)
+static bool selector_decode(const float* o, int64_t n_rows, int* strategy, int64_t* groups) {
+  for (int k = 0; k < NO; k++)
+    if (!std::isfinite(o[k])) return false;
+  int best = 0;
+  for (int k = 1; k < 3; k++)
+    if (o[k] > o[best]) best = k;
+  static const int map[3] = {PMB_STRATEGY_SMEM_HASH, PMB_STRATEGY_GLOBAL_HASH, PMB_STRATEGY_SORT};
+  *strategy = map[best];
+  const double g = std::exp2(std::min<double>(std::max<double>(o[3], 0.0), 40.0));
+  *groups = (int64_t)std::min<double>(g, (double)n_rows);
+  if (*groups < 1) *groups = 1;
+  return true;
+}
+
+// pmb_selector_pick in two halves around a synchronisation the caller makes anyway: the launch
+// queues the feature and MLP kernels and the copy of the outputs into the handle's pinned staging
+// (at PMB_SEL_PINNED_OFF); the read decodes them once the stream has been synchronised.
+bool pmb_selector_launch(pmb_handle* h, const CompiledQuery& cq) {
+  if (!h->selector || cq.dq.n_rows == 0) return false;
+  float* buf = (float*)pmb_ws_alloc(h, (NF + NO) * sizeof(float));
+  if (!buf) return false;
+  if (features_device(h, cq, buf) != PMB_OK) return false;
+  pmb_kernel_begin(h, "mlp_forward");
+  k_mlp_forward<<<1, NH, 0, h->stream>>>(h->selector, buf, 1, buf + NF);
+  pmb_kernel_end(h);
+  if (cudaGetLastError() != cudaSuccess) return false;
+  return cudaMemcpyAsync(h->pinned + PMB_SEL_PINNED_OFF, buf + NF, NO * sizeof(float), cudaMemcpyDeviceToHost,
+                         h->stream) == cudaSuccess;
+}
+
+bool pmb_selector_read(pmb_handle* h, const CompiledQuery& cq, int* strategy, int64_t* groups) {
+  float o[NO];
+  memcpy(o, h->pinned + PMB_SEL_PINNED_OFF, sizeof(o));
+  return selector_decode(o, cq.dq.n_rows, strategy, groups);
+}
+
 bool pmb_selector_pick(pmb_handle* h, const CompiledQuery& cq, int* strategy, int64_t* groups) {
   if (!h->selector || cq.dq.n_rows == 0) return false;
   float* buf = (float*)pmb_ws_alloc(h, (NF + NO) * sizeof(float));
@@ -320,17 +357,7 @@ bool pmb_selector_pick(pmb_handle* h, const CompiledQuery& cq, int* strategy, in
   float o[NO];
   if (cudaMemcpyAsync(o, buf + NF, sizeof(o), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess) return false;
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return false;
-  for (int k = 0; k < NO; k++)
-    if (!std::isfinite(o[k])) return false;
-  int best = 0;
-  for (int k = 1; k < 3; k++)
-    if (o[k] > o[best]) best = k;
-  static const int map[3] = {PMB_STRATEGY_SMEM_HASH, PMB_STRATEGY_GLOBAL_HASH, PMB_STRATEGY_SORT};
-  *strategy = map[best];
-  const double g = std::exp2(std::min<double>(std::max<double>(o[3], 0.0), 40.0));
-  *groups = (int64_t)std::min<double>(g, (double)cq.dq.n_rows);
-  if (*groups < 1) *groups = 1;
-  return true;
+  return selector_decode(o, cq.dq.n_rows, strategy, groups);
 }
 
 extern "C" int pmb_selector_features(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols,

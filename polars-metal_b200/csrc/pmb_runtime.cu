@@ -12,6 +12,8 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <chrono>
+#include <cstdio>
 #include <string>
 
 #include "pmb_internal.cuh"
@@ -118,7 +120,21 @@ static cudaEvent_t take_event(pmb_handle* h) {
   return h->event_pool[h->event_next++];
 }
 
+static double host_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void pmb_phase(pmb_handle* h, const char* name) {
+  if (!h->phase_timing) return;
+  const double t = host_ms();
+  h->phases.push_back({name, t - h->phase_t0});
+  h->phase_t0 = t;
+}
+
 void pmb_call_begin(pmb_handle* h) {
+  h->phase_timing = getenv("PMB_CALL_TIMING") != nullptr;
+  h->phases.clear();
+  if (h->phase_timing) h->phase_t0 = host_ms();
   h->timings.clear();
   h->event_next = 0;
   h->launches = 0;
@@ -168,6 +184,14 @@ void pmb_call_end(pmb_handle* h) {
     }
   }
   h->last_stats = s;
+  if (h->phase_timing) {
+    pmb_phase(h, "end");
+    double total = 0.0;
+    for (auto& ph : h->phases) total += ph.second;
+    fprintf(stderr, "pmb call %.3f ms host:", total);
+    for (auto& ph : h->phases) fprintf(stderr, " %s %.3f", ph.first, ph.second);
+    fprintf(stderr, "\n");
+  }
 }
 
 // ------------------------------------------------------------------ staging kernels
@@ -432,6 +456,12 @@ int pmb_set_stream(pmb_handle* h, void* stream) {
 int pmb_set_profiling(pmb_handle* h, int32_t enabled) {
   if (!h) return PMB_E_INVALID;
   h->profiling = enabled != 0;
+  return PMB_OK;
+}
+
+int pmb_set_batching(pmb_handle* h, int32_t enabled) {
+  if (!h) return PMB_E_INVALID;
+  h->batching = enabled != 0;
   return PMB_OK;
 }
 

@@ -217,6 +217,7 @@ SIGNATURES = {
     "pmb_last_error": (C.c_char_p, [_H]),
     "pmb_set_stream": (C.c_int, [_H, _P]),
     "pmb_set_profiling": (C.c_int, [_H, C.c_int32]),
+    "pmb_set_batching": (C.c_int, [_H, C.c_int32]),
     "pmb_last_stats": (C.c_int, [_H, C.POINTER(Stats)]),
     "pmb_version": (C.c_char_p, []),
     "pmb_groupby": (C.c_int, [_H, C.POINTER(Query), C.POINTER(Column), C.c_int32, C.POINTER(C.POINTER(Result))]),

@@ -97,6 +97,11 @@ class Handle:
     def set_profiling(self, on: bool) -> None:
         self.check(self._lib.pmb_set_profiling(self._h, 1 if on else 0))
 
+    def set_batching(self, on: bool) -> None:
+        """False: groupby_batched runs each query alone through pmb_groupby, looped inside the
+        library (host outputs only); True (default): it batches where it can."""
+        self.check(self._lib.pmb_set_batching(self._h, 1 if on else 0))
+
     def last_stats(self) -> dict:
         s = A.Stats()
         self.check(self._lib.pmb_last_stats(self._h, C.byref(s)))

@@ -301,7 +301,7 @@ def test_remainder_zero_tests_on_both_kernels(jit, monkeypatch):
     cols["y"][0][:4] = [np.iinfo(np.int64).min, np.iinfo(np.int64).max, -7, 0]
     col = lambda c: {"kind": "Column", "name": c}  # noqa: E731
     aggs = [("Sum", "x", "s"), ("Count", "y", "c"), ("Min", "y", "lo"), ("Len", None, "n")]
-    for c in (7, -7, 3, 2, -1, 1000003):
+    for c in (7, -7, 3, 2, -1, 1000003, 12, -(2**63), 3 * 2**40):
         for op in ("Eq", "Ne"):
             p = {"kind": "Compare", "op": op, "dtype": "I64",
                  "lhs": {"kind": "Arith", "op": "Mod", "lhs": col("y"), "rhs": {"kind": "LiteralI64", "value": c}},
