@@ -7,7 +7,8 @@
 //      singletons (the group estimate), the heaviest keys (the hot keys of the query) and the
 //      float-sum ranges; with an installed strategy selector its predicted group count can only
 //      enlarge the estimate;
-//   2. the host sizes every query's global table (2.5 slots per estimated group) inside one arena,
+//   2. the host sizes every query's global table (2.5 slots per estimated group, or the tuned
+//      count) inside one arena,
 //      cuts the queries into work items (query, range of 128-row units) and uploads them;
 //   3. one init kernel, the persistent run-time compiled kernel pmb_jit_batch_agg over the work
 //      queue, and k_batch_finalize (every query's occupied slots into its output columns, in slot
@@ -15,8 +16,9 @@
 //      stays the same;
 //   4. queries whose table overflowed or whose float sums left their range run again, alone in a
 //      second batch round with a larger table / wider range.
-// The item size and block size come from a small autotuner: the first batch of a signature
-// times each candidate on its real data and keeps the fastest for the process.
+// The block size, item size, unit buffers, warm rule, shared-table (warm) capacity and global-table
+// capacity come from a small autotuner: the first batch of a signature times each candidate on its
+// real data and keeps the fastest for the process.
 // Other queries (other signatures, 128-bit keys, no NVRTC) run one by one through pmb_groupby.
 #include <cuda_runtime.h>
 
@@ -310,6 +312,9 @@ struct TuneChoice {
   int nbuf = 2;       // unit buffers per warp
   int warm_rule = 1;  // 0: every query fills a warm table; 1: only queries whose groups fit it, or
                       // whose items hold at least as many rows as the query has groups
+  int warm_max = 0;   // shared-table capacity: CTA warm-table slots at most (0: the largest that fits);
+                      // a smaller table is cheaper to reset at every work item
+  int gslots_x2 = 5;  // global-table capacity: 2 x slots per estimated group (5 = 2.5 slots)
 };
 std::mutex g_tune_mu;
 std::map<std::string, TuneChoice> g_tuned;  // signature + size class -> choice
@@ -332,7 +337,7 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
   const CompiledQuery& c0 = cqs[qidx[0]];
   const int rec = c0.dq.rec_bytes;
   JitPlan J;
-  int rc = pmb_plan_jit_batch(h, c0, tc.nt, tc.nbuf, h->max_smem_optin, &J);
+  int rc = pmb_plan_jit_batch(h, c0, tc.nt, tc.nbuf, h->max_smem_optin, &J, tc.warm_max);
   if (rc) return rc;
   cudaKernel_t k = nullptr;
   rc = pmb_jit_batch_kernel(h, c0, J, &k);
@@ -342,7 +347,7 @@ static int batch_round(pmb_handle* h, std::vector<CompiledQuery>& cqs, const std
   std::vector<uint64_t> cap(nq);
   for (int i = 0; i < nq; i++) {
     const CompiledQuery& cq = cqs[qidx[i]];
-    uint64_t c = (uint64_t)std::max<int64_t>(est[qidx[i]] * 5 / 2, 1024);  // 2.5 slots per estimated group
+    uint64_t c = (uint64_t)std::max<int64_t>(est[qidx[i]] * tc.gslots_x2 / 2, 1024);  // tuned slots per group
     if (const char* e = getenv("PMB_GCAP_MULT")) {  // tuning override, as for single queries
       const double k = atof(e);
       if (k > 0) c = (uint64_t)std::max(1024.0, (double)c * k);
@@ -735,8 +740,14 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
       }
     }
     if (!have && !getenv("PMB_NO_AUTOTUNE")) {
-      static const TuneChoice cands[] = {{1024, 256, 1, 0}, {1024, 256, 2, 0}, {1024, 256, 2, 1}, {1024, 64, 2, 1},
-                                         {1024, 1024, 2, 1}, {512, 256, 2, 1},  {512, 1024, 2, 1}};
+      // block size, work-item size (rows of a query per item), unit buffers per warp, warm rule,
+      // shared-table capacity (warm slots) and global-table capacity (slots per estimated group);
+      // the reference fixes the counterparts (16 partitions, groupby.rs:533; 1024 threadgroup
+      // slots, groupby_build_partitioned_build.metal:36-37)
+      static const TuneChoice cands[] = {
+          {1024, 256, 1, 0, 0, 5},    {1024, 256, 2, 0, 0, 5},    {1024, 256, 2, 1, 0, 5},    {1024, 64, 2, 1, 0, 5},
+          {1024, 1024, 2, 1, 0, 5},   {512, 256, 2, 1, 0, 5},     {512, 1024, 2, 1, 0, 5},    {1024, 256, 2, 1, 4096, 5},
+          {1024, 256, 2, 1, 1024, 5}, {1024, 256, 2, 1, 0, 3},    {1024, 256, 2, 1, 0, 8}};
       float best = 1e30f;
       for (const TuneChoice& c : cands) {
         float ms = 0;
@@ -745,8 +756,8 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
         if (rc) return fail_all(rc);
         pmb_ws_release(h, mark);
         if (timing)
-          fprintf(stderr, "batch tuning candidate %d threads / %d units / %d buffers / warm rule %d: %.3f ms\n", c.nt,
-                  c.item_units, c.nbuf, c.warm_rule, ms);
+          fprintf(stderr, "batch tuning candidate %d threads / %d units / %d buffers / warm rule %d / warm max %d / "
+                  "slots x2 %d: %.3f ms\n", c.nt, c.item_units, c.nbuf, c.warm_rule, c.warm_max, c.gslots_x2, ms);
         if (ms < best) {
           best = ms;
           tc = c;
@@ -756,8 +767,8 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
       g_tuned[tkey] = tc;
     }
     if (timing)
-      fprintf(stderr, "batch tuning: %d threads, %d units per item, %d buffers, warm rule %d\n", tc.nt, tc.item_units,
-              tc.nbuf, tc.warm_rule);
+      fprintf(stderr, "batch tuning: %d threads, %d units per item, %d buffers, warm rule %d, warm max %d, slots x2 %d\n",
+              tc.nt, tc.item_units, tc.nbuf, tc.warm_rule, tc.warm_max, tc.gslots_x2);
     // 4. the rounds: queries grouped by record layout (a query whose float sums would have too few
     //    fraction bits sums them in double-double: another layout); queries that overflowed (3x
     //    table) or left their float-sum range (already widened) run again

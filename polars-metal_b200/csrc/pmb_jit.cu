@@ -882,7 +882,8 @@ int pmb_jit_hash_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J
   return jit_kernel(h, pmb_jit_source(cq, J), "pmb_jit_hash_agg", out);
 }
 
-int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf, int max_smem_optin, JitPlan* J) {
+int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf, int max_smem_optin, JitPlan* J,
+                       int warm_max) {
   const DQuery& q = cq.dq;
   memset(J, 0, sizeof(*J));
   J->nt = nt;
@@ -922,7 +923,8 @@ int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf,
   while (hot > 0 && (int)pmb_align((size_t)used, 16) + 64 + W * hot * J->srec > budget) hot /= 2;
   int warm = 0;
   for (int sw = 1 << 14; sw >= 64; sw /= 2)
-    if ((int)pmb_align((size_t)used, 16) + 8 * sw + 64 + (W * hot + sw) * J->srec <= budget) {
+    if ((warm_max <= 0 || sw <= warm_max) &&
+        (int)pmb_align((size_t)used, 16) + 8 * sw + 64 + (W * hot + sw) * J->srec <= budget) {
       warm = sw;
       break;
     }

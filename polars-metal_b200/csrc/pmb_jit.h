@@ -96,7 +96,9 @@ int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, b
 
 // the batched kernel (pmb_jit_batch.cuh): layout for `nt` threads with `nbuf` unit buffers per
 // warp, and its compiled kernel
-int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf, int max_smem_optin, JitPlan* J);
+// warm_max > 0 caps the CTA's warm table (slots; the largest power of two that fits otherwise)
+int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf, int max_smem_optin, JitPlan* J,
+                       int warm_max = 0);
 int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out);
 // launches over the global table and key lists set up in P (gkeys, grecs, gcap, status, lists)
 int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const JitPlan& J, const HashParams& P,
