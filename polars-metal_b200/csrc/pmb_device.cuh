@@ -78,10 +78,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// try_wait with a suspend-time hint: the thread may sleep up to `ns` nanoseconds for the phase
+// instead of spinning, which leaves the issue slots to the warps that have work
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(pmb_smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
 // bounded wait; returns false on timeout
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
   for (uint32_t it = 0; it < PMB_SPIN_LIMIT; it++)
     if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// bounded wait that sleeps between tests (at most PMB_SPIN_LIMIT tests of at most `ns` each)
+__device__ __forceinline__ bool mbar_wait_bounded_sleep(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  for (uint32_t it = 0; it < PMB_SPIN_LIMIT; it++)
+    if (mbar_try_wait_hint(bar, parity, ns)) return true;
   return false;
 }
 

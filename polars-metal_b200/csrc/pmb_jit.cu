@@ -149,8 +149,9 @@ struct Gen {
     return "reinterpret_cast<const " + std::string(ctype(C.dtype)) + "*>(st + " + d + ")[lr]";
   }
   std::string load_valid(int c) {
+    // the bit of row lr from the unit's 32-bit validity word of rows lr & ~31 (voff is 16-aligned)
     std::string vo = std::to_string(P.voff[c]);
-    return "(((st[" + vo + " + (lr >> 3)] >> (lr & 7)) & 1) != 0)";
+    return "(((reinterpret_cast<const unsigned int*>(st + " + vo + ")[lr >> 5] >> (lr & 31)) & 1u) != 0u)";
   }
 
   void row_struct() {
@@ -577,6 +578,7 @@ struct Gen {
     std::vector<bool> pk(q.n_cols, false), kc(q.n_cols, false);
     for (int c = 0; c < q.n_cols; c++) pk[c] = pred_col[c] || key_col[c];
     for (int k = 0; k < q.n_keys; k++) kc[q.key[k].col] = true;
+    o << "#define J_WAIT_NS " << P.wait_ns << "\n";
     o << "#define J_NT " << P.nt << "\n#define J_NBUF " << P.nbuf << "\n#define J_OFF_BARS " << P.off_bars
       << "\n#define J_OFF_BUF " << P.off_buf << "\n#define J_BUF_BYTES " << P.buf_bytes << "\n#define J_OFF_Q " << P.off_q
       << "\n#define J_OFF_TKEYS " << P.off_tkeys << "\n#define J_OFF_TVAL " << P.off_tval << "\n#define J_TKEY " << P.tkey
@@ -748,6 +750,8 @@ int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int m
   memset(J, 0, sizeof(*J));
   J->nt = 1024;
   J->nbuf = 1;
+  J->wait_ns = 0;
+  if (const char* e = getenv("PMB_WAIT_NS")) J->wait_ns = std::max(0, std::min(atoi(e), 100000));
   if (const char* e = getenv("PMB_NT")) {
     int v = atoi(e);
     if (v == 256 || v == 512 || v == 1024) J->nt = v;

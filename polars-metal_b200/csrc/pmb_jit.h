@@ -31,6 +31,7 @@ struct JitParams {
 // table of sampled keys, hot records (one per warp and key) and warm records (one per key)
 struct JitPlan {
   int nt, nbuf;       // threads per CTA; unit buffers per warp (2: the next unit is in flight)
+  int wait_ns;        // > 0: unit waits sleep up to this many ns per test instead of spinning
   int buf_bytes;      // one unit buffer
   int tx_bytes;       // bytes the bulk copies of one unit deliver
   int doff[16];       // column data offset inside a unit buffer

@@ -192,7 +192,11 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
     if (rows == J_UNIT) {
       bool ok = true;
       if (lane == 0) {
+#if J_WAIT_NS > 0
+        ok = mbar_wait_bounded_sleep(&bars[b], (parity >> b) & 1u, J_WAIT_NS);
+#else
         ok = mbar_wait_bounded(&bars[b], (parity >> b) & 1u);
+#endif
         if (ok) {
           parity ^= 1u << b;
           pending &= ~(1u << b);
