@@ -737,10 +737,26 @@ bool pmb_jit_enabled(int64_t n_rows) {
   return n_rows >= (1LL << 21);
 }
 
+// The hash kernel's skeleton text: the embedded one, or (for kernel development) the text of the
+// file PMB_JIT_SKELETON names, which must define the same kernel and parameter block
+static std::string hash_skeleton() {
+  if (const char* path = getenv("PMB_JIT_SKELETON")) {
+    if (FILE* f = fopen(path, "rb")) {
+      std::string t;
+      char buf[65536];
+      size_t n;
+      while ((n = fread(buf, 1, sizeof buf, f)) > 0) t.append(buf, n);
+      fclose(f);
+      if (t.find("__device__ __forceinline__ long long j_gresolve") != std::string::npos) return t;
+    }
+  }
+  return std::string(kSkeleton);
+}
+
 std::string pmb_jit_source(const CompiledQuery& cq, const JitPlan& J) {
   Gen g(cq.dq, J);
   // order: device helpers, the skeleton's parameter block, the generated row program, the kernel
-  std::string skel(kSkeleton);
+  std::string skel = hash_skeleton();
   size_t cut = skel.find("__device__ __forceinline__ long long j_gresolve");
   return std::string(kDeviceHeader) + "\n" + skel.substr(0, cut) + "\n" + g.build() + "\n" + skel.substr(cut);
 }
