@@ -128,11 +128,11 @@ __global__ void k_sketch_select(const unsigned long long* __restrict__ set_keys,
 
 // The run-time kernel's table of sampled keys, built on the device from the hot and warm lists so
 // the host never reads them back: `tnb` buckets of 4 slots, keys (4-byte keys when `narrow`, else
-// 8-byte) then 16-bit values (J_HOTBIT-style 0x8000 | hot index, or the warm index). A key goes to
-// the emptier of its two candidate buckets (the kernel's j_hash and the same two bucket choices),
-// hot keys first; a key that finds both buckets full is left out and its rows take the global
-// table, which gives the same results. Empty slots hold the value 0xFFFF, which the lookup reads as
-// a miss whatever their key word. One CTA.
+// 8-byte) then 16-bit values (0x8000 | hot index, or the warm index). A key takes a slot of its
+// first bucket (the kernel's j_hash) and, only when that bucket is full, of its second: so a first
+// bucket with an empty slot holds every key whose first choice it is, and the lookup stops there.
+// Hot keys go in first; a key that finds both buckets full is left out and its rows take the
+// global table, which gives the same results. Empty slots hold the value 0xFFFF. One CTA.
 __device__ __forceinline__ void sample_table_insert(unsigned long long k, unsigned short v, unsigned tnb, bool narrow,
                                                     unsigned char* tab, unsigned int* fill) {
   if (k == PMB_EMPTY64 || (narrow && k > 0xFFFFFFFFull)) return;  // never looked up in the table
@@ -143,17 +143,11 @@ __device__ __forceinline__ void sample_table_insert(unsigned long long k, unsign
   } else {
     hk = pmb_fmix64(k);
   }
-  const unsigned a = (unsigned)(hk >> 32), b = pmb_mix32b(a);
-  unsigned b1 = __umulhi(a, tnb), b2 = __umulhi(b, tnb);
-  if (*(volatile unsigned int*)&fill[b2] < *(volatile unsigned int*)&fill[b1]) {
-    const unsigned t = b1;
-    b1 = b2;
-    b2 = t;
-  }
-  unsigned bk = b1, sl = atomicAdd(&fill[b1], 1u);
+  const unsigned a = (unsigned)(hk >> 32);
+  unsigned bk = __umulhi(a, tnb), sl = atomicAdd(&fill[bk], 1u);
   if (sl >= 4u) {
-    bk = b2;
-    sl = atomicAdd(&fill[b2], 1u);
+    bk = __umulhi(pmb_mix32b(a), tnb);
+    sl = atomicAdd(&fill[bk], 1u);
     if (sl >= 4u) return;
   }
   const unsigned at = 4u * bk + sl;

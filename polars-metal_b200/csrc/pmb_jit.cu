@@ -807,9 +807,10 @@ int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int m
     J->nbuf = 1;
   }
   // hot keys: one record per warp each; warm keys: the largest count whose table and records fit.
-  // The sampled-key table: buckets of 4 keys and 4 16-bit values, filled to at most 80%.
+  // The sampled-key table: buckets of 4 keys and 4 16-bit values, filled to at most 50% (a key
+  // sits in its first bucket unless that one was full, so most lookups read one bucket).
   J->tkey = q.key_bits <= 32 ? 4 : 8;
-  auto buckets = [](int keys) { return keys ? ((keys * 5 / 16 + 2) + 1) & ~1 : 0; };
+  auto buckets = [](int keys) { return keys ? ((keys / 2 + 2) + 1) & ~1 : 0; };
   auto tbytes = [&](int keys) { return buckets(keys) * 4 * (J->tkey + 2); };
   int hot = have_sketch ? 8 : 0;
   if (const char* e = getenv("PMB_HOT")) hot = std::max(0, std::min(atoi(e), 64));

@@ -96,33 +96,52 @@ __device__ __forceinline__ long long j_gfind(const JParams& P, unsigned long lon
   return j_gresolve(P, key, h, claimed);
 }
 
-// The CTA's table of sampled keys (hot and warm), built on the device by k_sample_table: every
-// placed key sits in one of its two 4-slot buckets, so a lookup is two bucket loads and no loop.
-// Empty slots hold the value 0xFFFF (a miss whatever their key word). Returns the key's value
-// (J_HOTBIT | hot index, or warm index) or J_MISS.
+// The CTA's table of sampled keys (hot and warm), built on the device by k_sample_table: a key
+// sits in its first bucket (4 slots) unless that bucket was already full, then in its second.
+// Empty slots hold the value 0xFFFF (a miss whatever their key word), so a first bucket with an
+// empty slot ends a lookup: its keys never spilled over. A lookup reads the first bucket's keys
+// and values side by side, and the second bucket only when the first is full. Returns the key's
+// value (J_HOTBIT | hot index, or warm index) or J_MISS.
 __device__ __forceinline__ unsigned j_tvalue(unsigned short v) {
   return v == 0xFFFFu ? J_MISS : ((v & 0x8000u) ? (J_HOTBIT | (v & 0x7FFFu)) : (unsigned)v);
+}
+// the 16-bit value of slot s of a bucket whose values are (lo, hi)
+__device__ __forceinline__ unsigned short j_tslot(uint2 v, int s) {
+  const unsigned w = (s & 2) ? v.y : v.x;
+  return (unsigned short)((s & 1) ? (w >> 16) : (w & 0xFFFFu));
+}
+// true when a bucket's values hold an empty slot (0xFFFF)
+__device__ __forceinline__ bool j_tnotfull(uint2 v) {
+  return (v.x >> 16) == 0xFFFFu || (v.x & 0xFFFFu) == 0xFFFFu || (v.y >> 16) == 0xFFFFu || (v.y & 0xFFFFu) == 0xFFFFu;
 }
 __device__ __forceinline__ unsigned j_tfind(const unsigned char* tk, const unsigned short* tv, unsigned tnb,
                                             unsigned long long key, unsigned long long h) {
   if (tnb == 0u) return J_MISS;
-  const unsigned a = (unsigned)(h >> 32), b = pmb_mix32b(a);
-  const unsigned b1 = __umulhi(a, tnb), b2 = __umulhi(b, tnb);
+  const unsigned a = (unsigned)(h >> 32);
+  const unsigned b1 = __umulhi(a, tnb);
+  const uint2* vals = reinterpret_cast<const uint2*>(tv);
+  const uint2 vx = vals[b1];
 #if J_TKEY == 4
   const unsigned k = (unsigned)key;
-  const uint4 x = reinterpret_cast<const uint4*>(tk)[b1], y = reinterpret_cast<const uint4*>(tk)[b2];
+  const uint4 x = reinterpret_cast<const uint4*>(tk)[b1];
   int s = x.x == k ? 0 : x.y == k ? 1 : x.z == k ? 2 : x.w == k ? 3 : -1;
-  if (s >= 0) return j_tvalue(tv[4 * b1 + s]);
-  s = y.x == k ? 0 : y.y == k ? 1 : y.z == k ? 2 : y.w == k ? 3 : -1;
-  return s >= 0 ? j_tvalue(tv[4 * b2 + s]) : J_MISS;
 #else
   const ulonglong2* t = reinterpret_cast<const ulonglong2*>(tk);
-  const ulonglong2 x0 = t[2 * b1], x1 = t[2 * b1 + 1], y0 = t[2 * b2], y1 = t[2 * b2 + 1];
+  const ulonglong2 x0 = t[2 * b1], x1 = t[2 * b1 + 1];
   int s = x0.x == key ? 0 : x0.y == key ? 1 : x1.x == key ? 2 : x1.y == key ? 3 : -1;
-  if (s >= 0) return j_tvalue(tv[4 * b1 + s]);
-  s = y0.x == key ? 0 : y0.y == key ? 1 : y1.x == key ? 2 : y1.y == key ? 3 : -1;
-  return s >= 0 ? j_tvalue(tv[4 * b2 + s]) : J_MISS;
 #endif
+  if (s >= 0) return j_tvalue(j_tslot(vx, s));
+  if (j_tnotfull(vx)) return J_MISS;
+  const unsigned b2 = __umulhi(pmb_mix32b(a), tnb);
+  const uint2 vy = vals[b2];
+#if J_TKEY == 4
+  const uint4 y = reinterpret_cast<const uint4*>(tk)[b2];
+  s = y.x == k ? 0 : y.y == k ? 1 : y.z == k ? 2 : y.w == k ? 3 : -1;
+#else
+  const ulonglong2 y0 = t[2 * b2], y1 = t[2 * b2 + 1];
+  s = y0.x == key ? 0 : y0.y == key ? 1 : y1.x == key ? 2 : y1.y == key ? 3 : -1;
+#endif
+  return s >= 0 ? j_tvalue(j_tslot(vy, s)) : J_MISS;
 }
 
 __device__ __forceinline__ bool j_stop(const JParams& P) {
