@@ -118,6 +118,9 @@ __device__ __forceinline__ void pmb_red_add(unsigned int* p, unsigned int v) {
 __device__ __forceinline__ void pmb_red_or(unsigned int* p, unsigned int v) {
   asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v) : "memory");
 }
+__device__ __forceinline__ void pmb_red_or(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.or.b64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
+}
 __device__ __forceinline__ void pmb_red_min(long long* p, long long v) {
   asm volatile("red.relaxed.gpu.global.min.s64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v) : "memory");
 }
@@ -134,11 +137,23 @@ __device__ __forceinline__ void pmb_red_max(unsigned long long* p, unsigned long
 __device__ __forceinline__ void pmb_red_add(unsigned long long* p, unsigned long long v) { atomicAdd(p, v); }
 __device__ __forceinline__ void pmb_red_add(unsigned int* p, unsigned int v) { atomicAdd(p, v); }
 __device__ __forceinline__ void pmb_red_or(unsigned int* p, unsigned int v) { atomicOr(p, v); }
+__device__ __forceinline__ void pmb_red_or(unsigned long long* p, unsigned long long v) { atomicOr(p, v); }
 __device__ __forceinline__ void pmb_red_min(long long* p, long long v) { atomicMin(p, v); }
 __device__ __forceinline__ void pmb_red_max(long long* p, long long v) { atomicMax(p, v); }
 __device__ __forceinline__ void pmb_red_min(unsigned long long* p, unsigned long long v) { atomicMin(p, v); }
 __device__ __forceinline__ void pmb_red_max(unsigned long long* p, unsigned long long v) { atomicMax(p, v); }
 #endif
+
+// Global-table records update their 4-byte words (counters, float-sum flags) with 64-bit atomics
+// on the 8-byte word that holds them, so that two 4-byte fields sharing a word (a counter in an
+// exact float sum's spare word beside its flags) never meet atomics of different sizes.
+// Counters stay below 2^32 - 1 (a call has fewer rows), so an add never carries into the other half.
+__device__ __forceinline__ void pmb_rec_add32(unsigned char* rec, int off, unsigned int v) {
+  pmb_red_add(reinterpret_cast<unsigned long long*>(rec + (off & ~7)), (unsigned long long)v << ((off & 4) ? 32 : 0));
+}
+__device__ __forceinline__ void pmb_rec_or32(unsigned char* rec, int off, unsigned int v) {
+  pmb_red_or(reinterpret_cast<unsigned long long*>(rec + (off & ~7)), (unsigned long long)v << ((off & 4) ? 32 : 0));
+}
 
 __host__ __device__ __forceinline__ uint64_t pmb_fmix64(uint64_t k) {
   k ^= k >> 33;

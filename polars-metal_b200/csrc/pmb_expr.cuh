@@ -490,7 +490,7 @@ __device__ __forceinline__ void apply_row_global(const DQuery& q, const TileCtx&
         double x = pmb_bits_to_f64(b, dt);
         unsigned fl = pmb_fx_flag(x);
         if (fl) {
-          pmb_red_or((unsigned int*)(p + 16), fl);
+          pmb_rec_or32(rec, F.off + 16, fl);
         } else if (pmb_fx_in_range(x, q.fx_e[F.fx_slot])) {
           unsigned long long w0, w1;
           pmb_fx_words(x, F.fx, w0, w1);
@@ -542,7 +542,7 @@ __device__ __forceinline__ void merge_record(const DQuery& q, uint8_t* dst, cons
       case F_LEN:
       case F_CNT: {
         unsigned int v = *(const unsigned int*)s;
-        if (v) pmb_red_add((unsigned int*)d, v);
+        if (v) pmb_rec_add32(dst, F.off, v);
         break;
       }
       case F_SUM_DD: {
@@ -556,7 +556,7 @@ __device__ __forceinline__ void merge_record(const DQuery& q, uint8_t* dst, cons
         for (int w = 0; w < 2; w++)
           if (l[w]) pmb_red_add((unsigned long long*)d + w, l[w]);
         unsigned fl = *(const unsigned int*)(s + 16);
-        if (fl) pmb_red_or((unsigned int*)(d + 16), fl);
+        if (fl) pmb_rec_or32(dst, F.off + 16, fl);
         break;
       }
       case F_SUM_I: {

@@ -357,7 +357,7 @@ struct Gen {
         case F_SUM_FX: {
           std::string slot = std::to_string(F.fx_slot);
           b << "    double xv = (double)" << v(F.col) << ";\n    unsigned fl = pmb_fx_flag(xv);\n";
-          b << "    if (fl) pmb_red_or(" << at(F.off + 16, "unsigned int") << ", fl);\n";
+          b << "    if (fl) pmb_rec_or32(rec, " << F.off + 16 << ", fl);\n";
           b << "    else if (pmb_fx_in_range(xv, P.fx_e[" << slot << "])) {\n      unsigned long long w0, w1;\n";
           b << "      pmb_fx_words(xv, P.fx[" << slot << "], w0, w1);\n";
           b << "      if (w0) pmb_red_add(" << at(F.off, "unsigned long long") << ", w0);\n";
@@ -465,13 +465,11 @@ struct Gen {
       switch (F.kind) {
         case F_LEN:
         case F_CNT:
-          b << "  { unsigned int x = " << CU(so) << "; if (x) pmb_red_add(reinterpret_cast<unsigned int*>(d + " << gd
-            << "), x); }\n";
+          b << "  { unsigned int x = " << CU(so) << "; if (x) pmb_rec_add32(d, " << gd << ", x); }\n";
           break;
         case F_SUM_FX:
           // the 96-bit partial P: its low 32 bits, and P >> 32 as a signed 64-bit word
-          b << "  { unsigned fl = " << CU(so + 12) << "; if (fl) pmb_red_or(reinterpret_cast<unsigned int*>(d + "
-            << F.off + 16 << "), fl);\n";
+          b << "  { unsigned fl = " << CU(so + 12) << "; if (fl) pmb_rec_or32(d, " << F.off + 16 << ", fl);\n";
           b << "    unsigned w0 = " << CU(so) << ";\n    unsigned long long hi = ((unsigned long long)" << CU(so + 8)
             << " << 32) | " << CU(so + 4) << ";\n";
           b << "    if (w0) pmb_red_add(" << GU64(F.off) << ", (unsigned long long)w0);\n";

@@ -360,9 +360,12 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
   if (fields.size() > PMB_MAX_FIELDS) return pmb_fail(h, PMB_E_UNSUPPORTED, "too many aggregation state fields");
   // record layout: 24-byte fields (exact float sums), then 16-, 8- and 4-byte ones, so every
   // field stays aligned to its size (at most 8)
+  // (a 4-byte field first takes the spare last word of an exact float sum's 24 bytes, so the
+  // hash workload's record is 48 bytes: two 32-byte sectors wherever it sits)
   int rec = 0;
   static const int kSizes[4] = {24, 16, 8, 4};
   size_t placed = 0;
+  std::vector<int> spare;  // free 4-byte words inside placed fields
   for (int pass = 0; pass < 4; pass++) {
     int want = kSizes[pass];
     for (DField& f : fields) {
@@ -370,8 +373,14 @@ int pmb_compile_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* col
       int nw, bytes;
       field_identity(f.kind, &w0, &w1, &nw, &bytes);
       if (bytes != want) continue;
-      f.off = (int16_t)rec;
-      rec += bytes;
+      if (bytes == 4 && !spare.empty()) {
+        f.off = (int16_t)spare.back();
+        spare.pop_back();
+      } else {
+        f.off = (int16_t)rec;
+        rec += bytes;
+      }
+      if (f.kind == F_SUM_FX) spare.push_back(f.off + 20);
       placed++;
     }
   }
