@@ -157,8 +157,8 @@ def test_polars_types_wrap_and_round_on_the_gpu():
 def test_integer_literals_beyond_the_column_type_widen_on_the_gpu():
     # UInt8 * -1 is Int16 (not a wrapped UInt8), Int8 + 1000 is Int16, UInt32 * -1 is Int64,
     # UInt32 - 5_000_000_000 is UInt64 (a non-negative literal beside an unsigned column stays
-    # unsigned, and the difference wraps), a literal-only 3e9 + 1 is Int64: Polars' dynamic-integer
-    # rule
+    # unsigned, and the difference wraps), the folded literal 3e9 + 1 is UInt32 beside UInt8 and
+    # Int64 beside Int8: Polars' dynamic-integer rule
     rng = np.random.default_rng(37)
     n = 50_001
     u8 = rng.integers(0, 256, n).astype(np.uint8)
@@ -171,8 +171,10 @@ def test_integer_literals_beyond_the_column_type_widen_on_the_gpu():
         (_bin("Add", col("i8"), lit(1000)), A.I16, i8.astype(np.int16) + np.int16(1000)),
         (_bin("Mul", col("u32"), lit(-1)), A.I64, u32.astype(np.int64) * np.int64(-1)),
         (_bin("Sub", col("u32"), lit(5_000_000_000)), A.U64, u32.astype(np.uint64) - np.uint64(5_000_000_000)),
-        (_bin("Mul", col("u8"), _bin("Add", lit(3_000_000_000), lit(1))), A.I64,
-         u8.astype(np.int64) * np.int64(3_000_000_001)),
+        (_bin("Mul", col("u8"), _bin("Add", lit(3_000_000_000), lit(1))), A.U32,
+         u8.astype(np.uint32) * np.uint32(3_000_000_001)),
+        (_bin("Mul", col("i8"), _bin("Add", lit(3_000_000_000), lit(1))), A.I64,
+         i8.astype(np.int64) * np.int64(3_000_000_001)),
     ]
     for e, dt, want in cases:
         out = N.eval_expr(cols, e)
