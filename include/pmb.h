@@ -331,14 +331,16 @@ void pmb_result_free(pmb_result* r);
  * crates/polars-metal-kernels/src/groupby.rs:475-486). A query's features are computed on the
  * device from a 4096-row sample of its keys (HyperLogLog registers, hash-bucket occupancy, null
  * and filter fractions, sample frequency profile, key width); an MLP (PMB_SELECTOR_FEATURES ->
- * 64 -> 64 -> 4, fp32) maps them to three strategy scores (shared-memory hash, global hash, sort)
- * and log2 of the group count, which sizes the hash table. Without installed parameters, or for
- * a non-finite output, the plain cardinality heuristic decides. The strategy never changes a
- * result: every strategy is exact, and an undersized table is rebuilt larger. */
+ * 64 -> 64 -> 5, fp32) maps them to four strategy scores (shared-memory hash, global hash, sort,
+ * partitioned) and log2 of the group count, which sizes the hash table. Without installed
+ * parameters, or for a non-finite output, the plain cardinality heuristic decides (with its
+ * switch to the partitioned strategy for many groups and no heavy key). The strategy never
+ * changes a result: every strategy is exact, and an undersized table is rebuilt larger. */
 #define PMB_SELECTOR_FEATURES 24
 #define PMB_SELECTOR_HIDDEN 64
-#define PMB_SELECTOR_OUTPUTS 4
-/* parameter count: W1[64][24] b1[64] W2[64][64] b2[64] W3[4][64] b3[4], in that order */
+#define PMB_SELECTOR_STRATEGIES 4
+#define PMB_SELECTOR_OUTPUTS (PMB_SELECTOR_STRATEGIES + 1)
+/* parameter count: W1[64][24] b1[64] W2[64][64] b2[64] W3[5][64] b3[5], in that order */
 #define PMB_SELECTOR_PARAMS                                                                   \
   (PMB_SELECTOR_HIDDEN * PMB_SELECTOR_FEATURES + PMB_SELECTOR_HIDDEN +                       \
    PMB_SELECTOR_HIDDEN * PMB_SELECTOR_HIDDEN + PMB_SELECTOR_HIDDEN +                         \

@@ -2,8 +2,9 @@
 backward), the CPU oracle that the device kernels' gradients are checked against.
 
 Network (include/pmb.h, PMB_SELECTOR_*): x[24] -> relu(W1 x + b1)[64] -> relu(W2 h1 + b2)[64]
--> W3 h2 + b3 [4]; outputs 0-2 are strategy scores (softmax cross-entropy), output 3 predicts
-log2(group count) (squared error weighted by wreg). Per-sample weights sw scale both terms; the
+-> W3 h2 + b3 [5]; outputs 0-3 are strategy scores (shared-memory hash, global hash, sort,
+partitioned; softmax cross-entropy), output 4 predicts log2(group count) (squared error weighted
+by wreg). Per-sample weights sw scale both terms; the
 loss is their mean over the batch. Parameters are laid out W1, b1, W2, b2, W3, b3 (row-major, a
 row per output unit). The selector has no counterpart in the reference, so nothing here is pinned
 to reference vectors; the test pins this statement to finite differences instead.
@@ -13,7 +14,8 @@ from __future__ import annotations
 
 import numpy as np
 
-NF, NH, NO = 24, 64, 4
+NF, NH, NS = 24, 64, 4
+NO = NS + 1
 SIZES = [NH * NF, NH, NH * NH, NH, NO * NH, NO]
 N_PARAMS = sum(SIZES)
 
@@ -46,16 +48,16 @@ def loss_and_grad(p, X, cls, y, sw=None, wreg: float = 0.25):
     a2 = h1 @ W2.T + b2
     h2 = np.maximum(a2, 0.0)
     o = h2 @ W3.T + b3
-    z = o[:, :3] - o[:, :3].max(axis=1, keepdims=True)
+    z = o[:, :NS] - o[:, :NS].max(axis=1, keepdims=True)
     e = np.exp(z)
     prob = e / e.sum(axis=1, keepdims=True)
-    r = o[:, 3] - y
+    r = o[:, NS] - y
     w = sw / B
     loss = float(np.sum(w * (-np.log(np.maximum(prob[np.arange(B), cls], 1e-30)) + wreg * r * r)))
     dout = np.zeros_like(o)
-    dout[:, :3] = prob
+    dout[:, :NS] = prob
     dout[np.arange(B), cls] -= 1.0
-    dout[:, 3] = wreg * 2.0 * r
+    dout[:, NS] = wreg * 2.0 * r
     dout *= w[:, None]
     gW3 = dout.T @ h2
     gb3 = dout.sum(0)

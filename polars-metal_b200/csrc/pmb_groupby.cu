@@ -1156,15 +1156,15 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
       int s = 0;
       int64_t g = 0;
       if (sel && pmb_selector_read(h, cq, &s, &g)) {
-        strategy = s;
+        strategy = s;  // the network scores all four strategies
         if (est <= 0) est = std::max<int64_t>(e, std::min<int64_t>(g, cq.dq.n_rows));
       } else {
         if (est <= 0) est = e;
         strategy = pmb_choose_strategy(h, cq, sk, est);
+        if (pmb_prefer_partitioned(cq, sk, strategy, est)) strategy = PMB_STRATEGY_PARTITIONED;
       }
     }
     if (est <= 0) est = e;
-    if (q->strategy == PMB_STRATEGY_AUTO && pmb_prefer_partitioned(cq, sk, strategy, est)) strategy = PMB_STRATEGY_PARTITIONED;
     pmb_phase(h, "choose");
     if (strategy == PMB_STRATEGY_SORT) rc = pmb_groupby_sort(h, cq, r, 0);
     else if (strategy == PMB_STRATEGY_PARTITIONED) rc = pmb_groupby_sort(h, cq, r, std::max<int64_t>(est, 1));

@@ -19,6 +19,7 @@ namespace {
 constexpr int NF = PMB_SELECTOR_FEATURES;
 constexpr int NH = PMB_SELECTOR_HIDDEN;
 constexpr int NO = PMB_SELECTOR_OUTPUTS;
+constexpr int NS = PMB_SELECTOR_STRATEGIES;  // outputs 0..NS-1: strategy scores; output NS: log2(groups)
 constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + NH * NF, OFF_W2 = OFF_B1 + NH, OFF_B2 = OFF_W2 + NH * NH,
               OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + NO * NH, N_PARAMS = OFF_B3 + NO;
 static_assert(N_PARAMS == PMB_SELECTOR_PARAMS, "parameter layout");
@@ -203,14 +204,19 @@ __global__ void __launch_bounds__(NH) k_mlp_backward(const float* __restrict__ P
   mlp_layers(P, x, h1, h2, o);
   const float sw = (SW ? SW[b] : 1.f) / (float)B;
   if (j == 0) {
-    const float mx = fmaxf(o[0], fmaxf(o[1], o[2]));
-    const float e0 = expf(o[0] - mx), e1 = expf(o[1] - mx), e2 = expf(o[2] - mx), s = e0 + e1 + e2;
+    // softmax cross-entropy over the strategy scores, squared error of the group-count output
+    float mx = o[0];
+    for (int k = 1; k < NS; k++) mx = fmaxf(mx, o[k]);
+    float e[NS], s = 0.f;
+    for (int k = 0; k < NS; k++) {
+      e[k] = expf(o[k] - mx);
+      s += e[k];
+    }
     const int c = cls[b];
-    const float p[3] = {e0 / s, e1 / s, e2 / s};
-    for (int k = 0; k < 3; k++) dout[k] = sw * (p[k] - (k == c ? 1.f : 0.f));
-    const float r = o[3] - Y[b];
-    dout[3] = sw * wreg * 2.f * r;
-    atomicAdd(loss, sw * (-logf(fmaxf(p[c], 1e-30f)) + wreg * r * r));
+    for (int k = 0; k < NS; k++) dout[k] = sw * (e[k] / s - (k == c ? 1.f : 0.f));
+    const float r = o[NS] - Y[b];
+    dout[NS] = sw * wreg * 2.f * r;
+    atomicAdd(loss, sw * (-logf(fmaxf(e[c] / s, 1e-30f)) + wreg * r * r));
   }
   __syncthreads();
   // layer 3
@@ -298,7 +304,7 @@ bool pmb_selector_predict_batch(pmb_handle* h, const DQuery* d_qs, int nq, int64
     return false;
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return false;
   for (int i = 0; i < nq; i++) {
-    const float g = ho[(size_t)i * NO + 3];
+    const float g = ho[(size_t)i * NO + NS];
     out_groups[i] = std::isfinite(g) ? (int64_t)std::min<double>(std::exp2(std::min<double>(std::max<double>(g, 0.0), 40.0)),
                                                                  (double)n_rows[i])
                                      : 0;
@@ -313,11 +319,12 @@ static bool selector_decode(const float* o, int64_t n_rows, int* strategy, int64
   for (int k = 0; k < NO; k++)
     if (!std::isfinite(o[k])) return false;
   int best = 0;
-  for (int k = 1; k < 3; k++)
+  for (int k = 1; k < NS; k++)
     if (o[k] > o[best]) best = k;
-  static const int map[3] = {PMB_STRATEGY_SMEM_HASH, PMB_STRATEGY_GLOBAL_HASH, PMB_STRATEGY_SORT};
+  static const int map[NS] = {PMB_STRATEGY_SMEM_HASH, PMB_STRATEGY_GLOBAL_HASH, PMB_STRATEGY_SORT,
+                              PMB_STRATEGY_PARTITIONED};
   *strategy = map[best];
-  const double g = std::exp2(std::min<double>(std::max<double>(o[3], 0.0), 40.0));
+  const double g = std::exp2(std::min<double>(std::max<double>(o[NS], 0.0), 40.0));
   *groups = (int64_t)std::min<double>(g, (double)n_rows);
   if (*groups < 1) *groups = 1;
   return true;
@@ -416,10 +423,12 @@ extern "C" int pmb_selector_choose(pmb_handle* h, const pmb_query* q, const pmb_
   if (pmb_selector_pick(h, cq, &s, &g)) {
     g = std::max<int64_t>(e, std::min<int64_t>(g, cq.dq.n_rows));
   } else {
+    // the heuristic: cardinality, then the switch to the partitioned strategy (the network
+    // scores the partitioned strategy itself)
     g = e;
     s = pmb_choose_strategy(h, cq, sk, g);
+    if (pmb_prefer_partitioned(cq, sk, s, g)) s = PMB_STRATEGY_PARTITIONED;
   }
-  if (pmb_prefer_partitioned(cq, sk, s, g)) s = PMB_STRATEGY_PARTITIONED;
   *strategy = s;
   *groups = g;
   return PMB_OK;

@@ -260,11 +260,12 @@ SIGNATURES = {
 # learned strategy selector (include/pmb.h)
 SELECTOR_FEATURES = 24
 SELECTOR_HIDDEN = 64
-SELECTOR_OUTPUTS = 4
+SELECTOR_STRATEGIES_N = 4
+SELECTOR_OUTPUTS = SELECTOR_STRATEGIES_N + 1
 SELECTOR_PARAMS = (SELECTOR_HIDDEN * SELECTOR_FEATURES + SELECTOR_HIDDEN + SELECTOR_HIDDEN * SELECTOR_HIDDEN
                    + SELECTOR_HIDDEN + SELECTOR_OUTPUTS * SELECTOR_HIDDEN + SELECTOR_OUTPUTS)
 # strategy index of the selector's scores
-SELECTOR_STRATEGIES = ["smem_hash", "global_hash", "sort"]
+SELECTOR_STRATEGIES = ["smem_hash", "global_hash", "sort", "partitioned"]
 
 # largest n of pmb_cumsum_u8_to_u32_noalloc (its fixed scratch array)
 NOALLOC_MAX_ROWS = 1 << 27

@@ -1,8 +1,8 @@
 """The learned strategy selector: training data, training and evaluation.
 
 The network (include/pmb.h, PMB_SELECTOR_*) reads device-computed features of a 4096-row key
-sample and scores the three group-by strategies (shared-memory hash, global hash, sort) and
-predicts log2 of the group count. This module
+sample and scores the four group-by strategies (shared-memory hash, global hash, sort,
+partitioned) and predicts log2 of the group count. This module
 
   * generates synthetic tables like the learned-selection workload (rows log-uniform, key width
     int32 / int64 / 2 x int64, distinct count log-uniform, Zipf skew, null fraction);
@@ -335,7 +335,7 @@ def main(argv=None):
         p = np.load(a.params)
         tr, te = split(d["X"].shape[0])
         out = predict(p, d["X"][te])
-        print(evaluate(np.argmax(out[:, :3], axis=1), d["T"][te], d["H"][te]))
+        print(evaluate(np.argmax(out[:, :len(STRATEGIES)], axis=1), d["T"][te], d["H"][te]))
 
 
 if __name__ == "__main__":

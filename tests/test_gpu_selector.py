@@ -25,7 +25,7 @@ def test_forward_gradient_and_adam_match_the_oracle():
     h = Handle(0, selector=None)
     p = S.init_params(5)
     X = rng.random((200, mlp.NF)).astype(np.float32)
-    cls = rng.integers(0, 3, 200).astype(np.int32)
+    cls = rng.integers(0, mlp.NS, 200).astype(np.int32)
     y = (rng.random(200) * 25).astype(np.float32)
     sw = (rng.random(200) + 0.5).astype(np.float32)
     out = mlp_forward(_t(p), _t(X), handle=h).cpu().numpy()
@@ -45,11 +45,11 @@ def test_training_with_the_device_kernels_learns_a_rule():
     n = 2048
     X = rng.random((n, mlp.NF)).astype(np.float32)
     # the fastest strategy follows feature 4 (sample distinct fraction), like a cardinality rule
-    T = np.stack([1 + 4 * X[:, 4], 2 - X[:, 4], 1 + 3 * (1 - X[:, 4])], axis=1)
+    T = np.stack([1 + 4 * X[:, 4], 2 - X[:, 4], 1 + 3 * (1 - X[:, 4]), 1.5 + 2 * np.abs(X[:, 4] - 0.5)], axis=1)
     G = (2 ** (20 * X[:, 13])).astype(np.int64)
     p, hist = S.train(X, T, G, epochs=60, batch=256, lr=5e-3)
     assert hist[-1] < 0.5 * hist[0]
-    pred = np.argmax(mlp.forward(p, X)[:, :3], axis=1)
+    pred = np.argmax(mlp.forward(p, X)[:, :mlp.NS], axis=1)
     assert np.mean(pred == np.argmin(T, axis=1)) > 0.9
 
 

@@ -19,7 +19,7 @@ def test_oracle_gradient_matches_finite_differences():
     rng = np.random.default_rng(0)
     p = S.init_params(3).astype(np.float64)
     X = rng.random((16, mlp.NF))
-    cls = rng.integers(0, 3, 16)
+    cls = rng.integers(0, mlp.NS, 16)
     y = rng.random(16) * 20
     sw = rng.random(16) + 0.5
     loss, g = mlp.loss_and_grad(p, X, cls, y, sw, wreg=0.1)
@@ -47,11 +47,11 @@ def test_shipped_selector_gains_over_the_heuristic_on_held_out_tables():
     assert p is not None and p.size == A.SELECTOR_PARAMS
     tr, te = S.split(d["X"].shape[0])
     out = mlp.forward(p, d["X"][te])
-    rep = S.evaluate(np.argmax(out[:, :3], axis=1), d["T"][te], d["H"][te])
+    rep = S.evaluate(np.argmax(out[:, :mlp.NS], axis=1), d["T"][te], d["H"][te])
     print(rep)
     # never slower than the heuristic in total, and most of the way to the best pick per table
     assert rep["gain_vs_heuristic"] >= 1.0
     assert rep["learned_vs_best"] <= 1.25
     # the size prediction: log2(groups) within 1.5 on most held-out tables
-    err = np.abs(out[:, 3] - np.log2(np.maximum(d["G"][te], 1)))
+    err = np.abs(out[:, mlp.NS] - np.log2(np.maximum(d["G"][te], 1)))
     assert np.median(err) < 1.5
