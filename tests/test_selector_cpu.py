@@ -40,7 +40,7 @@ def test_labels_pick_the_fastest_strategy():
     assert list(cls) == [1, 0] and sw[0] == 3.0 and sw[1] == 9.0 and y[0] == pytest.approx(np.log2(7))
 
 
-@pytest.mark.skipif(not (S.DATASET_FILE.exists() and S.PARAMS_FILE.exists()), reason="no shipped selector")
+@pytest.mark.skipif(not (S.DATASET_FILE.exists() and S.default_params() is not None), reason="no shipped selector")
 def test_shipped_selector_gains_over_the_heuristic_on_held_out_tables():
     d = np.load(S.DATASET_FILE)
     p = S.default_params()
