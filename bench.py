@@ -845,6 +845,9 @@ def run_batch(args, device, rank: int, local_rank: int, world: int) -> None:
     h_plain.set_stream(stream.cuda_stream)
     cmp = batch_vs_plain(qs, rows, stream, h, h_plain, steps=args.steps)
     h_plain.close()
+    parity = None
+    if rank == 0 and not args.no_cpu_baseline:
+        parity = batch_parity(tables, qs, h, len(os.sched_getaffinity(0)))
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -874,6 +877,7 @@ def run_batch(args, device, rank: int, local_rank: int, world: int) -> None:
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "vs_plain": cmp,
+            "parity": parity,
         }
         print(json.dumps(line), flush=True)
     h.close()

@@ -125,9 +125,11 @@ def make_table(spec: TableSpec, device="cuda"):
     return cols, keys
 
 
-def collect(specs, reps: int = 2, log=None) -> dict:
+def collect(specs, reps: int = 2, log=None, budget_s: float = 0.0) -> dict:
     """Features, per-strategy device time (ms, best of `reps`), the heuristic's pick and the
-    exact group count of every table, measured on the current GPU."""
+    exact group count of every table, measured on the current GPU. With `budget_s` > 0 the
+    collection stops after the table that crosses that many seconds (`seconds` in the result
+    holds the time taken)."""
     import torch
 
     from ._native import Handle, groupby, selector_choose, selector_features
@@ -163,9 +165,11 @@ def collect(specs, reps: int = 2, log=None) -> dict:
         del cols
         if log and (i + 1) % 50 == 0:
             log(f"{i + 1}/{len(specs)} tables, {time.time() - t0:.0f} s")
+        if budget_s > 0 and time.time() - t0 > budget_s:
+            break
     h.close()
     return {"X": np.array(X, np.float32), "T": np.array(T, np.float64), "G": np.array(G, np.int64),
-            "H": np.array(H, np.int32), "S": np.array(S, np.float64)}
+            "H": np.array(H, np.int32), "S": np.array(S, np.float64), "seconds": np.float64(time.time() - t0)}
 
 
 def labels(T: np.ndarray, G: np.ndarray):
@@ -304,6 +308,7 @@ def main(argv=None):
     c.add_argument("--seed", type=int, default=1)
     c.add_argument("--max-rows", type=float, default=2e7)
     c.add_argument("--out", default=str(DATASET_FILE))
+    c.add_argument("--budget-s", type=float, default=0.0, help="stop after this many seconds of collection")
     t = sub.add_parser("train")
     t.add_argument("--data", default=str(DATASET_FILE))
     t.add_argument("--out", default=str(PARAMS_FILE))
@@ -319,7 +324,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     if a.cmd == "collect":
         specs = sample_specs(a.tables, a.seed, max_rows=a.max_rows)
-        d = collect(specs, log=print)
+        d = collect(specs, log=print, budget_s=a.budget_s)
+        print(f"collected {d['X'].shape[0]} tables in {float(d['seconds']):.0f} s")
         Path(a.out).parent.mkdir(parents=True, exist_ok=True)
         np.savez_compressed(a.out, **d)
         print("wrote", a.out)
