@@ -810,7 +810,9 @@ int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int m
   J->tkey = q.key_bits <= 32 ? 4 : 8;
   auto buckets = [](int keys) { return keys ? ((keys / 2 + 2) + 1) & ~1 : 0; };
   auto tbytes = [&](int keys) { return buckets(keys) * 4 * (J->tkey + 2); };
-  int hot = have_sketch ? 8 : 0;
+  // 24 hot keys (a record per warp each): measured best on the hash workload (100M rows, Zipf 1.1
+  // over 1M keys): 1.48 ms against 1.55 ms with 8 and 1.54 ms with 48
+  int hot = have_sketch ? 24 : 0;
   if (const char* e = getenv("PMB_HOT")) hot = std::max(0, std::min(atoi(e), 64));
   while (hot > 0 && (int)pmb_align((size_t)used, 16) + tbytes(hot) + 32 + W * hot * J->srec > budget) hot /= 2;
   int warm = 0;
