@@ -184,6 +184,7 @@ struct pmb_handle {
   // profiling
   bool profiling = false;
   bool batching = true;  // pmb_groupby_batched may batch (else: one pmb_groupby per query)
+  std::vector<std::pair<uintptr_t, uintptr_t>> ptr_ok;  // device ranges of the handle's GPU seen this call
   // host phases of a call (PMB_CALL_TIMING=1 prints them to stderr at the end of the call)
   bool phase_timing = false;
   std::vector<std::pair<const char*, double>> phases;

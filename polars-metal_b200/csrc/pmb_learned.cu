@@ -274,6 +274,7 @@ int stage_query(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32
   if (rc) return rc;
   rc = pmb_ws_begin(h);
   if (rc) return rc;
+  h->ptr_ok.clear();  // pointer checks start afresh for this call
   for (int c = 0; c < cq->dq.n_cols; c++) {
     rc = pmb_stage_column(h, cols[cq->map.user[c]], cq->dq.n_rows, &cq->dq.col[c]);
     if (rc) return rc;

@@ -7,6 +7,7 @@
 // workspace; each call bump-allocates from it and synchronises once at the end.
 #include <cuda_runtime.h>
 
+#include <dlfcn.h>
 #include <sys/mman.h>
 
 #include <algorithm>
@@ -132,6 +133,7 @@ void pmb_phase(pmb_handle* h, const char* name) {
 }
 
 void pmb_call_begin(pmb_handle* h) {
+  h->ptr_ok.clear();  // allocation ranges checked in this call (the caller's buffers live through it)
   h->phase_timing = getenv("PMB_CALL_TIMING") != nullptr;
   h->phases.clear();
   if (h->phase_timing) h->phase_t0 = host_ms();
@@ -257,19 +259,48 @@ static int stage_bits(pmb_handle* h, const uint8_t* base, int64_t offset, int64_
   return PMB_OK;
 }
 
+// The allocation range of a device pointer (driver's cuMemGetAddressRange, looked up with dlsym
+// so the library needs no link-time driver dependency); false when unavailable or not device memory
+static bool device_range(const void* p, uintptr_t* base, size_t* size) {
+  typedef int (*range_fn)(unsigned long long*, size_t*, unsigned long long);
+  static range_fn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    if (void* lib = dlopen("libcuda.so.1", RTLD_NOW | RTLD_LOCAL | RTLD_NOLOAD))
+      fn = (range_fn)dlsym(lib, "cuMemGetAddressRange_v2");
+  }
+  if (!fn) return false;
+  unsigned long long b = 0;
+  size_t n = 0;
+  if (fn(&b, &n, (unsigned long long)(uintptr_t)p) != 0 || n == 0) return false;
+  *base = (uintptr_t)b;
+  *size = n;
+  return true;
+}
+
+// A device column's pointer must be memory of the handle's GPU (or pinned host memory). The
+// answer is kept per allocation range for the rest of the call, so a batch of thousands of
+// columns carved from a few allocations costs a few driver queries.
 static int check_device_pointer(pmb_handle* h, const void* p) {
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+  const uintptr_t a = (uintptr_t)p;
+  for (const auto& r : h->ptr_ok)
+    if (a >= r.first && a < r.second) return PMB_OK;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
     cudaGetLastError();
     return pmb_fail(h, PMB_E_INVALID, "device column pointer is not CUDA memory");
   }
-  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) {
-    if (a.device != h->device)
-      return pmb_fail(h, PMB_E_INVALID, "device column lives on GPU " + std::to_string(a.device) +
+  if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) {
+    if (at.device != h->device)
+      return pmb_fail(h, PMB_E_INVALID, "device column lives on GPU " + std::to_string(at.device) +
                                             ", the handle on GPU " + std::to_string(h->device));
+    uintptr_t base;
+    size_t size;
+    if (h->ptr_ok.size() < 64 && device_range(p, &base, &size)) h->ptr_ok.push_back({base, base + size});
     return PMB_OK;
   }
-  if (a.type == cudaMemoryTypeHost) return PMB_OK;  // pinned host memory, mapped for the device
+  if (at.type == cudaMemoryTypeHost) return PMB_OK;  // pinned host memory, mapped for the device
   return pmb_fail(h, PMB_E_INVALID, "device column pointer is not CUDA memory (pageable host memory?)");
 }
 
