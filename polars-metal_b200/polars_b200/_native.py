@@ -608,14 +608,36 @@ def _batch_args(queries, output: str):
     return qrec, ptrs, ncols, keep, names
 
 
+class PreparedBatch:
+    """The C arguments of a batch of queries, built once (prepare_batched) and passed to
+    groupby_batched any number of times: the query and column structs point at the columns'
+    buffers, so they stay valid while those buffers stay where they are (their contents may change
+    between calls). It keeps the buffers alive."""
+
+    def __init__(self, queries, output: str):
+        self.n = len(queries)
+        self.output = output
+        self.qrec, self.ptrs, self.ncols, self.keep, self.names = _batch_args(queries, output)
+
+
+def prepare_batched(queries, output: str = "host") -> PreparedBatch:
+    """Marshals a batch for repeated groupby_batched calls (see PreparedBatch)."""
+    return PreparedBatch(queries, output)
+
+
 def groupby_batched(queries, output: str = "host", handle: Handle | None = None) -> list:
     """Many independent group-by queries in one call (pmb_groupby_batched).
 
-    queries: a list of (columns, keys, aggs, predicate) with the meanings of `groupby`. Queries of
-    one signature run in one persistent launch; the results come back in query order."""
+    queries: a list of (columns, keys, aggs, predicate) with the meanings of `groupby`, or a
+    PreparedBatch (its own output kind then applies). Queries of one signature run in one
+    persistent launch; the results come back in query order."""
     h = handle or default_handle()
-    n = len(queries)
-    qrec, ptrs, ncols, keep, names = _batch_args(queries, output)
+    if isinstance(queries, PreparedBatch):
+        n, output = queries.n, queries.output
+        qrec, ptrs, ncols, keep, names = queries.qrec, queries.ptrs, queries.ncols, queries.keep, queries.names
+    else:
+        n = len(queries)
+        qrec, ptrs, ncols, keep, names = _batch_args(queries, output)
     outs = (C.POINTER(A.Result) * max(1, n))()
     h.check(h._lib.pmb_groupby_batched(h.raw, qrec.ctypes.data_as(C.POINTER(A.Query)),
                                        ptrs.ctypes.data_as(C.POINTER(C.POINTER(A.Column))),
