@@ -97,3 +97,27 @@ def test_overflow_in_batch_reruns_larger(monkeypatch):
     queries = [_np_query(rng, 200_000, 150_000, 0.0), _np_query(rng, 50_000, 100, 1.0)]
     res = groupby_batched([_product(q) for q in queries], handle=Handle(0))
     _check(queries, res, "overflow")
+
+
+def test_prepared_batch_twice_and_the_plain_loop_switch():
+    # a batch prepared once gives the same results on two calls; with batching off the same
+    # batch runs query by query inside the library, with the same results again
+    from polars_b200._native import prepare_batched
+
+    rng = np.random.default_rng(41)
+    qs = []
+    for n, card, s in [(30_000, 50, 0.8), (120_000, 5_000, 0.0), (70_000, 900, 1.2)]:
+        cols, keys, aggs, pred = _np_query(rng, n, card, s)
+        qs.append(({k: ColumnData(*v) for k, v in cols.items()}, keys, aggs, pred))
+    prep = prepare_batched(qs, output="host")
+    first = groupby_batched(prep)
+    second = groupby_batched(prep)
+    h = Handle(0)
+    h.set_batching(False)
+    loop = groupby_batched(prep, handle=h)
+    h.close()
+    for (cols, keys, aggs, pred), a, b, c in zip(qs, first, second, loop):
+        np_cols = {k: (v.data, v.validity) for k, v in cols.items()}
+        want = pyoracle.groupby(np_cols, keys, aggs, pred)
+        for got, label in ((a, "prepared 1"), (b, "prepared 2"), (c, "plain loop")):
+            assert_results_match(as_dict(got), want, 1, aggs, label)
