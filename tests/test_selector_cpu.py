@@ -49,9 +49,13 @@ def test_shipped_selector_gains_over_the_heuristic_on_held_out_tables():
     out = mlp.forward(p, d["X"][te])
     rep = S.evaluate(np.argmax(out[:, :mlp.NS], axis=1), d["T"][te], d["H"][te])
     print(rep)
-    # never slower than the heuristic in total, and most of the way to the best pick per table
-    assert rep["gain_vs_heuristic"] >= 1.0
-    assert rep["learned_vs_best"] <= 1.25
-    # the size prediction: log2(groups) within 1.5 on most held-out tables
+    # the shipped network measured 1.32x over the heuristic on its 2500 held-out tables (of 10,000)
+    # and within 4% of the best strategy per table: hold it to most of that
+    assert rep["gain_vs_heuristic"] >= 1.2
+    assert rep["learned_vs_best"] <= 1.1
+    assert rep["accuracy_learned"] > rep["accuracy_heuristic"]
+    # the size prediction: log2(groups) within 0.5 on most held-out tables (measured median 0.25)
     err = np.abs(out[:, mlp.NS] - np.log2(np.maximum(d["G"][te], 1)))
-    assert np.median(err) < 1.5
+    assert np.median(err) < 0.5
+    # the evaluation covers the 10,000 tables of the learned-selection workload
+    assert d["X"].shape[0] == 10_000
