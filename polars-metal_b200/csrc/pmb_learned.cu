@@ -1,8 +1,8 @@
 // pmb_learned.cu — the learned strategy selector: sketch features of a 4096-row key sample, and a
-// small MLP (24 -> 64 -> 64 -> 4, fp32, CUDA cores) with hand-written forward, backward and Adam
+// small MLP (24 -> 64 -> 64 -> 5, fp32, CUDA cores) with hand-written forward, backward and Adam
 // kernels. The network is trained on timings and exact group counts that the engine measures on
-// synthetic tables (polars_b200/selector.py); its outputs are three strategy scores and log2 of
-// the group count. The reference routes by a row threshold and an estimated-cardinality gate
+// synthetic tables (polars_b200/selector.py); its outputs are four strategy scores (shared-memory
+// hash, global hash, sort, partitioned) and log2 of the group count. The reference routes by a row threshold and an estimated-cardinality gate
 // (crates/polars-metal-core/src/router/cost.rs:35-52, crates/polars-metal-kernels/src/groupby.rs:475-486);
 // that plain heuristic (pmb_choose_strategy) stays the fallback.
 #include <cuda_runtime.h>
