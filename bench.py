@@ -570,7 +570,11 @@ def run_reference(args) -> None:
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload][2], "rows_per_step": sample,
                    "note": "CPU restatement of the reference algorithm (oracle/oracle.cpp); the reference is Rust+Metal "
-                           "and cannot run here"},
+                           "and cannot run here. Each step is a bounded sample (the first rows of the same "
+                           "generator) rather than all rows of the workload, so that --steps K --warmup W ends "
+                           "within minutes (the oracle needs ~8 s per 100M rows on 16 threads); rows/s is "
+                           "per row, and the ours-arm line's parity check times the oracle on all rows "
+                           "(parity.oracle_s)"},
         "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
                          "sample": f"first {sample:,} rows of the workload generator (seed 99) per step"},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
