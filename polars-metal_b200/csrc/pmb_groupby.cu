@@ -1155,8 +1155,11 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
       // one only its initialisation
       int s = 0;
       int64_t g = 0;
-      if (sel && pmb_selector_read(h, cq, &s, &g)) {
-        strategy = s;  // the network scores all four strategies
+      if (sel && pmb_selector_read(h, cq, &s, &g) &&
+          !((s == PMB_STRATEGY_SORT || s == PMB_STRATEGY_PARTITIONED) && pmb_heavy_key(cq, sk))) {
+        // the network scores all four strategies; a sort or partitioned pick with a heavy key in
+        // the sample (one CTA's serial segment) is overruled by the heuristic below
+        strategy = s;
         if (est <= 0) est = std::max<int64_t>(e, std::min<int64_t>(g, cq.dq.n_rows));
       } else {
         if (est <= 0) est = e;
@@ -1194,9 +1197,8 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
 // groups on; 96-bit keys (the prebuilt 128-bit hash kernel) win 2x from 2M groups and tie at
 // 200K. A heavy key would make its partition one CTA's serial work, so the most frequent sampled
 // key must stand for at most 256K rows.
-bool pmb_prefer_partitioned(const CompiledQuery& cq, const SketchOut& sk, int strategy, int64_t est) {
-  if (strategy != PMB_STRATEGY_GLOBAL_HASH && strategy != PMB_STRATEGY_SORT) return false;
-  if (est < (cq.dq.key_bits > 64 ? 200000 : 500000) || sk.samples <= 0) return false;
+bool pmb_heavy_key(const CompiledQuery& cq, const SketchOut& sk) {
+  if (sk.samples <= 0) return false;
   int top = 0;
   for (int c = SK_HIST - 1; c > 0; c--)
     if (sk.hist[c]) {
@@ -1204,7 +1206,13 @@ bool pmb_prefer_partitioned(const CompiledQuery& cq, const SketchOut& sk, int st
       break;
     }
   const double top_rows = (double)top * (double)cq.dq.n_rows / (double)sk.samples;
-  return top < SK_HIST - 1 && top_rows <= 262144.0;
+  return top >= SK_HIST - 1 || top_rows > 262144.0;
+}
+
+bool pmb_prefer_partitioned(const CompiledQuery& cq, const SketchOut& sk, int strategy, int64_t est) {
+  if (strategy != PMB_STRATEGY_GLOBAL_HASH && strategy != PMB_STRATEGY_SORT) return false;
+  if (est < (cq.dq.key_bits > 64 ? 200000 : 500000) || sk.samples <= 0) return false;
+  return !pmb_heavy_key(cq, sk);
 }
 
 // Plain cardinality heuristic (the fallback of the learned selector): shared-memory tables

@@ -78,6 +78,9 @@ int64_t pmb_estimate_groups(const SketchOut& s, int64_t n_rows);
 int pmb_choose_strategy(pmb_handle* h, const CompiledQuery& cq, const SketchOut& sk, int64_t est);
 // AUTO's switch from a chosen global-table or sort strategy to the partitioned strategy
 bool pmb_prefer_partitioned(const CompiledQuery& cq, const SketchOut& sk, int strategy, int64_t est);
+// the most frequent sampled key stands for more than 256K rows: the sort's and the partitioned
+// strategy's work for it would be one CTA's serial segment
+bool pmb_heavy_key(const CompiledQuery& cq, const SketchOut& sk);
 int pmb_plan_hash(pmb_handle* h, int max_smem_optin, CompiledQuery& cq, int strategy, int64_t est, bool have_sketch,
                   HashParams& P, int& nt, int& smem);
 int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,

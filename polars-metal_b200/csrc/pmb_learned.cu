@@ -421,7 +421,8 @@ extern "C" int pmb_selector_choose(pmb_handle* h, const pmb_query* q, const pmb_
   rc = pmb_groupby_sketch(h, cq, &sk);
   if (rc) return rc;
   const int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
-  if (pmb_selector_pick(h, cq, &s, &g)) {
+  if (pmb_selector_pick(h, cq, &s, &g) &&
+      !((s == PMB_STRATEGY_SORT || s == PMB_STRATEGY_PARTITIONED) && pmb_heavy_key(cq, sk))) {
     g = std::max<int64_t>(e, std::min<int64_t>(g, cq.dq.n_rows));
   } else {
     // the heuristic: cardinality, then the switch to the partitioned strategy (the network

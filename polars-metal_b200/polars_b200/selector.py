@@ -33,6 +33,9 @@ from . import _abi as A
 PKG = Path(__file__).resolve().parent
 PARAMS_FILE = PKG / "data" / "selector_params.npy"
 DATASET_FILE = PKG / "data" / "selector_dataset.npz"
+# tables of the same distribution with a filter on most of them: the network is applied to filtered
+# queries too (the hash workload, the batched queries), so it trains on some
+FILTERED_FILE = PKG / "data" / "selector_dataset_filtered.npz"
 STRATEGIES = A.SELECTOR_STRATEGIES  # score index -> strategy name
 KEY_KINDS = ["i32", "i64", "2xi64"]
 _M64 = 0x9E3779B97F4A7C15 - (1 << 64)  # an odd 64-bit multiplier, as a signed int64
@@ -56,20 +59,37 @@ class TableSpec:
     zipf: float
     null_frac: float
     seed: int
+    keep: float = 1.0  # < 1: the query filters v > t, keeping this fraction of the rows
 
 
-def sample_specs(n: int, seed: int, min_rows: float = 1e5, max_rows: float = 1e8, max_distinct: float = 1e8):
+def predicate_of(spec: TableSpec) -> dict | None:
+    """The filter of a spec: v > t with P(v > t) = keep for v ~ N(0,1); None when keep is 1."""
+    if spec.keep >= 1.0:
+        return None
+    from statistics import NormalDist
+
+    t = NormalDist().inv_cdf(1.0 - spec.keep)
+    return {"kind": "Compare", "op": "Gt", "lhs": {"kind": "Column", "name": "v"},
+            "rhs": {"kind": "LiteralF64", "value": float(t)}}
+
+
+def sample_specs(n: int, seed: int, min_rows: float = 1e5, max_rows: float = 1e8, max_distinct: float = 1e8,
+                 filter_frac: float = 0.0):
     """Table specs of the learned-selection workload: rows log-uniform in [min_rows, max_rows],
     distinct count log-uniform in [10, min(max_distinct, rows)], Zipf s uniform in [0, 2], null
-    fraction uniform in [0, 0.2], key width uniform over int32 / int64 / 2 x int64."""
+    fraction uniform in [0, 0.2], key width uniform over int32 / int64 / 2 x int64. With
+    `filter_frac` > 0 that fraction of the tables also gets a filter keeping U[0.05, 1) of the rows
+    (drawn from a separate stream, so the tables themselves do not change)."""
     rng = np.random.default_rng(seed)
+    frng = np.random.default_rng(seed + 7919)
     out = []
     for i in range(n):
         rows = int(math.exp(rng.uniform(math.log(min_rows), math.log(max_rows))))
         hi = min(max_distinct, rows)
         distinct = int(math.exp(rng.uniform(math.log(10), math.log(max(hi, 11)))))
+        keep = float(frng.uniform(0.05, 1.0)) if frng.random() < filter_frac else 1.0
         out.append(TableSpec(rows, KEY_KINDS[rng.integers(0, 3)], max(1, distinct), float(rng.uniform(0, 2)),
-                             float(rng.uniform(0, 0.2)), int(rng.integers(0, 2**31 - 1))))
+                             float(rng.uniform(0, 0.2)), int(rng.integers(0, 2**31 - 1)), keep))
     return out
 
 
@@ -140,19 +160,20 @@ def collect(specs, reps: int = 2, log=None, budget_s: float = 0.0) -> dict:
     warmed = set()  # (key width, strategy): the run-time compile happens in the first such call
     for i, sp in enumerate(specs):
         cols, keys = make_table(sp)
+        pred = predicate_of(sp)
         torch.cuda.synchronize()
-        X.append(selector_features(cols, keys, AGGS, handle=h))
-        heur, _ = selector_choose(cols, keys, AGGS, handle=h)
+        X.append(selector_features(cols, keys, AGGS, pred, handle=h))
+        heur, _ = selector_choose(cols, keys, AGGS, pred, handle=h)
         H.append(STRATEGIES.index(heur) if heur in STRATEGIES else 1)
         times, groups = [], None
         for s in STRATEGIES:
             if (sp.key, s, sp.null_frac > 0) not in warmed:
-                groupby(cols, keys, AGGS, strategy=s, output="device", handle=h)  # warm-up (run-time compile)
+                groupby(cols, keys, AGGS, pred, strategy=s, output="device", handle=h)  # warm-up (run-time compile)
                 warmed.add((sp.key, s, sp.null_frac > 0))
             best = float("inf")
             h.set_profiling(True)
             for _ in range(reps):
-                res = groupby(cols, keys, AGGS, strategy=s, output="device", handle=h)
+                res = groupby(cols, keys, AGGS, pred, strategy=s, output="device", handle=h)
                 best = min(best, h.last_stats()["total_ms"])
             h.set_profiling(False)
             groups = res.n_groups if groups is None else groups
@@ -161,7 +182,7 @@ def collect(specs, reps: int = 2, log=None, budget_s: float = 0.0) -> dict:
             times.append(best)
         T.append(times)
         G.append(groups)
-        S.append([sp.rows, KEY_KINDS.index(sp.key), sp.distinct, sp.zipf, sp.null_frac])
+        S.append([sp.rows, KEY_KINDS.index(sp.key), sp.distinct, sp.zipf, sp.null_frac, sp.keep])
         del cols
         if log and (i + 1) % 50 == 0:
             log(f"{i + 1}/{len(specs)} tables, {time.time() - t0:.0f} s")
@@ -271,13 +292,14 @@ def evaluate_live(specs, params, reps: int = 2, log=None) -> dict:
     picks = {"learned": {}, "heuristic": {}}
     for i, sp in enumerate(specs):
         cols, keys = make_table(sp)
+        pred = predicate_of(sp)
         torch.cuda.synchronize()
         for name, h in (("learned", learned), ("heuristic", plain)):
-            groupby(cols, keys, AGGS, output="device", handle=h)
+            groupby(cols, keys, AGGS, pred, output="device", handle=h)
             h.set_profiling(True)
             best = float("inf")
             for _ in range(reps):
-                res = groupby(cols, keys, AGGS, output="device", handle=h)
+                res = groupby(cols, keys, AGGS, pred, output="device", handle=h)
                 best = min(best, h.last_stats()["total_ms"])
             h.set_profiling(False)
             tot[name] += best
@@ -309,6 +331,7 @@ def main(argv=None):
     c.add_argument("--max-rows", type=float, default=2e7)
     c.add_argument("--out", default=str(DATASET_FILE))
     c.add_argument("--budget-s", type=float, default=0.0, help="stop after this many seconds of collection")
+    c.add_argument("--filter-frac", type=float, default=0.0, help="fraction of the tables that get a filter")
     t = sub.add_parser("train")
     t.add_argument("--data", default=str(DATASET_FILE))
     t.add_argument("--out", default=str(PARAMS_FILE))
@@ -321,30 +344,38 @@ def main(argv=None):
     lv.add_argument("--tables", type=int, default=200)
     lv.add_argument("--seed", type=int, default=12345)
     lv.add_argument("--max-rows", type=float, default=1e8)
+    lv.add_argument("--filter-frac", type=float, default=0.0)
     a = ap.parse_args(argv)
     if a.cmd == "collect":
-        specs = sample_specs(a.tables, a.seed, max_rows=a.max_rows)
+        specs = sample_specs(a.tables, a.seed, max_rows=a.max_rows, filter_frac=a.filter_frac)
         d = collect(specs, log=print, budget_s=a.budget_s)
         print(f"collected {d['X'].shape[0]} tables in {float(d['seconds']):.0f} s")
         Path(a.out).parent.mkdir(parents=True, exist_ok=True)
         np.savez_compressed(a.out, **d)
         print("wrote", a.out)
     elif a.cmd == "train":
-        d = np.load(a.data)
-        tr, te = split(d["X"].shape[0])
-        p, hist = train(d["X"][tr], d["T"][tr], d["G"][tr], epochs=a.epochs, log=print)
+        # several datasets (comma-separated): the network trains on the training split of each
+        parts = [np.load(x) for x in a.data.split(",")]
+        X, T, G = [], [], []
+        for d in parts:
+            tr, _te = split(d["X"].shape[0])
+            X.append(d["X"][tr])
+            T.append(d["T"][tr])
+            G.append(d["G"][tr])
+        p, hist = train(np.concatenate(X), np.concatenate(T), np.concatenate(G), epochs=a.epochs, log=print)
         Path(a.out).parent.mkdir(parents=True, exist_ok=True)
         np.save(a.out, p)
         print("wrote", a.out, "final loss", hist[-1])
     elif a.cmd == "live":
-        specs = sample_specs(a.tables, a.seed, max_rows=a.max_rows)
+        specs = sample_specs(a.tables, a.seed, max_rows=a.max_rows, filter_frac=a.filter_frac)
         print(evaluate_live(specs, np.load(a.params), log=print))
     else:
-        d = np.load(a.data)
         p = np.load(a.params)
-        tr, te = split(d["X"].shape[0])
-        out = predict(p, d["X"][te])
-        print(evaluate(np.argmax(out[:, :len(STRATEGIES)], axis=1), d["T"][te], d["H"][te]))
+        for path in a.data.split(","):
+            d = np.load(path)
+            tr, te = split(d["X"].shape[0])
+            out = predict(p, d["X"][te])
+            print(Path(path).name, evaluate(np.argmax(out[:, :len(STRATEGIES)], axis=1), d["T"][te], d["H"][te]))
 
 
 if __name__ == "__main__":
