@@ -309,9 +309,10 @@ def filter_subrecord(t, cols, h, stream, threads: int | None) -> dict:
                         "frac": (in_bytes + out_bytes) / (kern[dom] / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
            "parity": None}
     # the u8 -> u32 inclusive scan (the reference's MLX cumsum), 100M device bytes in, 400 MB out
-    g = torch.Generator(device=t.columns["k"][0].device)
+    dev = next(iter(t.columns.values()))[0].device
+    g = torch.Generator(device=dev)
     g.manual_seed(5)
-    u8 = torch.randint(0, 256, (n,), dtype=torch.uint8, device=t.columns["k"][0].device, generator=g)
+    u8 = torch.randint(0, 256, (n,), dtype=torch.uint8, device=dev, generator=g)
     o32 = torch.empty(n, dtype=torch.int32, device=u8.device)
 
     def scan():

@@ -1156,9 +1156,9 @@ extern "C" int pmb_groupby(pmb_handle* h, const pmb_query* q, const pmb_column* 
       int s = 0;
       int64_t g = 0;
       if (sel && pmb_selector_read(h, cq, &s, &g) &&
-          !((s == PMB_STRATEGY_SORT || s == PMB_STRATEGY_PARTITIONED) && pmb_heavy_key(cq, sk))) {
-        // the network scores all four strategies; a sort or partitioned pick with a heavy key in
-        // the sample (one CTA's serial segment) is overruled by the heuristic below
+          !(pmb_selector_vetoed(cq, sk, s))) {
+        // the network scores all four strategies; pmb_selector_vetoed picks are overruled by the
+        // heuristic below
         strategy = s;
         if (est <= 0) est = std::max<int64_t>(e, std::min<int64_t>(g, cq.dq.n_rows));
       } else {
@@ -1207,6 +1207,17 @@ bool pmb_heavy_key(const CompiledQuery& cq, const SketchOut& sk) {
     }
   const double top_rows = (double)top * (double)cq.dq.n_rows / (double)sk.samples;
   return top >= SK_HIST - 1 || top_rows > 262144.0;
+}
+
+// A sort or partitioned pick of the network for a key of at most 64 packed bits with a heavy key
+// in the sample: over the 13,000 timed tables of the selector's training data, such queries never
+// ran faster than the run-time compiled hash kernel (vetoing them would have cost 22 ms of 1,520 ms
+// there), while a heavy key can make its segment one CTA's serial work (the hash workload: 27.8 ms
+// sorted against 2.0 ms hashed). Wider keys keep the network's pick: their hash path is the slower
+// prebuilt 128-bit kernel, and there the sort and partitioned strategies often win.
+bool pmb_selector_vetoed(const CompiledQuery& cq, const SketchOut& sk, int strategy) {
+  return (strategy == PMB_STRATEGY_SORT || strategy == PMB_STRATEGY_PARTITIONED) && cq.dq.key_bits <= 64 &&
+         pmb_heavy_key(cq, sk);
 }
 
 bool pmb_prefer_partitioned(const CompiledQuery& cq, const SketchOut& sk, int strategy, int64_t est) {

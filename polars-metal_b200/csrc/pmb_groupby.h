@@ -81,6 +81,8 @@ bool pmb_prefer_partitioned(const CompiledQuery& cq, const SketchOut& sk, int st
 // the most frequent sampled key stands for more than 256K rows: the sort's and the partitioned
 // strategy's work for it would be one CTA's serial segment
 bool pmb_heavy_key(const CompiledQuery& cq, const SketchOut& sk);
+// a learned pick that AUTO overrules with the heuristic (see pmb_groupby.cu)
+bool pmb_selector_vetoed(const CompiledQuery& cq, const SketchOut& sk, int strategy);
 int pmb_plan_hash(pmb_handle* h, int max_smem_optin, CompiledQuery& cq, int strategy, int64_t est, bool have_sketch,
                   HashParams& P, int& nt, int& smem);
 int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,

@@ -422,7 +422,7 @@ extern "C" int pmb_selector_choose(pmb_handle* h, const pmb_query* q, const pmb_
   if (rc) return rc;
   const int64_t e = pmb_estimate_groups(sk, cq.dq.n_rows);
   if (pmb_selector_pick(h, cq, &s, &g) &&
-      !((s == PMB_STRATEGY_SORT || s == PMB_STRATEGY_PARTITIONED) && pmb_heavy_key(cq, sk))) {
+      !(pmb_selector_vetoed(cq, sk, s))) {
     g = std::max<int64_t>(e, std::min<int64_t>(g, cq.dq.n_rows));
   } else {
     // the heuristic: cardinality, then the switch to the partitioned strategy (the network

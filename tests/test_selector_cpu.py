@@ -49,8 +49,8 @@ def test_shipped_selector_gains_over_the_heuristic_on_held_out_tables():
     out = mlp.forward(p, d["X"][te])
     rep = S.evaluate(np.argmax(out[:, :mlp.NS], axis=1), d["T"][te], d["H"][te])
     print(rep)
-    # the shipped network measured 1.32x over the heuristic on its 2500 held-out tables (of 10,000)
-    # and within 4% of the best strategy per table: hold it to most of that
+    # the shipped network measured 1.31x over the heuristic on its 2500 held-out tables (of 10,000)
+    # and within 5% of the best strategy per table: hold it to most of that
     assert rep["gain_vs_heuristic"] >= 1.2
     assert rep["learned_vs_best"] <= 1.1
     assert rep["accuracy_learned"] > rep["accuracy_heuristic"]
@@ -59,3 +59,17 @@ def test_shipped_selector_gains_over_the_heuristic_on_held_out_tables():
     assert np.median(err) < 0.5
     # the evaluation covers the 10,000 tables of the learned-selection workload
     assert d["X"].shape[0] == 10_000
+
+
+@pytest.mark.skipif(not (S.FILTERED_FILE.exists() and S.default_params() is not None), reason="no shipped selector")
+def test_shipped_selector_gains_on_filtered_tables():
+    # 3,000 tables of the same distribution, 80% of them filtered (v > t keeping 5-100% of the
+    # rows): the shipped network trained on their training split too; measured 1.27x over the
+    # heuristic and 1.037x of the best on the 750 held out
+    d = np.load(S.FILTERED_FILE)
+    p = S.default_params()
+    tr, te = S.split(d["X"].shape[0])
+    out = mlp.forward(p, d["X"][te])
+    rep = S.evaluate(np.argmax(out[:, :mlp.NS], axis=1), d["T"][te], d["H"][te])
+    assert rep["gain_vs_heuristic"] >= 1.15
+    assert rep["learned_vs_best"] <= 1.1
