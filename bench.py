@@ -379,6 +379,35 @@ def sort_extras(t, cols, h, stream, strategy: str, used: str, ms_group_by: float
     return sort_strategy, sorted_output
 
 
+def sort_parity_slice(got, table, threads: int, k2: int = 0) -> dict:
+    """Parity of the sort workload's group-by over one slice of its key space: the groups whose
+    second key equals `k2` are exactly the groups of the rows with that key, so the oracle's group-by
+    of those rows (1/64 of all rows) must equal the device result's groups with k2 == `k2`. Exact,
+    and a few seconds of CPU instead of the minutes of a 49M-group oracle run."""
+    import numpy as np
+
+    from oracle import pyoracle
+
+    t0 = time.perf_counter()
+    mask = table.columns["k2"][0] == k2
+    cols = {name: (d[mask].cpu().numpy(), None) for name, (d, v) in table.columns.items()}
+    want = pyoracle.groupby(cols, table.keys, table.aggs, None, n_threads=threads)
+    kcol = got.names.index("k2")
+    n = int(got.n_groups)
+    sel = np.nonzero(np.asarray(got.data[kcol])[:n] == k2)[0]
+    data, valid = [], []
+    for d, v in zip(got.data, got.validity):
+        data.append(np.asarray(d)[:n][sel])
+        bits = np.unpackbits(np.asarray(v, dtype=np.uint8), bitorder="little")[:n][sel]
+        valid.append(np.packbits(bits, bitorder="little"))
+    g = {"n_groups": len(sel), "names": got.names, "dtypes": got.dtypes, "data": data, "validity": valid}
+    rep = compare_results(g, want, len(table.keys), table.aggs)
+    rep["rows"] = int(mask.sum().item())
+    rep["slice"] = f"k2 == {k2}: 1/64 of the rows and of the groups"
+    rep["oracle_s"] = time.perf_counter() - t0
+    return rep
+
+
 def sort_subrecord(device, h, stream, threads: int | None) -> dict:
     """The sort workload (200M rows, two-column key, ~49M groups) on device-resident inputs: AUTO
     (the partitioned strategy), the sort strategy, the sorted group-by, its dominant kernel against
@@ -411,7 +440,7 @@ def sort_subrecord(device, h, stream, threads: int | None) -> dict:
            "sort_strategy": sort_strategy, "sorted_output": sorted_output, "parity": None}
     if threads:
         got = groupby(cols, t.keys, t.aggs, None, output="host", handle=h)
-        rec["parity"] = parity_against_oracle(got, t, threads)
+        rec["parity"] = sort_parity_slice(got, t, threads)
         del got
     del cols, t
     torch.cuda.synchronize()
@@ -468,15 +497,19 @@ def batch_vs_plain(qs, rows: int, stream, h_learned, h_plain, steps: int = 3, pl
 
     ms_b = time_calls(lambda: groupby_batched(prep_dev, handle=h_learned), stream, steps, 3)
     ms_bh = time_calls(lambda: groupby_batched(prep_dev, handle=h_plain), stream, steps, 3)
+    ms_bhh = time_calls(lambda: groupby_batched(prep_host, handle=h_plain), stream, plain_steps, 1)
     ms_c = time_calls(c_loop, stream, plain_steps, 1)
     ms_p = time_calls(plain, stream, plain_steps, 1)
     arm = lambda ms, st: {"rows_per_s": rows / (ms / 1e3), "ms_per_step": ms, "steps": st}  # noqa: E731
     return {"workload": BATCH_DESC, "queries": len(qs), "rows": rows,
             "batched_learned": arm(ms_b, steps), "batched_heuristic": arm(ms_bh, steps),
-            "plain_loop_c": arm(ms_c, plain_steps), "plain_heuristic": arm(ms_p, plain_steps),
-            "speedup": ms_p / ms_b, "speedup_vs_c_loop": ms_c / ms_b, "selector_gain": ms_bh / ms_b,
+            "batched_heuristic_host": arm(ms_bhh, plain_steps), "plain_loop_c": arm(ms_c, plain_steps),
+            "plain_heuristic": arm(ms_p, plain_steps),
+            "speedup": ms_p / ms_b, "speedup_vs_c_loop": ms_c / ms_bhh, "selector_gain": ms_bh / ms_b,
             "note": "the batched arms and the C loop take a batch prepared once before timing (prepare_batched: "
-                    "its C arguments built once); the Python loop makes one groupby call per query"}
+                    "its C arguments built once); the Python loop makes one groupby call per query with device "
+                    "outputs; the C loop has host outputs only, so speedup_vs_c_loop divides it by the batched "
+                    "heuristic arm with host outputs (batched_heuristic_host): the batching's own share"}
 
 
 def batch_parity(tables, qs, h, threads: int) -> dict:
