@@ -17,6 +17,7 @@
 #include <cstring>
 #include <string>
 
+#include "pmb_jit.h"
 #include "pmb_plan.h"
 
 namespace {
@@ -138,16 +139,21 @@ __global__ void __launch_bounds__(CT_NT) k_compact(const __grid_constant__ Compa
     if (lane == 0) s_cnt[j][warp] = __popc(b);
   }
   __syncthreads();
-  if (tid == 0) {
+  if (warp == 0) {
     int acc = 0;
-    for (int j = 0; j < CT_PER; j++)
-      for (int w = 0; w < CT_NT / 32; w++) {
-        s_off[j][w] = acc;
-        acc += s_cnt[j][w];
-      }
-    unsigned long long base = pmb_lookback(P.lb, tile, (unsigned long long)acc, P.status);
-    s_base = base;
-    if (tile == (long long)gridDim.x - 1) *P.n_out = base + acc;
+    if (lane == 0) {
+      for (int j = 0; j < CT_PER; j++)
+        for (int w = 0; w < CT_NT / 32; w++) {
+          s_off[j][w] = acc;
+          acc += s_cnt[j][w];
+        }
+    }
+    acc = __shfl_sync(0xffffffffu, acc, 0);
+    const unsigned long long base = pmb_lookback_warp(P.lb, tile, (unsigned long long)acc, P.status);
+    if (lane == 0) {
+      s_base = base;
+      if (tile == (long long)gridDim.x - 1) *P.n_out = base + acc;
+    }
   }
   __syncthreads();
   const unsigned long long base = s_base;
@@ -178,7 +184,7 @@ __global__ void __launch_bounds__(CT_NT) k_compact(const __grid_constant__ Compa
 }
 
 // ----------------------------------------------------------------- u8 -> u32 inclusive scan
-constexpr int SC_NT = 256;
+constexpr int SC_NT = 512;  // 8192 rows per tile: one look-back per 8 KB of input
 constexpr int SC_PER = 16;
 constexpr int SC_TILE = SC_NT * SC_PER;
 
@@ -220,14 +226,19 @@ __global__ void __launch_bounds__(SC_NT) k_cumsum_u8(const uint8_t* __restrict__
   }
   if (lane == 31) s_warp[warp] = x;
   __syncthreads();
-  if (tid == 0) {
-    uint32_t acc = 0;
-    for (int w = 0; w < SC_NT / 32; w++) {
-      uint32_t t = s_warp[w];
-      s_warp[w] = acc;
-      acc += t;
+  if (warp == 0) {
+    // warp 0: exclusive offsets of the warps' sums, then the tile's look-back with all 32 lanes
+    const uint32_t w_sum = lane < SC_NT / 32 ? s_warp[lane] : 0u;
+    uint32_t w_inc = w_sum;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, w_inc, d);
+      if (lane >= d) w_inc += y;
     }
-    s_base = pmb_lookback(lb, tile, acc, status);
+    const uint32_t total = __shfl_sync(0xffffffffu, w_inc, 31);
+    __syncwarp();
+    if (lane < SC_NT / 32) s_warp[lane] = w_inc - w_sum;
+    const unsigned long long base = pmb_lookback_warp(lb, tile, total, status);
+    if (lane == 0) s_base = base;
   }
   __syncthreads();
   uint32_t run = (uint32_t)s_base + s_warp[warp] + (x - sum);
@@ -287,7 +298,43 @@ int run_compact(pmb_handle* h, CompiledQuery& cq, const uint8_t* keep_d, const u
     cudaMemsetAsync(P.out_valid[c], 0, vb + 16, h->stream);
     if (!e) cudaMemsetAsync(P.out_data[c], 0, db + 16, h->stream);
   }
-  if (n > 0) {
+  // a predicate over many rows: the run-time compiled compaction (literal offsets and dtypes)
+  cudaKernel_t jk = nullptr;
+  if (n > 0 && !keep_d && pmb_jit_enabled(n)) {
+    std::string keep_err = h->err;
+    if (pmb_jit_compact_kernel(h, cq, n_out, &jk) != PMB_OK) jk = nullptr;  // prebuilt kernel: same results
+    h->err = keep_err;
+  }
+  if (n > 0 && jk) {
+    const int64_t jt = (n + JC_TILE_ROWS - 1) / JC_TILE_ROWS;
+    if (jt > tiles) {
+      pmb_result_free(r);
+      return pmb_fail(h, PMB_E_CUDA, "internal: compaction tiles");
+    }
+    JitCompactParams A;
+    memset(&A, 0, sizeof(A));
+    for (int c = 0; c < q.n_cols; c++) {
+      A.col_data[c] = q.col[c].data;
+      A.col_valid[c] = q.col[c].valid;
+    }
+    A.n_rows = n;
+    A.lb = P.lb;
+    A.ticket = P.ticket;
+    A.n_out = P.n_out;
+    A.status = P.status;
+    for (int c = 0; c < n_out; c++) {
+      A.out_data[c] = P.out_data[c];
+      A.out_valid[c] = P.out_valid[c];
+    }
+    void* args[] = {&A};
+    pmb_kernel_begin(h, "compact");
+    cudaError_t e = cudaLaunchKernel((const void*)jk, dim3((unsigned)jt), dim3(256), args, 0, h->stream);
+    pmb_kernel_end(h);
+    if (e != cudaSuccess) {
+      pmb_result_free(r);
+      return pmb_cuda_check(h, e, "pmb_jit_compact launch");
+    }
+  } else if (n > 0) {
     pmb_kernel_begin(h, "compact");
     k_compact<<<(unsigned)tiles, CT_NT, 0, h->stream>>>(P);
     pmb_kernel_end(h);

@@ -315,6 +315,47 @@ __device__ __forceinline__ unsigned long long pmb_lookback(unsigned long long* s
   return excl;
 }
 
+// pmb_lookback for a whole warp (every lane calls it; all get the tile's exclusive prefix): the
+// lanes read 32 predecessor states at once, so a look-back costs one L2 round trip per 32 tiles
+// instead of one per tile. The window is summed up to its nearest inclusive prefix; a window that
+// still holds an unpublished state before that point is read again (bounded: PMB_ST_TIMEOUT).
+__device__ __forceinline__ unsigned long long pmb_lookback_warp(unsigned long long* status, long long tile,
+                                                                unsigned long long count, unsigned int* st) {
+  const unsigned long long VAL = (1ULL << 62) - 1;
+  const int lane = threadIdx.x & 31;
+  if (tile == 0) {
+    if (lane == 0) atomicExch(&status[0], (2ULL << 62) | count);
+    return 0;
+  }
+  if (lane == 0) atomicExch(&status[tile], (1ULL << 62) | count);
+  unsigned long long excl = 0;
+  long long top = tile - 1;
+  uint32_t spins = 0;
+  for (;;) {
+    const long long t = top - lane;
+    const unsigned long long s = t >= 0 ? *((volatile unsigned long long*)&status[t]) : (2ULL << 62);
+    const unsigned flag = (unsigned)(s >> 62);
+    const unsigned incl = __ballot_sync(0xffffffffu, flag == 2u), none = __ballot_sync(0xffffffffu, flag == 0u);
+    const int first = incl ? __ffs(incl) - 1 : 32;
+    const unsigned need = first == 32 ? 0xffffffffu : (0xffffffffu >> (31 - first));  // lanes 0..first
+    if (none & need) {
+      if (++spins > PMB_SPIN_LIMIT) {
+        if (lane == 0) atomicOr(st, PMB_ST_TIMEOUT);
+        return 0;
+      }
+      continue;
+    }
+    unsigned long long v = lane <= first ? (s & VAL) : 0ULL;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    excl += v;
+    if (first < 32) break;
+    top -= 32;
+  }
+  if (lane == 0) atomicExch(&status[tile], (2ULL << 62) | (excl + count));
+  return excl;
+}
+
 // the same over states spaced `stride` apart (state of tile t at status[t * stride])
 __device__ __forceinline__ unsigned long long pmb_lookback_strided(unsigned long long* status, long long tile,
                                                                    long long stride, unsigned long long count,

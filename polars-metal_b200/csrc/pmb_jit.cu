@@ -25,7 +25,7 @@
 
 namespace {
 
-#include "pmb_jit_sources.inc"  // kDeviceHeader, kSkeleton (generated from the .cuh files by the build)
+#include "pmb_jit_sources.inc"  // kDeviceHeader, kSkeleton, ... (generated from the .cuh files by the build)
 
 // ---------------------------------------------------------------------------- NVRTC via dlopen
 typedef int nvrtcResult_t;
@@ -533,6 +533,49 @@ struct Gen {
     }
   }
 
+  // the top-level filter's row functions: the verdict of row `row` read straight from the
+  // predicate's columns, and the scatter of the first `n_out` columns to output position p
+  // (every lane of the warp calls j_scatter: the validity words are OR-ed warp-wide)
+  std::string compact_funcs(int n_out) {
+    std::ostringstream b;
+    mark();
+    std::ostringstream body;
+    std::string keep = predicate(body);
+    b << "__device__ __forceinline__ bool j_keep_row(const JCParams& P, long long row) {\n  JRow r;\n";
+    for (int c = 0; c < q.n_cols; c++) {
+      if (!pred_col[c]) continue;
+      const DCol& C = q.col[c];
+      const std::string cs = std::to_string(c);
+      if (C.dtype == PMB_BOOL)
+        b << "  r.v" << cs << " = ((P.col_data[" << cs << "][row >> 3] >> (row & 7)) & 1) != 0;\n";
+      else
+        b << "  r.v" << cs << " = reinterpret_cast<const " << ctype(C.dtype) << "*>(P.col_data[" << cs << "])[row];\n";
+      if (C.valid) b << "  r.ok" << cs << " = ((P.col_valid[" << cs << "][row >> 3] >> (row & 7)) & 1) != 0;\n";
+    }
+    b << body.str() << "  return " << keep << ";\n}\n";
+    b << "__device__ __forceinline__ void j_scatter(const JCParams& P, long long row, bool keep, long long p, "
+         "long long p_first) {\n";
+    for (int c = 0; c < n_out && c < q.n_cols; c++) {
+      const DCol& C = q.col[c];
+      const std::string cs = std::to_string(c);
+      if (C.dtype == PMB_BOOL) {
+        b << "  { const bool bv = keep && ((P.col_data[" << cs << "][row >> 3] >> (row & 7)) & 1) != 0;\n"
+          << "    jc_set_bits(reinterpret_cast<unsigned int*>(P.out_data[" << cs << "]), p, p_first, bv); }\n";
+      } else {
+        const std::string T = ctype(C.dtype);
+        b << "  if (keep) reinterpret_cast<" << T << "*>(P.out_data[" << cs << "])[p] = reinterpret_cast<const " << T
+          << "*>(P.col_data[" << cs << "])[row];\n";
+      }
+      if (C.valid)
+        b << "  jc_set_bits(P.out_valid[" << cs << "], p, p_first, keep && ((P.col_valid[" << cs
+          << "][row >> 3] >> (row & 7)) & 1) != 0);\n";
+      else
+        b << "  jc_set_bits(P.out_valid[" << cs << "], p, p_first, keep);\n";
+    }
+    b << "}\n";
+    return b.str();
+  }
+
   // the aggregated columns of row `row`, read straight from the columns (a gather)
   void gather(std::ostringstream& b) {
     for (int c = 0; c < q.n_cols; c++) {
@@ -977,6 +1020,27 @@ int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, b
   return jit_kernel(h, part_source(cq, *J, key_words, cas64 && key_words == 1), "pmb_jit_part_agg", out);
 }
 
+// the top-level filter's compaction (pmb_jit_compact.cuh): device helpers, the parameter block,
+// the generated row functions of the hash skeleton's prefix, the compaction's own parameter block
+// and helpers, its generated row functions, then its kernel
+std::string pmb_jit_compact_source(const CompiledQuery& cq, const JitPlan& J, int n_out) {
+  Gen g(cq.dq, J);
+  std::string skel(kSkeleton);
+  const size_t cut = skel.find("__device__ __forceinline__ long long j_gresolve");
+  std::string comp(kCompactSkeleton);
+  const size_t kcut = comp.find("extern \"C\" __global__");
+  Gen g2(cq.dq, J);
+  return std::string(kDeviceHeader) + "\n" + skel.substr(0, cut) + "\n" + g.build() + "\n" + comp.substr(0, kcut) +
+         "\n" + g2.compact_funcs(n_out) + "\n" + comp.substr(kcut);
+}
+
+int pmb_jit_compact_kernel(pmb_handle* h, const CompiledQuery& cq, int n_out, cudaKernel_t* out) {
+  JitPlan J;
+  int rc = pmb_plan_jit_batch(h, cq, 1024, 1, h->max_smem_optin, &J);
+  if (rc) return rc;
+  return jit_kernel(h, pmb_jit_compact_source(cq, J, n_out), "pmb_jit_compact", out);
+}
+
 int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out) {
   return jit_kernel(h, "#define PMB_EXPLICIT_RED 1\n" + pmb_jit_source(cq, J) + "\n" + std::string(kBatchSkeleton),
                     "pmb_jit_batch_agg", out);
@@ -1000,7 +1064,14 @@ static int debug_compile(const pmb_query* q, const pmb_column* cols, int32_t n_c
       cq.dq.col[c].data = dummy;
       cq.dq.col[c].valid = cols[cq.map.user[c]].validity ? dummy : nullptr;
     }
-    if (mode == 2) {
+    if (mode == 3) {
+      JitPlan J;
+      rc = pmb_plan_jit_batch(&h, cq, 1024, 1, 232448, &J);
+      if (rc != PMB_OK) msg = h.err;
+      std::vector<char> cubin;
+      if (rc == PMB_OK && !jit_compile(pmb_jit_compact_source(cq, J, cq.dq.n_cols), cubin, msg)) rc = PMB_E_UNSUPPORTED;
+      else if (rc == PMB_OK && getenv("PMB_JIT_DEBUG") && getenv("PMB_JIT_DEBUG")[0] == '2') fprintf(stderr, "%s\n", msg.c_str());
+    } else if (mode == 2) {
       JitPlan J;
       rc = pmb_plan_jit_batch(&h, cq, 1024, 1, 232448, &J);
       if (rc != PMB_OK) msg = h.err;
@@ -1046,6 +1117,12 @@ extern "C" int pmb_debug_jit_compile(const pmb_query* q, const pmb_column* cols,
 extern "C" int pmb_debug_jit_compile_batch(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,
                                            int64_t log_cap) {
   return debug_compile(q, cols, n_cols, log, log_cap, 1);
+}
+// the same for the top-level filter's compaction (pmb_jit_compact.cuh) of every column by the
+// query's predicate (keys and aggregates of the query are ignored)
+extern "C" int pmb_debug_jit_compile_compact(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,
+                                             int64_t log_cap) {
+  return debug_compile(q, cols, n_cols, log, log_cap, 3);
 }
 // the same for the partitioned strategy's aggregation kernel (pmb_jit_part.cuh)
 extern "C" int pmb_debug_jit_compile_part(const pmb_query* q, const pmb_column* cols, int32_t n_cols, char* log,

@@ -101,6 +101,24 @@ int pmb_jit_part_kernel(pmb_handle* h, const CompiledQuery& cq, int key_words, b
 int pmb_plan_jit_batch(pmb_handle* h, const CompiledQuery& cq, int nt, int nbuf, int max_smem_optin, JitPlan* J,
                        int warm_max = 0);
 int pmb_jit_batch_kernel(pmb_handle* h, const CompiledQuery& cq, const JitPlan& J, cudaKernel_t* out);
+// launch parameters of pmb_jit_compact (the layout of JCParams in pmb_jit_compact.cuh)
+struct JitCompactParams {
+  const unsigned char* col_data[16];
+  const unsigned char* col_valid[16];
+  long long n_rows;
+  unsigned long long* lb;
+  unsigned long long* ticket;
+  unsigned long long* n_out;
+  unsigned int* status;
+  unsigned char* out_data[16];
+  unsigned int* out_valid[16];
+};
+constexpr int JC_TILE_ROWS = 256 * 16;  // rows per tile of pmb_jit_compact (JC_TILE)
+
+// the top-level filter's compaction of the first n_out columns by the query's predicate
+// (pmb_jit_compact.cuh); the source alone for the compile checks
+std::string pmb_jit_compact_source(const CompiledQuery& cq, const JitPlan& J, int n_out);
+int pmb_jit_compact_kernel(pmb_handle* h, const CompiledQuery& cq, int n_out, cudaKernel_t* out);
 // launches over the global table and key lists set up in P (gkeys, grecs, gcap, status, lists)
 int pmb_jit_launch(pmb_handle* h, cudaKernel_t k, const CompiledQuery& cq, const JitPlan& J, const HashParams& P,
                    int grid, const uint8_t* ttab, int tnb);

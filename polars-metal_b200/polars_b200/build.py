@@ -36,7 +36,8 @@ SOURCES = [
 
 # device sources compiled at run time by NVRTC, embedded into the library as string literals
 JIT_EMBED = [("kDeviceHeader", "pmb_device.cuh"), ("kSkeleton", "pmb_jit_skeleton.cuh"),
-             ("kBatchSkeleton", "pmb_jit_batch.cuh"), ("kPartSkeleton", "pmb_jit_part.cuh")]
+             ("kBatchSkeleton", "pmb_jit_batch.cuh"), ("kPartSkeleton", "pmb_jit_part.cuh"),
+             ("kCompactSkeleton", "pmb_jit_compact.cuh")]
 
 
 def write_jit_sources() -> Path:

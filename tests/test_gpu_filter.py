@@ -126,3 +126,37 @@ def test_cumsum_u8_to_u32(n):
     a = rng.integers(0, 256, n).astype(np.uint8)
     got = N.cumsum_u8_to_u32(a)
     assert np.array_equal(got, pyoracle.cumsum_u8_to_u32(a))
+
+
+@pytest.mark.parametrize("n", [2_097_152, 3_000_017])
+def test_filter_columns_run_time_compiled_vs_oracle(n):
+    # above 2^21 rows the predicate path compiles its compaction at run time: every output dtype,
+    # nullable and not, a Bool column in the predicate, rows not a multiple of the tile
+    rng = np.random.default_rng(n)
+    cols_np = {
+        "i8": (rng.integers(-100, 100, n).astype(np.int8), pack(rng.random(n) > 0.1)),
+        "u16": (rng.integers(0, 60000, n).astype(np.uint16), None),
+        "i32": (rng.integers(-2**31, 2**31, n).astype(np.int32), pack(rng.random(n) > 0.05)),
+        "u64": (rng.integers(0, 2**63, n).astype(np.uint64), None),
+        "f32": (rng.standard_normal(n).astype(np.float32), pack(rng.random(n) > 0.2)),
+        "x": (rng.standard_normal(n), pack(rng.random(n) > 0.05)),
+        "y": (rng.integers(-10**9, 10**9, n).astype(np.int64), pack(rng.random(n) > 0.05)),
+        "b": (pack(rng.random(n) > 0.3), pack(rng.random(n) > 0.1), A.BOOL, n),
+    }
+    pred = {"kind": "And",
+            "lhs": {"kind": "Or", "lhs": {"kind": "Column", "name": "b"},
+                    "rhs": {"kind": "Compare", "op": "Gt", "lhs": {"kind": "Column", "name": "x"},
+                            "rhs": {"kind": "LiteralF64", "value": 0.5}}},
+            "rhs": {"kind": "Compare", "op": "Ne", "dtype": "I64",
+                    "lhs": {"kind": "Arith", "op": "Mod", "lhs": {"kind": "Column", "name": "y"},
+                            "rhs": {"kind": "LiteralI64", "value": 7}}, "rhs": {"kind": "LiteralI64", "value": 0}}}
+    keep = pyoracle.filter_mask(cols_np, pred)
+    m, want = pyoracle.filter_compact(keep, cols_np)
+    got = N.filter_columns({k: ColumnData(*v) for k, v in cols_np.items()}, pred)
+    assert got.n_groups == m == keep.sum()
+    for j, (dt, wd, wv) in enumerate(want):
+        assert np.array_equal(unpack(np.asarray(got.validity[j], np.uint8), m), unpack(wv, m)), got.names[j]
+        if dt == A.BOOL:
+            assert np.array_equal(unpack(np.asarray(got.data[j], np.uint8), m), unpack(wd, m))
+        else:
+            assert np.asarray(got.data[j])[:m].tobytes() == wd[:m].tobytes(), got.names[j]

@@ -20,7 +20,8 @@ def _lib():
     return L
 
 
-def jit_compile(cols: dict, keys, aggs, predicate=None, batch: bool = False, part: bool = False) -> tuple[int, str]:
+def jit_compile(cols: dict, keys, aggs, predicate=None, batch: bool = False, part: bool = False,
+                compact: bool = False) -> tuple[int, str]:
     L = _lib()
     names = list(cols)
     cds = [c if isinstance(c, ColumnData) else ColumnData(*c) for c in cols.values()]
@@ -39,7 +40,8 @@ def jit_compile(cols: dict, keys, aggs, predicate=None, batch: bool = False, par
     q.n_aggs = len(aggs)
     q.predicate = C.pointer(expr) if expr is not None else None
     buf = C.create_string_buffer(1 << 16)
-    fn = L.pmb_debug_jit_compile_part if part else L.pmb_debug_jit_compile_batch if batch else L.pmb_debug_jit_compile
+    fn = (L.pmb_debug_jit_compile_compact if compact else L.pmb_debug_jit_compile_part if part
+          else L.pmb_debug_jit_compile_batch if batch else L.pmb_debug_jit_compile)
     fn.argtypes = [C.POINTER(A.Query), C.POINTER(A.Column), C.c_int32, C.c_char_p, C.c_int64]
     rc = fn(C.byref(q), abi, len(names), buf, 1 << 16)
     return rc, buf.value.decode(errors="replace")
@@ -142,4 +144,31 @@ def test_partitioned_kernel_value_dtypes_compile():
     aggs = [("Sum", "f", "s"), ("Mean", "u", "m"), ("Min", "f", "mn"), ("Max", "u", "mx"), ("Count", "b", "c"),
             ("Sum", "b", "sb"), ("Len", None, "n")]
     rc, log = jit_compile(cols, ["k"], aggs, part=True)
+    assert rc == 0, log
+
+
+@pytest.mark.parametrize("maker", ["make_hash", "make_small"])
+def test_compaction_kernel_compiles(maker):
+    t = getattr(datagen, maker)(1024, seed=1)
+    cols = {k: ColumnData(d.numpy(), None if v is None else v.numpy()) for k, (d, v) in t.columns.items()}
+    rc, log = jit_compile(cols, t.keys, t.aggs, t.predicate, compact=True)
+    assert rc == 0, log
+
+
+def test_compaction_kernel_all_dtypes_compile():
+    # every output dtype (Bool bit-packed, 8- to 64-bit integers, floats), nullable or not, and a
+    # predicate over a Bool column and an integer modulo
+    rng = np.random.default_rng(3)
+    n = 64
+    cols = {"k": ColumnData(rng.integers(0, 5, n).astype(np.int32))}
+    for i, dt in enumerate([np.int8, np.uint8, np.int16, np.uint16, np.int32, np.uint32, np.int64, np.uint64,
+                            np.float32, np.float64]):
+        cols[f"c{i}"] = ColumnData(rng.integers(0, 100, n).astype(dt), np.packbits(rng.random(n) > 0.2, bitorder="little"))
+    cols["b"] = ColumnData(np.packbits(rng.random(n) > 0.5, bitorder="little"), None, dtype=A.BOOL, length=n)
+    pred = {"kind": "And", "lhs": {"kind": "Column", "name": "b"},
+            "rhs": {"kind": "Compare", "op": "Ne", "dtype": "I64",
+                    "lhs": {"kind": "Arith", "op": "Mod", "lhs": {"kind": "Column", "name": "c6"},
+                            "rhs": {"kind": "LiteralI64", "value": 3}},
+                    "rhs": {"kind": "LiteralI64", "value": 0}}}
+    rc, log = jit_compile(cols, ["k"], [("Len", None, "n")], pred, compact=True)
     assert rc == 0, log
