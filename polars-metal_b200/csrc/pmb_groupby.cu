@@ -560,16 +560,21 @@ __global__ void __launch_bounds__(NT) k_finalize(const __grid_constant__ FinPara
     if (lane == 0) s_cnt[j][warp] = __popc(b);
   }
   __syncthreads();
-  if (tid == 0) {
+  if (warp == 0) {
     int acc = 0;
-    for (int j = 0; j < PER; j++)
-      for (int w = 0; w < NT / 32; w++) {
-        s_off[j][w] = acc;
-        acc += s_cnt[j][w];
-      }
-    unsigned long long base = pmb_lookback(F.lb_status, tile, (unsigned long long)acc, F.status);
-    s_base = base;
-    if (tile == (long long)gridDim.x - 1) *F.n_groups = base + acc;
+    if (lane == 0) {
+      for (int j = 0; j < PER; j++)
+        for (int w = 0; w < NT / 32; w++) {
+          s_off[j][w] = acc;
+          acc += s_cnt[j][w];
+        }
+    }
+    acc = __shfl_sync(0xffffffffu, acc, 0);
+    const unsigned long long base = pmb_lookback_warp(F.lb_status, tile, (unsigned long long)acc, F.status);
+    if (lane == 0) {
+      s_base = base;
+      if (tile == (long long)gridDim.x - 1) *F.n_groups = base + acc;
+    }
   }
   __syncthreads();
   const unsigned long long base = s_base;
