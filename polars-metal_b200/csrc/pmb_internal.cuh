@@ -173,6 +173,7 @@ struct pmb_handle {
     size_t top;
   };
   std::vector<Block> ws;
+  size_t ws_cur = 0;  // block that pmb_ws_alloc bumps from (earlier blocks are full or in use)
   // pinned host staging (64 KiB) for status words, counts and the sketch histogram
   uint8_t* pinned = nullptr;
   std::string err;

@@ -625,7 +625,7 @@ struct Gen {
       << "\n#define J_OFF_TKEYS " << P.off_tkeys << "\n#define J_OFF_TVAL " << P.off_tval << "\n#define J_TKEY " << P.tkey
       << "\n#define J_TNB " << P.tnb
       << "\n#define J_OFF_SRECS " << P.off_srecs << "\n#define J_H " << P.hot_cap << "\n#define J_SW " << P.warm_cap
-      << "\n#define J_SREC " << S.bytes << "\n#define J_SREC_WORDS " << S.bytes / 4 << "\n#define J_LEN_SOFF " << S.off[0]
+      << "\n#define J_SREC " << S.bytes << "\n#define J_SREC_WORDS " << S.bytes / 4 << "\n#define J_LEN_SOFF " << (S.off.empty() ? 0 : S.off[0])
       << "\n#define J_REC " << q.rec_bytes << "\n";
     o << "__constant__ unsigned int J_SIDENT[" << S.ident.size() << "] = {";
     for (size_t i = 0; i < S.ident.size(); i++) o << (i ? ", " : "") << S.ident[i] << "u";
@@ -1065,11 +1065,26 @@ static int debug_compile(const pmb_query* q, const pmb_column* cols, int32_t n_c
       cq.dq.col[c].valid = cols[cq.map.user[c]].validity ? dummy : nullptr;
     }
     if (mode == 3) {
+      // the query of a top-level filter (pmb_filter.cu): every column an output, no keys or
+      // aggregates, the predicate only
+      CompiledQuery fq;
+      memset(&fq.dq, 0, sizeof(DQuery));
+      for (int c = 0; c < n_cols; c++) fq.map.user.push_back(c);
+      if (q->predicate) rc = pmb_compile_predicate(&h, q->predicate, &fq.map, cols, n_cols, &fq.dq.prog);
+      fq.dq.n_cols = (int)fq.map.user.size();
+      fq.dq.n_rows = n_cols ? cols[0].length : 0;
+      for (int c = 0; c < fq.dq.n_cols; c++) {
+        fq.dq.col[c].dtype = cols[fq.map.user[c]].dtype;
+        fq.dq.col[c].elem = pmb_dtype_bytes(fq.dq.col[c].dtype);
+        fq.dq.col[c].data = dummy;
+        fq.dq.col[c].valid = cols[fq.map.user[c]].validity ? dummy : nullptr;
+      }
+      cq = fq;
       JitPlan J;
-      rc = pmb_plan_jit_batch(&h, cq, 1024, 1, 232448, &J);
+      if (rc == PMB_OK) rc = pmb_plan_jit_batch(&h, cq, 1024, 1, 232448, &J);
       if (rc != PMB_OK) msg = h.err;
       std::vector<char> cubin;
-      if (rc == PMB_OK && !jit_compile(pmb_jit_compact_source(cq, J, cq.dq.n_cols), cubin, msg)) rc = PMB_E_UNSUPPORTED;
+      if (rc == PMB_OK && !jit_compile(pmb_jit_compact_source(cq, J, n_cols), cubin, msg)) rc = PMB_E_UNSUPPORTED;
       else if (rc == PMB_OK && getenv("PMB_JIT_DEBUG") && getenv("PMB_JIT_DEBUG")[0] == '2') fprintf(stderr, "%s\n", msg.c_str());
     } else if (mode == 2) {
       JitPlan J;

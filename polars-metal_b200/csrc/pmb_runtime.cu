@@ -34,6 +34,7 @@ int pmb_cuda_check(pmb_handle* h, cudaError_t e, const char* what) {
 static void ws_free_all(pmb_handle* h) {
   for (auto& b : h->ws) cudaFree(b.ptr);
   h->ws.clear();
+  h->ws_cur = 0;
 }
 
 int pmb_ws_begin(pmb_handle* h) {
@@ -51,6 +52,7 @@ int pmb_ws_begin(pmb_handle* h) {
     h->ws.push_back({p, total, 0});
   }
   for (auto& b : h->ws) b.top = 0;
+  h->ws_cur = 0;
   // the staging area grows between calls (the previous call's copies have completed by now)
   if (h->hstage_want > h->hstage_cap) {
     cudaError_t e = cudaStreamSynchronize(h->stream);
@@ -75,24 +77,32 @@ void* pmb_host_stage(pmb_handle* h, size_t bytes) {
   return p;
 }
 
-WsMark pmb_ws_mark(const pmb_handle* h) { return {h->ws.size(), h->ws.empty() ? 0 : h->ws.back().top}; }
+// the allocation position: the current block and its top (blocks after it are empty)
+WsMark pmb_ws_mark(const pmb_handle* h) {
+  if (h->ws.empty()) return {0, 0};
+  return {h->ws_cur + 1, h->ws[h->ws_cur].top};
+}
 
 void pmb_ws_release(pmb_handle* h, WsMark m) {
   if (m.blocks == 0) {
     for (auto& b : h->ws) b.top = 0;
+    h->ws_cur = 0;
     return;
   }
   h->ws[m.blocks - 1].top = m.top;
   for (size_t i = m.blocks; i < h->ws.size(); i++) h->ws[i].top = 0;
+  h->ws_cur = m.blocks - 1;  // the blocks given back are used again before new ones are added
 }
 
 void* pmb_ws_alloc(pmb_handle* h, size_t bytes) {
   bytes = pmb_align(bytes ? bytes : 1, 256);
-  if (!h->ws.empty()) {
-    auto& b = h->ws.back();
+  // bump allocation from the current block on (blocks before it are in use up to their top)
+  for (size_t i = h->ws_cur; i < h->ws.size(); i++) {
+    auto& b = h->ws[i];
     if (b.top + bytes <= b.cap) {
       void* p = b.ptr + b.top;
       b.top += bytes;
+      h->ws_cur = i;
       return p;
     }
   }
@@ -108,6 +118,7 @@ void* pmb_ws_alloc(pmb_handle* h, size_t bytes) {
     want = bytes;
   }
   h->ws.push_back({p, want, bytes});
+  h->ws_cur = h->ws.size() - 1;
   return p;
 }
 
