@@ -20,7 +20,8 @@
 // column chunks into one of the warp's J_NBUF buffers (one mbarrier each, bounded waits), so with
 // two buffers the next unit is in flight while this one is processed. Per unit:
 //   1. classify: each lane evaluates the filter and the key of rows lane, lane+32, lane+64,
-//      lane+96 and looks the key up in the CTA's read-only table of sampled keys. Rows of sampled
+//      lane+96 and looks the key up in the CTA's read-only table of sampled keys (every lane,
+//      kept row or not, so the lookup never diverges). Rows of sampled
 //      keys ("hot": the heaviest, with one record per warp; "warm": one record per CTA) and the
 //      other kept rows ("cold") are compacted with ballots into the warp's queue;
 //   2. the queued shared-tier rows are applied 32 at a time, every lane busy;
@@ -99,9 +100,8 @@ __device__ __forceinline__ long long j_gfind(const JParams& P, unsigned long lon
 // The CTA's table of sampled keys (hot and warm), built on the device by k_sample_table: a key
 // sits in its first bucket (4 slots) unless that bucket was already full, then in its second.
 // Empty slots hold the value 0xFFFF (a miss whatever their key word), so a first bucket with an
-// empty slot ends a lookup: its keys never spilled over. A lookup reads the first bucket's keys
-// and values side by side, and the second bucket only when the first is full. Returns the key's
-// value (J_HOTBIT | hot index, or warm index) or J_MISS.
+// empty slot ends a lookup: its keys never spilled over. A lookup reads a bucket's keys and values
+// side by side; the value is J_HOTBIT | hot index, a warm index, or J_MISS.
 __device__ __forceinline__ unsigned j_tvalue(unsigned short v) {
   return v == 0xFFFFu ? J_MISS : ((v & 0x8000u) ? (J_HOTBIT | (v & 0x7FFFu)) : (unsigned)v);
 }
@@ -114,34 +114,22 @@ __device__ __forceinline__ unsigned short j_tslot(uint2 v, int s) {
 __device__ __forceinline__ bool j_tnotfull(uint2 v) {
   return (v.x >> 16) == 0xFFFFu || (v.x & 0xFFFFu) == 0xFFFFu || (v.y >> 16) == 0xFFFFu || (v.y & 0xFFFFu) == 0xFFFFu;
 }
-__device__ __forceinline__ unsigned j_tfind(const unsigned char* tk, const unsigned short* tv, unsigned tnb,
-                                            unsigned long long key, unsigned long long h) {
-  if (tnb == 0u) return J_MISS;
-  const unsigned a = (unsigned)(h >> 32);
-  const unsigned b1 = __umulhi(a, tnb);
-  const uint2* vals = reinterpret_cast<const uint2*>(tv);
-  const uint2 vx = vals[b1];
+// bucket bk of the table: the key's value, or J_MISS; `full` tells whether the bucket had no
+// empty slot (then a missing key may sit in its second bucket). Straight-line code, no branch.
+__device__ __forceinline__ unsigned j_tprobe(const unsigned char* tk, const unsigned short* tv, unsigned bk,
+                                             unsigned long long key, bool& full) {
+  const uint2 vx = reinterpret_cast<const uint2*>(tv)[bk];
 #if J_TKEY == 4
   const unsigned k = (unsigned)key;
-  const uint4 x = reinterpret_cast<const uint4*>(tk)[b1];
-  int s = x.x == k ? 0 : x.y == k ? 1 : x.z == k ? 2 : x.w == k ? 3 : -1;
+  const uint4 x = reinterpret_cast<const uint4*>(tk)[bk];
+  const int s = x.x == k ? 0 : x.y == k ? 1 : x.z == k ? 2 : x.w == k ? 3 : -1;
 #else
   const ulonglong2* t = reinterpret_cast<const ulonglong2*>(tk);
-  const ulonglong2 x0 = t[2 * b1], x1 = t[2 * b1 + 1];
-  int s = x0.x == key ? 0 : x0.y == key ? 1 : x1.x == key ? 2 : x1.y == key ? 3 : -1;
+  const ulonglong2 x0 = t[2 * bk], x1 = t[2 * bk + 1];
+  const int s = x0.x == key ? 0 : x0.y == key ? 1 : x1.x == key ? 2 : x1.y == key ? 3 : -1;
 #endif
-  if (s >= 0) return j_tvalue(j_tslot(vx, s));
-  if (j_tnotfull(vx)) return J_MISS;
-  const unsigned b2 = __umulhi(pmb_mix32b(a), tnb);
-  const uint2 vy = vals[b2];
-#if J_TKEY == 4
-  const uint4 y = reinterpret_cast<const uint4*>(tk)[b2];
-  s = y.x == k ? 0 : y.y == k ? 1 : y.z == k ? 2 : y.w == k ? 3 : -1;
-#else
-  const ulonglong2 y0 = t[2 * b2], y1 = t[2 * b2 + 1];
-  s = y0.x == key ? 0 : y0.y == key ? 1 : y1.x == key ? 2 : y1.y == key ? 3 : -1;
-#endif
-  return s >= 0 ? j_tvalue(j_tslot(vy, s)) : J_MISS;
+  full = s < 0 && !j_tnotfull(vx);
+  return s >= 0 ? j_tvalue(j_tslot(vx, s)) : J_MISS;
 }
 
 __device__ __forceinline__ bool j_stop(const JParams& P) {
@@ -240,22 +228,26 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
     int ns = 0, nc = 0;
     const unsigned lt = (1u << lane) - 1u;
     unsigned ent[4];  // 0: dropped, J_MISS: cold, else shared-tier entry (record << 7 | row) + 1
+    // Every lane looks up the key of each of its rows in the first bucket, kept or not (a dropped
+    // row's answer is ignored), so the lookup runs with all lanes and no divergent exits; the
+    // second bucket, needed only behind a full first one, is taken by the whole warp together.
+    const unsigned tnb_eff = P.ttab ? tnb : 0u;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      const int lr = lane + 32 * j;
+      const int lr = lane + 32 * j;  // rows past a partial unit read stale buffer bytes, then drop
       JRow r;
-      const bool keep = lr < rows && j_load_pk(P, st, lr, r);
-      ent[j] = 0u;
-      if (keep) {
-        const unsigned long long key = j_key(r);
-        const unsigned v = j_tfind(tkeys, tval, P.ttab ? tnb : 0u, key, j_hash(key));
-        if (v != J_MISS) {
-          const unsigned rec = (v & J_HOTBIT) ? (unsigned)(warp * J_H) + (v & ~J_HOTBIT) : (unsigned)(W * J_H) + v;
-          ent[j] = ((rec << 7) | (unsigned)lr) + 1u;
-        } else {
-          ent[j] = J_MISS;
-        }
+      const bool keep = j_load_pk(P, st, lr, r) && lr < rows;
+      const unsigned long long key = j_key(r);
+      const unsigned a = (unsigned)(j_hash(key) >> 32);
+      unsigned v = J_MISS;
+      bool full = false;
+      if (tnb_eff) v = j_tprobe(tkeys, tval, __umulhi(a, tnb_eff), key, full);
+      if (__any_sync(0xffffffffu, keep && full)) {
+        bool full2;
+        if (keep && full) v = j_tprobe(tkeys, tval, __umulhi(pmb_mix32b(a), tnb_eff), key, full2);
       }
+      const unsigned rec = (v & J_HOTBIT) ? (unsigned)(warp * J_H) + (v & ~J_HOTBIT) : (unsigned)(W * J_H) + v;
+      ent[j] = !keep ? 0u : (v != J_MISS ? ((rec << 7) | (unsigned)lr) + 1u : J_MISS);
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -289,17 +281,31 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
       c_sh += c1 - c0;
       c0 = c1;
     }
-    // 3. cold tier: the probe load of every lane first, then resolve and apply
+    // 3. cold tier. Most cold keys already sit in their first bucket: that probe is straight-line
+    //    code, and the probing loop (claims, later buckets) only runs for the other lanes. The
+    //    lanes meet again before the record updates, so those run once for the whole round.
     for (int base = 0; base < nc; base += 32) {
-      if (base + lane < nc) {
+      const bool act = base + lane < nc;
+      const unsigned am = __ballot_sync(0xffffffffu, act);
+      if (act) {
         const int lr = (int)q[J_UNIT - 1 - (base + lane)];
         JRow r;
         j_load_key(P, st, lr, r);
         j_load_vals(P, st, lr, r);
         const unsigned long long key = j_key(r);
         j_fxcheck(P, r);
-        bool claimed;
-        const long long gi = j_gresolve(P, key, j_hash(key), claimed);
+        const unsigned long long hk = j_hash(key);
+        bool claimed = false;
+        long long gi = -1;
+        if (key != PMB_EMPTY64) {
+          const unsigned long long bk = pmb_slot(hk, P.gcap >> 2);
+          const ulonglong2* src = reinterpret_cast<const ulonglong2*>(P.gkeys + 4 * bk);
+          const ulonglong2 x0 = src[0], x1 = src[1];
+          const int s = x0.x == key ? 0 : x0.y == key ? 1 : x1.x == key ? 2 : x1.y == key ? 3 : -1;
+          if (s >= 0) gi = (long long)(4 * bk + s);
+        }
+        if (gi < 0) gi = j_gresolve(P, key, hk, claimed);
+        __syncwarp(am);
         if (gi >= 0) j_global(P, P.grecs + (unsigned long long)gi * J_REC, r);
         if (claimed && ((atomicAdd(&s_claims, 1u) + 1u) & 63u) == 0u) {
           // every 64 claims of this CTA: publish them; past the limit the table counts as full
