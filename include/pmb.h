@@ -325,6 +325,17 @@ int pmb_groupby_sorted(pmb_handle* h, const pmb_query* q, const pmb_column* cols
  * Device outputs live in the handle's workspace and are not freed here. */
 void pmb_result_free(pmb_result* r);
 
+/* ---- many results at once (bindings that read a batch's results) ----
+ * No counterpart in the reference, whose batch of one query per call returns one PyO3 tuple per
+ * call. pmb_results_pack copies the headers of n results into one array of 64-bit words: per
+ * result 4 words (n_groups; n_columns | strategy_used << 32; rehash_count; capacity), then 4 per
+ * column (data; validity; length; dtype | on_device << 32). A NULL result packs as 0 columns.
+ * It returns the words written, or -1 when they do not fit in cap_words. The addresses stay the
+ * results' own: pack before pmb_results_free, and read device addresses only while they are valid.
+ * pmb_results_free is pmb_result_free of each of the n results. */
+int64_t pmb_results_pack(pmb_result* const* rs, int32_t n, uint64_t* words, int64_t cap_words);
+void pmb_results_free(pmb_result* const* rs, int32_t n);
+
 /* ---- learned strategy selection ----
  * No counterpart in the reference, whose routing is a row-count threshold and an estimated-
  * cardinality gate (crates/polars-metal-core/src/router/cost.rs:35-52,

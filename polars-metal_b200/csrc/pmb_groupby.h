@@ -85,8 +85,10 @@ bool pmb_heavy_key(const CompiledQuery& cq, const SketchOut& sk);
 bool pmb_selector_vetoed(const CompiledQuery& cq, const SketchOut& sk, int strategy);
 int pmb_plan_hash(pmb_handle* h, int max_smem_optin, CompiledQuery& cq, int strategy, int64_t est, bool have_sketch,
                   HashParams& P, int& nt, int& smem);
+// est_learned: est is the larger of the sample estimate and the strategy selector's predicted
+// group count (two estimates, so the table is sized tighter: 2 slots per group instead of 4)
 int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int strategy, int64_t est,
-                     const SketchOut* sk, pmb_result* r);
+                     const SketchOut* sk, pmb_result* r, bool est_learned = false);
 // compiles the query again with cq.dd_user_cols, keeping the staged column pointers
 int recompile_dd(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32_t n_cols, CompiledQuery& cq);
 // keys = EMPTY, records = identity (k_table_init) on stream s

@@ -525,4 +525,31 @@ void pmb_result_free(pmb_result* r) {
   free(r);
 }
 
+int64_t pmb_results_pack(pmb_result* const* rs, int32_t n, uint64_t* words, int64_t cap_words) {
+  if (n < 0 || (n > 0 && (!rs || !words))) return -1;
+  int64_t w = 0;
+  for (int32_t i = 0; i < n; i++) {
+    const pmb_result* r = rs[i];
+    const int32_t nc = r ? r->n_columns : 0;
+    if (w + 4 + 4 * (int64_t)nc > cap_words) return -1;
+    words[w++] = r ? (uint64_t)r->n_groups : 0;
+    words[w++] = (uint64_t)(uint32_t)nc | ((uint64_t)(uint32_t)(r ? r->strategy_used : 0) << 32);
+    words[w++] = r ? (uint64_t)(uint32_t)r->rehash_count : 0;
+    words[w++] = r ? (uint64_t)r->capacity : 0;
+    for (int32_t c = 0; c < nc; c++) {
+      const pmb_out_column& o = r->columns[c];
+      words[w++] = (uint64_t)(uintptr_t)o.data;
+      words[w++] = (uint64_t)(uintptr_t)o.validity;
+      words[w++] = (uint64_t)o.length;
+      words[w++] = (uint64_t)(uint32_t)o.dtype | ((uint64_t)(uint32_t)o.on_device << 32);
+    }
+  }
+  return w;
+}
+
+void pmb_results_free(pmb_result* const* rs, int32_t n) {
+  if (!rs) return;
+  for (int32_t i = 0; i < n; i++) pmb_result_free(rs[i]);
+}
+
 }  // extern "C"

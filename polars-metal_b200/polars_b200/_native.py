@@ -26,7 +26,8 @@ import ctypes as C
 import threading
 import weakref
 from dataclasses import dataclass, field
-from typing import Any, Sequence
+from collections.abc import Sequence
+from typing import Any
 
 import numpy as np
 
@@ -625,12 +626,13 @@ def prepare_batched(queries, output: str = "host") -> PreparedBatch:
     return PreparedBatch(queries, output)
 
 
-def groupby_batched(queries, output: str = "host", handle: Handle | None = None) -> list:
+def groupby_batched(queries, output: str = "host", handle: Handle | None = None) -> Sequence:
     """Many independent group-by queries in one call (pmb_groupby_batched).
 
     queries: a list of (columns, keys, aggs, predicate) with the meanings of `groupby`, or a
     PreparedBatch (its own output kind then applies). Queries of one signature run in one
-    persistent launch; the results come back in query order."""
+    persistent launch; the results come back in query order: a list of GroupByResult for host
+    outputs, a BatchResults sequence of them for device outputs."""
     h = handle or default_handle()
     if isinstance(queries, PreparedBatch):
         n, output = queries.n, queries.output
@@ -642,33 +644,68 @@ def groupby_batched(queries, output: str = "host", handle: Handle | None = None)
     h.check(h._lib.pmb_groupby_batched(h.raw, qrec.ctypes.data_as(C.POINTER(A.Query)),
                                        ptrs.ctypes.data_as(C.POINTER(C.POINTER(A.Column))),
                                        ncols.ctypes.data_as(C.POINTER(C.c_int32)), n, outs))
-    addrs = list(C.cast(outs, C.POINTER(C.c_uint64 * max(1, n))).contents)[:n]
-    results = []
+    outs_p = C.cast(outs, C.c_void_p)
     try:
-        to_host = output != "device"
+        if output == "device":
+            # device outputs: every header in one array (one C call); the per-query result
+            # objects are built when they are read, so a batch of thousands of queries costs no
+            # Python object per query (nor the garbage collections that many objects set off)
+            n_out = [len(x) for x in names]
+            cap = 4 * n + 4 * sum(n_out)
+            words = np.empty(max(1, cap), dtype=np.uint64)
+            got = h._lib.pmb_results_pack(outs_p, n, words.ctypes.data, cap)
+            if got != cap:
+                raise RuntimeError("polars_b200: pmb_results_pack failed")
+            offs = np.zeros(n + 1, dtype=np.int64)
+            np.cumsum(4 + 4 * np.asarray(n_out, dtype=np.int64), out=offs[1:])
+            return BatchResults(words, offs, names)
+        addrs = list(C.cast(outs, C.POINTER(C.c_uint64 * max(1, n))).contents)[:n]
+        results = []
         head_at = (C.c_uint64 * 5).from_address  # a pmb_result read as 64-bit words (layout checked at import)
-        cols_at = {}
         for i in range(n):
             hw = head_at(addrs[i])[:]
-            nc = hw[1] & 0xFFFFFFFF
             su = hw[3] & 0xFFFFFFFF
-            if to_host:
-                data, valid, dts = _read_result(A.Result.from_address(addrs[i]), names[i], True)
-            else:
-                at = cols_at.get(nc)
-                if at is None:
-                    at = cols_at[nc] = (C.c_uint64 * (4 * nc)).from_address
-                cw = at(hw[2])[:]  # per column: data, validity, length, dtype
-                data, valid, dts = cw[0::4], cw[1::4], [x & 0xFFFFFFFF for x in cw[3::4]]
+            data, valid, dts = _read_result(A.Result.from_address(addrs[i]), names[i], True)
             results.append(GroupByResult(n_groups=hw[0], names=names[i], dtypes=dts, data=data, validity=valid,
                                          strategy=A.STRATEGY_NAMES.get(su, str(su)), rehash_count=hw[3] >> 32,
                                          capacity=hw[4]))
+        return results
     finally:
-        for i in range(n):
-            if outs[i]:
-                h._lib.pmb_result_free(outs[i])
+        h._lib.pmb_results_free(outs_p, n)
         del keep
-    return results
+
+
+class BatchResults(Sequence):
+    """The results of a batched call with device outputs, in query order: a sequence of
+    GroupByResult built on access from the packed headers (pmb_results_pack). Device addresses
+    stay valid until the next call on the same handle, as for any device output."""
+
+    def __init__(self, words: np.ndarray, offs: np.ndarray, names: list):
+        self._w = words
+        self._o = offs
+        self._names = names
+
+    def __len__(self) -> int:
+        return len(self._names)
+
+    def _one(self, i: int) -> GroupByResult:
+        o = int(self._o[i])
+        w = self._w
+        nc = int(w[o + 1]) & 0xFFFFFFFF
+        su = int(w[o + 1]) >> 32
+        cw = w[o + 4:o + 4 + 4 * nc].tolist()
+        return GroupByResult(n_groups=int(w[o]), names=self._names[i], dtypes=[x & 0xFFFFFFFF for x in cw[3::4]],
+                             data=cw[0::4], validity=cw[1::4], strategy=A.STRATEGY_NAMES.get(su, str(su)),
+                             rehash_count=int(w[o + 2]), capacity=int(w[o + 3]))
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self._one(j) for j in range(*i.indices(len(self)))]
+        if i < 0:
+            i += len(self)
+        if not 0 <= i < len(self):
+            raise IndexError("batch result index out of range")
+        return self._one(i)
 
 
 def _query_shape(names, keys, aggs, predicate):

@@ -162,3 +162,31 @@ def test_large_host_results_change_owner_small_ones_are_copied():
     assert np.all(view == 7)        # the buffer lives while any view of it does
     libc.free(oc.validity)
     assert N._host_out(A.OutColumn(), "data", 0, np.int64, 0).size == 0
+
+
+def test_results_pack_reads_headers_and_columns_in_one_array():
+    import numpy as np
+
+    from polars_b200._native import BatchResults
+
+    lib = A.lib()
+    cols = (A.OutColumn * 2)()
+    cols[0].data, cols[0].validity, cols[0].length, cols[0].dtype, cols[0].on_device = 0x1000, 0x2000, 5, 7, 1
+    cols[1].data, cols[1].validity, cols[1].length, cols[1].dtype, cols[1].on_device = 0x3000, 0x4000, 5, 11, 1
+    r = A.Result()
+    r.n_groups, r.n_columns, r.columns = 5, 2, C.cast(cols, C.POINTER(A.OutColumn))
+    r.strategy_used, r.rehash_count, r.capacity = 2, 1, 1024
+    rs = (C.POINTER(A.Result) * 2)(C.pointer(r), None)  # a NULL result packs as no columns
+    words = np.zeros(16, dtype=np.uint64)
+    assert lib.pmb_results_pack(C.cast(rs, C.c_void_p), 2, words.ctypes.data, 16) == 16
+    assert lib.pmb_results_pack(C.cast(rs, C.c_void_p), 2, words.ctypes.data, 15) == -1
+    assert words[:4].tolist() == [5, 2 | (2 << 32), 1, 1024]
+    assert words[4:12].tolist() == [0x1000, 0x2000, 5, 7 | (1 << 32), 0x3000, 0x4000, 5, 11 | (1 << 32)]
+    assert words[12:].tolist() == [0, 0, 0, 0]
+    res = BatchResults(words, np.array([0, 12, 16]), [["k", "s"], []])
+    assert len(res) == 2
+    g = res[0]
+    assert (g.n_groups, g.dtypes, g.data, g.validity, g.rehash_count, g.capacity) == (
+        5, [7, 11], [0x1000, 0x3000], [0x2000, 0x4000], 1, 1024)
+    assert res[-1].n_groups == 0 and res[1].data == []
+    assert [x.n_groups for x in res] == [5, 0]
