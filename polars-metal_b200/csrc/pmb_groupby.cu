@@ -132,7 +132,10 @@ __global__ void k_sketch_select(const unsigned long long* __restrict__ set_keys,
 // first bucket (the kernel's j_hash) and, only when that bucket is full, of its second: so a first
 // bucket with an empty slot holds every key whose first choice it is, and the lookup stops there.
 // Hot keys go in first; a key that finds both buckets full is left out and its rows take the
-// global table, which gives the same results. Empty slots hold the value 0xFFFF. One CTA.
+// global table, which gives the same results. Empty slots hold the value 0xFFFF. A bucket that
+// turned a key away (more than 4 keys tried it) gets bit 14 set in its first slot's value (a full
+// bucket's first slot is never empty, and indices stay below 2^14), so a lookup of an absent key
+// reads the second bucket only behind such a bucket, not behind every full one. One CTA.
 __device__ __forceinline__ void sample_table_insert(unsigned long long k, unsigned short v, unsigned tnb, bool narrow,
                                                     unsigned char* tab, unsigned int* fill) {
   if (k == PMB_EMPTY64 || (narrow && k > 0xFFFFFFFFull)) return;  // never looked up in the table
@@ -178,6 +181,10 @@ __global__ void __launch_bounds__(1024) k_sample_table(const unsigned long long*
   const unsigned nw = warm ? min(*warm_n, warm_cap) : 0u;
   for (unsigned i = threadIdx.x; i < nw; i += blockDim.x)
     sample_table_insert(warm[i], (unsigned short)i, tnb, narrow != 0, tab, fill);
+  __syncthreads();
+  unsigned short* vals = reinterpret_cast<unsigned short*>(tab + kb);
+  for (unsigned i = threadIdx.x; i < tnb; i += blockDim.x)
+    if (fill[i] > 4u) vals[4u * i] |= 0x4000u;
 }
 
 // ============================================================================ table init

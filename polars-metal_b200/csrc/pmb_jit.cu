@@ -860,6 +860,7 @@ int pmb_plan_jit(pmb_handle* h, const CompiledQuery& cq, bool have_sketch, int m
   while (hot > 0 && (int)pmb_align((size_t)used, 16) + tbytes(hot) + 32 + W * hot * J->srec > budget) hot /= 2;
   int warm = 0;
   if (have_sketch) {
+    // at most 2^14 warm keys: the sampled-key table's 16-bit values keep bits 14-15 for flags
     for (int sw = 16384; sw >= 32; sw -= 32) {
       int need = (int)pmb_align((size_t)used, 16) + tbytes(hot + sw) + 32 + (W * hot + sw) * J->srec;
       if (need <= budget) {

@@ -101,21 +101,18 @@ __device__ __forceinline__ long long j_gfind(const JParams& P, unsigned long lon
 // sits in its first bucket (4 slots) unless that bucket was already full, then in its second.
 // Empty slots hold the value 0xFFFF (a miss whatever their key word), so a first bucket with an
 // empty slot ends a lookup: its keys never spilled over. A lookup reads a bucket's keys and values
-// side by side; the value is J_HOTBIT | hot index, a warm index, or J_MISS.
+// side by side; the value is J_HOTBIT | hot index, a warm index, or J_MISS. Bit 14 of a bucket's
+// first value marks a bucket that turned a key away to its second bucket.
 __device__ __forceinline__ unsigned j_tvalue(unsigned short v) {
-  return v == 0xFFFFu ? J_MISS : ((v & 0x8000u) ? (J_HOTBIT | (v & 0x7FFFu)) : (unsigned)v);
+  return v == 0xFFFFu ? J_MISS : ((v & 0x8000u) ? (J_HOTBIT | (v & 0x3FFFu)) : (unsigned)(v & 0x3FFFu));
 }
 // the 16-bit value of slot s of a bucket whose values are (lo, hi)
 __device__ __forceinline__ unsigned short j_tslot(uint2 v, int s) {
   const unsigned w = (s & 2) ? v.y : v.x;
   return (unsigned short)((s & 1) ? (w >> 16) : (w & 0xFFFFu));
 }
-// true when a bucket's values hold an empty slot (0xFFFF)
-__device__ __forceinline__ bool j_tnotfull(uint2 v) {
-  return (v.x >> 16) == 0xFFFFu || (v.x & 0xFFFFu) == 0xFFFFu || (v.y >> 16) == 0xFFFFu || (v.y & 0xFFFFu) == 0xFFFFu;
-}
-// bucket bk of the table: the key's value, or J_MISS; `full` tells whether the bucket had no
-// empty slot (then a missing key may sit in its second bucket). Straight-line code, no branch.
+// bucket bk of the table: the key's value, or J_MISS; `full` tells whether the bucket turned a
+// key away (then a missing key may sit in its second bucket). Straight-line code, no branch.
 __device__ __forceinline__ unsigned j_tprobe(const unsigned char* tk, const unsigned short* tv, unsigned bk,
                                              unsigned long long key, bool& full) {
   const uint2 vx = reinterpret_cast<const uint2*>(tv)[bk];
@@ -128,7 +125,8 @@ __device__ __forceinline__ unsigned j_tprobe(const unsigned char* tk, const unsi
   const ulonglong2 x0 = t[2 * bk], x1 = t[2 * bk + 1];
   const int s = x0.x == key ? 0 : x0.y == key ? 1 : x1.x == key ? 2 : x1.y == key ? 3 : -1;
 #endif
-  full = s < 0 && !j_tnotfull(vx);
+  const unsigned v0 = vx.x & 0xFFFFu;
+  full = s < 0 && v0 != 0xFFFFu && (v0 & 0x4000u) != 0u;
   return s >= 0 ? j_tvalue(j_tslot(vx, s)) : J_MISS;
 }
 
