@@ -274,16 +274,18 @@ int run_compact(pmb_handle* h, CompiledQuery& cq, const uint8_t* keep_d, const u
   P.keep_data = keep_d;
   P.keep_valid = keep_v;
   P.n_out_cols = n_out;
-  P.lb = (unsigned long long*)pmb_ws_alloc(h, (size_t)tiles * 8 + 64);
+  // look-back states for whichever kernel runs (the run-time compiled one has smaller tiles)
+  const int64_t lb_tiles = std::max<int64_t>(tiles, (n + JC_TILE_ROWS - 1) / JC_TILE_ROWS);
+  P.lb = (unsigned long long*)pmb_ws_alloc(h, (size_t)lb_tiles * 8 + 64);
   unsigned int* status = (unsigned int*)pmb_ws_alloc(h, 64);
   if (!P.lb || !status) {
     pmb_result_free(r);
     return pmb_fail(h, PMB_E_OOM, "workspace exhausted (compaction)");
   }
-  P.ticket = P.lb + tiles;
-  P.n_out = P.lb + tiles + 1;
+  P.ticket = P.lb + lb_tiles;
+  P.n_out = P.lb + lb_tiles + 1;
   P.status = status;
-  cudaMemsetAsync(P.lb, 0, (size_t)tiles * 8 + 64, h->stream);
+  cudaMemsetAsync(P.lb, 0, (size_t)lb_tiles * 8 + 64, h->stream);
   cudaMemsetAsync(status, 0, 64, h->stream);
   for (int c = 0; c < n_out; c++) {
     int e = q.col[c].elem;
@@ -307,7 +309,7 @@ int run_compact(pmb_handle* h, CompiledQuery& cq, const uint8_t* keep_d, const u
   }
   if (n > 0 && jk) {
     const int64_t jt = (n + JC_TILE_ROWS - 1) / JC_TILE_ROWS;
-    if (jt > tiles) {
+    if (jt > lb_tiles) {
       pmb_result_free(r);
       return pmb_fail(h, PMB_E_CUDA, "internal: compaction tiles");
     }

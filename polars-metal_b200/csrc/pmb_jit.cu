@@ -533,17 +533,29 @@ struct Gen {
     }
   }
 
-  // the top-level filter's row functions: the verdict of row `row` read straight from the
-  // predicate's columns, and the scatter of the first `n_out` columns to output position p
-  // (every lane of the warp calls j_scatter: the validity words are OR-ed warp-wide)
+  // the top-level filter's row functions. A row's values (the predicate's columns and the first
+  // `n_out` columns, the outputs) are read once into a JCRow (j_cload), its verdict is taken from
+  // those registers (j_ckeep), and the kept row is written from them (j_cscatter; every lane of
+  // the warp calls it: the validity words are OR-ed warp-wide). Reading the columns once matters:
+  // a second read at the scatter, after the tile's look-back, mostly missed L2 (1.48x the
+  // algorithmic DRAM reads on the hash workload's filter).
   std::string compact_funcs(int n_out) {
     std::ostringstream b;
     mark();
     std::ostringstream body;
     std::string keep = predicate(body);
-    b << "__device__ __forceinline__ bool j_keep_row(const JCParams& P, long long row) {\n  JRow r;\n";
+    std::vector<bool> use(q.n_cols, false);
+    for (int c = 0; c < q.n_cols; c++) use[c] = pred_col[c] || c < n_out;
+    b << "struct JCRow {\n";
     for (int c = 0; c < q.n_cols; c++) {
-      if (!pred_col[c]) continue;
+      if (!use[c]) continue;
+      b << "  " << (q.col[c].dtype == PMB_BOOL ? "bool" : ctype(q.col[c].dtype)) << " v" << c << ";\n";
+      if (q.col[c].valid) b << "  bool ok" << c << ";\n";
+    }
+    b << "};\n";
+    b << "__device__ __forceinline__ void j_cload(const JCParams& P, long long row, JCRow& r) {\n";
+    for (int c = 0; c < q.n_cols; c++) {
+      if (!use[c]) continue;
       const DCol& C = q.col[c];
       const std::string cs = std::to_string(c);
       if (C.dtype == PMB_BOOL)
@@ -552,23 +564,22 @@ struct Gen {
         b << "  r.v" << cs << " = reinterpret_cast<const " << ctype(C.dtype) << "*>(P.col_data[" << cs << "])[row];\n";
       if (C.valid) b << "  r.ok" << cs << " = ((P.col_valid[" << cs << "][row >> 3] >> (row & 7)) & 1) != 0;\n";
     }
-    b << body.str() << "  return " << keep << ";\n}\n";
-    b << "__device__ __forceinline__ void j_scatter(const JCParams& P, long long row, bool keep, long long p, "
+    b << "}\n";
+    b << "__device__ __forceinline__ bool j_ckeep(const JCRow& r) {\n" << body.str() << "  return " << keep << ";\n}\n";
+    b << "__device__ __forceinline__ void j_cscatter(const JCParams& P, const JCRow& r, bool keep, long long p, "
          "long long p_first) {\n";
     for (int c = 0; c < n_out && c < q.n_cols; c++) {
       const DCol& C = q.col[c];
       const std::string cs = std::to_string(c);
       if (C.dtype == PMB_BOOL) {
-        b << "  { const bool bv = keep && ((P.col_data[" << cs << "][row >> 3] >> (row & 7)) & 1) != 0;\n"
-          << "    jc_set_bits(reinterpret_cast<unsigned int*>(P.out_data[" << cs << "]), p, p_first, bv); }\n";
+        b << "  jc_set_bits(reinterpret_cast<unsigned int*>(P.out_data[" << cs << "]), p, p_first, keep && r.v" << cs
+          << ");\n";
       } else {
         const std::string T = ctype(C.dtype);
-        b << "  if (keep) reinterpret_cast<" << T << "*>(P.out_data[" << cs << "])[p] = reinterpret_cast<const " << T
-          << "*>(P.col_data[" << cs << "])[row];\n";
+        b << "  if (keep) reinterpret_cast<" << T << "*>(P.out_data[" << cs << "])[p] = r.v" << cs << ";\n";
       }
       if (C.valid)
-        b << "  jc_set_bits(P.out_valid[" << cs << "], p, p_first, keep && ((P.col_valid[" << cs
-          << "][row >> 3] >> (row & 7)) & 1) != 0);\n";
+        b << "  jc_set_bits(P.out_valid[" << cs << "], p, p_first, keep && r.ok" << cs << ");\n";
       else
         b << "  jc_set_bits(P.out_valid[" << cs << "], p, p_first, keep);\n";
     }

@@ -113,7 +113,7 @@ struct JitCompactParams {
   unsigned char* out_data[16];
   unsigned int* out_valid[16];
 };
-constexpr int JC_TILE_ROWS = 256 * 16;  // rows per tile of pmb_jit_compact (JC_TILE)
+constexpr int JC_TILE_ROWS = 256 * 4;  // rows per tile of pmb_jit_compact (JC_TILE)
 
 // the top-level filter's compaction of the first n_out columns by the query's predicate
 // (pmb_jit_compact.cuh); the source alone for the compile checks

@@ -1,8 +1,8 @@
 // pmb_jit_compact.cuh — the top-level filter's compaction compiled at run time for one query
-// signature (NVRTC): every row's predicate in registers with literal column offsets and dtypes
-// (j_keep_row, generated), then the kept rows of every output column scattered in row order
-// (j_scatter, generated). This text follows pmb_device.cuh, the parameter block of
-// pmb_jit_skeleton.cuh and the generated row functions.
+// signature (NVRTC): every row's values read once into registers with literal column offsets and
+// dtypes (j_cload, generated), its predicate taken from them (j_ckeep), then the kept rows of every
+// output column scattered in row order from the same registers (j_cscatter). This text follows
+// pmb_device.cuh, the parameter block of pmb_jit_skeleton.cuh and the generated row functions.
 //
 // Structure (as the prebuilt k_compact, pmb_filter.cu): a CTA takes tiles of JC_TILE rows in
 // ticket order; every warp ballots its rows' verdicts, the CTA's warp counts give each warp its
@@ -11,7 +11,7 @@
 // 32-bit words; a warp's 32 consecutive outputs span at most two words.
 
 #define JC_NT 256
-#define JC_PER 16
+#define JC_PER 4  // a thread's rows stay in registers from the verdict to the scatter
 #define JC_TILE (JC_NT * JC_PER)
 
 struct JCParams {
@@ -85,10 +85,16 @@ extern "C" __global__ void __launch_bounds__(JC_NT) pmb_jit_compact(const __grid
   const long long tile = s_tile;
   const long long row0 = tile * JC_TILE;
   unsigned keepm = 0;  // bit j: row row0 + j * JC_NT + tid is kept
+  JCRow x[JC_PER];
 #pragma unroll
   for (int j = 0; j < JC_PER; j++) {
     const long long r = row0 + (long long)j * JC_NT + tid;
-    const bool k = r < P.n_rows && j_keep_row(P, r);
+    if (r < P.n_rows) j_cload(P, r, x[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < JC_PER; j++) {
+    const long long r = row0 + (long long)j * JC_NT + tid;
+    const bool k = r < P.n_rows && j_ckeep(x[j]);
     if (k) keepm |= 1u << j;
     const unsigned b = __ballot_sync(0xffffffffu, k);
     if (lane == 0) s_cnt[j][warp] = __popc(b);
@@ -113,14 +119,13 @@ extern "C" __global__ void __launch_bounds__(JC_NT) pmb_jit_compact(const __grid
   __syncthreads();
   const unsigned long long base = s_base;
   const unsigned lt = (1u << lane) - 1u;
-#pragma unroll 1
+#pragma unroll
   for (int j = 0; j < JC_PER; j++) {
     const bool k = (keepm >> j) & 1u;
     const unsigned b = __ballot_sync(0xffffffffu, k);
     if (b == 0) continue;
-    const long long r = row0 + (long long)j * JC_NT + tid;
     const long long p_first = (long long)(base + (unsigned long long)s_off[j][warp]);
     const long long p = p_first + __popc(b & lt);
-    j_scatter(P, r, k, p, p_first);
+    j_cscatter(P, x[j], k, p, p_first);
   }
 }
