@@ -336,6 +336,13 @@ void pmb_result_free(pmb_result* r);
 int64_t pmb_results_pack(pmb_result* const* rs, int32_t n, uint64_t* words, int64_t cap_words);
 void pmb_results_free(pmb_result* const* rs, int32_t n);
 
+/* Releases one host buffer of a result column that the caller took over: it copied the column's
+ * data or validity pointer and set it to NULL in the result, so pmb_result_free leaves it. Host
+ * buffers of 1 MB and more are page-locked blocks of a pool that the library recycles (the copy
+ * back from the device then needs no staging and no page faults); they must come back through
+ * here, not through free(). No counterpart in the reference, whose results are PyO3 objects. */
+void pmb_host_buffer_free(void* p);
+
 /* ---- learned strategy selection ----
  * No counterpart in the reference, whose routing is a row-count threshold and an estimated-
  * cardinality gate (crates/polars-metal-core/src/router/cost.rs:35-52,

@@ -11,6 +11,9 @@
 #include <sys/mman.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <unordered_map>
 #include <cstdlib>
 #include <cstring>
 #include <chrono>
@@ -367,20 +370,68 @@ pmb_result* pmb_result_new(int32_t n_columns) {
   return r;
 }
 
-// host memory for a result buffer, released with free(). Large buffers are 2 MB aligned and asked
-// for transparent huge pages, so that the copy into them takes one page fault per 2 MB instead of
-// one per 4 KB (fresh pages every call: the caller frees each result)
+// Host memory for result buffers. Buffers of 1 MB and more come from a process-wide pool of pinned
+// (page-locked) blocks that are recycled when results are freed: the copy back from the device then
+// runs at the host link's speed into pages that are already resident, instead of through the
+// driver's staging into fresh pageable pages that fault on first touch (the hash workload's 46 MB
+// result took ~9 ms that way). Freed blocks are kept for reuse up to PMB_PINNED_CACHE_MB (default
+// 2048) megabytes; a request takes the smallest cached block that holds it if that block is at
+// most twice its size. Smaller buffers, and any buffer when pinned memory cannot be had, come
+// from malloc. host_release() frees either kind.
+namespace {
+std::mutex g_pool_mu;
+std::unordered_map<void*, size_t> g_pool_size;  // every pinned block handed out or cached
+std::multimap<size_t, void*> g_pool_free;       // cached blocks by size
+size_t g_pool_cached = 0;
+constexpr size_t POOL_MIN = (size_t)1 << 20;
+
+size_t pool_cache_cap() {
+  static size_t cap = [] {
+    const char* e = getenv("PMB_PINNED_CACHE_MB");
+    return (size_t)(e ? std::max(0, atoi(e)) : 2048) << 20;
+  }();
+  return cap;
+}
+}  // namespace
+
 static void* host_alloc(size_t bytes) {
-  constexpr size_t HUGE_PAGE = (size_t)2 << 20;
-  if (bytes >= 2 * HUGE_PAGE) {
-    const size_t rounded = (bytes + HUGE_PAGE - 1) & ~(HUGE_PAGE - 1);
-    void* p = nullptr;
-    if (posix_memalign(&p, HUGE_PAGE, rounded) == 0) {
-      madvise(p, rounded, MADV_HUGEPAGE);  // a hint: without huge pages the buffer works the same
+  if (bytes >= POOL_MIN) {
+    const size_t rounded = (bytes + POOL_MIN - 1) & ~(POOL_MIN - 1);
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    auto it = g_pool_free.lower_bound(rounded);
+    if (it != g_pool_free.end() && it->first <= 2 * rounded) {
+      void* p = it->second;
+      g_pool_cached -= it->first;
+      g_pool_free.erase(it);
       return p;
     }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, rounded, cudaHostAllocPortable) == cudaSuccess) {
+      g_pool_size[p] = rounded;
+      return p;
+    }
+    cudaGetLastError();  // no pinned memory: a pageable buffer works the same, only slower
   }
   return malloc(bytes ? bytes : 1);
+}
+
+void host_release(void* p) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    auto it = g_pool_size.find(p);
+    if (it != g_pool_size.end()) {
+      if (g_pool_cached + it->second <= pool_cache_cap()) {
+        g_pool_free.emplace(it->second, p);
+        g_pool_cached += it->second;
+        return;
+      }
+      g_pool_size.erase(it);
+      cudaFreeHost(p);
+      return;
+    }
+  }
+  free(p);
 }
 
 static size_t bitmap_bytes(int64_t n) {
@@ -403,8 +454,8 @@ int pmb_finish_outputs(pmb_handle* h, pmb_result* r, bool to_host) {
     void* hd = host_alloc(db);
     uint8_t* hv = (uint8_t*)host_alloc(vb);
     if (!hd || !hv) {
-      free(hd);
-      free(hv);
+      host_release(hd);
+      host_release(hv);
       return pmb_fail(h, PMB_E_OOM, "host output allocation failed");
     }
     // the copies below fill every byte but the padding of the bitmaps, which is zeroed here
@@ -517,8 +568,8 @@ void pmb_result_free(pmb_result* r) {
   if (!r) return;
   for (int c = 0; c < r->n_columns; c++) {
     if (!r->columns[c].on_device) {
-      free(r->columns[c].data);
-      free(r->columns[c].validity);
+      host_release(r->columns[c].data);
+      host_release(r->columns[c].validity);
     }
   }
   free(r->columns);
@@ -546,6 +597,8 @@ int64_t pmb_results_pack(pmb_result* const* rs, int32_t n, uint64_t* words, int6
   }
   return w;
 }
+
+void pmb_host_buffer_free(void* p) { host_release(p); }
 
 void pmb_results_free(pmb_result* const* rs, int32_t n) {
   if (!rs) return;

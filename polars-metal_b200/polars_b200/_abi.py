@@ -229,6 +229,7 @@ SIGNATURES = {
     "pmb_result_free": (None, [C.POINTER(Result)]),
     "pmb_results_pack": (C.c_int64, [_P, C.c_int32, _P, C.c_int64]),
     "pmb_results_free": (None, [_P, C.c_int32]),
+    "pmb_host_buffer_free": (None, [_P]),
     "pmb_column_from_arrow": (C.c_int, [C.POINTER(ArrowArray), C.POINTER(ArrowSchema), C.POINTER(Column)]),
     "pmb_column_from_arrow_device": (C.c_int, [C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema),
                                                C.POINTER(Column)]),

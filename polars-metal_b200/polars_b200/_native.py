@@ -300,21 +300,15 @@ def _host_copy(addr: int, nbytes: int, dtype) -> np.ndarray:
     return np.frombuffer((C.c_char * nbytes).from_address(addr), dtype=dtype).copy()
 
 
-_free = None
 _TAKE_MIN = 1 << 20  # host result buffers of at least this size are taken over instead of copied
 
 
 def _host_take(addr: int, nbytes: int, dtype) -> np.ndarray:
-    """A numpy array over host memory that libpmb malloc'd for a result, without a copy: the array
-    owns the buffer, which is freed (libc free) when the last view of it is collected."""
-    global _free
-    if _free is None:
-        libc = C.CDLL(None)
-        libc.free.argtypes = [C.c_void_p]
-        libc.free.restype = None
-        _free = libc.free
+    """A numpy array over a host buffer of a result, without a copy: the array owns the buffer,
+    which goes back to libpmb (pmb_host_buffer_free: its pinned pool, or free) when the last view
+    of it is collected."""
     buf = (C.c_char * nbytes).from_address(addr)
-    weakref.finalize(buf, _free, addr)
+    weakref.finalize(buf, A.lib().pmb_host_buffer_free, addr)
     return np.frombuffer(buf, dtype=dtype)
 
 
