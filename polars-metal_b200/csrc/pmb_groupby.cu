@@ -188,19 +188,39 @@ __global__ void __launch_bounds__(1024) k_sample_table(const unsigned long long*
 }
 
 // ============================================================================ table init
+// Regions of 32-bit words to clear in the same launch as the table (a call's status words,
+// look-back states and output bitmaps), instead of one cudaMemsetAsync each.
+struct ZeroList {
+  int n;
+  unsigned int* p[24];
+  int64_t words[24];
+};
+// adds `bytes` (a multiple of 4) at p; false when the list is full (the caller clears it itself)
+static bool zl_add(ZeroList& z, void* p, size_t bytes) {
+  if (z.n == 24 || (bytes & 3u) || ((uintptr_t)p & 3u)) return false;
+  z.p[z.n] = (unsigned int*)p;
+  z.words[z.n++] = (int64_t)(bytes / 4);
+  return true;
+}
+
 __global__ void k_table_init(unsigned long long* __restrict__ keys, int64_t key_words, uint64_t* __restrict__ recs,
-                             int64_t n_recs, int rec_words, const __grid_constant__ RecInit ri) {
+                             int64_t n_recs, int rec_words, const __grid_constant__ RecInit ri,
+                             const __grid_constant__ ZeroList z) {
   int64_t stride = (int64_t)gridDim.x * blockDim.x;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   for (int64_t k = i; k < key_words; k += stride) keys[k] = PMB_EMPTY64;
   int64_t total = n_recs * rec_words;
   for (int64_t w = i; w < total; w += stride) recs[w] = ri.w[w % rec_words];
+  for (int j = 0; j < z.n; j++)
+    for (int64_t w = i; w < z.words[j]; w += stride) z.p[j][w] = 0u;
 }
 
 // launcher of k_table_init for other translation units (batched tables)
 void k_table_init_pub(unsigned long long* keys, int64_t key_words, uint64_t* recs, int64_t n_recs, int rec_words,
                       const RecInit& ri, int blocks, cudaStream_t s) {
-  k_table_init<<<blocks, 256, 0, s>>>(keys, key_words, recs, n_recs, rec_words, ri);
+  ZeroList z;
+  z.n = 0;
+  k_table_init<<<blocks, 256, 0, s>>>(keys, key_words, recs, n_recs, rec_words, ri, z);
 }
 
 // ============================================================================ global table
@@ -975,24 +995,27 @@ int pmb_groupby_hash(pmb_handle* h, CompiledQuery& cq, const pmb_query* uq, int 
     FinParams F;
     memset(&F, 0, sizeof(F));
     F.q = q;
+    ZeroList zl;  // cleared by the table init's launch
+    zl.n = 0;
     for (int c = 0; c < n_out; c++) {
       int dt = r->columns[c].dtype;
       size_t db = dt == PMB_BOOL ? (size_t)((nslots + 31) / 32 * 4) : (size_t)nslots * pmb_dtype_bytes(dt);
       F.out_data[c] = (uint8_t*)pmb_ws_alloc(h, db + 16);
       F.out_valid[c] = (uint8_t*)pmb_ws_alloc(h, (size_t)((nslots + 31) / 32 * 4) + 16);
       if (!F.out_data[c] || !F.out_valid[c]) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (outputs)");
-      PMB_CUDA(h, cudaMemsetAsync(F.out_valid[c], 0, (size_t)((nslots + 31) / 32 * 4), h->stream));
-      if (dt == PMB_BOOL) PMB_CUDA(h, cudaMemsetAsync(F.out_data[c], 0, db, h->stream));
+      if (!zl_add(zl, F.out_valid[c], (size_t)((nslots + 31) / 32 * 4)))
+        PMB_CUDA(h, cudaMemsetAsync(F.out_valid[c], 0, (size_t)((nslots + 31) / 32 * 4), h->stream));
+      if (dt == PMB_BOOL && !zl_add(zl, F.out_data[c], db)) PMB_CUDA(h, cudaMemsetAsync(F.out_data[c], 0, db, h->stream));
     }
-    PMB_CUDA(h, cudaMemsetAsync(status, 0, 64, h->stream));
-    PMB_CUDA(h, cudaMemsetAsync(lb, 0, (size_t)fin_tiles * 8 + 64, h->stream));
+    if (!zl_add(zl, status, 64)) PMB_CUDA(h, cudaMemsetAsync(status, 0, 64, h->stream));
+    if (!zl_add(zl, lb, (size_t)fin_tiles * 8 + 64)) PMB_CUDA(h, cudaMemsetAsync(lb, 0, (size_t)fin_tiles * 8 + 64, h->stream));
     // table init
     {
       int64_t work = std::max<int64_t>((int64_t)(cap + 1) * key_words, (int64_t)(cap + 1) * cq.rec_words);
       int blocks = (int)std::min<int64_t>((work + 255) / 256, (int64_t)h->sm_count * 16);
       pmb_kernel_begin(h, "table_init");
       k_table_init<<<blocks, 256, 0, h->stream>>>(gkeys, (int64_t)(cap + 1) * key_words, (uint64_t*)grecs,
-                                                  (int64_t)(cap + 1), cq.rec_words, P.rec_init);
+                                                  (int64_t)(cap + 1), cq.rec_words, P.rec_init, zl);
       pmb_kernel_end(h);
       PMB_CUDA(h, cudaGetLastError());
     }

@@ -374,21 +374,23 @@ pmb_result* pmb_result_new(int32_t n_columns) {
 // (page-locked) blocks that are recycled when results are freed: the copy back from the device then
 // runs at the host link's speed into pages that are already resident, instead of through the
 // driver's staging into fresh pageable pages that fault on first touch (the hash workload's 46 MB
-// result took ~9 ms that way). Freed blocks are kept for reuse up to PMB_PINNED_CACHE_MB (default
-// 2048) megabytes; a request takes the smallest cached block that holds it if that block is at
-// most twice its size. Smaller buffers, and any buffer when pinned memory cannot be had, come
-// from malloc. host_release() frees either kind.
+// result took ~9 ms that way). The pool holds at most PMB_PINNED_POOL_MB (default 1024) megabytes,
+// handed out or cached: pinning pages is slow (a batch of 4,096 host results pinned afresh on every
+// call ran 1.6x slower than with pageable buffers), so beyond that budget buffers come from malloc,
+// and blocks are never unpinned, only reused. A request takes the smallest cached block that holds
+// it if that block is at most twice its size. Smaller buffers, and any buffer when pinned memory
+// cannot be had, come from malloc. host_release() frees either kind.
 namespace {
 std::mutex g_pool_mu;
 std::unordered_map<void*, size_t> g_pool_size;  // every pinned block handed out or cached
 std::multimap<size_t, void*> g_pool_free;       // cached blocks by size
-size_t g_pool_cached = 0;
+size_t g_pool_total = 0;                        // bytes of all pinned blocks (handed out or cached)
 constexpr size_t POOL_MIN = (size_t)1 << 20;
 
-size_t pool_cache_cap() {
+size_t pool_budget() {
   static size_t cap = [] {
-    const char* e = getenv("PMB_PINNED_CACHE_MB");
-    return (size_t)(e ? std::max(0, atoi(e)) : 2048) << 20;
+    const char* e = getenv("PMB_PINNED_POOL_MB");
+    return (size_t)(e ? std::max(0, atoi(e)) : 1024) << 20;
   }();
   return cap;
 }
@@ -401,16 +403,18 @@ static void* host_alloc(size_t bytes) {
     auto it = g_pool_free.lower_bound(rounded);
     if (it != g_pool_free.end() && it->first <= 2 * rounded) {
       void* p = it->second;
-      g_pool_cached -= it->first;
       g_pool_free.erase(it);
       return p;
     }
     void* p = nullptr;
-    if (cudaHostAlloc(&p, rounded, cudaHostAllocPortable) == cudaSuccess) {
-      g_pool_size[p] = rounded;
-      return p;
+    if (g_pool_total + rounded <= pool_budget()) {
+      if (cudaHostAlloc(&p, rounded, cudaHostAllocPortable) == cudaSuccess) {
+        g_pool_size[p] = rounded;
+        g_pool_total += rounded;
+        return p;
+      }
+      cudaGetLastError();  // no pinned memory: a pageable buffer works the same, only slower
     }
-    cudaGetLastError();  // no pinned memory: a pageable buffer works the same, only slower
   }
   return malloc(bytes ? bytes : 1);
 }
@@ -421,13 +425,7 @@ void host_release(void* p) {
     std::lock_guard<std::mutex> lock(g_pool_mu);
     auto it = g_pool_size.find(p);
     if (it != g_pool_size.end()) {
-      if (g_pool_cached + it->second <= pool_cache_cap()) {
-        g_pool_free.emplace(it->second, p);
-        g_pool_cached += it->second;
-        return;
-      }
-      g_pool_size.erase(it);
-      cudaFreeHost(p);
+      g_pool_free.emplace(it->second, p);
       return;
     }
   }
