@@ -278,19 +278,20 @@ def shape_table(case: dict):
 
 def arrow_to_oracle_columns(table, dict_columns=()):
     """Oracle inputs of an Arrow table: numeric columns as (values, validity bitmap | None), Bool
-    columns bit-packed, and the named string columns as their sorted-dictionary codes through the
-    product's host encoder (polars_b200.arrow._dictionary_key). Returns (columns, dictionaries)."""
+    columns bit-packed, and the named string columns as dictionary codes from pyarrow's own
+    `dictionary_encode` (first-appearance order), independent of the product's encoder: the oracle
+    groups by the codes and the caller decodes them through the dictionary. Returns (columns,
+    dictionaries)."""
     import pyarrow as pa
-
-    from polars_b200.arrow import _dictionary_key
 
     cols, dicts = {}, {}
     for name in table.column_names:
         col = table.column(name)
         if name in dict_columns:
-            codes, values = _dictionary_key(col)
-            dicts[name] = values
-            arr = codes
+            flat = col.combine_chunks() if col.num_chunks else pa.array([], type=col.type)
+            enc = flat.dictionary_encode()
+            dicts[name] = enc.dictionary
+            arr = enc.indices
         else:
             arr = col.combine_chunks() if col.num_chunks else pa.array([], type=col.type)
         n = len(arr)
