@@ -691,6 +691,8 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
     k_batch_sketch<<<nb, BS_NT, sk_smem, h->stream>>>(d_all, d_sk, fxc);
     pmb_kernel_end(h);
     PMB_CUDA(h, cudaGetLastError());
+    // the selector's kernels go in before the sketch's readback, whose synchronisation serves both
+    const float* sel_out = pmb_selector_batch_launch(h, d_all, nb);
     std::vector<BatchSketch> skb(nb);
     PMB_CUDA(h, cudaMemcpyAsync(skb.data(), d_sk, sizeof(BatchSketch) * nb, cudaMemcpyDeviceToHost, h->stream));
     PMB_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -698,7 +700,8 @@ extern "C" int pmb_groupby_batched(pmb_handle* h, const pmb_query* qs, const pmb
     // 2. estimates (the selector's prediction can only enlarge them) and float-sum ranges
     std::vector<int64_t> nrows(nb), pred(nb, 0);
     for (int j = 0; j < nb; j++) nrows[j] = cqs[batch[j]].dq.n_rows;
-    pmb_selector_predict_batch(h, d_all, nb, pred.data(), nrows.data());
+    if (sel_out) pmb_selector_batch_groups(sel_out, nb, pred.data(), nrows.data());
+    else pmb_selector_predict_batch(h, d_all, nb, pred.data(), nrows.data());
     std::vector<int64_t> est(n_queries, 0);
     std::vector<BatchSketch> sk(n_queries);
     int64_t total_rows = 0;

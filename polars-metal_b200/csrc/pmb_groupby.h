@@ -117,6 +117,8 @@ bool pmb_selector_read(pmb_handle* h, const CompiledQuery& cq, int* strategy, in
 // group counts the selector predicts for a batch of queries (device DQuery array); false without
 // an installed selector
 bool pmb_selector_predict_batch(pmb_handle* h, const DQuery* d_qs, int nq, int64_t* out_groups, const int64_t* n_rows);
+const float* pmb_selector_batch_launch(pmb_handle* h, const DQuery* d_qs, int nq);
+void pmb_selector_batch_groups(const float* ho, int nq, int64_t* out_groups, const int64_t* n_rows);
 
 // Sets bit p of a bitmap for every lane whose `bit` is true. The warp's positions are
 // consecutive from p_first, so they touch at most two 32-bit words: one atomicOr each.

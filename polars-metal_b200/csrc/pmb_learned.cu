@@ -286,6 +286,44 @@ int stage_query(pmb_handle* h, const pmb_query* q, const pmb_column* cols, int32
 
 // Group counts predicted by the installed selector for the queries of a batch (device DQuery
 // array): out_groups[i] (host) = 2^(output 3), or 0 when unusable; false without a selector.
+// group count of query i from the network's outputs o[i * NO ...] (0 when not finite)
+static int64_t batch_groups(const float* o, int i, int64_t n_rows) {
+  const float g = o[(size_t)i * NO + NS];
+  return std::isfinite(g) ? (int64_t)std::min<double>(std::exp2(std::min<double>(std::max<double>(g, 0.0), 40.0)),
+                                                      (double)n_rows)
+                          : 0;
+}
+
+// features and MLP forward of every query of a batch, queued on the stream; the outputs are copied
+// into pinned staging, so the caller's next stream synchronisation (the batch sketch's readback)
+// serves both. nullptr when no selector is installed or no staging is available yet (then
+// pmb_selector_predict_batch runs synchronously).
+const float* pmb_selector_batch_launch(pmb_handle* h, const DQuery* d_qs, int nq) {
+  if (!h->selector || nq <= 0) return nullptr;
+  float* ho = (float*)pmb_host_stage(h, (size_t)nq * NO * sizeof(float));
+  if (!ho) return nullptr;
+  float* feat = (float*)pmb_ws_alloc(h, (size_t)nq * NF * sizeof(float));
+  float* o = (float*)pmb_ws_alloc(h, (size_t)nq * NO * sizeof(float));
+  if (!feat || !o) return nullptr;
+  const int smem = TSLOTS * 8;
+  if (cudaFuncSetAttribute(k_features_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return nullptr;
+  pmb_kernel_begin(h, "features");
+  k_features_batch<<<nq, F_NT, smem, h->stream>>>(d_qs, feat);
+  pmb_kernel_end(h);
+  pmb_kernel_begin(h, "mlp_forward");
+  k_mlp_forward<<<nq, NH, 0, h->stream>>>(h->selector, feat, nq, o);
+  pmb_kernel_end(h);
+  if (cudaGetLastError() != cudaSuccess) return nullptr;
+  if (cudaMemcpyAsync(ho, o, (size_t)nq * NO * sizeof(float), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+    return nullptr;
+  return ho;
+}
+
+// the group counts from the staged outputs of pmb_selector_batch_launch, after a synchronisation
+void pmb_selector_batch_groups(const float* ho, int nq, int64_t* out_groups, const int64_t* n_rows) {
+  for (int i = 0; i < nq; i++) out_groups[i] = batch_groups(ho, i, n_rows[i]);
+}
+
 bool pmb_selector_predict_batch(pmb_handle* h, const DQuery* d_qs, int nq, int64_t* out_groups, const int64_t* n_rows) {
   if (!h->selector || nq <= 0) return false;
   float* feat = (float*)pmb_ws_alloc(h, (size_t)nq * NF * sizeof(float));
@@ -304,12 +342,7 @@ bool pmb_selector_predict_batch(pmb_handle* h, const DQuery* d_qs, int nq, int64
   if (cudaMemcpyAsync(ho.data(), o, ho.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
     return false;
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return false;
-  for (int i = 0; i < nq; i++) {
-    const float g = ho[(size_t)i * NO + NS];
-    out_groups[i] = std::isfinite(g) ? (int64_t)std::min<double>(std::exp2(std::min<double>(std::max<double>(g, 0.0), 40.0)),
-                                                                 (double)n_rows[i])
-                                     : 0;
-  }
+  for (int i = 0; i < nq; i++) out_groups[i] = batch_groups(ho.data(), i, n_rows[i]);
   return true;
 }
 
