@@ -89,15 +89,29 @@ __global__ void __launch_bounds__(OR_NT) k_order_range(const __grid_constant__ S
   for (int c = 0; c < C.n; c++) {
     unsigned long long lo = ~0ULL, hi = 0, nul = 0;
     unsigned any = 0;
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
-      if (!pmb_valid_bit(C.valid[c], r)) {
-        nul++;
-        continue;
+    const uint8_t* data = C.data[c];
+    const uint8_t* valid = C.valid[c];
+    const int elem = C.elem[c], dtype = C.dtype[c];
+    // four rows per step, their loads issued together (one row at a time left the kernel latency-bound)
+    for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r0 < n; r0 += 4 * stride) {
+      uint64_t b[4];
+      bool in[4], v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int64_t r = r0 + u * stride;
+        in[u] = r < n;
+        v[u] = in[u] && pmb_valid_bit(valid, r);
+        b[u] = in[u] ? pmb_load_bits(data, elem, r) : 0;
       }
-      const unsigned long long o = order_key(pmb_load_bits(C.data[c], C.elem[c], r), C.dtype[c]);
-      lo = min(lo, o);
-      hi = max(hi, o);
-      any = 1;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (in[u] && !v[u]) nul++;
+        if (!v[u]) continue;
+        const unsigned long long o = order_key(b[u], dtype);
+        lo = min(lo, o);
+        hi = max(hi, o);
+        any = 1;
+      }
     }
     lo = warp_min64(lo);
     hi = warp_max64(hi);

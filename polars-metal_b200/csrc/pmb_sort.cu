@@ -86,51 +86,48 @@ __device__ __forceinline__ uint64_t from_ordered(unsigned long long o, int dt) {
 
 __global__ void __launch_bounds__(ST_NT) k_key_range(const __grid_constant__ SortKeyLayout L, int64_t n,
                                                      RangeOut* out) {
-  unsigned long long lo[PMB_MAX_KEYS], hi[PMB_MAX_KEYS];
-  unsigned nul[PMB_MAX_KEYS], any[PMB_MAX_KEYS];
-  for (int k = 0; k < L.n_keys; k++) {
-    lo[k] = ~0ULL;
-    hi[k] = 0;
-    nul[k] = any[k] = 0;
-  }
-  // four rows per step, their loads issued together
+  // one key column at a time with scalar accumulators (per-key arrays indexed at run time would
+  // live in local memory); four rows per step, their loads issued together
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r0 < n; r0 += 4 * stride) {
-    for (int k = 0; k < L.n_keys; k++) {
+  for (int k = 0; k < L.n_keys; k++) {
+    unsigned long long lo = ~0ULL, hi = 0;
+    unsigned nul = 0, any = 0;
+    const uint8_t* data = L.data[k];
+    const uint8_t* valid = L.valid[k];
+    const int elem = L.elem[k], dtype = L.dtype[k];
+    for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r0 < n; r0 += 4 * stride) {
       uint64_t b[4];
       bool v[4];
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const int64_t r = r0 + u * stride;
-        v[u] = r < n && pmb_valid_bit(L.valid[k], r);
-        b[u] = r < n ? pmb_load_bits(L.data[k], L.elem[k], r) : 0;
-        nul[k] |= (r < n && !v[u]) ? 1u : 0u;
+        v[u] = r < n && pmb_valid_bit(valid, r);
+        b[u] = r < n ? pmb_load_bits(data, elem, r) : 0;
+        nul |= (r < n && !v[u]) ? 1u : 0u;
       }
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         if (!v[u]) continue;
-        const unsigned long long o = ordered_bits(b[u], L.dtype[k]);
-        lo[k] = o < lo[k] ? o : lo[k];
-        hi[k] = o > hi[k] ? o : hi[k];
-        any[k] = 1;
+        const unsigned long long o = ordered_bits(b[u], dtype);
+        lo = o < lo ? o : lo;
+        hi = o > hi ? o : hi;
+        any = 1;
       }
     }
-  }
-  for (int k = 0; k < L.n_keys; k++) {
     for (int o = 16; o; o >>= 1) {
-      unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[k], o), b = __shfl_xor_sync(0xffffffffu, hi[k], o);
-      lo[k] = a < lo[k] ? a : lo[k];
-      hi[k] = b > hi[k] ? b : hi[k];
-      nul[k] |= __shfl_xor_sync(0xffffffffu, nul[k], o);
-      any[k] |= __shfl_xor_sync(0xffffffffu, any[k], o);
+      const unsigned long long x = __shfl_xor_sync(0xffffffffu, lo, o), y = __shfl_xor_sync(0xffffffffu, hi, o);
+      lo = x < lo ? x : lo;
+      hi = y > hi ? y : hi;
+      nul |= __shfl_xor_sync(0xffffffffu, nul, o);
+      any |= __shfl_xor_sync(0xffffffffu, any, o);
     }
     if ((threadIdx.x & 31) == 0) {
-      if (any[k]) {
-        atomicMin(&out->lo[k], lo[k]);
-        atomicMax(&out->hi[k], hi[k]);
+      if (any) {
+        atomicMin(&out->lo[k], lo);
+        atomicMax(&out->hi[k], hi);
         atomicOr(&out->any[k], 1u);
       }
-      if (nul[k]) atomicOr(&out->nulls[k], 1u);
+      if (nul) atomicOr(&out->nulls[k], 1u);
     }
   }
 }
