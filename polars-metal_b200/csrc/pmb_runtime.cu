@@ -381,10 +381,18 @@ pmb_result* pmb_result_new(int32_t n_columns) {
 // it if that block is at most twice its size. Smaller buffers, and any buffer when pinned memory
 // cannot be had, come from malloc. host_release() frees either kind.
 namespace {
-std::mutex g_pool_mu;
-std::unordered_map<void*, size_t> g_pool_size;  // every pinned block handed out or cached
-std::multimap<size_t, void*> g_pool_free;       // cached blocks by size
-size_t g_pool_total = 0;                        // bytes of all pinned blocks (handed out or cached)
+// the pool's state is never destroyed: a binding may release a buffer from a finalizer that runs
+// late in the process's exit, after static objects would have been torn down
+struct PinnedPool {
+  std::mutex mu;
+  std::unordered_map<void*, size_t> size;  // every pinned block handed out or cached
+  std::multimap<size_t, void*> free;       // cached blocks by size
+  size_t total = 0;                        // bytes of all pinned blocks (handed out or cached)
+};
+PinnedPool& pool() {
+  static PinnedPool* p = new PinnedPool();
+  return *p;
+}
 constexpr size_t POOL_MIN = (size_t)1 << 20;
 
 size_t pool_budget() {
@@ -399,18 +407,19 @@ size_t pool_budget() {
 static void* host_alloc(size_t bytes) {
   if (bytes >= POOL_MIN) {
     const size_t rounded = (bytes + POOL_MIN - 1) & ~(POOL_MIN - 1);
-    std::lock_guard<std::mutex> lock(g_pool_mu);
-    auto it = g_pool_free.lower_bound(rounded);
-    if (it != g_pool_free.end() && it->first <= 2 * rounded) {
+    PinnedPool& P = pool();
+    std::lock_guard<std::mutex> lock(P.mu);
+    auto it = P.free.lower_bound(rounded);
+    if (it != P.free.end() && it->first <= 2 * rounded) {
       void* p = it->second;
-      g_pool_free.erase(it);
+      P.free.erase(it);
       return p;
     }
     void* p = nullptr;
-    if (g_pool_total + rounded <= pool_budget()) {
+    if (P.total + rounded <= pool_budget()) {
       if (cudaHostAlloc(&p, rounded, cudaHostAllocPortable) == cudaSuccess) {
-        g_pool_size[p] = rounded;
-        g_pool_total += rounded;
+        P.size[p] = rounded;
+        P.total += rounded;
         return p;
       }
       cudaGetLastError();  // no pinned memory: a pageable buffer works the same, only slower
@@ -422,10 +431,11 @@ static void* host_alloc(size_t bytes) {
 void host_release(void* p) {
   if (!p) return;
   {
-    std::lock_guard<std::mutex> lock(g_pool_mu);
-    auto it = g_pool_size.find(p);
-    if (it != g_pool_size.end()) {
-      g_pool_free.emplace(it->second, p);
+    PinnedPool& P = pool();
+    std::lock_guard<std::mutex> lock(P.mu);
+    auto it = P.size.find(p);
+    if (it != P.size.end()) {
+      P.free.emplace(it->second, p);
       return;
     }
   }

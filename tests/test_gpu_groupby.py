@@ -347,3 +347,26 @@ def test_float_sum_outlier_beyond_the_fixed_point(strategy, n):
     cols = {"k": (rng.integers(0, 1000, n).astype(np.int32), None), "v": (v, pack(rng.random(n) > 0.05))}
     aggs = [("Sum", "v", "s"), ("Mean", "v", "m"), ("Len", None, "n")]
     run_both(cols, ["k"], aggs, None, strategy, f"outlier {strategy} n={n}")
+
+
+def test_pinned_result_buffers_are_not_shared_between_live_results():
+    # host results of 1 MB and more come from a recycled pool of pinned blocks: results kept alive
+    # across later calls, and results dropped between calls (their blocks reused), must all still
+    # hold their own values
+    import gc
+
+    tables = [datagen.make_hash(1_000_000, seed=300 + i, device="cpu", n_values=2_000_000, s=0.2) for i in range(3)]
+    wants = [pyoracle.groupby(datagen.to_numpy_columns(t), t.keys, t.aggs, t.predicate) for t in tables]
+    kept = []
+    for rep in range(3):
+        for t, want in zip(tables, wants):
+            got = groupby(datagen.to_column_data(t), t.keys, t.aggs, t.predicate, output="host")
+            assert max(np.asarray(d).nbytes for d in got.data) >= 1 << 20  # a pooled buffer is involved
+            if rep == 0:
+                kept.append((got, want, t))
+            else:
+                assert_results_match(as_dict(got), want, 1, t.aggs, f"pooled rep {rep}")
+            del got
+            gc.collect()
+    for got, want, t in kept:
+        assert_results_match(as_dict(got), want, 1, t.aggs, "pooled, kept alive")
