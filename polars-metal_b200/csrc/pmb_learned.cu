@@ -37,8 +37,36 @@ struct FeatParams {
 
 __device__ __forceinline__ float lg2p1(double x) { return (float)log2(x + 1.0); }
 
-// the features of query q into out[NF]; called by one whole CTA of F_NT threads
-__device__ __forceinline__ void features_body(const DQuery& q, float* out) {
+// sample i of query q (rows evenly spaced over the input): its key hash, never 0, or 0 when the
+// filter drops the row or i is past the sample; `nul` tells whether a key column is null there.
+// One thread per sample, so the sample's loads are all in flight at once.
+__device__ __forceinline__ void sample_one(const DQuery& q, int i, unsigned long long& hv, unsigned char& nul) {
+  hv = 0ULL;
+  nul = 0;
+  const int64_t n = q.n_rows;
+  const int m = (int)(n < SAMPLE ? n : SAMPLE);
+  if (i >= m) return;
+  const TileCtx t{nullptr, nullptr, nullptr, 0};
+  const int64_t r = (int64_t)((__int128)i * n / m);  // evenly spaced rows
+  if (q.prog.n_ops > 0 && !eval_keep(q, t, r)) return;
+  bool anynull = false;
+  for (int k = 0; k < q.n_keys; k++) anynull |= !tc_isvalid(q, t, q.key[k].col, r);
+  unsigned long long lo, hi = 0;
+  if (q.key_bits > 64) {
+    Key128 kk = pack_key128(q, t, r);
+    lo = kk.lo;
+    hi = kk.hi;
+  } else {
+    lo = pack_key64(q, t, r);
+  }
+  hv = pmb_fmix64(lo ^ pmb_fmix64(hi + 0x9E3779B97F4A7C15ULL)) | 1ULL;  // never 0 (empty)
+  nul = anynull ? 1 : 0;
+}
+
+// the features of query q into out[NF] from its samples (hs, ns: SAMPLE entries written by
+// sample_one); called by one whole CTA of F_NT threads
+__device__ __forceinline__ void features_body(const DQuery& q, const unsigned long long* __restrict__ hs,
+                                              const unsigned char* __restrict__ ns, float* out) {
   extern __shared__ unsigned long long s_slot[];  // TSLOTS
   __shared__ unsigned int s_hll[HLL];
   __shared__ unsigned int s_bkt[BUCKETS];
@@ -51,25 +79,12 @@ __device__ __forceinline__ void features_body(const DQuery& q, float* out) {
   __syncthreads();
   const int64_t n = q.n_rows;
   const int m = (int)(n < SAMPLE ? n : SAMPLE);
-  const TileCtx t{nullptr, nullptr, nullptr, 0};
-  const bool k128 = q.key_bits > 64;
   const bool pred = q.prog.n_ops > 0;
   for (int i = tid; i < m; i += F_NT) {
-    const int64_t r = (int64_t)((__int128)i * n / m);  // evenly spaced rows
-    if (pred && !eval_keep(q, t, r)) continue;
+    const unsigned long long h = hs[i];
+    if (h == 0ULL) continue;  // dropped by the filter
     atomicAdd(&s_acc[0], 1u);  // kept
-    bool anynull = false;
-    for (int k = 0; k < q.n_keys; k++) anynull |= !tc_isvalid(q, t, q.key[k].col, r);
-    if (anynull) atomicAdd(&s_acc[1], 1u);
-    unsigned long long lo, hi = 0;
-    if (k128) {
-      Key128 kk = pack_key128(q, t, r);
-      lo = kk.lo;
-      hi = kk.hi;
-    } else {
-      lo = pack_key64(q, t, r);
-    }
-    const unsigned long long h = pmb_fmix64(lo ^ pmb_fmix64(hi + 0x9E3779B97F4A7C15ULL)) | 1ULL;  // never 0 (empty)
+    if (ns[i]) atomicAdd(&s_acc[1], 1u);
     // HyperLogLog register: index from the top 8 bits, rank of the rest
     const unsigned reg = (unsigned)(h >> 56);
     const unsigned rank = (unsigned)__clzll((h << 8) | 0xFFULL) + 1u;
@@ -153,11 +168,37 @@ __device__ __forceinline__ void features_body(const DQuery& q, float* out) {
   }
 }
 
-__global__ void __launch_bounds__(F_NT) k_features(const __grid_constant__ FeatParams F) { features_body(F.q, F.out); }
+constexpr int SAMPLE_NT = 256;  // threads (samples) per CTA of the sampling kernels
 
-// one CTA per query of a batch
-__global__ void __launch_bounds__(F_NT) k_features_batch(const DQuery* __restrict__ qs, float* __restrict__ out) {
-  features_body(qs[blockIdx.x], out + (size_t)blockIdx.x * NF);
+__global__ void __launch_bounds__(SAMPLE_NT) k_feat_sample(const __grid_constant__ FeatParams F,
+                                                           unsigned long long* __restrict__ hs,
+                                                           unsigned char* __restrict__ ns) {
+  const int i = blockIdx.x * SAMPLE_NT + threadIdx.x;
+  if (i < SAMPLE) sample_one(F.q, i, hs[i], ns[i]);
+}
+
+__global__ void __launch_bounds__(F_NT) k_features(const __grid_constant__ FeatParams F,
+                                                   const unsigned long long* __restrict__ hs,
+                                                   const unsigned char* __restrict__ ns) {
+  features_body(F.q, hs, ns, F.out);
+}
+
+// a batch: SAMPLE / SAMPLE_NT sampling CTAs per query, then one feature CTA per query
+__global__ void __launch_bounds__(SAMPLE_NT) k_feat_sample_batch(const DQuery* __restrict__ qs,
+                                                                 unsigned long long* __restrict__ hs,
+                                                                 unsigned char* __restrict__ ns) {
+  constexpr int per_q = SAMPLE / SAMPLE_NT;
+  const int qi = blockIdx.x / per_q;
+  const int i = (blockIdx.x % per_q) * SAMPLE_NT + threadIdx.x;
+  sample_one(qs[qi], i, hs[(size_t)qi * SAMPLE + i], ns[(size_t)qi * SAMPLE + i]);
+}
+
+__global__ void __launch_bounds__(F_NT) k_features_batch(const DQuery* __restrict__ qs,
+                                                         const unsigned long long* __restrict__ hs,
+                                                         const unsigned char* __restrict__ ns,
+                                                         float* __restrict__ out) {
+  const size_t qi = blockIdx.x;
+  features_body(qs[qi], hs + qi * SAMPLE, ns + qi * SAMPLE, out + qi * NF);
 }
 
 // ---------------------------------------------------------------- MLP (one CTA of 64 threads per sample)
@@ -261,9 +302,13 @@ int features_device(pmb_handle* h, const CompiledQuery& cq, float* dev_out) {
   F.q = cq.dq;
   F.out = dev_out;
   const int smem = TSLOTS * 8;
+  unsigned long long* hs = (unsigned long long*)pmb_ws_alloc(h, (size_t)SAMPLE * 9);
+  if (!hs) return pmb_fail(h, PMB_E_OOM, "workspace exhausted (selector sample)");
+  unsigned char* ns = reinterpret_cast<unsigned char*>(hs + SAMPLE);
   PMB_CUDA(h, cudaFuncSetAttribute(k_features, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   pmb_kernel_begin(h, "features");
-  k_features<<<1, F_NT, smem, h->stream>>>(F);
+  k_feat_sample<<<SAMPLE / SAMPLE_NT, SAMPLE_NT, 0, h->stream>>>(F, hs, ns);
+  k_features<<<1, F_NT, smem, h->stream>>>(F, hs, ns);
   pmb_kernel_end(h);
   PMB_CUDA(h, cudaGetLastError());
   return PMB_OK;
@@ -307,8 +352,12 @@ const float* pmb_selector_batch_launch(pmb_handle* h, const DQuery* d_qs, int nq
   if (!feat || !o) return nullptr;
   const int smem = TSLOTS * 8;
   if (cudaFuncSetAttribute(k_features_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return nullptr;
+  unsigned long long* hs = (unsigned long long*)pmb_ws_alloc(h, (size_t)nq * SAMPLE * 9);
+  if (!hs) return nullptr;
+  unsigned char* ns = reinterpret_cast<unsigned char*>(hs + (size_t)nq * SAMPLE);
   pmb_kernel_begin(h, "features");
-  k_features_batch<<<nq, F_NT, smem, h->stream>>>(d_qs, feat);
+  k_feat_sample_batch<<<nq * (SAMPLE / SAMPLE_NT), SAMPLE_NT, 0, h->stream>>>(d_qs, hs, ns);
+  k_features_batch<<<nq, F_NT, smem, h->stream>>>(d_qs, hs, ns, feat);
   pmb_kernel_end(h);
   pmb_kernel_begin(h, "mlp_forward");
   k_mlp_forward<<<nq, NH, 0, h->stream>>>(h->selector, feat, nq, o);
@@ -331,8 +380,12 @@ bool pmb_selector_predict_batch(pmb_handle* h, const DQuery* d_qs, int nq, int64
   if (!feat || !o) return false;
   const int smem = TSLOTS * 8;
   if (cudaFuncSetAttribute(k_features_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return false;
+  unsigned long long* hs = (unsigned long long*)pmb_ws_alloc(h, (size_t)nq * SAMPLE * 9);
+  if (!hs) return false;
+  unsigned char* ns = reinterpret_cast<unsigned char*>(hs + (size_t)nq * SAMPLE);
   pmb_kernel_begin(h, "features");
-  k_features_batch<<<nq, F_NT, smem, h->stream>>>(d_qs, feat);
+  k_feat_sample_batch<<<nq * (SAMPLE / SAMPLE_NT), SAMPLE_NT, 0, h->stream>>>(d_qs, hs, ns);
+  k_features_batch<<<nq, F_NT, smem, h->stream>>>(d_qs, hs, ns, feat);
   pmb_kernel_end(h);
   pmb_kernel_begin(h, "mlp_forward");
   k_mlp_forward<<<nq, NH, 0, h->stream>>>(h->selector, feat, nq, o);
