@@ -228,7 +228,8 @@ extern "C" __global__ void __launch_bounds__(J_NT, 1) pmb_jit_hash_agg(const __g
     unsigned ent[4];  // 0: dropped, J_MISS: cold, else shared-tier entry (record << 7 | row) + 1
     // Every lane looks up the key of each of its rows in the first bucket, kept or not (a dropped
     // row's answer is ignored), so the lookup runs with all lanes and no divergent exits; the
-    // second bucket, needed only behind a full first one, is taken by the whole warp together.
+    // second bucket, needed only behind a bucket that turned a key away, is taken by the whole
+    // warp together.
     const unsigned tnb_eff = P.ttab ? tnb : 0u;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
